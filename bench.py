@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Headline benchmark: DGEMM TFLOP/s (FP64-accurate, emulated vs native).
+
+Workload (N=1): cblas_dgemm NN, M = N = K = 16384, FP64 column-major,
+entries U[-0.5,0.5]*exp(phi*g), g~N(0,1) (phi = 0 by default), alpha = 1,
+beta = 0.5 -- the emulated-vs-native DGEMM configuration at 16384^3. One step
+is one full GEMM.
+
+* ``value``: device-resident operands (2 GiB each, larger than the 126 MB L2,
+  so no flush is needed), timed with CUDA events on the launching stream over
+  exactly --steps calls of ``blasx_dgemm_device``, max over ranks.
+* ``e2e``: the same GEMM through the drop-in ``cblas_dgemm`` with pinned host
+  buffers; every step copies A, B, C host->device and C device->host inside
+  the timed region (the call is synchronous; host wall clock per call).
+* ``native``: the same device-resident GEMM forced onto the native FP64 path.
+* ``roofline``: the dominant kernel's achieved rate against the measured peak
+  of its pipe (cuBLAS on this box, measured in this run).
+* ``cpu_baseline``: the reference's CPU implementation (its own library,
+  compiled from its sources into oracle/_ref, CPU path: every call <= 1000 per
+  dimension, which it hands to OpenBLAS) on a bounded slab of the same GEMM.
+
+``--impl reference`` times that reference CPU implementation alone on the
+same metric. With --gpus N > 1 (torchrun) every rank runs an independent
+replica: the GEMM path has no data exchange between GPUs (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PUBLISHED_BLASX_1GPU_16384_GFLOPS = 1153.4  # performance_data/GEMM.xlsx row 17 col D
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=16384)
+    p.add_argument("--phi", type=float, default=0.0)
+    p.add_argument("--mode", default="auto", choices=["auto", "native", "ozaki"])
+    p.add_argument("--cpu-seconds", type=float, default=8.0, help="target CPU time per reference sample")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU implementation (oracle/_ref) on a bounded sample
+# ---------------------------------------------------------------------------
+
+def reference_cpu_sample(n: int, seconds: float, cores: int, steps: int = 1, warmup: int = 0):
+    """Time the reference library's CPU path on a slab C[:, :ns] of the n^3 GEMM.
+
+    The reference dispatches calls with every dimension <= 1000 to its CPU BLAS
+    (blas/dgemm.c:61-75), so the slab is computed as 1000-sized tile calls
+    through its public cblas_dgemm, accumulating over K with beta = 1 after the
+    first K-step. Returns (tflops_per_step list, sample description, kind).
+    """
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
+    import numpy as np
+
+    import oracle
+    try:
+        ref = oracle.Reference()
+        kind = "reference"
+        gemm = ref.gemm
+    except (FileNotFoundError, OSError):
+        ref = oracle.OpenBLAS()
+        kind = "reference-cpublas"
+        gemm = ref.gemm
+    T = 1000
+
+    def run(ns):
+        A = oracle.spread((n, n), 1, 0.0)
+        B = oracle.spread((n, ns), 2, 0.0)
+        C = oracle.spread((n, ns), 3, 0.0)
+        t0 = time.perf_counter()
+        for j0 in range(0, ns, T):
+            nj = min(T, ns - j0)
+            for i0 in range(0, n, T):
+                mi = min(T, n - i0)
+                for k0 in range(0, n, T):
+                    kk = min(T, n - k0)
+                    beta = 0.5 if k0 == 0 else 1.0
+                    gemm("N", "N", mi, nj, kk, 1.0, A[i0:, k0:], n, B[k0:, j0:], n, beta, C[i0:, j0:], n)
+        return time.perf_counter() - t0
+
+    t = run(min(n, 1000))  # calibration slab
+    rate = 2.0 * n * n * min(n, 1000) / t
+    ns = int(max(1000, min(n, rate * seconds / (2.0 * n * n))) // 1000 * 1000)
+    out = []
+    for s in range(warmup + steps):
+        dt = run(ns)
+        if s >= warmup:
+            out.append(2.0 * n * n * ns / dt / 1e12)
+    sample = (f"C[:, :{ns}] of the {n}^3 DGEMM ({2.0 * n * n * ns / 1e12:.2f} TFLOP) as {T}-sized tile calls "
+              f"through the reference's cblas_dgemm CPU path")
+    return out, sample, kind, (ref.name if hasattr(ref, "name") else oracle.REF_PATH)
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cores = os.cpu_count() or 1
+    n = args.size
+    config = {"workload": f"cblas_dgemm NN M=N=K={n} FP64 col-major, U[-0.5,0.5]*exp({args.phi}*g), "
+                          "alpha=1 beta=0.5",
+              "phi": args.phi, "mode": args.mode, "M": n, "N": n, "K": n,
+              "l2": "operands 2 GiB each > 126 MB L2: no flush between steps",
+              "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        vals, sample, kind, lib = reference_cpu_sample(n, args.cpu_seconds, cores, args.steps, args.warmup)
+        v = statistics.median(vals)
+        line = {"impl": "reference", "metric": "DGEMM TFLOP/s (FP64-accurate, emulated vs native)",
+                "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 2.0 * n ** 3 / (v * 1e12) * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": kind, "sample": sample,
+                                 "library": lib},
+                "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    os.environ["BLASX_DEVICE"] = str(local)
+    import numpy as np
+    import torch
+
+    import blasx_b200 as bx
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    mode = {"auto": bx.MODE_AUTO, "native": bx.MODE_NATIVE, "ozaki": bx.MODE_OZAKI}[args.mode]
+    bx.set_dgemm_mode(mode)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- inputs (device-resident), C3 distribution ---
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+
+    def gen():
+        u = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g) - 0.5
+        if args.phi != 0:
+            u *= torch.exp(args.phi * torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g))
+        return u
+
+    A, B, C = gen(), gen(), gen()
+    stream = torch.cuda.current_stream()
+    flops = 2.0 * n ** 3
+
+    def step():
+        st = bx.gemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.5, C, n, stream=stream)
+        if st != 0:
+            raise RuntimeError(bx.last_error())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stats = bx.call_stats()
+
+    # --- timed region (device-resident) ---
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = bx.kernel_launch_count()
+    with ClockSampler(local) as clk:
+        barrier(); torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize(); barrier()
+    launches = bx.kernel_launch_count() - launches0
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    value = world * flops / (ms * 1e-3) / 1e12
+
+    # --- native FP64 path on the same inputs ---
+    native = None
+    if mode != bx.MODE_NATIVE:
+        bx.set_dgemm_mode(bx.MODE_NATIVE)
+        step(); torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ns = max(1, min(args.steps, 2))
+        barrier(); e0.record(stream)
+        for _ in range(ns):
+            step()
+        e1.record(stream); torch.cuda.synchronize(); barrier()
+        nms = max_over_ranks(e0.elapsed_time(e1) / ns)
+        native = {"value": world * flops / (nms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": nms}
+        bx.set_dgemm_mode(mode)
+
+    # --- pipe peak: cuBLAS DGEMM on this box, measured now ---
+    x = torch.rand((8192, 8192), dtype=torch.float64, device="cuda")
+    y = torch.rand((8192, 8192), dtype=torch.float64, device="cuda")
+    torch.matmul(x, y); torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        torch.matmul(x, y)
+    e1.record(); torch.cuda.synchronize()
+    fp64_peak = 3 * 2.0 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    del x, y
+
+    per_gpu = flops / (ms * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "pipe": "fp64 (DMMA)", "kernel": "whole DGEMM step",
+                "achieved": per_gpu, "peak": fp64_peak, "unit": "TFLOP/s", "frac": per_gpu / fp64_peak,
+                "peak_source": "cuBLAS DGEMM 8192^3 via torch.matmul, measured in this run",
+                "traffic": None}
+
+    # --- e2e through the drop-in ABI with pinned host buffers ---
+    e2e = None
+    if not args.no_e2e:
+        Ah = torch.empty((n, n), dtype=torch.float64, pin_memory=True); Ah.copy_(A)
+        Bh = torch.empty((n, n), dtype=torch.float64, pin_memory=True); Bh.copy_(B)
+        Ch = torch.empty((n, n), dtype=torch.float64, pin_memory=True); Ch.copy_(C)
+        torch.cuda.synchronize()
+
+        def host_step():
+            bx.cblas_dgemm(bx.CblasColMajor, bx.CblasNoTrans, bx.CblasNoTrans, n, n, n, 1.0, Ah.data_ptr(), n,
+                           Bh.data_ptr(), n, 0.5, Ch.data_ptr(), n)
+            if bx.last_status() != 0:
+                raise RuntimeError(bx.last_error())
+
+        host_step()
+        ts = []
+        for _ in range(max(1, min(args.steps, 3))):
+            barrier()
+            t0 = time.perf_counter()
+            host_step()
+            ts.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks(statistics.median(ts))
+        hs = bx.call_stats()
+        e2e = {"value": world * flops / e2e_s / 1e12, "unit": "TFLOP/s", "ms_per_step": e2e_s * 1e3,
+               "h2d_bytes_per_step": int(hs["h2d_bytes"]), "d2h_bytes_per_step": int(hs["d2h_bytes"]),
+               "timing": "host wall clock around the synchronous cblas_dgemm call, median"}
+        del Ah, Bh, Ch
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        vals, sample, kind, lib = reference_cpu_sample(n, args.cpu_seconds, cores, 1, 0)
+        cpu = {"value": vals[0], "unit": "TFLOP/s", "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {"metric": "DGEMM TFLOP/s (FP64-accurate, emulated vs native)", "value": value, "unit": "TFLOP/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config,
+                "path": {1: "native", 2: "ozaki", 3: "scale"}.get(stats["path"], str(stats["path"])),
+                "moduli": stats["moduli"], "native": native, "e2e": e2e, "roofline": roofline,
+                "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary(),
+                "vs_published_blasx_1gpu_16384": value * 1e3 / PUBLISHED_BLASX_1GPU_16384_GFLOPS}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,217 @@
+"""blasx_b200 -- B200-native tiled GEMM runtime behind the BLASX C ABI.
+
+The product is the shared library ``libblasx_b200.so`` built from ``csrc/``
+(CUDA C++ for sm_100a). Its C ABI is declared in ``include/blasx_b200.h`` and
+replaces the GEMM entry points of linnanwang/BLASX: ``cblas_sgemm``,
+``cblas_dgemm``, ``cblas_zgemm`` (include/cblas.h:424/454/514) and the F77
+wrappers ``sgemm_``, ``dgemm_``, ``zgemm_`` (blas/dgemm.c:131-154).
+
+This module is the Python host mirror of that interface (ctypes, no torch in
+the signatures): the same names, argument order and meaning, and the same
+error behaviour (``xerbla_`` text on stdout, C untouched). It loads the
+in-tree library and raises if it is missing -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libblasx_b200.so")
+HEADER = os.path.join(ROOT, "include", "blasx_b200.h")
+
+CblasRowMajor, CblasColMajor = 101, 102
+CblasNoTrans, CblasTrans, CblasConjTrans = 111, 112, 113
+TRANS = {"N": CblasNoTrans, "T": CblasTrans, "C": CblasConjTrans}
+
+BLASX_OK, BLASX_ERR_ARG, BLASX_ERR_CUDA, BLASX_ERR_NOMEM = 0, 1, 2, 3
+BLASX_ERR_NODEVICE, BLASX_ERR_TIMEOUT, BLASX_ERR_UNSUPPORTED, BLASX_ERR_CLOSED = 4, 5, 6, 7
+
+MODE_AUTO, MODE_NATIVE, MODE_OZAKI = 0, 1, 2
+
+_P, _I, _D, _F = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float
+_lib = None
+
+
+class CallStats(ctypes.Structure):
+    _fields_ = [("seconds", _D), ("h2d_bytes", _D), ("d2h_bytes", _D), ("cache_hits", _D),
+                ("cache_misses", _D), ("evictions", _D), ("path", _I), ("moduli", _I),
+                ("tile", _I), ("reserved", _I)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+def build(verbose: bool = False) -> str:
+    from . import _build
+    return _build.build(verbose=verbose)
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded libblasx_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m blasx_b200._build` "
+                              "(the GEMM path has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+        L.cblas_sgemm.argtypes = [_I] * 6 + [_F, _P, _I, _P, _I, _F, _P, _I]
+        L.cblas_dgemm.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _D, _P, _I]
+        L.cblas_zgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
+        for f in ("sgemm_", "dgemm_", "zgemm_"):
+            getattr(L, f).argtypes = [_P] * 13
+        L.xerbla_.argtypes = [ctypes.c_char_p, _P]
+        L.blasx_last_status.restype = _I
+        L.blasx_last_error.restype = ctypes.c_char_p
+        L.blasx_set_dgemm_mode.argtypes = [_I]
+        L.blasx_set_hbm_budget.argtypes = [ctypes.c_size_t]
+        L.blasx_set_tile.argtypes = [_I]
+        L.blasx_get_call_stats.argtypes = [ctypes.POINTER(CallStats)]
+        L.blasx_dgemm_device.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
+        L.blasx_sgemm_device.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I, _P]
+        L.blasx_zgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
+        L.blasx_kernel_launch_count.restype = ctypes.c_uint64
+        _lib = L
+    return _lib
+
+
+def kernel_launch_count() -> int:
+    """Kernels launched by the library so far (all threads)."""
+    return int(lib().blasx_kernel_launch_count())
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/blasx_b200.h (the C ABI)."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", text, flags=re.M)
+    return sorted({n for n in names if not n.startswith("__")})
+
+
+def _addr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    raise TypeError(f"cannot take the address of {type(x)}")
+
+
+def _cpair(v) -> np.ndarray:
+    v = complex(v)
+    return np.array([v.real, v.imag], dtype=np.float64)
+
+
+# ---------------------------------------------------------------------------
+# CBLAS mirror (include/cblas.h:424/454/514)
+# ---------------------------------------------------------------------------
+
+def cblas_sgemm(Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    lib().cblas_sgemm(Order, TransA, TransB, M, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta,
+                      _addr(C), ldc)
+
+
+def cblas_dgemm(Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    lib().cblas_dgemm(Order, TransA, TransB, M, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta,
+                      _addr(C), ldc)
+
+
+def cblas_zgemm(Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    al, be = _cpair(alpha), _cpair(beta)
+    lib().cblas_zgemm(Order, TransA, TransB, M, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb,
+                      be.ctypes.data, _addr(C), ldc)
+
+
+def _f77(fn, ctype, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cplx=False):
+    ta = ctypes.c_char(transa.encode() if isinstance(transa, str) else transa)
+    tb = ctypes.c_char(transb.encode() if isinstance(transb, str) else transb)
+    ints = [ctypes.c_int(v) for v in (m, n, k, lda, ldb, ldc)]
+    if cplx:
+        al, be = _cpair(alpha), _cpair(beta)
+        pa, pb = al.ctypes.data, be.ctypes.data
+    else:
+        al, be = ctype(alpha), ctype(beta)
+        pa, pb = ctypes.addressof(al), ctypes.addressof(be)
+    r = ctypes.byref
+    fn(r(ta), r(tb), r(ints[0]), r(ints[1]), r(ints[2]), pa, _addr(A), r(ints[3]), _addr(B),
+       r(ints[4]), pb, _addr(C), r(ints[5]))
+
+
+def sgemm_(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    _f77(lib().sgemm_, ctypes.c_float, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+
+
+def dgemm_(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    _f77(lib().dgemm_, ctypes.c_double, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+
+
+def zgemm_(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    _f77(lib().zgemm_, None, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cplx=True)
+
+
+def gemm(transa, transb, alpha, A, B, beta, C):
+    """C <- alpha op(A) op(B) + beta C on Fortran-ordered numpy arrays."""
+    M, N = C.shape
+    K = A.shape[1] if transa == "N" else A.shape[0]
+    args = (CblasColMajor, TRANS[transa], TRANS[transb], M, N, K, alpha, A, max(1, A.shape[0]),
+            B, max(1, B.shape[0]), beta, C, max(1, M))
+    {np.float32: cblas_sgemm, np.float64: cblas_dgemm, np.complex128: cblas_zgemm}[C.dtype.type](*args)
+    return C
+
+
+# ---------------------------------------------------------------------------
+# extensions
+# ---------------------------------------------------------------------------
+
+def gemm_device(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, stream=None,
+                dtype="d"):
+    """Device-resident GEMM on device pointers (ints or tensors with data_ptr)."""
+    L = lib()
+    s = _addr(stream) if stream is not None and not hasattr(stream, "cuda_stream") else \
+        (stream.cuda_stream if stream is not None else None)
+    ta = TRANS[transa] if isinstance(transa, str) else transa
+    tb = TRANS[transb] if isinstance(transb, str) else transb
+    if dtype == "d":
+        return L.blasx_dgemm_device(ta, tb, M, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta, _addr(C), ldc, s)
+    if dtype == "s":
+        return L.blasx_sgemm_device(ta, tb, M, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta, _addr(C), ldc, s)
+    al, be = _cpair(alpha), _cpair(beta)
+    return L.blasx_zgemm_device(ta, tb, M, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb,
+                                be.ctypes.data, _addr(C), ldc, s)
+
+
+def last_status() -> int:
+    return lib().blasx_last_status()
+
+
+def last_error() -> str:
+    return lib().blasx_last_error().decode()
+
+
+def call_stats() -> dict:
+    s = CallStats()
+    lib().blasx_get_call_stats(ctypes.byref(s))
+    return s.as_dict()
+
+
+def set_dgemm_mode(mode: int) -> int:
+    return lib().blasx_set_dgemm_mode(mode)
+
+
+def set_hbm_budget(nbytes: int) -> int:
+    return lib().blasx_set_hbm_budget(nbytes)
+
+
+def set_tile(tile: int) -> int:
+    return lib().blasx_set_tile(tile)
+
+
+def finalize() -> int:
+    return lib().blasx_finalize()

@@ -1,0 +1,187 @@
+// kernels_simt.cu -- portable SIMT GEMM kernel and the beta-scale kernel.
+//
+// The SIMT kernel is the correctness baseline of the device path: any dtype,
+// any transpose, ragged edges, BLAS alpha/beta semantics (C not read when
+// beta == 0). Fast paths live in kernels_dmma.cu (FP64 pipe) and the Ozaki
+// INT8 tensor-core path.
+#include "kernels.h"
+
+namespace bx {
+
+namespace {
+
+struct z2 {
+    double re, im;
+};
+
+template <typename T> struct Arith;
+
+template <> struct Arith<float> {
+    using V = float;
+    __device__ static V zero() { return 0.f; }
+    __device__ static V fma(V a, V b, V c) { return fmaf(a, b, c); }
+    __device__ static V conj(V a) { return a; }
+    __device__ static V mul(V a, V b) { return a * b; }
+    __device__ static V add(V a, V b) { return a + b; }
+};
+template <> struct Arith<double> {
+    using V = double;
+    __device__ static V zero() { return 0.0; }
+    __device__ static V fma(V a, V b, V c) { return ::fma(a, b, c); }
+    __device__ static V conj(V a) { return a; }
+    __device__ static V mul(V a, V b) { return a * b; }
+    __device__ static V add(V a, V b) { return a + b; }
+};
+template <> struct Arith<z2> {
+    using V = z2;
+    __device__ static V zero() { return {0.0, 0.0}; }
+    __device__ static V fma(V a, V b, V c) {
+        c.re = ::fma(a.re, b.re, c.re);
+        c.re = ::fma(-a.im, b.im, c.re);
+        c.im = ::fma(a.re, b.im, c.im);
+        c.im = ::fma(a.im, b.re, c.im);
+        return c;
+    }
+    __device__ static V conj(V a) { return {a.re, -a.im}; }
+    __device__ static V mul(V a, V b) {
+        return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+    }
+    __device__ static V add(V a, V b) { return {a.re + b.re, a.im + b.im}; }
+};
+
+template <typename T> __host__ T from_cplx(cplx c);
+template <> __host__ float from_cplx<float>(cplx c) { return float(c.re); }
+template <> __host__ double from_cplx<double>(cplx c) { return c.re; }
+template <> __host__ z2 from_cplx<z2>(cplx c) { return {c.re, c.im}; }
+
+constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(NT)
+    gemm_simt_kernel(int ta, int tb, int M, int N, int K, T alpha, const T *__restrict__ A,
+                     int64_t lda, const T *__restrict__ B, int64_t ldb, T beta, T *__restrict__ C,
+                     int64_t ldc, int beta_zero) {
+    using Ar = Arith<T>;
+    __shared__ T As[BK][BM + 1];
+    __shared__ T Bs[BK][BN + 1];
+    const int tid = threadIdx.x;
+    const int tx = tid % 16, ty = tid / 16;
+    const int64_t m0 = int64_t(blockIdx.x) * BM, n0 = int64_t(blockIdx.y) * BN;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = Ar::zero();
+
+    for (int64_t k0 = 0; k0 < K; k0 += BK) {
+        for (int e = tid; e < BM * BK; e += NT) {
+            int mm, kk;
+            if (ta == NoTrans) { mm = e % BM; kk = e / BM; }
+            else { kk = e % BK; mm = e / BK; }
+            const int64_t gm = m0 + mm, gk = k0 + kk;
+            T v = Ar::zero();
+            if (gm < M && gk < K) {
+                v = ta == NoTrans ? A[gm + gk * lda] : A[gk + gm * lda];
+                if (ta == ConjT) v = Ar::conj(v);
+            }
+            As[kk][mm] = v;
+        }
+        for (int e = tid; e < BN * BK; e += NT) {
+            int nn, kk;
+            if (tb == NoTrans) { kk = e % BK; nn = e / BK; }
+            else { nn = e % BN; kk = e / BN; }
+            const int64_t gn = n0 + nn, gk = k0 + kk;
+            T v = Ar::zero();
+            if (gn < N && gk < K) {
+                v = tb == NoTrans ? B[gk + gn * ldb] : B[gn + gk * ldb];
+                if (tb == ConjT) v = Ar::conj(v);
+            }
+            Bs[kk][nn] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = Ar::fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t gn = n0 + ty + 16 * j;
+        if (gn >= N) continue;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int64_t gm = m0 + tx + 16 * i;
+            if (gm >= M) continue;
+            T *cp = &C[gm + gn * ldc];
+            T v = Ar::mul(alpha, acc[i][j]);
+            if (!beta_zero) v = Ar::add(v, Ar::mul(beta, *cp));
+            *cp = v;
+        }
+    }
+}
+
+template <typename T>
+__global__ void scale_kernel(int M, int N, T beta, T *__restrict__ C, int64_t ldc, int beta_zero) {
+    using Ar = Arith<T>;
+    const int64_t total = int64_t(M) * N;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = t % M, j = t / M;
+        T *cp = &C[i + j * ldc];
+        *cp = beta_zero ? Ar::zero() : Ar::mul(beta, *cp);
+    }
+}
+
+template <typename T> int launch_simt_t(const Gemm &g, cudaStream_t s) {
+    dim3 grid(unsigned((g.M + BM - 1) / BM), unsigned((g.N + BN - 1) / BN));
+    if (grid.y > 65535) return set_error(BLASX_ERR_UNSUPPORTED, "N too large for SIMT grid");
+    gemm_simt_kernel<T><<<grid, NT, 0, s>>>(
+        g.ta, g.tb, int(g.M), int(g.N), int(g.K), from_cplx<T>(g.alpha),
+        static_cast<const T *>(g.A), g.lda, static_cast<const T *>(g.B), g.ldb,
+        from_cplx<T>(g.beta), static_cast<T *>(g.C), g.ldc, g.beta_zero() ? 1 : 0);
+    BX_CUDA(cudaGetLastError());
+    count_launch();
+    return BLASX_OK;
+}
+
+template <typename T> int launch_scale_t(const Gemm &g, cudaStream_t s) {
+    const int64_t total = g.M * g.N;
+    int blocks = int((total + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    scale_kernel<T><<<blocks, 256, 0, s>>>(int(g.M), int(g.N), from_cplx<T>(g.beta),
+                                            static_cast<T *>(g.C), g.ldc, g.beta_zero() ? 1 : 0);
+    BX_CUDA(cudaGetLastError());
+    count_launch();
+    return BLASX_OK;
+}
+
+}  // namespace
+
+int launch_gemm_simt(const Gemm &g, cudaStream_t s) {
+    switch (g.dt) {
+        case DType::F32: return launch_simt_t<float>(g, s);
+        case DType::F64: return launch_simt_t<double>(g, s);
+        default: return launch_simt_t<z2>(g, s);
+    }
+}
+
+int launch_scale(const Gemm &g, cudaStream_t s) {
+    if (g.M == 0 || g.N == 0) return BLASX_OK;
+    switch (g.dt) {
+        case DType::F32: return launch_scale_t<float>(g, s);
+        case DType::F64: return launch_scale_t<double>(g, s);
+        default: return launch_scale_t<z2>(g, s);
+    }
+}
+
+}  // namespace bx

@@ -1,0 +1,108 @@
+// runtime.h -- shared types of the B200 GEMM runtime: problem description,
+// status recording, the per-process device context and its configuration.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../include/blasx_b200.h"
+
+namespace bx {
+
+enum class DType : int { F32 = 0, F64 = 1, C128 = 2 };
+
+inline size_t elem_size(DType t) {
+    return t == DType::F32 ? 4 : (t == DType::F64 ? 8 : 16);
+}
+
+struct cplx {
+    double re, im;
+};
+
+enum Trans : int { NoTrans = 111, TransT = 112, ConjT = 113 };
+
+// One column-major GEMM C = alpha op(A) op(B) + beta C. Pointers are host or
+// device addresses depending on the caller; leading dimensions in elements.
+struct Gemm {
+    DType dt;
+    int ta, tb;
+    int64_t M, N, K;
+    cplx alpha, beta;
+    const void *A;
+    int64_t lda;
+    const void *B;
+    int64_t ldb;
+    void *C;
+    int64_t ldc;
+
+    bool alpha_zero() const { return alpha.re == 0 && alpha.im == 0; }
+    bool beta_zero() const { return beta.re == 0 && beta.im == 0; }
+    bool beta_one() const { return beta.re == 1 && beta.im == 0; }
+    // stored (column-major) shapes of A and B
+    int64_t rows_a() const { return ta == NoTrans ? M : K; }
+    int64_t cols_a() const { return ta == NoTrans ? K : M; }
+    int64_t rows_b() const { return tb == NoTrans ? K : N; }
+    int64_t cols_b() const { return tb == NoTrans ? N : K; }
+    double flops() const {
+        return (dt == DType::C128 ? 8.0 : 2.0) * double(M) * double(N) * double(K);
+    }
+};
+
+// Records `status` and a formatted message for the calling thread, prints it
+// to stderr and returns `status`.
+int set_error(int status, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+void clear_error();
+int last_status();
+
+#define BX_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t bx_e_ = (call);                                                    \
+        if (bx_e_ != cudaSuccess)                                                      \
+            return ::bx::set_error(bx_e_ == cudaErrorMemoryAllocation ? BLASX_ERR_NOMEM \
+                                                                      : BLASX_ERR_CUDA, \
+                                   "%s:%d: %s failed: %s", __FILE__, __LINE__, #call,  \
+                                   cudaGetErrorString(bx_e_));                         \
+    } while (0)
+
+#define BX_TRY(expr)                     \
+    do {                                 \
+        int bx_s_ = (expr);              \
+        if (bx_s_ != BLASX_OK) return bx_s_; \
+    } while (0)
+
+// Library configuration, read once from the environment at first use and
+// adjustable through the blasx_set_* calls.
+struct Config {
+    std::atomic<int> dgemm_mode{0};    // 0 auto, 1 native, 2 ozaki
+    std::atomic<size_t> hbm_budget{0}; // 0 = default
+    std::atomic<int> tile{0};          // 0 = automatic
+};
+Config &config();
+
+// Per-process device state. Created lazily on the first GPU call.
+struct Context {
+    int device = 0;
+    int num_sms = 0;
+    size_t total_mem = 0;
+    cudaStream_t compute = nullptr;  // kernels
+    cudaStream_t h2d = nullptr;      // host -> device copies
+    cudaStream_t d2h = nullptr;      // device -> host copies
+    std::mutex host_mu;              // serialises host-pipeline calls
+};
+
+// Returns the context or nullptr (status recorded) when no GPU is usable.
+Context *context();
+int release_context();
+
+// Counts every kernel launch of the library (blasx_kernel_launch_count).
+void count_launch(int n = 1);
+
+// Thread-local statistics of the last host call.
+blasx_call_stats &call_stats();
+
+}  // namespace bx

@@ -1,0 +1,151 @@
+/*
+ * blasx_b200.h -- C ABI of the B200-native GEMM runtime.
+ *
+ * The first block is the drop-in boundary: the CBLAS and Fortran-77 GEMM
+ * symbols of linnanwang/BLASX, with the same signatures, enum values, argument
+ * meaning and xerbla_ error reporting. Operands are host-resident and
+ * column-major (row-major is accepted too, see below); the call is
+ * synchronous: C is complete when it returns.
+ *
+ * Differences from the reference, on purpose:
+ *   - every call with M, N > 0 runs on the GPU (no CPU BLAS, no size
+ *     threshold; the reference sends calls with all dims <= 1000 to a CPU
+ *     BLAS, blas/dgemm.c:61-64);
+ *   - CblasRowMajor is honoured (the reference ignores Order on its GPU path,
+ *     blas/dgemm.c:107), using the identity C^T = op(B)^T op(A)^T;
+ *   - the calls are thread-safe and re-entrant;
+ *   - internal CUDA failures never abort the process: the call reports to
+ *     stderr and records the status for blasx_last_status().
+ */
+#ifndef BLASX_B200_H
+#define BLASX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Enum values of the reference's include/cblas.h:11-12. */
+#ifndef CBLAS_ENUM_DEFINED_H
+#define CBLAS_ENUM_DEFINED_H
+enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
+enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 };
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in boundary                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces cblas_sgemm, include/cblas.h:424 (implementation blas/sgemm.c:16). */
+void cblas_sgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K,
+                 const float alpha, const float *A, const int lda, const float *B,
+                 const int ldb, const float beta, float *C, const int ldc);
+
+/* Replaces cblas_dgemm, include/cblas.h:454 (implementation blas/dgemm.c:18-128). */
+void cblas_dgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K,
+                 const double alpha, const double *A, const int lda, const double *B,
+                 const int ldb, const double beta, double *C, const int ldc);
+
+/* Replaces cblas_zgemm, include/cblas.h:514 (implementation blas/zgemm.c:16-130).
+ * alpha, beta, A, B, C point to interleaved (re, im) double pairs. */
+void cblas_zgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K,
+                 const void *alpha, const void *A, const int lda, const void *B,
+                 const int ldb, const void *beta, void *C, const int ldc);
+
+/* Replace the F77 wrappers sgemm_ (blas/sgemm.c), dgemm_ (blas/dgemm.c:131-154)
+ * and zgemm_ (blas/zgemm.c:133-156): every argument by pointer, trans chars
+ * 'N'/'T'/'C' in either case, column-major. */
+void sgemm_(char *transa, char *transb, int *m, int *n, int *k, float *alpha, float *A,
+            int *lda, float *B, int *ldb, float *beta, float *C, int *ldc);
+void dgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, double *A,
+            int *lda, double *B, int *ldb, double *beta, double *C, int *ldc);
+void zgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, double *A,
+            int *lda, double *B, int *ldb, double *beta, double *C, int *ldc);
+
+/* Replaces xerbla_, blas/error.c:5: prints
+ * " ** On entry to <NAME> parameter number <info> had an illegal value".
+ * Exported weak, so an application's own xerbla_ takes precedence. */
+void xerbla_(char *name, int *info);
+
+/* ------------------------------------------------------------------------ */
+/* Extensions (no counterpart in the reference)                              */
+/* ------------------------------------------------------------------------ */
+
+/* Status codes returned by the blasx_* calls and recorded per thread. */
+enum blasx_status {
+    BLASX_OK = 0,
+    BLASX_ERR_ARG = 1,      /* illegal argument (xerbla_ was called) */
+    BLASX_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+    BLASX_ERR_NOMEM = 3,    /* device allocation or budget exhausted */
+    BLASX_ERR_NODEVICE = 4, /* no usable GPU */
+    BLASX_ERR_TIMEOUT = 5,  /* a bounded device wait ran out */
+    BLASX_ERR_UNSUPPORTED = 6,
+    BLASX_ERR_CLOSED = 7    /* the serving loop was shut down */
+};
+
+/* Status of the calling thread's last GEMM call and its message. */
+int blasx_last_status(void);
+const char *blasx_last_error(void);
+
+/* DGEMM/ZGEMM precision mode: 0 = auto (Ozaki emulation when the measured
+ * exponent spread allows FP64 accuracy, native FP64 otherwise),
+ * 1 = native FP64 only, 2 = Ozaki emulation whenever it is feasible.
+ * Also read once from the environment variable BLASX_DGEMM_MODE
+ * (auto|native|ozaki). Returns the previous mode. */
+int blasx_set_dgemm_mode(int mode);
+
+/* Device tile-cache byte budget (0 = default: 90% of free HBM at first use;
+ * env BLASX_HBM_BUDGET, bytes, suffixes K/M/G accepted). Takes effect for
+ * calls that start after it returns. Returns 0 on success. */
+int blasx_set_hbm_budget(size_t bytes);
+
+/* Tile edge (rows = cols) used by the host pipeline, 0 = automatic
+ * (env BLASX_TILE). Multiple of 256, between 256 and 16384. */
+int blasx_set_tile(int tile);
+
+/* Per-call statistics of the calling thread's last host GEMM call. */
+typedef struct blasx_call_stats {
+    double seconds;           /* wall time of the call */
+    double h2d_bytes;         /* bytes copied host -> device */
+    double d2h_bytes;         /* bytes copied device -> host */
+    double cache_hits;        /* operand tiles found resident */
+    double cache_misses;      /* operand tiles copied in */
+    double evictions;         /* operand tiles evicted */
+    int path;                 /* 1 native, 2 Ozaki emulation, 3 scale-only */
+    int moduli;               /* Ozaki moduli used (0 when native) */
+    int tile;                 /* tile edge used */
+    int reserved;
+} blasx_call_stats;
+void blasx_get_call_stats(blasx_call_stats *out);
+
+/* Device-resident GEMM: A, B, C are device pointers (column-major), the call
+ * is enqueued on `stream` (a cudaStream_t, NULL = the library's own stream)
+ * and returns without waiting. Scalars are host values. Used by callers whose
+ * operands already live in HBM. Returns a blasx_status. */
+int blasx_dgemm_device(int transa, int transb, int M, int N, int K, double alpha,
+                       const double *A, int lda, const double *B, int ldb, double beta,
+                       double *C, int ldc, void *stream);
+int blasx_sgemm_device(int transa, int transb, int M, int N, int K, float alpha,
+                       const float *A, int lda, const float *B, int ldb, float beta, float *C,
+                       int ldc, void *stream);
+int blasx_zgemm_device(int transa, int transb, int M, int N, int K, const void *alpha,
+                       const void *A, int lda, const void *B, int ldb, const void *beta,
+                       void *C, int ldc, void *stream);
+
+/* Number of kernels this library has launched since it was loaded (all
+ * threads); lets a caller count the GPU work of a region. */
+uint64_t blasx_kernel_launch_count(void);
+
+/* Release all device memory and streams held by the library (the next call
+ * re-initialises). Returns a blasx_status. */
+int blasx_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLASX_B200_H */
