@@ -233,7 +233,11 @@ def main():
         return u
 
     A, B, C = gen(), gen(), gen()
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream: the library enqueues on it, and the
+    # CUDA events below are recorded on the same stream
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    torch.cuda.synchronize()
     flops = 2.0 * n ** 3
 
     def step():

@@ -94,7 +94,8 @@ int device_entry(DType dt, int ta, int tb, int M, int N, int K, cplx alpha, cons
     if (g.M == 0 || g.N == 0) return BLASX_OK;
     Context *c = context();
     if (!c) return last_status();
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->compute;
+    // NULL is the CUDA legacy default stream, as everywhere in the CUDA API
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (g.alpha_zero() || g.K == 0) return launch_scale(g, s);
     return device_gemm(g, s);
 }

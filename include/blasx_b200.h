@@ -124,7 +124,7 @@ typedef struct blasx_call_stats {
 void blasx_get_call_stats(blasx_call_stats *out);
 
 /* Device-resident GEMM: A, B, C are device pointers (column-major), the call
- * is enqueued on `stream` (a cudaStream_t, NULL = the library's own stream)
+ * is enqueued on `stream` (a cudaStream_t; NULL = the CUDA default stream)
  * and returns without waiting. Scalars are host values. Used by callers whose
  * operands already live in HBM. Returns a blasx_status. */
 int blasx_dgemm_device(int transa, int transb, int M, int N, int K, double alpha,
