@@ -74,6 +74,12 @@ int host_gemm(const Gemm &g) {
                               cudaMemcpyDeviceToHost, s));
     st.d2h_bytes += double(es) * g.M * g.N;
     BX_CUDA(cudaStreamSynchronize(s));
+    if (st.path == 2) {
+        resolve_decision(st);
+        if (*c->last_error_flag)
+            return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
+                             *c->last_error_flag);
+    }
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return BLASX_OK;
 }

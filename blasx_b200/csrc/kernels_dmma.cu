@@ -61,6 +61,7 @@ struct DmmaParams {
     int beta_zero;
     int tiles_m, tiles_n;
     int vec_a, vec_b;  // 16-byte copies allowed (ld even, base 16-byte aligned)
+    const int *guard;  // when set, run only if *guard == 0
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(kThreads, 1) dmma_gemm_kernel(const DmmaParams
     constexpr int A_STAGE = PLANES * SA::plane, B_STAGE = PLANES * SB::plane;  // doubles
     constexpr int IM = CPLX ? 1 : 0;
 
+    if (p.guard && *p.guard != 0) return;  // the emulated path produced C
     extern __shared__ __align__(16) double smem[];
     double *sA = smem;
     double *sB = smem + STAGES * A_STAGE;
@@ -365,6 +367,7 @@ template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
     p.tiles_n = int((g.N + TL::BN - 1) / TL::BN);
     p.vec_a = (g.lda % 2 == 0) && (reinterpret_cast<uintptr_t>(g.A) % 16 == 0);
     p.vec_b = (g.ldb % 2 == 0) && (reinterpret_cast<uintptr_t>(g.B) % 16 == 0);
+    p.guard = g.guard;
     if (int64_t(p.tiles_m) * p.tiles_n > INT32_MAX)
         return set_error(BLASX_ERR_UNSUPPORTED, "DMMA grid too large");
     const bool akc = g.ta != NoTrans;  // op(A) = A^T: stored K x M, k contiguous

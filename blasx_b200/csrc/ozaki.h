@@ -1,0 +1,80 @@
+// ozaki.h -- FP64/FP32/complex GEMM emulated with INT8 tensor-core GEMMs
+// (Ozaki scheme II: integer scaling + Chinese-remainder reconstruction).
+//
+// Method (Ozaki, Uchino, Imamura, "Ozaki Scheme II: A GEMM-oriented emulation
+// of floating-point matrix multiplication using an integer modular
+// technique", 2025), restated for this runtime:
+//   1. every row of op(A) and column of op(B) is scaled by a power of two and
+//      rounded to an integer (|a'| < 2^62, row 2-norm < 2^Q) so that every
+//      dot product of scaled rows is bounded by M/4, M = prod of the moduli;
+//   2. for each modulus m_l (pairwise coprime, <= 256) the scaled integers are
+//      reduced to symmetric residues in int8;
+//   3. one INT8 GEMM per modulus on the tcgen05 tensor cores accumulates in
+//      INT32 exactly (|residue| <= 128, K <= 65536); its epilogue reduces the
+//      accumulator mod m_l to a uint8 residue;
+//   4. the residues are recombined exactly by the CRT in multi-limb integer
+//      arithmetic, converted to floating point, unscaled, and the alpha/beta
+//      epilogue is applied in FP64.
+// The number of moduli is chosen on the device from the measured spread of
+// the operands (row/column norm ratios); when no count up to kMaxModuli can
+// reach the target accuracy the call falls back to the native FP64 kernel,
+// also decided on the device (no host synchronisation).
+#pragma once
+
+#include <cstdint>
+
+#include "runtime.h"
+
+namespace bx {
+namespace oz {
+
+constexpr int kMaxModuli = 20;
+constexpr int kMinModuli = 6;
+constexpr int kLimbs = 6;  // 32-bit limbs of CRT weights / products (M < 2^160)
+constexpr int kMaxK = 65536;  // INT32-exact accumulation bound (complex uses 2K)
+
+// Padded extents used by the INT8 GEMM tiles.
+constexpr int kTileJ = 128;  // MMA M (rows = columns of C)
+constexpr int kTileI = 256;  // MMA N (rows of C)
+constexpr int kTileK = 128;  // bytes of K per pipeline stage
+
+inline int64_t pad(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Device-side decision record written by the decide kernel.
+struct Decision {
+    int nmod;      // 0 = native fallback
+    int q;         // norm exponent bound Q
+    double estimate;  // estimated max normalised error (units of the dtype's u)
+    int nonfinite;
+    int pad;
+};
+
+// Row/column statistics of one operand (R rows of op(X), each over K).
+struct RowStats {
+    double *amax;    // max |x|
+    double *sumsq;   // sum x^2
+    double *sumabs;  // sum |x|
+    int *flags;      // bit 0: non-finite value seen
+};
+
+// INT8 residue GEMM: for every modulus l < *nmod,
+//   U_l[j][i] = (sum_k X_l[j][k] * Y_l[i][k]) mod m_l   (uint8, ldu = Ip)
+// X: [kMaxModuli][Jp][Kp] int8, Y: [kMaxModuli][Ip][Kp] int8 (K-major).
+// Kp multiple of 128, Jp of 128, Ip of 256. Returns a blasx status.
+int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
+                        int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
+                        cudaStream_t s);
+
+// Host-side CRT constant tables (uploaded once to constant memory).
+int upload_crt_tables();
+
+// The moduli (largest first).
+extern const int kModuli[kMaxModuli];
+
+}  // namespace oz
+
+// Emulated GEMM on device-resident operands. Chooses the modulus count on
+// the device; falls back to the native kernel on the device when needed.
+int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode);
+
+}  // namespace bx

@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "ozaki.h"
 #include "runtime.h"
 
 namespace bx {
@@ -77,6 +78,13 @@ blasx_call_stats &call_stats() { return t_stats; }
 
 void count_launch(int n) { g_launches.fetch_add(uint64_t(n), std::memory_order_relaxed); }
 
+void resolve_decision(blasx_call_stats &st) {
+    if (st.path != 2 || !g_ctx) return;
+    const oz::Decision *d = static_cast<const oz::Decision *>(g_ctx->last_decision);
+    st.moduli = d->nmod;
+    if (d->nmod == 0) st.path = 4;  // native fallback chosen on the device
+}
+
 Context *context() {
     std::lock_guard<std::mutex> lk(g_ctx_mu);
     if (g_ctx) {
@@ -113,6 +121,15 @@ Context *context() {
     }
     c->num_sms = prop.multiProcessorCount;
     c->total_mem = prop.totalGlobalMem;
+    void *pinned = nullptr;
+    if ((e = cudaHostAlloc(&pinned, 256, cudaHostAllocDefault)) != cudaSuccess) {
+        set_error(BLASX_ERR_CUDA, "pinned slot allocation failed: %s", cudaGetErrorString(e));
+        delete c;
+        return nullptr;
+    }
+    memset(pinned, 0, 256);
+    c->last_decision = pinned;
+    c->last_error_flag = reinterpret_cast<int *>(static_cast<char *>(pinned) + 128);
     // keep freed pool memory cached in the device pool between calls
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) {
@@ -131,6 +148,7 @@ int release_context() {
     cudaStreamDestroy(g_ctx->compute);
     cudaStreamDestroy(g_ctx->h2d);
     cudaStreamDestroy(g_ctx->d2h);
+    cudaFreeHost(g_ctx->last_decision);
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, g_ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     delete g_ctx;
@@ -163,7 +181,9 @@ int blasx_set_tile(int tile) {
 }
 
 void blasx_get_call_stats(blasx_call_stats *out) {
-    if (out) *out = bx::call_stats();
+    if (!out) return;
+    *out = bx::call_stats();
+    bx::resolve_decision(*out);
 }
 
 int blasx_finalize(void) { return bx::release_context(); }

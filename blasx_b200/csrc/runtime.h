@@ -39,6 +39,9 @@ struct Gemm {
     int64_t ldb;
     void *C;
     int64_t ldc;
+    // Device pointer; when set, the native kernels return at once unless
+    // *guard == 0 (the emulated path chose its native fallback on the device).
+    const int *guard = nullptr;
 
     bool alpha_zero() const { return alpha.re == 0 && alpha.im == 0; }
     bool beta_zero() const { return beta.re == 0 && beta.im == 0; }
@@ -93,6 +96,10 @@ struct Context {
     cudaStream_t h2d = nullptr;      // host -> device copies
     cudaStream_t d2h = nullptr;      // device -> host copies
     std::mutex host_mu;              // serialises host-pipeline calls
+    // pinned host slots the emulated path copies its device decision and
+    // error flag into (valid once the stream has passed the copy)
+    void *last_decision = nullptr;   // oz::Decision
+    int *last_error_flag = nullptr;
 };
 
 // Returns the context or nullptr (status recorded) when no GPU is usable.
@@ -104,5 +111,8 @@ void count_launch(int n = 1);
 
 // Thread-local statistics of the last host call.
 blasx_call_stats &call_stats();
+// Fills the modulus count / fallback of an emulated call from the pinned
+// decision slot (valid once the stream has passed the call).
+void resolve_decision(blasx_call_stats &st);
 
 }  // namespace bx

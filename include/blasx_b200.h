@@ -116,7 +116,9 @@ typedef struct blasx_call_stats {
     double cache_hits;        /* operand tiles found resident */
     double cache_misses;      /* operand tiles copied in */
     double evictions;         /* operand tiles evicted */
-    int path;                 /* 1 native, 2 Ozaki emulation, 3 scale-only */
+    int path;                 /* 1 native, 2 Ozaki emulation, 3 scale-only,
+                                 4 emulation requested, native chosen on the
+                                 device (spread too wide or non-finite input) */
     int moduli;               /* Ozaki moduli used (0 when native) */
     int tile;                 /* tile edge used */
     int reserved;
