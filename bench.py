@@ -166,6 +166,20 @@ def reference_cpu_sample(n: int, seconds: float, cores: int, steps: int = 1, war
     return out, sample, kind, (ref.name if hasattr(ref, "name") else oracle.REF_PATH)
 
 
+def traffic_for(kernel: str, n: int):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any.
+
+    profiles/roofline_traffic.json maps "<kernel>@<n>" to the
+    dram__bytes_read.sum + dram__bytes_write.sum of one captured launch."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        with open(path) as f:
+            table = json.load(f)
+        return table.get(f"{kernel}@{n}")
+    except (OSError, ValueError):
+        return None
+
+
 # ---------------------------------------------------------------------------
 
 def main():
@@ -253,6 +267,7 @@ def main():
     # --- timed region (device-resident) ---
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = bx.kernel_launch_count()
+    bx.profile_enable(True)  # per-phase CUDA events on the launching stream
     with ClockSampler(local) as clk:
         barrier(); torch.cuda.synchronize()
         ev0.record(stream)
@@ -261,6 +276,9 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize(); barrier()
     launches = bx.kernel_launch_count() - launches0
+    phases = bx.profile_read()
+    bx.profile_enable(False)
+    stats = bx.call_stats()
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
     value = world * flops / (ms * 1e-3) / 1e12
 
@@ -279,23 +297,46 @@ def main():
         native = {"value": world * flops / (nms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": nms}
         bx.set_dgemm_mode(mode)
 
-    # --- pipe peak: cuBLAS DGEMM on this box, measured now ---
+    # --- pipe peaks on this box, measured now with the vendor library ---
+    def lib_rate(fn, ops, reps=3):
+        fn(); torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record(); torch.cuda.synchronize()
+        return reps * ops / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
     x = torch.rand((8192, 8192), dtype=torch.float64, device="cuda")
-    y = torch.rand((8192, 8192), dtype=torch.float64, device="cuda")
-    torch.matmul(x, y); torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(3):
-        torch.matmul(x, y)
-    e1.record(); torch.cuda.synchronize()
-    fp64_peak = 3 * 2.0 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
-    del x, y
+    fp64_peak = lib_rate(lambda: torch.matmul(x, x), 2.0 * 8192 ** 3)
+    del x
+    xi = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+    yi = xi.t().contiguous().t()
+    int8_peak = lib_rate(lambda: torch._int_mm(xi, yi), 2.0 * 8192 ** 3)
+    del xi, yi
 
     per_gpu = flops / (ms * 1e-3) / 1e12
-    roofline = {"bound": "tensor", "pipe": "fp64 (DMMA)", "kernel": "whole DGEMM step",
-                "achieved": per_gpu, "peak": fp64_peak, "unit": "TFLOP/s", "frac": per_gpu / fp64_peak,
-                "peak_source": "cuBLAS DGEMM 8192^3 via torch.matmul, measured in this run",
-                "traffic": None}
+    path = {1: "native", 2: "ozaki", 3: "scale", 4: "native (device fallback)"}.get(stats["path"], "?")
+    phase_ms = {k: v["ms"] / max(1, args.steps) for k, v in phases.items()}
+    if stats["path"] == 2:
+        gemm_ms = phase_ms["residue_gemm"]
+        int8_ops = 2.0 * n ** 3 * stats["moduli"]  # one M x N x K INT8 GEMM per modulus
+        achieved = int8_ops / (gemm_ms * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "pipe": "int8 (tcgen05.mma kind::i8)",
+                    "kernel": "residue_gemm_kernel (all moduli of one step)",
+                    "achieved": achieved, "peak": int8_peak, "unit": "TOP/s", "frac": achieved / int8_peak,
+                    "peak_source": "cuBLASLt INT8 GEMM 8192^3 (torch._int_mm), measured in this run",
+                    "algorithmic_ops_per_launch": int8_ops, "ms_per_launch": gemm_ms,
+                    "traffic": traffic_for("residue_gemm_kernel", n)}
+    else:
+        kms = phase_ms["native"] or ms
+        achieved = flops / (kms * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "pipe": "fp64 (DMMA mma.sync)", "kernel": "dmma_gemm_kernel",
+                    "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                    "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul), measured in this run",
+                    "algorithmic_ops_per_launch": flops, "ms_per_launch": kms,
+                    "traffic": traffic_for("dmma_gemm_kernel", n)}
+    fp64_equiv = {"value": per_gpu, "frac_of_fp64_peak": per_gpu / fp64_peak, "fp64_peak": fp64_peak}
 
     # --- e2e through the drop-in ABI with pinned host buffers ---
     e2e = None
@@ -335,8 +376,8 @@ def main():
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": config,
-                "path": {1: "native", 2: "ozaki", 3: "scale"}.get(stats["path"], str(stats["path"])),
-                "moduli": stats["moduli"], "native": native, "e2e": e2e, "roofline": roofline,
+                "path": path, "moduli": stats["moduli"], "phases_ms_per_step": phase_ms,
+                "fp64_equivalent": fp64_equiv, "native": native, "e2e": e2e, "roofline": roofline,
                 "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary(),
                 "vs_published_blasx_1gpu_16384": value * 1e3 / PUBLISHED_BLASX_1GPU_16384_GFLOPS}
         print(json.dumps(line), flush=True)

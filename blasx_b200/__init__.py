@@ -75,6 +75,8 @@ def lib() -> ctypes.CDLL:
         L.blasx_sgemm_device.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I, _P]
         L.blasx_zgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
         L.blasx_kernel_launch_count.restype = ctypes.c_uint64
+        L.blasx_profile_enable.argtypes = [_I]
+        L.blasx_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long), _I]
         _lib = L
     return _lib
 
@@ -215,3 +217,19 @@ def set_tile(tile: int) -> int:
 
 def finalize() -> int:
     return lib().blasx_finalize()
+
+
+PHASES = ("slice", "residue_gemm", "reconstruct", "native")
+
+
+def profile_enable(on: bool = True) -> bool:
+    """Turn per-phase CUDA-event timing on/off (resets the totals)."""
+    return bool(lib().blasx_profile_enable(1 if on else 0))
+
+
+def profile_read() -> dict:
+    """Per-phase device time (ms) and span counts since profile_enable."""
+    ms = (ctypes.c_double * 4)()
+    cnt = (ctypes.c_long * 4)()
+    lib().blasx_profile_read(ms, cnt, 4)
+    return {p: {"ms": ms[i], "count": cnt[i]} for i, p in enumerate(PHASES)}

@@ -9,6 +9,7 @@
 //   ozaki   -- the Ozaki path whenever K is within its exact range.
 #include "kernels.h"
 #include "ozaki.h"
+#include "profile.h"
 
 namespace bx {
 
@@ -34,8 +35,10 @@ int device_gemm(const Gemm &g, cudaStream_t s) {
     if (oz) return ozaki_gemm(g, s, mode);
     call_stats().path = 1;
     call_stats().moduli = 0;
-    if (dmma_supported(g)) return launch_gemm_dmma(g, s);
-    return launch_gemm_simt(g, s);
+    cudaEvent_t e0 = prof::mark(s);
+    const int st = dmma_supported(g) ? launch_gemm_dmma(g, s) : launch_gemm_simt(g, s);
+    prof::span(prof::kNative, e0, prof::mark(s));
+    return st;
 }
 
 }  // namespace bx

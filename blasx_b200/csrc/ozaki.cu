@@ -16,6 +16,7 @@
 
 #include "kernels.h"
 #include "ozaki.h"
+#include "profile.h"
 
 namespace bx {
 namespace oz {
@@ -721,6 +722,7 @@ template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
     int8_t *X = cv.take<int8_t>(size_t(L) * Jx * Kp);
     uint8_t *U = cv.take<uint8_t>(size_t(L) * Jx * Ip);
     const size_t stats_bytes = reinterpret_cast<char *>(ea) - static_cast<char *>(ws);
+    cudaEvent_t ev0 = prof::mark(s);
     BX_CUDA(cudaMemsetAsync(ws, 0, stats_bytes, s));
     BX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
 
@@ -744,7 +746,9 @@ template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
         BX_TRY((launch_slice<T, 0>(va, akc, sa, dec, ea, oy, Kc, s)));
         BX_TRY((launch_slice<T, 0>(vb, bkc, sb, dec, fb, ox, Kc, s)));
     }
+    cudaEvent_t ev1 = prof::mark(s);
     BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, ctx->num_sms, s));
+    cudaEvent_t ev2 = prof::mark(s);
 
     dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(N));
     if constexpr (CPLX) {
@@ -760,11 +764,18 @@ template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
     BX_CUDA(cudaGetLastError());
     count_launch();
 
+    cudaEvent_t ev3 = prof::mark(s);
+
     // native fallback, decided on the device (runs only when nmod == 0)
     Gemm gn = g;
     gn.guard = &dec->nmod;
     if (g.dt == DType::F32) BX_TRY(launch_gemm_simt(gn, s));
     else BX_TRY(launch_gemm_dmma(gn, s));
+    cudaEvent_t ev4 = prof::mark(s);
+    prof::span(prof::kSlice, ev0, ev1);
+    prof::span(prof::kResidueGemm, ev1, ev2);
+    prof::span(prof::kReconstruct, ev2, ev3);
+    prof::span(prof::kNative, ev3, ev4);
 
     // record the decision for blasx_get_call_stats (lands when the stream does)
     BX_CUDA(cudaMemcpyAsync(ctx->last_decision, dec, sizeof(oz::Decision), cudaMemcpyDeviceToHost, s));

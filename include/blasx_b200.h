@@ -143,6 +143,16 @@ int blasx_zgemm_device(int transa, int transb, int M, int N, int K, const void *
  * threads); lets a caller count the GPU work of a region. */
 uint64_t blasx_kernel_launch_count(void);
 
+/* Per-phase device timing. When enabled, every GEMM records CUDA events on
+ * its own stream around its phases: 0 slicing (emulated path: statistics,
+ * modulus decision, scaling, residues), 1 INT8 residue GEMMs, 2 CRT
+ * reconstruction and epilogue, 3 native kernel. blasx_profile_enable resets
+ * the totals and returns the previous setting; blasx_profile_read waits for
+ * the recorded events, writes up to n totals (milliseconds) and span counts,
+ * and returns the number of phases. */
+int blasx_profile_enable(int on);
+int blasx_profile_read(double *ms, long *count, int n);
+
 /* Release all device memory and streams held by the library (the next call
  * re-initialises). Returns a blasx_status. */
 int blasx_finalize(void);
