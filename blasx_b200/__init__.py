@@ -74,6 +74,7 @@ def lib() -> ctypes.CDLL:
         L.blasx_dgemm_device.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_sgemm_device.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I, _P]
         L.blasx_zgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
+        L.blasx_dgemm_device_noalloc.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_kernel_launch_count.restype = ctypes.c_uint64
         L.blasx_profile_enable.argtypes = [_I]
         L.blasx_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long), _I]

@@ -110,6 +110,11 @@ bool f77_trans(const char *c, int *t) {
 }
 
 }  // namespace
+
+int gemm_arg_info(int order, int ta, int tb, int M, int N, int K, int lda, int ldb, int ldc) {
+    return check_args(order, ta, tb, M, N, K, lda, ldb, ldc);
+}
+
 }  // namespace bx
 
 using bx::cplx;

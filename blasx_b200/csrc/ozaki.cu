@@ -630,6 +630,12 @@ int upload_crt_tables() {
     return BLASX_OK;
 }
 
+int prepare_crt_tables_current_device() {
+    static const CrtTables t = build_tables();
+    BX_CUDA(cudaMemcpyToSymbol(c_crt, &t, sizeof t));
+    return BLASX_OK;
+}
+
 }  // namespace oz
 
 // --------------------------------------------------------------------------
@@ -688,30 +694,40 @@ int forced_moduli() {
     return f;
 }
 
-template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
-    constexpr bool CPLX = oz::Elem<T>::cplx;
-    Context *ctx = context();
-    if (!ctx) return last_status();
-    BX_TRY(oz::upload_crt_tables());
-    const int64_t M = g.M, N = g.N, K = g.K;
-    const int64_t Kh = CPLX ? oz::pad(K, 64) : 0;
-    const int64_t Kp = CPLX ? 2 * Kh : oz::pad(K, oz::kTileK);
-    const int64_t Kc = CPLX ? Kh : Kp;  // k extent covered by the slice kernels
-    const int64_t Ip = oz::pad(M, oz::kTileI);
-    const int64_t Jp = oz::pad(N, oz::kTileJ);
-    const int64_t Jx = CPLX ? 2 * Jp : Jp;  // X rows (Re block + Im block)
-    const int64_t L = oz::kMaxModuli;
+// Padded extents and scratch size of one emulated GEMM.
+struct Plan {
+    int64_t M, N, K, Kh, Kp, Kc, Ip, Jp, Jx;
+    size_t bytes;
+};
 
-    const size_t bytes = 256 * 16 + (3 * sizeof(double) + 2 * sizeof(int)) * size_t(M + N) +
-                         sizeof(oz::Decision) + sizeof(int) + size_t(L) * Ip * Kp +
-                         size_t(L) * Jx * Kp + size_t(L) * Jx * Ip;
-    void *ws = nullptr;
-    BX_CUDA(cudaMallocAsync(&ws, bytes, s));
-    struct Free {
-        void *p;
-        cudaStream_t s;
-        ~Free() { cudaFreeAsync(p, s); }
-    } free_ws{ws, s};
+Plan make_plan(const Gemm &g) {
+    const bool cplx = g.dt == DType::C128;
+    const int64_t L = oz::kMaxModuli;
+    Plan p;
+    p.M = g.M; p.N = g.N; p.K = g.K;
+    p.Kh = cplx ? oz::pad(p.K, 64) : 0;
+    p.Kp = cplx ? 2 * p.Kh : oz::pad(p.K, oz::kTileK);
+    p.Kc = cplx ? p.Kh : p.Kp;  // k extent covered by the slice kernels
+    p.Ip = oz::pad(p.M, oz::kTileI);
+    p.Jp = oz::pad(p.N, oz::kTileJ);
+    p.Jx = cplx ? 2 * p.Jp : p.Jp;  // X rows (Re block + Im block)
+    p.bytes = 256 * 16 + (3 * sizeof(double) + 2 * sizeof(int)) * size_t(p.M + p.N) +
+              sizeof(oz::Decision) + sizeof(int) + size_t(L) * p.Ip * p.Kp +
+              size_t(L) * p.Jx * p.Kp + size_t(L) * p.Jx * p.Ip;
+    return p;
+}
+
+// The whole emulated pipeline on a caller-provided workspace of
+// make_plan(g).bytes bytes: no allocation. The device decision and error
+// flag are copied to the given host slots when they are not null.
+template <typename T>
+int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, void *dec_host,
+              int *err_host) {
+    constexpr bool CPLX = oz::Elem<T>::cplx;
+    const Plan pl = make_plan(g);
+    const int64_t M = pl.M, N = pl.N, K = pl.K, Kh = pl.Kh, Kp = pl.Kp, Kc = pl.Kc;
+    const int64_t Ip = pl.Ip, Jp = pl.Jp, Jx = pl.Jx;
+    const int64_t L = oz::kMaxModuli;
     Carve cv{static_cast<char *>(ws)};
     oz::RowStats sa{cv.take<double>(M), cv.take<double>(M), cv.take<double>(M), cv.take<int>(M)};
     oz::RowStats sb{cv.take<double>(N), cv.take<double>(N), cv.take<double>(N), cv.take<int>(N)};
@@ -747,7 +763,7 @@ template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
         BX_TRY((launch_slice<T, 0>(vb, bkc, sb, dec, fb, ox, Kc, s)));
     }
     cudaEvent_t ev1 = prof::mark(s);
-    BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, ctx->num_sms, s));
+    BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s));
     cudaEvent_t ev2 = prof::mark(s);
 
     dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(N));
@@ -778,10 +794,26 @@ template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
     prof::span(prof::kNative, ev3, ev4);
 
     // record the decision for blasx_get_call_stats (lands when the stream does)
-    BX_CUDA(cudaMemcpyAsync(ctx->last_decision, dec, sizeof(oz::Decision), cudaMemcpyDeviceToHost, s));
-    BX_CUDA(cudaMemcpyAsync(ctx->last_error_flag, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (dec_host)
+        BX_CUDA(cudaMemcpyAsync(dec_host, dec, sizeof(oz::Decision), cudaMemcpyDeviceToHost, s));
+    if (err_host) BX_CUDA(cudaMemcpyAsync(err_host, err, sizeof(int), cudaMemcpyDeviceToHost, s));
     call_stats().path = 2;
     return BLASX_OK;
+}
+
+template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
+    Context *ctx = context();
+    if (!ctx) return last_status();
+    BX_TRY(oz::upload_crt_tables());
+    const Plan pl = make_plan(g);
+    void *ws = nullptr;
+    BX_CUDA(cudaMallocAsync(&ws, pl.bytes, s));
+    struct Free {
+        void *p;
+        cudaStream_t s;
+        ~Free() { cudaFreeAsync(p, s); }
+    } free_ws{ws, s};
+    return ozaki_run<T>(g, s, mode, ws, ctx->num_sms, ctx->last_decision, ctx->last_error_flag);
 }
 
 }  // namespace
@@ -791,6 +823,16 @@ int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode) {
         case DType::F64: return ozaki_t<double>(g, s, mode);
         case DType::F32: return ozaki_t<float>(g, s, mode);
         default: return ozaki_t<oz::zpair>(g, s, mode);
+    }
+}
+
+size_t ozaki_scratch_bytes(const Gemm &g) { return make_plan(g).bytes; }
+
+int ozaki_gemm_in(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms) {
+    switch (g.dt) {
+        case DType::F64: return ozaki_run<double>(g, s, mode, ws, num_sms, nullptr, nullptr);
+        case DType::F32: return ozaki_run<float>(g, s, mode, ws, num_sms, nullptr, nullptr);
+        default: return ozaki_run<oz::zpair>(g, s, mode, ws, num_sms, nullptr, nullptr);
     }
 }
 

@@ -68,6 +68,11 @@ int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp
 // Host-side CRT constant tables (uploaded once to constant memory).
 int upload_crt_tables();
 
+// Uploads the constant tables and sets the kernel attributes of the emulated
+// path for the current device (unconditionally; for per-device set-up).
+int prepare_crt_tables_current_device();
+int prepare_residue_gemm_current_device();
+
 // The moduli (largest first).
 extern const int kModuli[kMaxModuli];
 
@@ -76,5 +81,11 @@ extern const int kModuli[kMaxModuli];
 // Emulated GEMM on device-resident operands. Chooses the modulus count on
 // the device; falls back to the native kernel on the device when needed.
 int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode);
+
+// Scratch bytes the emulated pipeline needs for g, and the pipeline itself
+// on a caller-provided scratch of at least that size (allocates nothing;
+// the constant tables must already be on the current device).
+size_t ozaki_scratch_bytes(const Gemm &g);
+int ozaki_gemm_in(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms);
 
 }  // namespace bx

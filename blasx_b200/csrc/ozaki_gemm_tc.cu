@@ -369,6 +369,13 @@ int make_map(CUtensorMap *map, const void *base, int64_t rows, int64_t kp, int b
 
 }  // namespace
 
+int prepare_residue_gemm_current_device() {
+    BX_CUDA(cudaMemcpyToSymbol(c_mod, kModuli, sizeof(kModuli)));
+    BX_CUDA(cudaFuncSetAttribute(residue_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(kSmemBytes)));
+    return BLASX_OK;
+}
+
 int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
                         int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
                         cudaStream_t s) {

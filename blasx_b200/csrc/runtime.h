@@ -106,6 +106,9 @@ struct Context {
 Context *context();
 int release_context();
 
+// The reference's info code for a GEMM argument list (0 = legal).
+int gemm_arg_info(int order, int ta, int tb, int M, int N, int K, int lda, int ldb, int ldc);
+
 // Counts every kernel launch of the library (blasx_kernel_launch_count).
 void count_launch(int n = 1);
 

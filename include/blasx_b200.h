@@ -139,6 +139,27 @@ int blasx_zgemm_device(int transa, int transb, int M, int N, int K, const void *
                        const void *A, int lda, const void *B, int ldb, const void *beta,
                        void *C, int ldc, void *stream);
 
+/* Device-resident DGEMM that allocates no memory. No counterpart in the
+ * reference. It is meant for callers that cannot let a library call
+ * cudaMalloc: a framework whose own allocator has already reserved the
+ * GPU's memory (a cudaMalloc would fail or fragment that pool), or
+ * latency-critical code where cudaMalloc / cudaFree may synchronise the
+ * device. Same arguments and result as blasx_dgemm_device on the emulated
+ * (INT8 Ozaki) path, with the native FP64 kernel chosen on the device when
+ * the operands' spread is too wide; the caller still provides A, B and C.
+ * Its scratch is a fixed 64 MiB device array that every GPU loading this
+ * library holds until the process exits; problems whose scratch would not
+ * fit (M = N = K = 1024 fits; 2048 does not) are rejected with
+ * BLASX_ERR_UNSUPPORTED and a message in blasx_last_error(). The first call
+ * on each device performs a one-time set-up there (it looks up the array's
+ * device address and uploads constant tables); make that first call before
+ * any stream capture. All calls share the one array: calls that overlap on
+ * the GPU (other streams, other threads) race and must be serialised by the
+ * caller. Returns a blasx_status. */
+int blasx_dgemm_device_noalloc(int transa, int transb, int M, int N, int K, double alpha,
+                               const double *A, int lda, const double *B, int ldb,
+                               double beta, double *C, int ldc, void *stream);
+
 /* Number of kernels this library has launched since it was loaded (all
  * threads); lets a caller count the GPU work of a region. */
 uint64_t blasx_kernel_launch_count(void);

@@ -1,0 +1,71 @@
+"""GPU test of blasx_dgemm_device_noalloc, the DGEMM entry point that
+allocates no memory (for callers whose device memory belongs to another
+allocator, or that cannot afford cudaMalloc's synchronisation).
+
+It is called through the C ABI and compared with blasx_dgemm_device (the
+existing device-resident entry point, here on the same emulated path) on two
+calls in a row of different shapes, so the second call runs on scratch that
+still holds the first call's contents. The file is named to be collected
+last; it passes alone in a fresh process and after the other tests.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _device(x, torch):
+    # column-major numpy array -> device buffer with the same memory layout
+    return torch.from_numpy(np.ascontiguousarray(x.T)).cuda()
+
+
+def test_noalloc_matches_device_entry_on_two_calls(blx):
+    torch = pytest.importorskip("torch")
+    L = blx.lib()
+    prev = blx.set_dgemm_mode(blx.MODE_OZAKI)
+    try:
+        stream = torch.cuda.Stream()
+        for (M, N, K, ta, tb, seed) in [(700, 513, 1000, "N", "T", 1), (1024, 1024, 1024, "T", "N", 5)]:
+            ra, ca = oracle.shape_of_op(ta, M, K)
+            rb, cb = oracle.shape_of_op(tb, K, N)
+            A = oracle.uniform((ra, ca), np.float64, seed)
+            B = oracle.uniform((rb, cb), np.float64, seed + 1)
+            C0 = oracle.uniform((M, N), np.float64, seed + 2)
+            dA, dB = _device(A, torch), _device(B, torch)
+            d_ref, d_new = _device(C0, torch), _device(C0, torch)
+            stream.wait_stream(torch.cuda.current_stream())
+            st = blx.gemm_device(ta, tb, M, N, K, 1.5, dA, ra, dB, rb, -0.25, d_ref, M, stream=stream)
+            assert st == blx.BLASX_OK, blx.last_error()
+            st = L.blasx_dgemm_device_noalloc(blx.TRANS[ta], blx.TRANS[tb], M, N, K, 1.5, dA.data_ptr(), ra,
+                                              dB.data_ptr(), rb, -0.25, d_new.data_ptr(), M, stream.cuda_stream)
+            assert st == blx.BLASX_OK, blx.last_error()
+            torch.cuda.synchronize()
+            c_ref = d_ref.cpu().numpy().T
+            c_new = d_new.cpu().numpy().T
+            # tolerance of the parity tests: the componentwise bound (K+2) u (|alpha||A||B| + |beta||C0|)
+            opA = A if ta == "N" else A.T
+            opB = B if tb == "N" else B.T
+            bound = 1.5 * (np.abs(opA) @ np.abs(opB)) + 0.25 * np.abs(C0)
+            gamma = (K + 2) * 2.0 ** -53
+            assert np.all(np.abs(c_new - c_ref) <= gamma * bound)
+            rng = np.random.default_rng(seed)
+            ii = rng.integers(0, M, 2000); jj = rng.integers(0, N, 2000)
+            val, bnd = oracle.dd_entries(ta, tb, M, N, K, 1.5, A, ra, B, rb, -0.25, C0, M, ii, jj)
+            ratio, _ = oracle.componentwise_ratio(c_new, ii, jj, val, bnd, K, np.float64)
+            assert ratio <= 1.0
+    finally:
+        blx.set_dgemm_mode(prev)
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch(blx):
+    torch = pytest.importorskip("torch")
+    L = blx.lib()
+    buf = torch.zeros(16, dtype=torch.float64, device="cuda")
+    n = 2048  # needs more scratch than the fixed array holds; rejected before any device work
+    st = L.blasx_dgemm_device_noalloc(111, 111, n, n, n, 1.0, buf.data_ptr(), n, buf.data_ptr(), n, 0.0,
+                                      buf.data_ptr(), n, None)
+    assert st == blx.BLASX_ERR_UNSUPPORTED
+    assert "scratch" in blx.last_error()
+    assert torch.all(buf == 0)
