@@ -276,19 +276,46 @@ __device__ __forceinline__ uint32_t modulus_of(int l) {
     }
 }
 
-// Symmetric residue of a (|v| < 2^63) modulo the l-th modulus, as int8. With
-// l a compile-time constant after unrolling, the divisions by m become
-// multiply-high sequences.
-__device__ __forceinline__ int32_t sym_residue(int64_t v, int l) {
+// v + 2^62 (|v| < 2^62, so the biased value is in [0, 2^63)) split into
+// 21-bit digits, computed once per element and shared by all moduli.
+struct Digits {
+    uint32_t d0, d1, d2;
+};
+__device__ __forceinline__ Digits digits_of(int64_t v) {
+    const uint64_t a = uint64_t(v) + (uint64_t(1) << 62);
+    return {uint32_t(a) & 0x1FFFFFu, uint32_t(a >> 21) & 0x1FFFFFu, uint32_t(a >> 42)};
+}
+
+// Residue in [0, m) of the biased value minus the bias, for the l-th modulus:
+//   t = d2 (2^42 mod m) + d1 (2^21 mod m) + d0 + (-2^62 mod m) < 2^31,
+//   t mod m = floor(t ceil(2^39/m) / 2^39), exact for t < 2^31 and m <= 256
+// (the rounding error of the magic multiplier stays below 1/m). With l a
+// compile-time constant after unrolling, every constant folds: two IMADs,
+// one multiply-high, one shift, one IMAD.
+__device__ __forceinline__ uint32_t residue_u(const Digits &x, int l) {
     const uint32_t m = modulus_of(l);
-    const uint32_t c32 = uint32_t((uint64_t(1) << 32) % m);
-    const uint64_t a = v < 0 ? uint64_t(-v) : uint64_t(v);
-    const uint32_t hi = uint32_t(a >> 32), lo = uint32_t(a);
-    uint32_t r = ((hi % m) * c32 + (lo % m)) % m;
-    if (v < 0 && r) r = m - r;
-    int32_t s = int32_t(r);
-    if (s > int32_t(m - 1) / 2) s -= int32_t(m);
-    return s;
+    const uint32_t c21 = uint32_t((uint64_t(1) << 21) % m);
+    const uint32_t c42 = uint32_t((uint64_t(1) << 42) % m);
+    const uint32_t cb = uint32_t((m - (uint64_t(1) << 62) % m) % m);
+    const uint32_t magic = uint32_t(((uint64_t(1) << 39) + m - 1) / m);
+    const uint32_t t = x.d2 * c42 + x.d1 * c21 + (x.d0 + cb);  // < 2^21 * 512 + 256 < 2^31
+    const uint32_t q = __umulhi(t, magic) >> 7;
+    return t - q * m;
+}
+
+// Four residues packed as bytes, mapped to the symmetric int8 range:
+// bytes above (m-1)/2 take m off (mod 256), 4 at a time with SIMD byte ops.
+// For m = 256 the byte already is the two's complement of the symmetric
+// residue.
+__device__ __forceinline__ uint32_t pack4_sym(const Digits &a, const Digits &b, const Digits &c,
+                                              const Digits &d, int l) {
+    const uint32_t m = modulus_of(l);
+    const uint32_t w = residue_u(a, l) + (residue_u(b, l) << 8) + (residue_u(c, l) << 16) +
+                       (residue_u(d, l) << 24);
+    if (m == 256) return w;
+    const uint32_t half = ((m - 1) / 2) * 0x01010101u;
+    const uint32_t over = __vcmpgtu4(w, half);  // 0xff in every byte above (m-1)/2
+    return __vadd4(w, over & ((256 - m) * 0x01010101u));
 }
 
 __device__ __forceinline__ int64_t scale_round(double x, int e) {
@@ -308,214 +335,220 @@ struct SliceOut {
     int64_t plane;   // bytes per modulus plane
 };
 
+// Packs the symmetric residues of 16 consecutive elements for modulus l.
+__device__ __forceinline__ uint4 pack16(const Digits (&x)[16], int l) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        w[q] = pack4_sym(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3], l);
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+__device__ __forceinline__ uint4 neg16(uint4 a) {  // residue of -x, byte-wise
+    return make_uint4(__vneg4(a.x), __vneg4(a.y), __vneg4(a.z), __vneg4(a.w));
+}
+
+// Writes the residues of 16 consecutive k (k0 multiple of 16) of row r.
 template <int ROLE>
-__device__ __forceinline__ void put4(const SliceOut &o, int l, int64_t r, int64_t k,
-                                     const int32_t (&re)[4], const int32_t (&im)[4]) {
-    auto pack = [](int32_t a, int32_t b, int32_t c, int32_t d) {
-        return (uint32_t(a) & 0xff) | ((uint32_t(b) & 0xff) << 8) | ((uint32_t(c) & 0xff) << 16) |
-               ((uint32_t(d) & 0xff) << 24);
-    };
+__device__ __forceinline__ void store16(const SliceOut &o, int l, int64_t r, int64_t k0,
+                                        const Digits (&re)[16], const Digits (&im)[16]) {
     int8_t *base = o.p + int64_t(l) * o.plane;
-    *reinterpret_cast<uint32_t *>(base + r * o.Kp + k) = pack(re[0], re[1], re[2], re[3]);
+    const uint4 wr = pack16(re, l);
+    *reinterpret_cast<uint4 *>(base + r * o.Kp + k0) = wr;
     if (ROLE == 1) {
-        *reinterpret_cast<uint32_t *>(base + r * o.Kp + o.Kh + k) = pack(im[0], im[1], im[2], im[3]);
+        *reinterpret_cast<uint4 *>(base + r * o.Kp + o.Kh + k0) = pack16(im, l);
     } else if (ROLE == 2) {
-        *reinterpret_cast<uint32_t *>(base + r * o.Kp + o.Kh + k) =
-            pack(-im[0], -im[1], -im[2], -im[3]);
-        *reinterpret_cast<uint32_t *>(base + (o.Rp + r) * o.Kp + k) =
-            pack(im[0], im[1], im[2], im[3]);
-        *reinterpret_cast<uint32_t *>(base + (o.Rp + r) * o.Kp + o.Kh + k) =
-            pack(re[0], re[1], re[2], re[3]);
+        const uint4 wi = pack16(im, l);
+        *reinterpret_cast<uint4 *>(base + r * o.Kp + o.Kh + k0) = neg16(wi);
+        *reinterpret_cast<uint4 *>(base + (o.Rp + r) * o.Kp + k0) = wi;
+        *reinterpret_cast<uint4 *>(base + (o.Rp + r) * o.Kp + o.Kh + k0) = wr;
     }
 }
 
-// k-contiguous source: a thread scales 4 consecutive k of one row and writes
-// their residues for every modulus as one 4-byte word per plane.
-// grid (Kc/64, Rp/16), block 256 = 16 (k groups of 4) x 16 rows.
+template <int ROLE>
+__device__ __forceinline__ void store_all(const SliceOut &o, int nmod, int64_t r, int64_t k0,
+                                          const Digits (&re)[16], const Digits (&im)[16]) {
+#pragma unroll
+    for (int l = 0; l < kMaxModuli; ++l)
+        if (l < nmod) store16<ROLE>(o, l, r, k0, re, im);
+}
+
+// k-contiguous source: a thread scales 16 consecutive k of one row and
+// writes one 16-byte word per modulus (and component).
+// grid (Kc/64, Rp/64), block 256: row = tid / 4, k = 16 (tid % 4).
 template <typename T, int ROLE>
-__global__ void slice_kc_kernel(View v, RowStats st, const Decision *dec, int *expo, SliceOut o) {
+__global__ void __launch_bounds__(256) slice_kc_kernel(View v, RowStats st, const Decision *dec,
+                                                       int *expo, SliceOut o) {
     const int nmod = dec->nmod;
     if (nmod == 0) return;
     const int Q = dec->q;
-    const int64_t r = int64_t(blockIdx.y) * 16 + (threadIdx.x >> 4);
-    const int64_t k = int64_t(blockIdx.x) * 64 + (threadIdx.x & 15) * 4;
+    const int64_t r = int64_t(blockIdx.y) * 64 + (threadIdx.x >> 2);
+    const int64_t k0 = int64_t(blockIdx.x) * 64 + (threadIdx.x & 3) * 16;
     int e = 0;
     if (r < v.R) e = row_exponent(st.amax[r], st.sumsq[r], Q, v.K);
-    if (blockIdx.x == 0 && (threadIdx.x & 15) == 0 && r < v.R) expo[r] = e;
-    int64_t vr[4], vi[4];
+    if (blockIdx.x == 0 && (threadIdx.x & 3) == 0 && r < v.R) expo[r] = e;
+    Digits dr[16], di[16];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 16; ++q) {
         double re = 0, im = 0;
-        if (r < v.R && k + q < v.K) load_elem<T>(v, r, k + q, true, re, im);
-        vr[q] = scale_round(re, e);
-        vi[q] = scale_round(im, e);
+        if (r < v.R && k0 + q < v.K) load_elem<T>(v, r, k0 + q, true, re, im);
+        dr[q] = digits_of(scale_round(re, e));
+        di[q] = digits_of(scale_round(im, e));
     }
-#pragma unroll
-    for (int l = 0; l < kMaxModuli; ++l) {
-        if (l < nmod) {
-            int32_t rr[4], ri[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                rr[q] = sym_residue(vr[q], l);
-                ri[q] = ROLE ? sym_residue(vi[q], l) : 0;
-            }
-            put4<ROLE>(o, l, r, k, rr, ri);
-        }
-    }
+    store_all<ROLE>(o, nmod, r, k0, dr, di);
 }
 
-// row-contiguous source: a 64 (rows) x 64 (k) tile is read along rows,
-// scaled, and its residues are transposed through shared memory so that the
-// k-contiguous output rows are written with 4-byte words.
+// row-contiguous source: a 64-row x KT-k tile is read along rows, scaled,
+// and its integers are transposed once through shared memory; then a thread
+// owns 16 consecutive k of one row, as in the k-contiguous kernel.
+// grid (Kc/KT, Rp/64), block 256.
 template <typename T, int ROLE>
-__global__ void slice_rc_kernel(View v, RowStats st, const Decision *dec, int *expo, SliceOut o) {
+__global__ void __launch_bounds__(256) slice_rc_kernel(View v, RowStats st, const Decision *dec,
+                                                       int *expo, SliceOut o) {
+    constexpr int KT = ROLE ? 32 : 64;
+    constexpr int CPL = ROLE ? 2 : 1;
+    __shared__ int64_t tile[CPL][KT][64 + 1];
+    __shared__ int s_e[64];
     const int nmod = dec->nmod;
     if (nmod == 0) return;
     const int Q = dec->q;
-    constexpr int CPL = ROLE ? 2 : 1;  // components
-    __shared__ int8_t tile[CPL][64][64 + 4];
-    __shared__ int s_e[64];
-    const int64_t r0 = int64_t(blockIdx.y) * 64, k0 = int64_t(blockIdx.x) * 64;
-    const int tr = threadIdx.x & 63, tk = threadIdx.x >> 6;  // tk in 0..3
-    const int64_t r = r0 + tr;
-    if (tk == 0) {
+    const int64_t r0 = int64_t(blockIdx.y) * 64, k0 = int64_t(blockIdx.x) * KT;
+    const int tid = threadIdx.x;
+    if (tid < 64) {
+        const int64_t r = r0 + tid;
         int e = 0;
         if (r < v.R) e = row_exponent(st.amax[r], st.sumsq[r], Q, v.K);
-        s_e[tr] = e;
+        s_e[tid] = e;
         if (blockIdx.x == 0 && r < v.R) expo[r] = e;
     }
     __syncthreads();
-    const int e = s_e[tr];
-    int64_t vr[16], vi[16];
+    {
+        const int tr = tid & 63, tk = tid >> 6;  // tk in 0..3
+        const int64_t r = r0 + tr;
+        const int e = s_e[tr];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int64_t k = k0 + tk + 4 * i;
-        double re = 0, im = 0;
-        if (r < v.R && k < v.K) load_elem<T>(v, r, k, false, re, im);
-        vr[i] = scale_round(re, e);
-        vi[i] = scale_round(im, e);
-    }
-    // writer mapping: thread -> (row wr, 4 consecutive k at wk)
-    const int wr = threadIdx.x >> 2, wk = (threadIdx.x & 3) * 16;
-#pragma unroll
-    for (int l = 0; l < kMaxModuli; ++l) {
-        if (l < nmod) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                tile[0][tk + 4 * i][tr] = int8_t(sym_residue(vr[i], l));
-                if (ROLE) tile[CPL - 1][tk + 4 * i][tr] = int8_t(sym_residue(vi[i], l));
-            }
-            __syncthreads();
-            // thread writes 16 k of row (r0 + wr): 4 words per component
-#pragma unroll
-            for (int q = 0; q < 16; q += 4) {
-                int32_t re4[4], im4[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    re4[u] = tile[0][wk + q + u][wr];
-                    im4[u] = ROLE ? tile[CPL - 1][wk + q + u][wr] : 0;
-                }
-                put4<ROLE>(o, l, r0 + wr, k0 + wk + q, re4, im4);
-            }
-            __syncthreads();
+        for (int i = 0; i < KT / 4; ++i) {
+            const int kk = tk + 4 * i;
+            double re = 0, im = 0;
+            if (r < v.R && k0 + kk < v.K) load_elem<T>(v, r, k0 + kk, false, re, im);
+            tile[0][kk][tr] = scale_round(re, e);
+            if (ROLE) tile[CPL - 1][kk][tr] = scale_round(im, e);
         }
+    }
+    __syncthreads();
+    constexpr int TPR = KT / 16;  // threads per row in the residue phase
+    if (tid < 64 * TPR) {
+        const int wr = tid / TPR, wk = (tid % TPR) * 16;
+        Digits dr[16], di[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            dr[q] = digits_of(tile[0][wk + q][wr]);
+            di[q] = ROLE ? digits_of(tile[CPL - 1][wk + q][wr]) : digits_of(0);
+        }
+        store_all<ROLE>(o, nmod, r0 + wr, k0 + wk, dr, di);
     }
 }
 
 // ---- reconstruction -----------------------------------------------------------
 
-// CRT value of the residues u[0..n) for modulus count n, as a double
-// (correctly rounded from the exact symmetric integer).
-__device__ double crt_to_double(const uint32_t *u, int n) {
-    const int ni = n - kMinModuli;
-    uint64_t acc[kLimbs];
+// 32-bit limbs that hold sum_l u_l w_l < N 2^8 M for N moduli.
+__host__ __device__ constexpr int limbs_for(int n) {
+    return n <= 6 ? 2 : n <= 10 ? 3 : n <= 14 ? 4 : n <= 18 ? 5 : 6;
+}
+
+// x * 2^e for a normal x: one multiply by a constructed power of two when
+// 2^e is a normal double, ldexp otherwise.
+__device__ __forceinline__ double scale_pow2(double x, int e) {
+    if (e >= -1022 && e <= 1023) return x * __longlong_as_double(int64_t(e + 1023) << 52);
+    return ldexp(x, e);
+}
+
+// CRT value of the residues u[0..N) times 2^scale as a double, correctly
+// rounded from the exact symmetric integer X in (-M/2, M/2] (the scaling by
+// a power of two is exact unless the result leaves the normal range):
+//   S = sum_l u_l w_l (multi-limb), X = S mod M, X -= M if 2X >= M.
+template <int N>
+__device__ __forceinline__ double crt_to_double(const uint32_t (&u)[N], int scale) {
+    constexpr int L = limbs_for(N);
+    constexpr int ni = N - kMinModuli;
+    uint64_t acc[L];
 #pragma unroll
-    for (int t = 0; t < kLimbs; ++t) acc[t] = 0;
-    for (int l = 0; l < n; ++l) {
-        const uint32_t ul = u[l];
+    for (int t = 0; t < L; ++t) acc[t] = 0;
 #pragma unroll
-        for (int t = 0; t < kLimbs; ++t) acc[t] += uint64_t(ul) * c_crt.w[ni][l][t];
-    }
-    // normalise to 32-bit limbs (S < 2^13 M < 2^192)
-    uint32_t s[kLimbs];
+    for (int l = 0; l < N; ++l)
+#pragma unroll
+        for (int t = 0; t < L; ++t) acc[t] += uint64_t(u[l]) * c_crt.w[ni][l][t];
+    uint32_t s[L];
     uint64_t carry = 0;
 #pragma unroll
-    for (int t = 0; t < kLimbs; ++t) {
+    for (int t = 0; t < L; ++t) {
         const uint64_t v = acc[t] + carry;
         s[t] = uint32_t(v);
         carry = v >> 32;
     }
-    // q = floor(S / M), estimated in double and corrected below
+    // q = floor(S / M) estimated in double (S / M < N 2^8, so the estimate is
+    // off by at most one), then corrected exactly
     double sd = 0;
 #pragma unroll
-    for (int t = kLimbs - 1; t >= 0; --t) sd = sd * 4294967296.0 + double(s[t]);
-    sd += double(carry) * 6277101735386680763835789423207666416102355444464034512896.0;  // 2^192
-    int64_t q = int64_t(floor(sd * c_crt.invMd[ni]));
-    if (q < 0) q = 0;
-    // X = S - q M (may be negative by < M, or >= M by < M)
+    for (int t = L - 1; t >= 0; --t) sd = sd * 4294967296.0 + double(s[t]);
+    const uint32_t q = uint32_t(fmax(0.0, floor(sd * c_crt.invMd[ni])));
+    uint32_t x[L];
     int64_t borrow = 0;
-    uint32_t x[kLimbs];
-    {
-        uint64_t qc = 0;
+    uint64_t qc = 0;
 #pragma unroll
-        for (int t = 0; t < kLimbs; ++t) {
-            const uint64_t qm = uint64_t(q) * c_crt.M[ni][t] + qc;
-            qc = qm >> 32;
-            const int64_t d = int64_t(s[t]) - int64_t(uint32_t(qm)) - borrow;
-            x[t] = uint32_t(d);
-            borrow = d < 0 ? 1 : 0;
-        }
-        borrow = borrow + int64_t(qc) - int64_t(carry);  // > 0: X negative
+    for (int t = 0; t < L; ++t) {
+        const uint64_t qm = uint64_t(q) * c_crt.M[ni][t] + qc;
+        qc = qm >> 32;
+        const int64_t d = int64_t(s[t]) - int64_t(uint32_t(qm)) - borrow;
+        x[t] = uint32_t(d);
+        borrow = d < 0 ? 1 : 0;
     }
-    auto add_m = [&](int sign) {  // x += sign * M
-        int64_t c = 0;
+    if (borrow + int64_t(qc) > 0) {  // X < 0: add M
+        uint64_t c = 0;
 #pragma unroll
-        for (int t = 0; t < kLimbs; ++t) {
-            const int64_t d = int64_t(x[t]) + sign * int64_t(c_crt.M[ni][t]) + c;
-            x[t] = uint32_t(d);
-            c = d >> 32;
+        for (int t = 0; t < L; ++t) {
+            const uint64_t v = uint64_t(x[t]) + c_crt.M[ni][t] + c;
+            x[t] = uint32_t(v);
+            c = v >> 32;
         }
-        return c;
+    }
+    auto cmp_ge_M = [&](const uint32_t (&y)[L]) {
+        bool ge = true, decided = false;
+#pragma unroll
+        for (int t = L - 1; t >= 0; --t) {
+            if (!decided && y[t] != c_crt.M[ni][t]) {
+                ge = y[t] > c_crt.M[ni][t];
+                decided = true;
+            }
+        }
+        return ge;
     };
-    if (borrow > 0) add_m(1);  // X < 0
-    // X >= M ?
-    bool ge = true;
+    if (cmp_ge_M(x)) {  // X >= M: subtract M
+        int64_t b = 0;
 #pragma unroll
-    for (int t = kLimbs - 1; t >= 0; --t) {
-        if (x[t] != c_crt.M[ni][t]) {
-            ge = x[t] > c_crt.M[ni][t];
-            break;
+        for (int t = 0; t < L; ++t) {
+            const int64_t d = int64_t(x[t]) - int64_t(c_crt.M[ni][t]) - b;
+            x[t] = uint32_t(d);
+            b = d < 0 ? 1 : 0;
         }
     }
-    if (ge) add_m(-1);
-    // symmetric: X >= M/2 -> X - M (use 2X >= M)
-    bool neg = false;
+    // symmetric representative: 2X >= M -> magnitude M - X, negative
+    uint32_t x2[L];
     {
-        uint32_t x2[kLimbs];
         uint32_t c = 0;
 #pragma unroll
-        for (int t = 0; t < kLimbs; ++t) {
+        for (int t = 0; t < L; ++t) {
             x2[t] = (x[t] << 1) | c;
             c = x[t] >> 31;
         }
-        bool gem = true;
+    }
+    const bool neg = cmp_ge_M(x2);
+    if (neg) {
+        int64_t b = 0;
 #pragma unroll
-        for (int t = kLimbs - 1; t >= 0; --t) {
-            if (x2[t] != c_crt.M[ni][t]) {
-                gem = x2[t] > c_crt.M[ni][t];
-                break;
-            }
-        }
-        if (gem) {
-            // |X - M| = M - X
-            int64_t b = 0;
-#pragma unroll
-            for (int t = 0; t < kLimbs; ++t) {
-                const int64_t d = int64_t(c_crt.M[ni][t]) - int64_t(x[t]) - b;
-                x[t] = uint32_t(d);
-                b = d < 0 ? 1 : 0;
-            }
-            neg = true;
+        for (int t = 0; t < L; ++t) {
+            const int64_t d = int64_t(c_crt.M[ni][t]) - int64_t(x[t]) - b;
+            x[t] = uint32_t(d);
+            b = d < 0 ? 1 : 0;
         }
     }
     // magnitude -> double, correctly rounded: a 64-bit window whose bit 63 is
@@ -523,97 +556,129 @@ __device__ double crt_to_double(const uint32_t *u, int n) {
     // below the 53-bit rounding point, so round-to-nearest-even stays exact)
     int top = -1;
 #pragma unroll
-    for (int t = kLimbs - 1; t >= 0; --t)
+    for (int t = L - 1; t >= 0; --t)
         if (top < 0 && x[t]) top = t;
     if (top < 0) return 0.0;
-    const uint64_t hi64 = (uint64_t(x[top]) << 32) | (top >= 1 ? x[top - 1] : 0u);
-    const uint32_t lo32 = top >= 2 ? x[top - 2] : 0u;
-    uint32_t sticky = 0;
-    for (int t = top - 3; t >= 0; --t) sticky |= x[t];
-    const int lz = __clzll(hi64);  // < 32 because x[top] != 0
+    uint32_t xt = 0, xt1 = 0, xt2 = 0, sticky = 0;
+#pragma unroll
+    for (int t = 0; t < L; ++t) {
+        if (t == top) xt = x[t];
+        if (t == top - 1) xt1 = x[t];
+        if (t == top - 2) xt2 = x[t];
+        if (t < top - 2) sticky |= x[t];
+    }
+    const uint64_t hi64 = (uint64_t(xt) << 32) | xt1;
+    const int lz = __clzll(hi64);  // < 32 because xt != 0
     uint64_t win = hi64 << lz;
     if (lz) {
-        win |= uint64_t(lo32) >> (32 - lz);
-        sticky |= lo32 << lz;
+        win |= uint64_t(xt2) >> (32 - lz);
+        sticky |= xt2 << lz;
     } else {
-        sticky |= lo32;
+        sticky |= xt2;
     }
     if (sticky) win |= 1;
-    const double d = ldexp(__ull2double_rn(win), 32 * (top - 1) - lz);
+    const double d = scale_pow2(__ull2double_rn(win), 32 * (top - 1) - lz + scale);
     return neg ? -d : d;
 }
 
-template <typename T> struct OutT;
-template <> struct OutT<double> { using type = double; };
-template <> struct OutT<float> { using type = float; };
-
-// Real outputs: thread -> 4 consecutive rows i of one column j.
-template <typename T>
-__global__ void reconstruct_real_kernel(const uint8_t *U, int64_t Jp, int64_t Ip, int64_t M,
-                                        int64_t N, const int *ea, const int *fb, const Decision *dec,
-                                        double alpha, double beta, int beta_zero, T *C,
-                                        int64_t ldc) {
-    const int n = dec->nmod;
-    if (n == 0) return;
-    const int64_t j = blockIdx.y;
-    const int64_t i0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
-    if (i0 >= M || j >= N) return;
-    uint32_t u[4][kMaxModuli];
-    for (int l = 0; l < n; ++l) {
-        const uchar4 w = *reinterpret_cast<const uchar4 *>(U + int64_t(l) * Jp * Ip + j * Ip + i0);
-        u[0][l] = w.x; u[1][l] = w.y; u[2][l] = w.z; u[3][l] = w.w;
-    }
-    const int fj = fb[j];
+// Gathers 4 consecutive rows' residues of one column: w[l] packs the uint8
+// residues of rows i0..i0+3 for modulus l.
+template <int N>
+__device__ __forceinline__ void gather4(const uint8_t *U, int64_t plane, int64_t row_off,
+                                        uint32_t (&w)[N]) {
 #pragma unroll
+    for (int l = 0; l < N; ++l) w[l] = *reinterpret_cast<const uint32_t *>(U + l * plane + row_off);
+}
+template <int N>
+__device__ __forceinline__ void unpack(const uint32_t (&w)[N], int q, uint32_t (&u)[N]) {
+#pragma unroll
+    for (int l = 0; l < N; ++l) u[l] = (w[l] >> (8 * q)) & 0xffu;
+}
+
+struct ReconArgs {
+    const uint8_t *U;
+    int64_t Jp, Ip, M, N;
+    const int *ea, *fb;
+    double ar, ai, br, bi;
+    int beta_zero;
+    void *C;
+    int64_t ldc;
+};
+
+template <typename T, int N>
+__device__ __forceinline__ void recon_real(const ReconArgs &a, int64_t i0, int64_t j) {
+    uint32_t w[N];
+    gather4<N>(a.U, a.Jp * a.Ip, j * a.Ip + i0, w);
+    const int fj = a.fb[j];
+    T *C = static_cast<T *>(a.C);
+#pragma unroll 1
     for (int q = 0; q < 4; ++q) {
         const int64_t i = i0 + q;
-        if (i >= M) break;
-        const double val = ldexp(crt_to_double(u[q], n), -(ea[i] + fj));
-        T *cp = C + i + j * ldc;
-        double r = alpha * val;
-        if (!beta_zero) r = fma(beta, double(*cp), r);
+        if (i >= a.M) break;
+        uint32_t u[N];
+        unpack<N>(w, q, u);
+        const double val = crt_to_double<N>(u, -(a.ea[i] + fj));
+        T *cp = C + i + j * a.ldc;
+        double r = a.ar * val;
+        if (!a.beta_zero) r = fma(a.br, double(*cp), r);
         *cp = T(r);
     }
 }
 
-// Complex outputs: the residue block of Re(C) is rows [0, Jp) of U, Im(C)
-// rows [Jp, 2Jp).
-__global__ void reconstruct_cplx_kernel(const uint8_t *U, int64_t Jp, int64_t Ip, int64_t M,
-                                        int64_t N, const int *ea, const int *fb,
-                                        const Decision *dec, double ar, double ai, double br,
-                                        double bi, int beta_zero, double *C, int64_t ldc) {
-    const int n = dec->nmod;
-    if (n == 0) return;
-    const int64_t j = blockIdx.y;
-    const int64_t i0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
-    if (i0 >= M || j >= N) return;
-    const int64_t plane = 2 * Jp * Ip;
-    const int fj = fb[j];
-    uint32_t ur[4][kMaxModuli], ui[4][kMaxModuli];
-    for (int l = 0; l < n; ++l) {
-        const uchar4 a = *reinterpret_cast<const uchar4 *>(U + int64_t(l) * plane + j * Ip + i0);
-        const uchar4 b =
-            *reinterpret_cast<const uchar4 *>(U + int64_t(l) * plane + (Jp + j) * Ip + i0);
-        ur[0][l] = a.x; ur[1][l] = a.y; ur[2][l] = a.z; ur[3][l] = a.w;
-        ui[0][l] = b.x; ui[1][l] = b.y; ui[2][l] = b.z; ui[3][l] = b.w;
-    }
+// Complex outputs: residues of Re(C) are rows [0, Jp) of U, Im(C) rows
+// [Jp, 2 Jp); U planes are 2 Jp x Ip.
+template <int N>
+__device__ __forceinline__ void recon_cplx(const ReconArgs &a, int64_t i0, int64_t j) {
+    const int64_t plane = 2 * a.Jp * a.Ip;
+    uint32_t wr[N], wi[N];
+    gather4<N>(a.U, plane, j * a.Ip + i0, wr);
+    gather4<N>(a.U, plane, (a.Jp + j) * a.Ip + i0, wi);
+    const int fj = a.fb[j];
+    double *C = static_cast<double *>(a.C);
 #pragma unroll 1
     for (int q = 0; q < 4; ++q) {
         const int64_t i = i0 + q;
-        if (i >= M) break;
-        const int sc = -(ea[i] + fj);
-        const double xr = ldexp(crt_to_double(ur[q], n), sc);
-        const double xi = ldexp(crt_to_double(ui[q], n), sc);
-        double *cp = C + 2 * (i + j * ldc);
-        double vr = ar * xr - ai * xi, vi = ar * xi + ai * xr;
-        if (!beta_zero) {
+        if (i >= a.M) break;
+        uint32_t u[N];
+        const int sc = -(a.ea[i] + fj);
+        unpack<N>(wr, q, u);
+        const double xr = crt_to_double<N>(u, sc);
+        unpack<N>(wi, q, u);
+        const double xi = crt_to_double<N>(u, sc);
+        double *cp = C + 2 * (i + j * a.ldc);
+        double vr = a.ar * xr - a.ai * xi, vi = a.ar * xi + a.ai * xr;
+        if (!a.beta_zero) {
             const double cr = cp[0], ci = cp[1];
-            vr += br * cr - bi * ci;
-            vi += br * ci + bi * cr;
+            vr += a.br * cr - a.bi * ci;
+            vi += a.br * ci + a.bi * cr;
         }
         cp[0] = vr;
         cp[1] = vi;
     }
+}
+
+// One thread per 4 consecutive rows i of a column j. The modulus count is
+// read on the device; the switch is uniform, each case fully unrolled.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(128) reconstruct_kernel(const ReconArgs a, const Decision *dec) {
+    const int n = dec->nmod;
+    if (n == 0) return;
+    const int64_t j = blockIdx.y;
+    const int64_t i0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
+    if (i0 >= a.M || j >= a.N) return;
+#define BX_RECON_CASE(NN)                                     \
+    case NN:                                                  \
+        if constexpr (CPLX) recon_cplx<NN>(a, i0, j);         \
+        else recon_real<T, NN>(a, i0, j);                     \
+        break;
+    switch (n) {
+        BX_RECON_CASE(6) BX_RECON_CASE(7) BX_RECON_CASE(8) BX_RECON_CASE(9) BX_RECON_CASE(10)
+        BX_RECON_CASE(11) BX_RECON_CASE(12) BX_RECON_CASE(13) BX_RECON_CASE(14)
+        BX_RECON_CASE(15) BX_RECON_CASE(16) BX_RECON_CASE(17) BX_RECON_CASE(18)
+        BX_RECON_CASE(19) BX_RECON_CASE(20)
+        default: break;
+    }
+#undef BX_RECON_CASE
 }
 
 std::once_flag g_tables_once;
@@ -674,10 +739,11 @@ template <typename T, int ROLE>
 int launch_slice(const oz::View &v, bool kc, const oz::RowStats &st, const oz::Decision *dec,
                  int *expo, const oz::SliceOut &o, int64_t Kc, cudaStream_t s) {
     if (kc) {
-        dim3 grid(unsigned(Kc / 64), unsigned(o.Rp / 16));
+        dim3 grid(unsigned(Kc / 64), unsigned(o.Rp / 64));
         oz::slice_kc_kernel<T, ROLE><<<grid, 256, 0, s>>>(v, st, dec, expo, o);
     } else {
-        dim3 grid(unsigned(Kc / 64), unsigned(o.Rp / 64));
+        const int kt = ROLE ? 32 : 64;
+        dim3 grid(unsigned(Kc / kt), unsigned(o.Rp / 64));
         oz::slice_rc_kernel<T, ROLE><<<grid, 256, 0, s>>>(v, st, dec, expo, o);
     }
     BX_CUDA(cudaGetLastError());
@@ -767,16 +833,9 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
     cudaEvent_t ev2 = prof::mark(s);
 
     dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(N));
-    if constexpr (CPLX) {
-        oz::reconstruct_cplx_kernel<<<rgrid, 128, 0, s>>>(U, Jp, Ip, M, N, ea, fb, dec, g.alpha.re,
-                                                          g.alpha.im, g.beta.re, g.beta.im,
-                                                          g.beta_zero() ? 1 : 0,
-                                                          static_cast<double *>(g.C), g.ldc);
-    } else {
-        oz::reconstruct_real_kernel<T><<<rgrid, 128, 0, s>>>(
-            U, Jx, Ip, M, N, ea, fb, dec, g.alpha.re, g.beta.re, g.beta_zero() ? 1 : 0,
-            static_cast<T *>(g.C), g.ldc);
-    }
+    oz::ReconArgs ra{U, Jp, Ip, M, N, ea, fb, g.alpha.re, g.alpha.im, g.beta.re, g.beta.im,
+                     g.beta_zero() ? 1 : 0, g.C, g.ldc};
+    oz::reconstruct_kernel<T, CPLX><<<rgrid, 128, 0, s>>>(ra, dec);
     BX_CUDA(cudaGetLastError());
     count_launch();
 
