@@ -37,6 +37,16 @@ _P, _I, _D, _F = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float
 _lib = None
 
 
+class TilePlanStats(ctypes.Structure):
+    _fields_ = [("tiles_m", _I), ("tiles_n", _I), ("tiles_k", _I), ("slots", _I),
+                ("steps", ctypes.c_longlong), ("tile_loads", ctypes.c_longlong),
+                ("tile_hits", ctypes.c_longlong), ("evictions", ctypes.c_longlong),
+                ("operand_h2d_bytes", _D), ("min_operand_h2d_bytes", _D)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class CallStats(ctypes.Structure):
     _fields_ = [("seconds", _D), ("h2d_bytes", _D), ("d2h_bytes", _D), ("cache_hits", _D),
                 ("cache_misses", _D), ("evictions", _D), ("path", _I), ("moduli", _I),
@@ -76,6 +86,7 @@ def lib() -> ctypes.CDLL:
         L.blasx_zgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
         L.blasx_dgemm_device_noalloc.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_kernel_launch_count.restype = ctypes.c_uint64
+        L.blasx_tile_plan.argtypes = [ctypes.c_longlong] * 5 + [_I, _I, ctypes.POINTER(TilePlanStats)]
         L.blasx_profile_enable.argtypes = [_I]
         L.blasx_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long), _I]
         _lib = L
@@ -218,6 +229,18 @@ def set_tile(tile: int) -> int:
 
 def finalize() -> int:
     return lib().blasx_finalize()
+
+
+POLICY_BELADY, POLICY_LRU = 0, 1
+
+
+def tile_plan(M, N, K, tile, budget_bytes, elem_bytes=8, policy=POLICY_BELADY) -> dict:
+    """Host-only schedule of an out-of-core GEMM (no GPU needed)."""
+    s = TilePlanStats()
+    rc = lib().blasx_tile_plan(M, N, K, tile, budget_bytes, elem_bytes, policy, ctypes.byref(s))
+    if rc != 0:
+        raise ValueError(f"blasx_tile_plan failed ({rc})")
+    return s.as_dict()
 
 
 PHASES = ("slice", "residue_gemm", "reconstruct", "native")

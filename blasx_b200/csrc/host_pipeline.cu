@@ -1,12 +1,29 @@
-// host_pipeline.cu -- host-resident GEMM: copy operands into HBM, compute,
-// copy C back.
+// host_pipeline.cu -- GEMM on host-resident operands.
 //
-// Replaces the reference's per-call flow of blas/dgemm.c:88-121 (pin A/B/C,
-// build per-GPU caches, run the tiled runtime, unpin).
+// Replaces the reference's per-call flow (blas/dgemm.c:88-121: pin A/B/C,
+// build per-GPU caches, run the tiled runtime, unpin) with two paths:
+//
+//   in-core   A, B, C (and the emulated path's scratch) fit the HBM budget:
+//             C is processed in column panels. The H2D stream copies A, then
+//             for every panel its B columns (and C columns when beta != 0);
+//             the compute stream runs the panel as soon as its operands have
+//             landed; the D2H stream writes the panel back while later panels
+//             compute. The emulated path slices A and B once (its statistics
+//             need the whole operands), then runs the residue GEMMs and the
+//             reconstruction panel by panel with the same write-back overlap.
+//   tiled     otherwise: the HBM tile cache with an explicit byte budget
+//             (tile_engine.cu), native kernels.
+//
+// Host buffers that are not pinned are registered for the call (full
+// ld x columns extent) so that every copy is an asynchronous DMA.
+#include <algorithm>
 #include <chrono>
+#include <vector>
 
 #include "host_pipeline.h"
 #include "kernels.h"
+#include "ozaki.h"
+#include "tile_engine.h"
 
 namespace bx {
 
@@ -14,18 +31,203 @@ namespace {
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
-struct DevBuf {
-    void *p = nullptr;
-    cudaStream_t s = nullptr;
-    ~DevBuf() {
-        if (p) cudaFreeAsync(p, s);
+struct Events {
+    std::vector<cudaEvent_t> evs;
+    ~Events() {
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
     }
-    int alloc(size_t bytes, cudaStream_t st) {
-        s = st;
-        BX_CUDA(cudaMallocAsync(&p, bytes ? bytes : 256, st));
-        return BLASX_OK;
+    cudaEvent_t make() {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) evs.push_back(e);
+        return e;
     }
 };
+
+// Device copies of the operands, laid out column-major with ld padded to 32.
+struct DeviceOps {
+    void *A = nullptr, *B = nullptr, *C = nullptr, *ws = nullptr;
+    int64_t lda = 0, ldb = 0, ldc = 0;
+    cudaStream_t s = nullptr;
+    ~DeviceOps() {
+        for (void *p : {A, B, C, ws})
+            if (p) cudaFreeAsync(p, s);
+    }
+};
+
+size_t default_budget(const Context *c) {
+    size_t b = config().hbm_budget.load();
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return b ? b : c->total_mem / 2;
+    // the tile arena the library already holds is reusable, count it as free
+    const size_t cap = size_t(double(free_b) * 0.9);
+    return b ? std::min(b, total_b) : cap;
+}
+
+int pick_tile(const Gemm &g) {
+    const int t = config().tile.load();
+    if (t) return t;
+    return g.dt == DType::F32 ? 4096 : (g.dt == DType::F64 ? 4096 : 2048);
+}
+
+// Copies the column panel [j0, j1) of op(B) (and of C) host -> device.
+int copy_panel_in(const Gemm &g, const DeviceOps &d, int64_t j0, int64_t j1, bool need_b,
+                  bool read_c, cudaStream_t s, blasx_call_stats &st) {
+    const size_t es = elem_size(g.dt);
+    const int64_t w = j1 - j0;
+    if (need_b) {
+        const char *hb = static_cast<const char *>(g.B);
+        char *db = static_cast<char *>(d.B);
+        if (g.tb == NoTrans) {  // K x N stored: columns j0..j1
+            BX_CUDA(cudaMemcpy2DAsync(db + j0 * d.ldb * es, d.ldb * es, hb + j0 * g.ldb * es,
+                                      g.ldb * es, g.K * es, w, cudaMemcpyHostToDevice, s));
+        } else {  // N x K stored: rows j0..j1
+            BX_CUDA(cudaMemcpy2DAsync(db + j0 * es, d.ldb * es, hb + j0 * es, g.ldb * es, w * es,
+                                      g.K, cudaMemcpyHostToDevice, s));
+        }
+        st.h2d_bytes += double(w) * g.K * es;
+    }
+    if (read_c) {
+        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.C) + j0 * d.ldc * es, d.ldc * es,
+                                  static_cast<const char *>(g.C) + j0 * g.ldc * es, g.ldc * es,
+                                  g.M * es, w, cudaMemcpyHostToDevice, s));
+        st.h2d_bytes += double(w) * g.M * es;
+    }
+    return BLASX_OK;
+}
+
+int copy_panel_out(const Gemm &g, const DeviceOps &d, int64_t j0, int64_t j1, cudaStream_t s,
+                   blasx_call_stats &st) {
+    const size_t es = elem_size(g.dt);
+    BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(g.C) + j0 * g.ldc * es, g.ldc * es,
+                              static_cast<const char *>(d.C) + j0 * d.ldc * es, d.ldc * es,
+                              g.M * es, j1 - j0, cudaMemcpyDeviceToHost, s));
+    st.d2h_bytes += double(j1 - j0) * g.M * es;
+    return BLASX_OK;
+}
+
+int panel_count(const Gemm &g) {
+    // panels of >= 1024 columns, at most 8
+    return int(std::max<int64_t>(1, std::min<int64_t>(8, g.N / 1024)));
+}
+
+// ---- in-core, native kernels ----------------------------------------------
+int incore_native(const Gemm &g, Context *c, DeviceOps &d, bool need_ab, bool read_c,
+                  blasx_call_stats &st) {
+    Events ev;
+    const size_t es = elem_size(g.dt);
+    cudaEvent_t start = ev.make();
+    BX_CUDA(cudaEventRecord(start, c->compute));  // device buffers allocated on compute
+    BX_CUDA(cudaStreamWaitEvent(c->h2d, start, 0));
+    BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
+    if (need_ab) {
+        BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
+                                  cudaMemcpyHostToDevice, c->h2d));
+        st.h2d_bytes += double(es) * g.rows_a() * g.cols_a();
+    }
+    const int panels = panel_count(g);
+    for (int p = 0; p < panels; ++p) {
+        const int64_t j0 = g.N * p / panels, j1 = g.N * (p + 1) / panels;
+        BX_TRY(copy_panel_in(g, d, j0, j1, need_ab, read_c, c->h2d, st));
+        cudaEvent_t in = ev.make();
+        BX_CUDA(cudaEventRecord(in, c->h2d));
+        BX_CUDA(cudaStreamWaitEvent(c->compute, in, 0));
+        Gemm p_g = g;
+        p_g.N = j1 - j0;
+        p_g.A = d.A; p_g.lda = d.lda;
+        p_g.B = static_cast<char *>(d.B) + (g.tb == NoTrans ? j0 * d.ldb : j0) * es;
+        p_g.ldb = d.ldb;
+        p_g.C = static_cast<char *>(d.C) + j0 * d.ldc * es;
+        p_g.ldc = d.ldc;
+        if (need_ab) {
+            BX_TRY(dmma_supported(p_g) ? launch_gemm_dmma(p_g, c->compute)
+                                       : launch_gemm_simt(p_g, c->compute));
+        } else {
+            BX_TRY(launch_scale(p_g, c->compute));
+        }
+        cudaEvent_t done = ev.make();
+        BX_CUDA(cudaEventRecord(done, c->compute));
+        BX_CUDA(cudaStreamWaitEvent(c->d2h, done, 0));
+        BX_TRY(copy_panel_out(g, d, j0, j1, c->d2h, st));
+    }
+    BX_CUDA(cudaStreamSynchronize(c->h2d));
+    BX_CUDA(cudaStreamSynchronize(c->compute));
+    BX_CUDA(cudaStreamSynchronize(c->d2h));
+    st.path = need_ab ? 1 : 3;
+    return BLASX_OK;
+}
+
+// ---- in-core, emulated path -------------------------------------------------
+struct OzPanelCtx {
+    const Gemm *g;
+    const DeviceOps *d;
+    Context *c;
+    Events *ev;
+    blasx_call_stats *st;
+};
+
+int oz_after_panel(void *vctx, int64_t j0, int64_t j1) {
+    auto *x = static_cast<OzPanelCtx *>(vctx);
+    cudaEvent_t done = x->ev->make();
+    BX_CUDA(cudaEventRecord(done, x->c->compute));
+    BX_CUDA(cudaStreamWaitEvent(x->c->d2h, done, 0));
+    return copy_panel_out(*x->g, *x->d, j0, j1, x->c->d2h, *x->st);
+}
+
+// C panel copy-in, queued behind A and B on the H2D stream; only this
+// panel's reconstruction waits for it.
+int oz_before_reconstruct(void *vctx, int64_t j0, int64_t j1) {
+    auto *x = static_cast<OzPanelCtx *>(vctx);
+    BX_TRY(copy_panel_in(*x->g, *x->d, j0, j1, false, true, x->c->h2d, *x->st));
+    cudaEvent_t in = x->ev->make();
+    BX_CUDA(cudaEventRecord(in, x->c->h2d));
+    BX_CUDA(cudaStreamWaitEvent(x->c->compute, in, 0));
+    return BLASX_OK;
+}
+
+int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
+                 blasx_call_stats &st) {
+    Events ev;
+    const size_t es = elem_size(g.dt);
+    cudaEvent_t start = ev.make();
+    BX_CUDA(cudaEventRecord(start, c->compute));
+    BX_CUDA(cudaStreamWaitEvent(c->h2d, start, 0));
+    BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
+    // A and B first (the slicing needs them whole); C follows panel by panel,
+    // each reconstruction waiting only for its own panel
+    BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
+                              cudaMemcpyHostToDevice, c->h2d));
+    BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
+                              cudaMemcpyHostToDevice, c->h2d));
+    st.h2d_bytes += double(es) * (g.rows_a() * g.cols_a() + g.rows_b() * g.cols_b());
+    cudaEvent_t ab = ev.make();
+    BX_CUDA(cudaEventRecord(ab, c->h2d));
+    BX_CUDA(cudaStreamWaitEvent(c->compute, ab, 0));
+    Gemm dg = g;
+    dg.A = d.A; dg.lda = d.lda;
+    dg.B = d.B; dg.ldb = d.ldb;
+    dg.C = d.C; dg.ldc = d.ldc;
+    OzPanelCtx pctx{&g, &d, c, &ev, &st};
+    PanelHooks hooks{panel_count(g), read_c ? &oz_before_reconstruct : nullptr, &oz_after_panel,
+                     &pctx};
+    BX_TRY(ozaki_gemm_panels(dg, c->compute, mode, d.ws, c->num_sms, hooks));
+    BX_CUDA(cudaStreamSynchronize(c->h2d));
+    BX_CUDA(cudaStreamSynchronize(c->compute));
+    BX_CUDA(cudaStreamSynchronize(c->d2h));
+    st.path = 2;
+    resolve_decision(st);
+    if (*c->last_error_flag)
+        return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
+                         *c->last_error_flag);
+    return BLASX_OK;
+}
+
+bool want_ozaki(const Gemm &g, int mode) {
+    const int64_t kmax = g.dt == DType::C128 ? oz::kMaxK / 2 : oz::kMaxK;
+    if (g.K > kmax) return false;
+    const double work = double(g.M) * double(g.N) * double(g.K);
+    const bool worth = work >= double(1 << 27) && g.M >= 64 && g.N >= 64 && g.K >= 32;
+    return mode == 2 || (mode == 0 && worth);
+}
 
 }  // namespace
 
@@ -37,51 +239,45 @@ int host_gemm(const Gemm &g) {
     Context *c = context();
     if (!c) return last_status();
     std::lock_guard<std::mutex> lk(c->host_mu);
-    cudaStream_t s = c->compute;
     const size_t es = elem_size(g.dt);
     const bool need_ab = !(g.alpha_zero() || g.K == 0);
     const bool read_c = !g.beta_zero();
+    const int mode = config().dgemm_mode.load();
+    const bool oz = need_ab && want_ozaki(g, mode);
 
-    Gemm d = g;
-    DevBuf bA, bB, bC;
+    DeviceOps d;
+    d.s = c->compute;
+    d.lda = round_up(g.rows_a(), 32);
+    d.ldb = round_up(g.rows_b(), 32);
+    d.ldc = round_up(g.M, 32);
+    const size_t bytes_a = need_ab ? size_t(d.lda) * g.cols_a() * es : 0;
+    const size_t bytes_b = need_ab ? size_t(d.ldb) * g.cols_b() * es : 0;
+    const size_t bytes_c = size_t(d.ldc) * g.N * es;
+    Gemm probe = g;
+    probe.lda = d.lda; probe.ldb = d.ldb; probe.ldc = d.ldc;
+    const size_t bytes_ws = oz ? ozaki_scratch_bytes(probe) : 0;
+    const size_t budget = default_budget(c);
+
+    HostPin pins;
+    if (bytes_a + bytes_b + bytes_c + bytes_ws > budget && need_ab) {
+        // out-of-core: HBM tile cache under the byte budget, native kernels
+        const int st_code = tiled_host_gemm(g, c, budget, pick_tile(g), 0);
+        st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return st_code;
+    }
+    BX_TRY(pins.pin(g.A, need_ab ? host_extent(g.lda, g.rows_a(), g.cols_a(), es) : 0));
+    BX_TRY(pins.pin(g.B, need_ab ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
+    BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
     if (need_ab) {
-        const int64_t lda = round_up(g.rows_a(), 32), ldb = round_up(g.rows_b(), 32);
-        BX_TRY(bA.alloc(size_t(lda) * g.cols_a() * es, s));
-        BX_TRY(bB.alloc(size_t(ldb) * g.cols_b() * es, s));
-        BX_CUDA(cudaMemcpy2DAsync(bA.p, lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
-                                  cudaMemcpyHostToDevice, s));
-        BX_CUDA(cudaMemcpy2DAsync(bB.p, ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
-                                  cudaMemcpyHostToDevice, s));
-        d.A = bA.p; d.lda = lda;
-        d.B = bB.p; d.ldb = ldb;
-        st.h2d_bytes += double(es) * (g.rows_a() * g.cols_a() + g.rows_b() * g.cols_b());
+        BX_CUDA(cudaMallocAsync(&d.A, bytes_a ? bytes_a : 256, c->compute));
+        BX_CUDA(cudaMallocAsync(&d.B, bytes_b ? bytes_b : 256, c->compute));
     }
-    const int64_t ldc = round_up(g.M, 32);
-    BX_TRY(bC.alloc(size_t(ldc) * g.N * es, s));
-    if (read_c) {
-        BX_CUDA(cudaMemcpy2DAsync(bC.p, ldc * es, g.C, g.ldc * es, g.M * es, g.N,
-                                  cudaMemcpyHostToDevice, s));
-        st.h2d_bytes += double(es) * g.M * g.N;
-    }
-    d.C = bC.p; d.ldc = ldc;
-    if (need_ab) {
-        BX_TRY(device_gemm(d, s));
-    } else {
-        BX_TRY(launch_scale(d, s));
-        st.path = 3;
-    }
-    BX_CUDA(cudaMemcpy2DAsync(g.C, g.ldc * es, bC.p, ldc * es, g.M * es, g.N,
-                              cudaMemcpyDeviceToHost, s));
-    st.d2h_bytes += double(es) * g.M * g.N;
-    BX_CUDA(cudaStreamSynchronize(s));
-    if (st.path == 2) {
-        resolve_decision(st);
-        if (*c->last_error_flag)
-            return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
-                             *c->last_error_flag);
-    }
+    BX_CUDA(cudaMallocAsync(&d.C, bytes_c, c->compute));
+    if (oz) BX_CUDA(cudaMallocAsync(&d.ws, bytes_ws, c->compute));
+    const int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
+                      : incore_native(g, c, d, need_ab, read_c, st);
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    return BLASX_OK;
+    return rc;
 }
 
 }  // namespace bx

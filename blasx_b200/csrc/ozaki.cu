@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <type_traits>
 
@@ -603,6 +604,7 @@ struct ReconArgs {
     int beta_zero;
     void *C;
     int64_t ldc;
+    int64_t j0;  // first column of this launch
 };
 
 template <typename T, int N>
@@ -663,7 +665,7 @@ template <typename T, bool CPLX>
 __global__ void __launch_bounds__(128) reconstruct_kernel(const ReconArgs a, const Decision *dec) {
     const int n = dec->nmod;
     if (n == 0) return;
-    const int64_t j = blockIdx.y;
+    const int64_t j = a.j0 + blockIdx.y;
     const int64_t i0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
     if (i0 >= a.M || j >= a.N) return;
 #define BX_RECON_CASE(NN)                                     \
@@ -788,7 +790,7 @@ Plan make_plan(const Gemm &g) {
 // flag are copied to the given host slots when they are not null.
 template <typename T>
 int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, void *dec_host,
-              int *err_host) {
+              int *err_host, const PanelHooks *hooks = nullptr) {
     constexpr bool CPLX = oz::Elem<T>::cplx;
     const Plan pl = make_plan(g);
     const int64_t M = pl.M, N = pl.N, K = pl.K, Kh = pl.Kh, Kp = pl.Kp, Kc = pl.Kc;
@@ -828,24 +830,54 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         BX_TRY((launch_slice<T, 0>(va, akc, sa, dec, ea, oy, Kc, s)));
         BX_TRY((launch_slice<T, 0>(vb, bkc, sb, dec, fb, ox, Kc, s)));
     }
-    cudaEvent_t ev1 = prof::mark(s);
-    BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s));
-    cudaEvent_t ev2 = prof::mark(s);
-
-    dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(N));
-    oz::ReconArgs ra{U, Jp, Ip, M, N, ea, fb, g.alpha.re, g.alpha.im, g.beta.re, g.beta.im,
-                     g.beta_zero() ? 1 : 0, g.C, g.ldc};
-    oz::reconstruct_kernel<T, CPLX><<<rgrid, 128, 0, s>>>(ra, dec);
-    BX_CUDA(cudaGetLastError());
-    count_launch();
+    // residue GEMMs and reconstruction, in column panels of C when asked
+    const int64_t tiles_j = Jp / oz::kTileJ;
+    const int panels = (CPLX || !hooks) ? 1 : int(std::max<int64_t>(1, std::min<int64_t>(hooks->panels, tiles_j)));
+    cudaEvent_t ev1 = prof::mark(s), ev2 = nullptr;
+    for (int pnl = 0; pnl < panels; ++pnl) {
+        const int64_t tj0 = tiles_j * pnl / panels, tj1 = tiles_j * (pnl + 1) / panels;
+        const int64_t j0 = tj0 * oz::kTileJ, j1 = std::min<int64_t>(N, tj1 * oz::kTileJ);
+        if (panels == 1) {
+            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s));
+        } else {
+            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s, tj0, tj1 - tj0));
+        }
+        if (pnl == 0) ev2 = prof::mark(s);
+        if (hooks && hooks->before_reconstruct && j1 > j0)
+            BX_TRY(hooks->before_reconstruct(hooks->ctx, j0, j1));
+        if (j1 > j0) {
+            dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(j1 - j0));
+            oz::ReconArgs ra{U, Jp, Ip, M, N, ea, fb, g.alpha.re, g.alpha.im, g.beta.re, g.beta.im,
+                             g.beta_zero() ? 1 : 0, g.C, g.ldc, j0};
+            oz::reconstruct_kernel<T, CPLX><<<rgrid, 128, 0, s>>>(ra, dec);
+            BX_CUDA(cudaGetLastError());
+            count_launch();
+        }
+        if (hooks && j1 > j0) {
+            // native fallback for this panel's columns (runs only when nmod == 0),
+            // so that the panel's write-back also follows the fallback
+            Gemm gp = g;
+            gp.N = j1 - j0;
+            gp.B = static_cast<const char *>(g.B) +
+                   (g.tb == NoTrans ? j0 * g.ldb : j0) * int64_t(elem_size(g.dt));
+            gp.C = static_cast<char *>(g.C) + j0 * g.ldc * int64_t(elem_size(g.dt));
+            gp.guard = &dec->nmod;
+            if (g.dt == DType::F32) BX_TRY(launch_gemm_simt(gp, s));
+            else BX_TRY(launch_gemm_dmma(gp, s));
+        }
+        if (hooks && hooks->after_panel) BX_TRY(hooks->after_panel(hooks->ctx, j0, j1));
+    }
 
     cudaEvent_t ev3 = prof::mark(s);
 
-    // native fallback, decided on the device (runs only when nmod == 0)
-    Gemm gn = g;
-    gn.guard = &dec->nmod;
-    if (g.dt == DType::F32) BX_TRY(launch_gemm_simt(gn, s));
-    else BX_TRY(launch_gemm_dmma(gn, s));
+    // native fallback, decided on the device (runs only when nmod == 0);
+    // with panels it already ran panel by panel
+    if (!hooks) {
+        Gemm gn = g;
+        gn.guard = &dec->nmod;
+        if (g.dt == DType::F32) BX_TRY(launch_gemm_simt(gn, s));
+        else BX_TRY(launch_gemm_dmma(gn, s));
+    }
     cudaEvent_t ev4 = prof::mark(s);
     prof::span(prof::kSlice, ev0, ev1);
     prof::span(prof::kResidueGemm, ev1, ev2);
@@ -886,6 +918,22 @@ int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode) {
 }
 
 size_t ozaki_scratch_bytes(const Gemm &g) { return make_plan(g).bytes; }
+
+int ozaki_gemm_panels(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms,
+                      const PanelHooks &hooks) {
+    Context *ctx = context();
+    if (!ctx) return last_status();
+    BX_TRY(oz::upload_crt_tables());
+    switch (g.dt) {
+        case DType::F64:
+            return ozaki_run<double>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks);
+        case DType::F32:
+            return ozaki_run<float>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks);
+        default:
+            return ozaki_run<oz::zpair>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag,
+                                        &hooks);
+    }
+}
 
 int ozaki_gemm_in(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms) {
     switch (g.dt) {

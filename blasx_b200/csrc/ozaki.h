@@ -61,9 +61,11 @@ struct RowStats {
 //   U_l[j][i] = (sum_k X_l[j][k] * Y_l[i][k]) mod m_l   (uint8, ldu = Ip)
 // X: [kMaxModuli][Jp][Kp] int8, Y: [kMaxModuli][Ip][Kp] int8 (K-major).
 // Kp multiple of 128, Jp of 128, Ip of 256. Returns a blasx status.
+// tj_begin / tj_count: the range of 128-row X tiles (columns of C) to
+// compute; tj_count < 0 covers all of them.
 int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
                         int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
-                        cudaStream_t s);
+                        cudaStream_t s, int64_t tj_begin = 0, int64_t tj_count = -1);
 
 // Host-side CRT constant tables (uploaded once to constant memory).
 int upload_crt_tables();
@@ -87,5 +89,20 @@ int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode);
 // the constant tables must already be on the current device).
 size_t ozaki_scratch_bytes(const Gemm &g);
 int ozaki_gemm_in(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms);
+
+// Column panels of C for the host pipeline: the residue GEMMs and the
+// reconstruction run panel by panel (real types; complex runs one panel).
+// before_reconstruct(ctx, j0, j1) is called before panel [j0, j1) reads C
+// (the host enqueues that panel's copy and makes the stream wait for it);
+// after_panel(ctx, j0, j1) once the panel has been enqueued, so that its
+// write-back can be ordered behind it. Either may be null.
+struct PanelHooks {
+    int panels;
+    int (*before_reconstruct)(void *ctx, int64_t j0, int64_t j1);
+    int (*after_panel)(void *ctx, int64_t j0, int64_t j1);
+    void *ctx;
+};
+int ozaki_gemm_panels(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms,
+                      const PanelHooks &hooks);
 
 }  // namespace bx

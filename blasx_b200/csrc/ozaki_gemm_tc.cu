@@ -50,6 +50,7 @@ struct TcArgs {
     uint8_t *U;
     const Decision *dec;
     int *err;
+    int tj0, tjn;  // range of j-tiles (128 columns of C each) this launch covers
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
@@ -161,7 +162,7 @@ __device__ __forceinline__ uint32_t mod_small(int32_t x, int32_t m, float inv_m)
 struct TileCoord {
     int l, tj, ti;
 };
-__device__ __forceinline__ TileCoord decode(int64_t tile, int tiles_j, int tiles_i) {
+__device__ __forceinline__ TileCoord decode(int64_t tile, int tiles_j, int tiles_i, int tj0) {
     constexpr int GJ = 16;  // j-tiles per raster group (operand panels stay in L2)
     const int64_t per_mod = int64_t(tiles_j) * tiles_i;
     TileCoord c;
@@ -172,7 +173,7 @@ __device__ __forceinline__ TileCoord decode(int64_t tile, int tiles_j, int tiles
     const int first = group * GJ;
     const int gsize = min(GJ, tiles_j - first);
     const int64_t in = t % per_group;
-    c.tj = first + int(in % gsize);
+    c.tj = tj0 + first + int(in % gsize);
     c.ti = int(in / gsize);
     return c;
 }
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     residue_gemm_kernel(const __grid_constant__ CUtensorMap mapX,
                         const __grid_constant__ CUtensorMap mapY, const TcArgs a) {
     const int nmod = a.dec->nmod;
-    const int tiles_j = int(a.Jp / kTileJ), tiles_i = int(a.Ip / kTileI);
+    const int tiles_j = a.tjn, tiles_i = int(a.Ip / kTileI);
     const int64_t total = int64_t(nmod) * tiles_j * tiles_i;
     if (total == 0) return;  // native fallback chosen on the device
     const int num_kb = int(a.Kp / kTileK);
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             uint32_t issued = 0, par = 0;  // bit s: stage s has a load issued / its parity
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
-                const TileCoord c = decode(tile, tiles_j, tiles_i);
+                const TileCoord c = decode(tile, tiles_j, tiles_i, a.tj0);
                 for (int kb = 0; kb < num_kb; ++kb) {
                     if (!mbar_wait(empty0 + 8 * stage, phase ^ 1, abort_flag)) { ok = false; break; }
                     const uint32_t fb = full0 + 8 * stage;
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int64_t tile = blockIdx.x; tile < total; tile += gridDim.x) {
-            const TileCoord c = decode(tile, tiles_j, tiles_i);
+            const TileCoord c = decode(tile, tiles_j, tiles_i, a.tj0);
             const int32_t m = c_mod[c.l];
             const float inv_m = 1.0f / float(m);
             if (!mbar_wait(tfull0 + 8 * acc, acc_phase, abort_flag)) {
@@ -378,7 +379,7 @@ int prepare_residue_gemm_current_device() {
 
 int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
                         int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
-                        cudaStream_t s) {
+                        cudaStream_t s, int64_t tj_begin, int64_t tj_count) {
     if (Jp % kTileJ || Ip % kTileI || Kp % kTileK || Kp > int64_t(kMaxK) * 2)
         return set_error(BLASX_ERR_UNSUPPORTED, "residue GEMM: bad padded extents");
     static std::once_flag once;
@@ -393,8 +394,15 @@ int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp
     CUtensorMap mx, my;
     BX_TRY(make_map(&mx, X, Jp, Kp, kTileJ));
     BX_TRY(make_map(&my, Y, Ip, Kp, kTileI));
-    TcArgs a{Jp, Ip, Kp, U, dec, err_flag};
-    const int64_t tiles_upper = int64_t(kMaxModuli) * (Jp / kTileJ) * (Ip / kTileI);
+    if (tj_count < 0) {
+        tj_begin = 0;
+        tj_count = Jp / kTileJ;
+    }
+    if (tj_begin < 0 || tj_begin + tj_count > Jp / kTileJ)
+        return set_error(BLASX_ERR_ARG, "residue GEMM: j-tile range out of bounds");
+    TcArgs a{Jp, Ip, Kp, U, dec, err_flag, int(tj_begin), int(tj_count)};
+    const int64_t tiles_upper = int64_t(kMaxModuli) * tj_count * (Ip / kTileI);
+    if (tiles_upper == 0) return BLASX_OK;
     const int grid = int(tiles_upper < num_sms ? tiles_upper : num_sms);
     residue_gemm_kernel<<<grid, kThreadsTC, kSmemBytes, s>>>(mx, my, a);
     BX_CUDA(cudaGetLastError());

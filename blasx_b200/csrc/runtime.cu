@@ -13,6 +13,7 @@
 
 #include "ozaki.h"
 #include "runtime.h"
+#include "tile_engine.h"
 
 namespace bx {
 
@@ -145,6 +146,7 @@ int release_context() {
     if (!g_ctx) return BLASX_OK;
     cudaSetDevice(g_ctx->device);
     cudaDeviceSynchronize();
+    release_tile_arena();
     cudaStreamDestroy(g_ctx->compute);
     cudaStreamDestroy(g_ctx->h2d);
     cudaStreamDestroy(g_ctx->d2h);

@@ -1,0 +1,219 @@
+// tile_engine.cu -- executes a TilePlan for a host GEMM larger than the HBM
+// budget (out-of-core), on the native kernels.
+//
+// Replaces the reference's worker loop (blas/blasx_dgemm.c:98-248: batches
+// of 4 tasks, a host busy-wait on an event, cudaStreamSynchronize after the
+// copies of every tile-step, serial write-back of C) with a plan enqueued in
+// one pass over three streams, ordered only by events:
+//   H2D stream      operand tile -> its slot; C tile -> a C slot (beta != 0);
+//                   a reload into a slot first waits for the slot's last use;
+//   compute stream  waits for the tile's ready event, runs the K-step GEMM
+//                   (beta on the first K-step, 1 afterwards as in
+//                   blas/blasx_dgemm.c:82), records the slot's last use;
+//   D2H stream      writes a finished C tile back to the host.
+// The host thread never blocks until the final synchronisation, so copies
+// run ahead of compute as far as slot reuse allows. Host operands that are
+// not pinned are registered for the duration of the call over their full
+// ld x columns extent (the reference registers rows x columns,
+// blas/dgemm.c:88-90, which misses the ld padding).
+#include <chrono>
+#include <mutex>
+#include <vector>
+
+#include "kernels.h"
+#include "tile_engine.h"
+#include "tile_plan.h"
+
+namespace bx {
+
+namespace {
+
+constexpr int kCSlots = kCTileSlots;
+
+std::mutex g_arena_mu;
+void *g_arena = nullptr;
+size_t g_arena_bytes = 0;
+
+int ensure_arena(size_t bytes) {
+    if (g_arena && g_arena_bytes >= bytes) return BLASX_OK;
+    if (g_arena) {
+        cudaFree(g_arena);
+        g_arena = nullptr;
+        g_arena_bytes = 0;
+    }
+    BX_CUDA(cudaMalloc(&g_arena, bytes));
+    g_arena_bytes = bytes;
+    return BLASX_OK;
+}
+
+struct EventPool {
+    std::vector<cudaEvent_t> evs;
+    ~EventPool() {
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    }
+    int make(cudaEvent_t *out) {
+        BX_CUDA(cudaEventCreateWithFlags(out, cudaEventDisableTiming));
+        evs.push_back(*out);
+        return BLASX_OK;
+    }
+};
+
+}  // namespace
+
+int HostPin::pin(const void *p, size_t bytes) {
+    if (!p || !bytes) return BLASX_OK;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) == cudaSuccess && attr.type == cudaMemoryTypeHost)
+        return BLASX_OK;  // already pinned by the caller
+    cudaGetLastError();
+    if (cudaHostRegister(const_cast<void *>(p), bytes, cudaHostRegisterDefault) == cudaSuccess) {
+        regs.push_back(const_cast<void *>(p));
+    } else {
+        cudaGetLastError();  // not registrable: copies fall back to staged transfers
+    }
+    return BLASX_OK;
+}
+
+HostPin::~HostPin() {
+    for (void *p : regs) cudaHostUnregister(p);
+}
+
+size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es) {
+    if (rows <= 0 || cols <= 0) return 0;
+    return (size_t(ld) * size_t(cols - 1) + size_t(rows)) * es;
+}
+
+int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy) {
+    blasx_call_stats &st = call_stats();
+    const size_t es = elem_size(g.dt);
+    const size_t slot_bytes = size_t(T) * T * es;
+    const int64_t total_slots = int64_t(budget / slot_bytes);
+    const int op_slots = int(total_slots - kCSlots);
+    if (op_slots < 2)
+        return set_error(BLASX_ERR_NOMEM, "HBM budget %zu B holds fewer than %d tiles of %d^2",
+                         budget, kCSlots + 2, T);
+    TilePlan plan;
+    if (!plan_tiles(g.M, g.N, g.K, T, op_slots, policy, &plan))
+        return set_error(BLASX_ERR_ARG, "tile plan failed");
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        BX_TRY(ensure_arena(size_t(op_slots + kCSlots) * slot_bytes));
+    }
+    char *arena = static_cast<char *>(g_arena);
+    auto op_ptr = [&](int s) { return arena + size_t(s) * slot_bytes; };
+    auto c_ptr = [&](int s) { return arena + size_t(op_slots + s) * slot_bytes; };
+
+    HostPin pins;
+    BX_TRY(pins.pin(g.A, host_extent(g.lda, g.rows_a(), g.cols_a(), es)));
+    BX_TRY(pins.pin(g.B, host_extent(g.ldb, g.rows_b(), g.cols_b(), es)));
+    BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
+
+    EventPool pool;
+    std::vector<cudaEvent_t> ready(static_cast<size_t>(op_slots)), lastuse(static_cast<size_t>(op_slots));
+    std::vector<bool> used(static_cast<size_t>(op_slots), false);
+    cudaEvent_t c_ready[kCSlots], c_done[kCSlots], c_out[kCSlots];
+    bool c_used[kCSlots] = {false, false, false};
+    for (int s = 0; s < op_slots; ++s) {
+        BX_TRY(pool.make(&ready[size_t(s)]));
+        BX_TRY(pool.make(&lastuse[size_t(s)]));
+    }
+    for (int s = 0; s < kCSlots; ++s) {
+        BX_TRY(pool.make(&c_ready[s]));
+        BX_TRY(pool.make(&c_done[s]));
+        BX_TRY(pool.make(&c_out[s]));
+    }
+    cudaEvent_t start_ev;
+    BX_TRY(pool.make(&start_ev));
+    BX_CUDA(cudaEventRecord(start_ev, c->compute));
+    BX_CUDA(cudaStreamWaitEvent(c->h2d, start_ev, 0));
+    BX_CUDA(cudaStreamWaitEvent(c->d2h, start_ev, 0));
+
+    auto ext = [&](int idx, int64_t n) { return std::min<int64_t>(T, n - int64_t(idx) * T); };
+    const char *hA = static_cast<const char *>(g.A);
+    const char *hB = static_cast<const char *>(g.B);
+    char *hC = static_cast<char *>(g.C);
+
+    // host address and extent of an operand tile (stored layout)
+    auto load_tile = [&](const TileUse &u, const TileStep &s) -> int {
+        const bool isA = u.key.op == 0;
+        const int64_t rows_op = isA ? ext(s.i, g.M) : ext(s.k, g.K);  // op() rows
+        const int64_t cols_op = isA ? ext(s.k, g.K) : ext(s.j, g.N);
+        const int64_t r0 = int64_t(isA ? s.i : s.k) * T, c0 = int64_t(isA ? s.k : s.j) * T;
+        const bool tr = isA ? g.ta != NoTrans : g.tb != NoTrans;
+        const int64_t srow = tr ? c0 : r0, scol = tr ? r0 : c0;
+        const int64_t nrow = tr ? cols_op : rows_op, ncol = tr ? rows_op : cols_op;
+        const int64_t ld = isA ? g.lda : g.ldb;
+        const char *src = (isA ? hA : hB) + (srow + scol * ld) * int64_t(es);
+        if (used[size_t(u.slot)]) BX_CUDA(cudaStreamWaitEvent(c->h2d, lastuse[size_t(u.slot)], 0));
+        BX_CUDA(cudaMemcpy2DAsync(op_ptr(u.slot), size_t(T) * es, src, size_t(ld) * es,
+                                  size_t(nrow) * es, size_t(ncol), cudaMemcpyHostToDevice, c->h2d));
+        BX_CUDA(cudaEventRecord(ready[size_t(u.slot)], c->h2d));
+        st.h2d_bytes += double(nrow) * ncol * es;
+        return BLASX_OK;
+    };
+
+    int ctile = -1;
+    for (const TileStep &s : plan.steps) {
+        if (s.a.load) BX_TRY(load_tile(s.a, s));
+        if (s.b.load) BX_TRY(load_tile(s.b, s));
+        const int64_t m = ext(s.i, g.M), n = ext(s.j, g.N), k = ext(s.k, g.K);
+        if (s.first_k) {
+            ++ctile;
+            const int cs = ctile % kCSlots;
+            if (c_used[cs]) {  // previous occupant written back before reuse
+                BX_CUDA(cudaStreamWaitEvent(c->h2d, c_out[cs], 0));
+                BX_CUDA(cudaStreamWaitEvent(c->compute, c_out[cs], 0));
+            }
+            c_used[cs] = true;
+            if (!g.beta_zero()) {
+                char *src = hC + (int64_t(s.i) * T + int64_t(s.j) * T * g.ldc) * int64_t(es);
+                BX_CUDA(cudaMemcpy2DAsync(c_ptr(cs), size_t(T) * es, src, size_t(g.ldc) * es,
+                                          size_t(m) * es, size_t(n), cudaMemcpyHostToDevice, c->h2d));
+                BX_CUDA(cudaEventRecord(c_ready[cs], c->h2d));
+                BX_CUDA(cudaStreamWaitEvent(c->compute, c_ready[cs], 0));
+                st.h2d_bytes += double(m) * n * es;
+            }
+        }
+        const int cs = ctile % kCSlots;
+        BX_CUDA(cudaStreamWaitEvent(c->compute, ready[size_t(s.a.slot)], 0));
+        BX_CUDA(cudaStreamWaitEvent(c->compute, ready[size_t(s.b.slot)], 0));
+        Gemm d = g;
+        d.M = m; d.N = n; d.K = k;
+        d.A = op_ptr(s.a.slot); d.lda = T;
+        d.B = op_ptr(s.b.slot); d.ldb = T;
+        d.C = c_ptr(cs); d.ldc = T;
+        if (!s.first_k) d.beta = cplx{1.0, 0.0};
+        d.guard = nullptr;
+        BX_TRY(dmma_supported(d) ? launch_gemm_dmma(d, c->compute) : launch_gemm_simt(d, c->compute));
+        BX_CUDA(cudaEventRecord(lastuse[size_t(s.a.slot)], c->compute));
+        BX_CUDA(cudaEventRecord(lastuse[size_t(s.b.slot)], c->compute));
+        used[size_t(s.a.slot)] = used[size_t(s.b.slot)] = true;
+        if (s.last_k) {
+            BX_CUDA(cudaEventRecord(c_done[cs], c->compute));
+            BX_CUDA(cudaStreamWaitEvent(c->d2h, c_done[cs], 0));
+            char *dst = hC + (int64_t(s.i) * T + int64_t(s.j) * T * g.ldc) * int64_t(es);
+            BX_CUDA(cudaMemcpy2DAsync(dst, size_t(g.ldc) * es, c_ptr(cs), size_t(T) * es,
+                                      size_t(m) * es, size_t(n), cudaMemcpyDeviceToHost, c->d2h));
+            BX_CUDA(cudaEventRecord(c_out[cs], c->d2h));
+            st.d2h_bytes += double(m) * n * es;
+        }
+    }
+    BX_CUDA(cudaStreamSynchronize(c->h2d));
+    BX_CUDA(cudaStreamSynchronize(c->compute));
+    BX_CUDA(cudaStreamSynchronize(c->d2h));
+    st.cache_hits = double(plan.hits);
+    st.cache_misses = double(plan.loads);
+    st.evictions = double(plan.evictions);
+    st.tile = T;
+    st.path = 1;
+    return BLASX_OK;
+}
+
+void release_tile_arena() {
+    std::lock_guard<std::mutex> lk(g_arena_mu);
+    if (g_arena) cudaFree(g_arena);
+    g_arena = nullptr;
+    g_arena_bytes = 0;
+}
+
+}  // namespace bx

@@ -1,0 +1,29 @@
+// tile_engine.h -- out-of-core execution of a host GEMM through the HBM tile
+// cache, and host-memory pinning helpers shared by the host pipelines.
+#pragma once
+
+#include <vector>
+
+#include "runtime.h"
+
+namespace bx {
+
+// Pins host ranges for the lifetime of the object (no-op for memory that is
+// already pinned); unregisters what it registered on destruction.
+struct HostPin {
+    std::vector<void *> regs;
+    int pin(const void *p, size_t bytes);
+    ~HostPin();
+};
+
+// Bytes spanned by a column-major rows x cols matrix with leading dimension ld.
+size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es);
+
+// Host GEMM through tile x tile operand tiles cached in an HBM arena of
+// `budget` bytes (policy: 0 Belady, 1 LRU). Synchronous.
+int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int tile, int policy);
+
+// Frees the arena (blasx_finalize).
+void release_tile_arena();
+
+}  // namespace bx

@@ -125,6 +125,26 @@ typedef struct blasx_call_stats {
 } blasx_call_stats;
 void blasx_get_call_stats(blasx_call_stats *out);
 
+/* Tile schedule of a host GEMM that does not fit the HBM budget, computed on
+ * the host without touching a GPU (no counterpart in the reference; it
+ * replaces the reference's task queue and LRU tile cache,
+ * blas/blasx_task_queue.c, blas/LRU.c). C is cut into tile x tile blocks
+ * visited in snake order; operand tiles occupy budget_bytes / (tile^2 *
+ * elem_bytes) - 3 slots (3 hold C tiles); policy 0 = Belady (farthest next
+ * use), 1 = LRU. */
+typedef struct blasx_tile_plan_stats {
+    int tiles_m, tiles_n, tiles_k, slots;
+    long long steps;           /* GEMM launches (C tiles x K-steps) */
+    long long tile_loads;      /* operand tiles copied host -> device */
+    long long tile_hits;       /* operand uses served from HBM */
+    long long evictions;
+    double operand_h2d_bytes;  /* bytes of A and B tiles copied in */
+    double min_operand_h2d_bytes;  /* each element of A and B copied once */
+} blasx_tile_plan_stats;
+int blasx_tile_plan(long long M, long long N, long long K, long long tile,
+                    long long budget_bytes, int elem_bytes, int policy,
+                    blasx_tile_plan_stats *out);
+
 /* Device-resident GEMM: A, B, C are device pointers (column-major), the call
  * is enqueued on `stream` (a cudaStream_t; NULL = the CUDA default stream)
  * and returns without waiting. Scalars are host values. Used by callers whose

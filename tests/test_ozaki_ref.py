@@ -1,0 +1,48 @@
+"""CPU tests of the Ozaki scheme II restatement (oracle/ozaki_ref.py):
+exactness of the CRT reconstruction and the accuracy levels that calibrate
+the device-side modulus-count estimate."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import ozaki_ref
+
+
+def test_crt_constants():
+    for n in range(6, 21):
+        ms, M, w, Q = ozaki_ref.crt(n)
+        for a in range(len(ms)):
+            for b in range(a + 1, len(ms)):
+                assert math.gcd(ms[a], ms[b]) == 1
+        for m, wl in zip(ms, w):
+            assert wl % m == 1 and all(wl % m2 == 0 for m2 in ms if m2 != m)
+        assert 4 * 2 ** (2 * Q) <= M
+
+
+def test_reconstruction_is_exact():
+    A = oracle.spread((6, 300), 11, 1.0)
+    B = oracle.spread((300, 5), 12, 1.0)
+    for n in (8, 12, 15):
+        ozaki_ref.emulate(A, B, n, verify=True)
+
+
+def _normerr(C, A, B):
+    M, K = A.shape
+    N = B.shape[1]
+    ii, jj = np.indices((M, N))
+    ii, jj = ii.ravel(), jj.ravel()
+    val, bound = oracle.dd_entries("N", "N", M, N, K, 1.0, np.asfortranarray(A), M,
+                                   np.asfortranarray(B), K, 0.0, None, M, ii, jj)
+    return float(np.max(np.abs(C[ii, jj] - val) / bound)) / 2.0 ** -53
+
+
+@pytest.mark.parametrize("phi,n", [(0.0, 15), (1.0, 16)])
+def test_calibrated_modulus_counts_beat_native(phi, n):
+    # the modulus counts the device estimate picks for these spreads are at
+    # least as accurate as a plain FP64 dot product on the same inputs
+    A = oracle.spread((12, 2048), 5, phi)
+    B = oracle.spread((2048, 10), 6, phi)
+    C, _ = ozaki_ref.emulate(A, B, n)
+    assert _normerr(C, A, B) <= _normerr(A @ B, A, B) + 1e-3
