@@ -27,8 +27,9 @@
 extern "C" {
 #endif
 
-/* Enum values of the reference's include/cblas.h:11-12. */
-#ifndef CBLAS_ENUM_DEFINED_H
+/* Enum values of the reference's include/cblas.h:11-12 (skipped when a
+ * cblas.h guarded by CBLAS_H was included first). */
+#if !defined(CBLAS_H) && !defined(CBLAS_ENUM_DEFINED_H)
 #define CBLAS_ENUM_DEFINED_H
 enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
 enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 };
