@@ -47,6 +47,18 @@ class TilePlanStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("cache_hits", ctypes.c_longlong),
+                ("cache_misses", ctypes.c_longlong), ("grouped_launches", ctypes.c_longlong),
+                ("grouped_requests", ctypes.c_longlong), ("max_inflight_seen", _I), ("reserved", _I),
+                ("p50_ms", _D), ("p99_ms", _D), ("mean_ms", _D), ("max_ms", _D),
+                ("flops", _D), ("seconds", _D), ("tflops", _D)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class CallStats(ctypes.Structure):
     _fields_ = [("seconds", _D), ("h2d_bytes", _D), ("d2h_bytes", _D), ("cache_hits", _D),
                 ("cache_misses", _D), ("evictions", _D), ("path", _I), ("moduli", _I),
@@ -87,6 +99,9 @@ def lib() -> ctypes.CDLL:
         L.blasx_dgemm_device_noalloc.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_kernel_launch_count.restype = ctypes.c_uint64
         L.blasx_tile_plan.argtypes = [ctypes.c_longlong] * 5 + [_I, _I, ctypes.POINTER(TilePlanStats)]
+        L.blasx_serve_start.argtypes = [ctypes.c_size_t, ctypes.c_size_t, _I]
+        L.blasx_serve_invalidate.argtypes = [_P]
+        L.blasx_serve_get_stats.argtypes = [ctypes.POINTER(ServeStats)]
         L.blasx_profile_enable.argtypes = [_I]
         L.blasx_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long), _I]
         _lib = L
@@ -229,6 +244,30 @@ def set_tile(tile: int) -> int:
 
 def finalize() -> int:
     return lib().blasx_finalize()
+
+
+def serve_start(hbm_budget: int = 0, cache_bytes: int = 0, max_inflight: int = 0) -> int:
+    """Route host GEMM calls of all threads through the serving loop."""
+    return lib().blasx_serve_start(hbm_budget, cache_bytes, max_inflight)
+
+
+def serve_stop() -> int:
+    return lib().blasx_serve_stop()
+
+
+def serve_invalidate(host_buffer) -> int:
+    """Drop cached device copies of an operand modified in place."""
+    return lib().blasx_serve_invalidate(_addr(host_buffer))
+
+
+def serve_stats() -> dict:
+    s = ServeStats()
+    lib().blasx_serve_get_stats(ctypes.byref(s))
+    return s.as_dict()
+
+
+def serve_reset_stats() -> int:
+    return lib().blasx_serve_reset_stats()
 
 
 POLICY_BELADY, POLICY_LRU = 0, 1

@@ -11,6 +11,7 @@
 #include "host_pipeline.h"
 #include "kernels.h"
 #include "runtime.h"
+#include "serving.h"
 
 extern "C" __attribute__((weak)) void xerbla_(char *name, int *info) {
     // Same text as the reference, blas/error.c:5-8.
@@ -82,7 +83,9 @@ void host_entry(const char *name, DType dt, int order, int ta, int tb, int M, in
         return;
     }
     Gemm g = make_gemm(dt, order, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-    host_gemm(g);  // records its own status
+    if (g.M == 0 || g.N == 0) return;  // quick return, as in BLAS
+    if (serve::active()) serve::submit(g);  // records its own status
+    else host_gemm(g);
 }
 
 int device_entry(DType dt, int ta, int tb, int M, int N, int K, cplx alpha, const void *A,

@@ -153,8 +153,9 @@ __device__ __forceinline__ void load_tile(uint32_t sbase, const double *src, int
     }
 }
 
+// One C tile of one problem (`tile` in the grouped raster order below).
 template <bool CPLX, bool AKC, bool BKC, int KI>
-__global__ void __launch_bounds__(kThreads, 1) dmma_gemm_kernel(const DmmaParams p) {
+__device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, double *smem) {
     using TL = Tile<CPLX>;
     constexpr int BM = TL::BM, BN = TL::BN, MT = TL::MT, NT = TL::NT, BK = TL::BK;
     constexpr int STAGES = TL::STAGES;
@@ -164,13 +165,10 @@ __global__ void __launch_bounds__(kThreads, 1) dmma_gemm_kernel(const DmmaParams
     constexpr int A_STAGE = PLANES * SA::plane, B_STAGE = PLANES * SB::plane;  // doubles
     constexpr int IM = CPLX ? 1 : 0;
 
-    if (p.guard && *p.guard != 0) return;  // the emulated path produced C
-    extern __shared__ __align__(16) double smem[];
     double *sA = smem;
     double *sB = smem + STAGES * A_STAGE;
 
     // grouped rasterisation: 8 tile-rows per group keeps A panels hot in L2
-    const int tile = blockIdx.x;
     constexpr int GROUP = 8;
     const int per_group = GROUP * p.tiles_n;
     const int group = tile / per_group;
@@ -314,6 +312,50 @@ __global__ void __launch_bounds__(kThreads, 1) dmma_gemm_kernel(const DmmaParams
 }
 
 template <bool CPLX, bool AKC, bool BKC, int KI>
+__global__ void __launch_bounds__(kThreads, 1) dmma_gemm_kernel(const DmmaParams p) {
+    if (p.guard && *p.guard != 0) return;  // the emulated path produced C
+    extern __shared__ __align__(16) double smem[];
+    dmma_tile<CPLX, AKC, BKC, KI>(p, blockIdx.x, smem);
+}
+
+// Several problems in one launch: CTA b works on tile b - start[q] of the
+// problem q with start[q] <= b < start[q + 1]; the operand layouts of each
+// problem are chosen at run time (uniform within a CTA).
+// Problem table of a grouped launch, passed by value as a kernel parameter
+// (no device allocation): problem q owns CTAs [start[q], start[q + 1]).
+struct GroupTable {
+    int n;
+    int start[kMaxGroup + 1];
+    DmmaParams p[kMaxGroup];
+};
+
+// Several problems in one launch: CTA b works on tile b - start[q] of the
+// problem q with start[q] <= b < start[q + 1]; the operand layouts of each
+// problem are chosen at run time (uniform within a CTA).
+template <bool CPLX, int KI>
+__global__ void __launch_bounds__(kThreads, 1)
+    dmma_grouped_kernel(const __grid_constant__ GroupTable tab) {
+    extern __shared__ __align__(16) double smem[];
+    const int b = int(blockIdx.x);
+    int lo = 0, hi = tab.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (tab.start[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const DmmaParams p = tab.p[lo];
+    const int tile = b - tab.start[lo];
+    const bool akc = p.ta != NoTrans, bkc = p.tb == NoTrans;
+    if (akc) {
+        if (bkc) dmma_tile<CPLX, true, true, KI>(p, tile, smem);
+        else dmma_tile<CPLX, true, false, KI>(p, tile, smem);
+    } else {
+        if (bkc) dmma_tile<CPLX, false, true, KI>(p, tile, smem);
+        else dmma_tile<CPLX, false, false, KI>(p, tile, smem);
+    }
+}
+
+template <bool CPLX, bool AKC, bool BKC, int KI>
 int launch_cfg(const DmmaParams &p, cudaStream_t s) {
     using TL = Tile<CPLX>;
     constexpr int PLANES = CPLX ? 2 : 1;
@@ -352,7 +394,7 @@ template <bool CPLX, bool AKC, bool BKC> int launch_k(const DmmaParams &p, cudaS
     }
 }
 
-template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
+template <bool CPLX> DmmaParams make_params(const Gemm &g) {
     using TL = Tile<CPLX>;
     DmmaParams p;
     p.M = int(g.M); p.N = int(g.N); p.K = int(g.K);
@@ -368,6 +410,11 @@ template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
     p.vec_a = (g.lda % 2 == 0) && (reinterpret_cast<uintptr_t>(g.A) % 16 == 0);
     p.vec_b = (g.ldb % 2 == 0) && (reinterpret_cast<uintptr_t>(g.B) % 16 == 0);
     p.guard = g.guard;
+    return p;
+}
+
+template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
+    const DmmaParams p = make_params<CPLX>(g);
     if (int64_t(p.tiles_m) * p.tiles_n > INT32_MAX)
         return set_error(BLASX_ERR_UNSUPPORTED, "DMMA grid too large");
     const bool akc = g.ta != NoTrans;  // op(A) = A^T: stored K x M, k contiguous
@@ -376,10 +423,56 @@ template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
     return bkc ? launch_k<CPLX, false, true>(p, s) : launch_k<CPLX, false, false>(p, s);
 }
 
+template <bool CPLX, int KI> int launch_grouped_t(const GroupTable &tab, int tiles, cudaStream_t s) {
+    using TL = Tile<CPLX>;
+    constexpr int PLANES = CPLX ? 2 : 1;
+    constexpr int pa = SmemOp<TL::BM, TL::BK, true>::plane > SmemOp<TL::BM, TL::BK, false>::plane
+                           ? SmemOp<TL::BM, TL::BK, true>::plane
+                           : SmemOp<TL::BM, TL::BK, false>::plane;
+    constexpr int pb = SmemOp<TL::BN, TL::BK, true>::plane > SmemOp<TL::BN, TL::BK, false>::plane
+                           ? SmemOp<TL::BN, TL::BK, true>::plane
+                           : SmemOp<TL::BN, TL::BK, false>::plane;
+    // each layout combination places sB after its own A stages: size for the largest
+    constexpr size_t smem = size_t(TL::STAGES) * PLANES * (pa + pb) * sizeof(double);
+    static_assert(smem <= 227 * 1024, "shared memory budget");
+    auto kern = dmma_grouped_kernel<CPLX, KI>;
+    BX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kern<<<unsigned(tiles), kThreads, smem, s>>>(tab);
+    BX_CUDA(cudaGetLastError());
+    count_launch();
+    return BLASX_OK;
+}
+
 }  // namespace
 
 bool dmma_supported(const Gemm &g) {
     return g.dt != DType::F32 && g.M <= INT32_MAX && g.N <= INT32_MAX && g.K <= INT32_MAX;
+}
+
+int launch_gemm_dmma_grouped(const Gemm *gs, int n, cudaStream_t s) {
+    if (n <= 0) return BLASX_OK;
+    if (n > kMaxGroup) return set_error(BLASX_ERR_ARG, "grouped launch of %d > %d problems", n, kMaxGroup);
+    const bool cplx = gs[0].dt == DType::C128;
+    GroupTable tab;
+    tab.n = n;
+    int64_t tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        if (gs[i].dt != gs[0].dt || gs[i].dt == DType::F32)
+            return set_error(BLASX_ERR_ARG, "grouped launch needs one FP64 or complex128 dtype");
+        tab.p[i] = cplx ? make_params<true>(gs[i]) : make_params<false>(gs[i]);
+        tab.p[i].guard = nullptr;
+        tab.start[i] = int(tiles);
+        tiles += int64_t(tab.p[i].tiles_m) * tab.p[i].tiles_n;
+    }
+    tab.start[n] = int(tiles);
+    if (tiles == 0) return BLASX_OK;
+    if (tiles > INT32_MAX) return set_error(BLASX_ERR_UNSUPPORTED, "grouped launch too large");
+    if (cplx) return launch_grouped_t<true, 4>(tab, int(tiles), s);
+    switch (dmma_k()) {
+        case 4: return launch_grouped_t<false, 4>(tab, int(tiles), s);
+        case 8: return launch_grouped_t<false, 8>(tab, int(tiles), s);
+        default: return launch_grouped_t<false, 16>(tab, int(tiles), s);
+    }
 }
 
 int launch_gemm_dmma(const Gemm &g, cudaStream_t s) {

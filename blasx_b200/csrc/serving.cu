@@ -1,0 +1,668 @@
+// serving.cu -- continuous batching of host GEMM calls from many threads.
+//
+// When the serving loop runs (blasx_serve_start), cblas_?gemm / ?gemm_ calls
+// from any number of host threads become requests in one queue, served by a
+// single scheduler thread that owns the device:
+//
+//   admission   FIFO; a request is admitted when an in-flight slot is free and
+//               its device bytes (A, B, C copies and the emulated path's
+//               scratch) fit the HBM budget; a B operand found in the operand
+//               cache is not copied again and not charged again;
+//   in flight   every admitted request gets its own stream: its copies in,
+//               compute and copy out overlap with other requests' on the
+//               device, and requests that arrive meanwhile are admitted as
+//               slots and memory free up;
+//   mixing      small native FP64 / complex128 requests wait for their
+//               operands and are then run together by ONE grouped kernel
+//               launch whose grid holds the tiles of all of them;
+//   completion  detected by polling each request's last event; device memory
+//               is released, the B copy is kept in the operand cache (LRU,
+//               byte budget, pinned while in use) and the caller wakes up.
+//
+// Operand-cache identity rule: a cached device copy of B is reused when the
+// host pointer, leading dimension, stored shape and dtype match AND a
+// fingerprint of the contents matches -- an FNV-1a hash over 1024 elements
+// sampled at fixed, evenly spread positions plus the first and last column.
+// A change to the host buffer that touches none of the sampled elements is
+// not detected; callers that modify an operand in place between calls must
+// call blasx_serve_invalidate(ptr) (the reference has no cross-call cache at
+// all: it rebuilds its per-GPU caches on every call, blas/dgemm.c:106,114).
+//
+// Latency of a request = submit -> completion detected by the scheduler.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <future>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "kernels.h"
+#include "ozaki.h"
+#include "serving.h"
+#include "tile_engine.h"
+
+namespace bx {
+namespace serve {
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double now_s() {
+    return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
+}
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// ---- host-buffer pinning shared by all requests --------------------------------
+std::mutex g_pin_mu;
+std::map<const void *, std::pair<int, bool>> g_pins;  // ptr -> (users, registered by us)
+
+void pin_acquire(const void *p, size_t bytes) {
+    if (!p || !bytes) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_pins.find(p);
+    if (it != g_pins.end()) {
+        it->second.first++;
+        return;
+    }
+    bool ours = false;
+    cudaPointerAttributes attr;
+    if (!(cudaPointerGetAttributes(&attr, p) == cudaSuccess && attr.type == cudaMemoryTypeHost)) {
+        cudaGetLastError();
+        ours = cudaHostRegister(const_cast<void *>(p), bytes, cudaHostRegisterDefault) == cudaSuccess;
+        if (!ours) cudaGetLastError();
+    }
+    g_pins[p] = {1, ours};
+}
+
+void pin_release(const void *p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_pins.find(p);
+    if (it == g_pins.end()) return;
+    if (--it->second.first == 0) {
+        if (it->second.second) cudaHostUnregister(const_cast<void *>(p));
+        g_pins.erase(it);
+    }
+}
+
+// ---- operand cache ------------------------------------------------------------------
+struct Key {
+    const void *ptr;
+    int64_t ld, rows, cols;
+    int dt;
+    uint64_t fp;
+    bool operator==(const Key &o) const {
+        return ptr == o.ptr && ld == o.ld && rows == o.rows && cols == o.cols && dt == o.dt &&
+               fp == o.fp;
+    }
+};
+struct KeyHash {
+    size_t operator()(const Key &k) const {
+        return std::hash<const void *>()(k.ptr) ^ (size_t(k.fp) * 31u) ^ size_t(k.ld * 131 + k.cols);
+    }
+};
+struct Entry {
+    Key key;
+    void *dev = nullptr;
+    int64_t dld = 0;
+    size_t bytes = 0;
+    int users = 0;
+    bool stale = false;
+    std::list<Entry *>::iterator lru;
+};
+
+uint64_t fingerprint(const void *p, int64_t ld, int64_t rows, int64_t cols, size_t es) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const unsigned char *b) {
+        for (size_t i = 0; i < es; ++i) {
+            h ^= b[i];
+            h *= 1099511628211ull;
+        }
+    };
+    const unsigned char *base = static_cast<const unsigned char *>(p);
+    const int64_t n = rows * cols;
+    if (n == 0) return h;
+    auto at = [&](int64_t r, int64_t c) { return base + (r + c * ld) * int64_t(es); };
+    for (int t = 0; t < 1024; ++t) {
+        const int64_t idx = (int64_t(t) * (n - 1)) / 1023;
+        mix(at(idx % rows, idx / rows));
+    }
+    for (int64_t r = 0; r < rows; ++r) {
+        mix(at(r, 0));
+        mix(at(r, cols - 1));
+    }
+    return h;
+}
+
+// ---- requests -----------------------------------------------------------------------
+struct Request {
+    Gemm g;
+    double t_submit = 0, t_done = 0;
+    std::promise<int> done;
+    int status = BLASX_OK;
+    // device side
+    void *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    int64_t lda = 0, ldb = 0, ldc = 0;
+    Entry *bcache = nullptr;  // cached B in use
+    Key bkey{};
+    bool bkey_valid = false;
+    size_t charged = 0;        // bytes counted against the budget
+    bool grouped = false;
+    int stream_slot = -1;
+    cudaEvent_t ev_in = nullptr, ev_done = nullptr;
+    int stage = 0;  // 1 copying in (grouped: waiting for operands), 3 in flight to completion
+    double flops = 0;
+    blasx_call_stats stats{};
+};
+
+struct Server {
+    size_t budget = 0, cache_budget = 0;
+    int max_inflight = 8;
+    double group_flops = 4e9;
+
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<std::shared_ptr<Request>> queue;
+    bool stopping = false;
+    std::thread thread;
+
+    // scheduler-owned
+    std::vector<cudaStream_t> streams;
+    std::vector<bool> stream_busy;
+    cudaStream_t batch_stream = nullptr;
+    std::vector<std::shared_ptr<Request>> pending, inflight;
+    size_t used = 0;  // bytes of in-flight device copies (excluding cached operands)
+
+    std::mutex cache_mu;
+    std::unordered_map<Key, Entry *, KeyHash> cache;
+    std::list<Entry *> lru;  // front = most recent
+    size_t cache_bytes = 0;
+
+    // statistics
+    std::mutex stat_mu;
+    std::vector<double> latencies;
+    double flops = 0, t_first = 0, t_last = 0;
+    long long submitted = 0, completed = 0, hits = 0, misses = 0, grouped_launches = 0,
+              grouped_requests = 0, failed = 0;
+    int max_seen = 0;
+};
+
+std::mutex g_server_mu;
+Server *g_server = nullptr;
+std::atomic<bool> g_active{false};
+
+size_t device_bytes(const Request &r, bool need_b) {
+    const Gemm &g = r.g;
+    const size_t es = elem_size(g.dt);
+    const bool need_ab = !(g.alpha_zero() || g.K == 0);
+    size_t b = size_t(round_up(g.M, 32)) * g.N * es;
+    if (need_ab) {
+        b += size_t(round_up(g.rows_a(), 32)) * g.cols_a() * es;
+        if (need_b) b += size_t(round_up(g.rows_b(), 32)) * g.cols_b() * es;
+        const int mode = config().dgemm_mode.load();
+        const int64_t kmax = g.dt == DType::C128 ? oz::kMaxK / 2 : oz::kMaxK;
+        const double work = double(g.M) * double(g.N) * double(g.K);
+        const bool worth = work >= double(1 << 27) && g.M >= 64 && g.N >= 64 && g.K >= 32;
+        if (g.K <= kmax && (mode == 2 || (mode == 0 && worth))) {
+            Gemm probe = g;
+            b += ozaki_scratch_bytes(probe);
+        }
+    }
+    return b;
+}
+
+// Evicts unused cache entries (LRU first) until `need` more bytes fit.
+// Drops unused cache entries from the least recently used end while `over`
+// holds (caller holds cache_mu).
+template <typename Pred> void evict_lru(Server &s, cudaStream_t st, Pred over) {
+    auto it = s.lru.end();
+    while (it != s.lru.begin() && over()) {
+        --it;
+        Entry *e = *it;
+        if (e->users) continue;
+        it = s.lru.erase(it);  // next element: already visited going backwards
+        s.cache.erase(e->key);
+        s.cache_bytes -= e->bytes;
+        cudaFreeAsync(e->dev, st);
+        delete e;
+    }
+}
+
+void cache_make_room(Server &s, size_t need, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(s.cache_mu);
+    evict_lru(s, st, [&] { return s.used + s.cache_bytes + need > s.budget; });
+}
+
+int admit(Server &s, Request *r, int slot) {
+    Gemm &g = r->g;
+    const size_t es = elem_size(g.dt);
+    cudaStream_t st = s.streams[size_t(slot)];
+    r->stream_slot = slot;
+    const bool need_ab = !(g.alpha_zero() || g.K == 0);
+    const bool read_c = !g.beta_zero();
+    r->lda = round_up(g.rows_a(), 32);
+    r->ldb = round_up(g.rows_b(), 32);
+    r->ldc = round_up(g.M, 32);
+    BX_CUDA(cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming));
+    BX_CUDA(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
+    if (need_ab) {
+        BX_CUDA(cudaMallocAsync(&r->dA, size_t(r->lda) * g.cols_a() * es, st));
+        BX_CUDA(cudaMemcpy2DAsync(r->dA, r->lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
+                                  cudaMemcpyHostToDevice, st));
+        r->stats.h2d_bytes += double(es) * g.rows_a() * g.cols_a();
+        if (r->bcache) {
+            r->dB = r->bcache->dev;
+            r->ldb = r->bcache->dld;
+            r->stats.cache_hits += 1;
+        } else {
+            BX_CUDA(cudaMallocAsync(&r->dB, size_t(r->ldb) * g.cols_b() * es, st));
+            BX_CUDA(cudaMemcpy2DAsync(r->dB, r->ldb * es, g.B, g.ldb * es, g.rows_b() * es,
+                                      g.cols_b(), cudaMemcpyHostToDevice, st));
+            r->stats.h2d_bytes += double(es) * g.rows_b() * g.cols_b();
+            r->stats.cache_misses += 1;
+        }
+    }
+    BX_CUDA(cudaMallocAsync(&r->dC, size_t(r->ldc) * g.N * es, st));
+    if (read_c) {
+        BX_CUDA(cudaMemcpy2DAsync(r->dC, r->ldc * es, g.C, g.ldc * es, g.M * es, g.N,
+                                  cudaMemcpyHostToDevice, st));
+        r->stats.h2d_bytes += double(es) * g.M * g.N;
+    }
+    BX_CUDA(cudaEventRecord(r->ev_in, st));
+    if (r->grouped) {
+        r->stage = 1;  // compute joins the next grouped launch once the copies landed
+        return BLASX_OK;
+    }
+    Gemm d = g;
+    d.A = r->dA; d.lda = r->lda;
+    d.B = r->dB; d.ldb = r->ldb;
+    d.C = r->dC; d.ldc = r->ldc;
+    BX_TRY(device_gemm(d, st));
+    r->stats.path = call_stats().path;
+    r->stats.moduli = 0;
+    BX_CUDA(cudaMemcpy2DAsync(g.C, g.ldc * es, r->dC, r->ldc * es, g.M * es, g.N,
+                              cudaMemcpyDeviceToHost, st));
+    r->stats.d2h_bytes += double(es) * g.M * g.N;
+    BX_CUDA(cudaEventRecord(r->ev_done, st));
+    r->stage = 3;
+    return BLASX_OK;
+}
+
+// One grouped launch for every grouped request whose operands have landed.
+int launch_groups(Server &s) {
+    for (DType dt : {DType::F64, DType::C128}) {
+        std::vector<Request *> ready;
+        for (const auto &r : s.inflight)
+            if (r->grouped && r->stage == 1 && r->g.dt == dt && cudaEventQuery(r->ev_in) == cudaSuccess)
+                ready.push_back(r.get());
+        cudaGetLastError();
+        for (size_t off = 0; off < ready.size(); off += kMaxGroup) {
+            const size_t n = std::min(ready.size() - off, size_t(kMaxGroup));
+            std::vector<Gemm> gs;
+            for (size_t i = 0; i < n; ++i) {
+                Request *r = ready[off + i];
+                Gemm d = r->g;
+                d.A = r->dA; d.lda = r->lda;
+                d.B = r->dB; d.ldb = r->ldb;
+                d.C = r->dC; d.ldc = r->ldc;
+                gs.push_back(d);
+            }
+            BX_TRY(launch_gemm_dmma_grouped(gs.data(), int(n), s.batch_stream));
+            cudaEvent_t ev;
+            BX_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            BX_CUDA(cudaEventRecord(ev, s.batch_stream));
+            for (size_t i = 0; i < n; ++i) {
+                Request *r = ready[off + i];
+                cudaStream_t st = s.streams[size_t(r->stream_slot)];
+                const size_t es = elem_size(r->g.dt);
+                BX_CUDA(cudaStreamWaitEvent(st, ev, 0));
+                BX_CUDA(cudaMemcpy2DAsync(r->g.C, r->g.ldc * es, r->dC, r->ldc * es,
+                                          r->g.M * es, r->g.N, cudaMemcpyDeviceToHost, st));
+                r->stats.d2h_bytes += double(es) * r->g.M * r->g.N;
+                BX_CUDA(cudaEventRecord(r->ev_done, st));
+                r->stats.path = 1;
+                r->stage = 3;
+            }
+            cudaEventDestroy(ev);
+            std::lock_guard<std::mutex> lk(s.stat_mu);
+            s.grouped_launches += 1;
+            s.grouped_requests += static_cast<long long>(n);
+        }
+    }
+    return BLASX_OK;
+}
+
+void finish(Server &s, Request *r, int status) {
+    cudaStream_t st = s.streams[size_t(r->stream_slot)];
+    const Gemm &g = r->g;
+    const size_t es = elem_size(g.dt);
+    if (r->dA) cudaFreeAsync(r->dA, st);
+    if (r->dC) cudaFreeAsync(r->dC, st);
+    {
+        std::lock_guard<std::mutex> lk(s.cache_mu);
+        if (r->bcache) {
+            r->bcache->users--;
+            if (r->bcache->stale && r->bcache->users == 0) {
+                s.lru.erase(r->bcache->lru);
+                s.cache.erase(r->bcache->key);
+                s.cache_bytes -= r->bcache->bytes;
+                cudaFreeAsync(r->bcache->dev, st);
+                delete r->bcache;
+            }
+        } else if (r->dB) {
+            const size_t bytes = size_t(r->ldb) * g.cols_b() * es;
+            const bool keep = status == BLASX_OK && r->bkey_valid && bytes <= s.cache_budget &&
+                              s.cache.find(r->bkey) == s.cache.end();
+            if (keep)  // make room inside the cache budget (least recently used, unused first)
+                evict_lru(s, st, [&] { return s.cache_bytes + bytes > s.cache_budget; });
+            if (keep && s.cache_bytes + bytes <= s.cache_budget) {
+                Entry *e = new Entry;
+                e->key = r->bkey;
+                e->dev = r->dB;
+                e->dld = r->ldb;
+                e->bytes = bytes;
+                s.lru.push_front(e);
+                e->lru = s.lru.begin();
+                s.cache[e->key] = e;
+                s.cache_bytes += bytes;
+            } else {
+                cudaFreeAsync(r->dB, st);
+            }
+        }
+    }
+    s.used -= r->charged;
+    s.stream_busy[size_t(r->stream_slot)] = false;
+    if (r->ev_in) cudaEventDestroy(r->ev_in);
+    if (r->ev_done) cudaEventDestroy(r->ev_done);
+    r->t_done = now_s();
+    r->stats.seconds = r->t_done - r->t_submit;
+    {
+        std::lock_guard<std::mutex> lk(s.stat_mu);
+        s.completed += 1;
+        if (status != BLASX_OK) s.failed += 1;
+        s.latencies.push_back(r->t_done - r->t_submit);
+        s.flops += g.flops();
+        s.t_last = r->t_done;
+    }
+    r->status = status;
+    r->done.set_value(status);
+}
+
+void loop(Server *sp) {
+    Server &s = *sp;
+    Context *c = context();
+    if (c) cudaSetDevice(c->device);
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(s.mu);
+            if (s.pending.empty() && s.inflight.empty()) {
+                s.cv.wait(lk, [&] { return s.stopping || !s.queue.empty(); });
+                if (s.stopping && s.queue.empty()) return;
+            }
+            while (!s.queue.empty()) {
+                s.pending.push_back(s.queue.front());
+                s.queue.pop_front();
+            }
+        }
+        bool progress = false;
+        // completions
+        for (size_t i = 0; i < s.inflight.size();) {
+            Request *r = s.inflight[i].get();
+            if (r->stage == 3) {
+                const cudaError_t q = cudaEventQuery(r->ev_done);
+                if (q == cudaSuccess || (q != cudaErrorNotReady)) {
+                    if (q != cudaSuccess) cudaGetLastError();
+                    finish(s, r, q == cudaSuccess ? BLASX_OK : BLASX_ERR_CUDA);
+                    s.inflight.erase(s.inflight.begin() + long(i));
+                    progress = true;
+                    continue;
+                }
+            }
+            ++i;
+        }
+        // grouped launches of small native requests whose operands landed
+        launch_groups(s);
+        // admission (FIFO)
+        while (!s.pending.empty() && int(s.inflight.size()) < s.max_inflight) {
+            std::shared_ptr<Request> rp = s.pending.front();
+            Request *r = rp.get();
+            // operand cache lookup for B
+            Entry *hit = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(s.cache_mu);
+                if (r->bkey_valid) {
+                    auto it = s.cache.find(r->bkey);
+                    if (it != s.cache.end() && !it->second->stale) {
+                        hit = it->second;
+                        hit->users++;
+                        s.lru.splice(s.lru.begin(), s.lru, hit->lru);
+                    }
+                }
+            }
+            const size_t need = device_bytes(*r, hit == nullptr);
+            if (s.used + s.cache_bytes + need > s.budget) cache_make_room(s, need, s.batch_stream);
+            if (s.used + need > s.budget && !s.inflight.empty()) {
+                if (hit) {
+                    std::lock_guard<std::mutex> lk(s.cache_mu);
+                    hit->users--;
+                }
+                break;  // wait for memory to free up
+            }
+            int slot = -1;
+            for (size_t k = 0; k < s.stream_busy.size(); ++k)
+                if (!s.stream_busy[k]) { slot = int(k); break; }
+            if (slot < 0) {
+                if (hit) {
+                    std::lock_guard<std::mutex> lk(s.cache_mu);
+                    hit->users--;
+                }
+                break;
+            }
+            s.pending.erase(s.pending.begin());
+            s.stream_busy[size_t(slot)] = true;
+            r->bcache = hit;
+            r->charged = need;
+            s.used += need;
+            {
+                std::lock_guard<std::mutex> lk(s.stat_mu);
+                if (r->bkey_valid && !(r->g.alpha_zero() || r->g.K == 0)) (hit ? s.hits : s.misses) += 1;
+            }
+            const int st = admit(s, r, slot);
+            s.inflight.push_back(rp);
+            s.max_seen = std::max(s.max_seen, int(s.inflight.size()));
+            if (st != BLASX_OK) {
+                s.inflight.pop_back();
+                finish(s, r, st);
+            }
+            progress = true;
+        }
+        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+}  // namespace
+
+bool active() { return g_active.load(std::memory_order_acquire); }
+
+int submit(const Gemm &g) {
+    Server *s;
+    {
+        std::lock_guard<std::mutex> lk(g_server_mu);
+        s = g_server;
+    }
+    if (!s) return set_error(BLASX_ERR_CLOSED, "serving loop is not running");
+    const size_t es = elem_size(g.dt);
+    const bool need_ab = !(g.alpha_zero() || g.K == 0);
+    // shared by the caller and the scheduler: whichever lets go last frees it
+    auto rp = std::make_shared<Request>();
+    Request *r = rp.get();
+    r->g = g;
+    r->t_submit = now_s();
+    // small native requests are mixed into grouped launches
+    r->flops = 0;
+    r->grouped = false;
+    if (g.dt != DType::F32 && need_ab) {
+        const int mode = config().dgemm_mode.load();
+        const double work = double(g.M) * double(g.N) * double(g.K);
+        const bool emulated = mode == 2 || (mode == 0 && work >= double(1 << 27) && g.M >= 64 &&
+                                            g.N >= 64 && g.K >= 32);
+        r->grouped = !emulated && g.flops() <= s->group_flops;
+    }
+    if (need_ab) {
+        r->bkey = Key{g.B, g.ldb, g.rows_b(), g.cols_b(), int(g.dt),
+                      fingerprint(g.B, g.ldb, g.rows_b(), g.cols_b(), es)};
+        r->bkey_valid = true;
+    }
+    pin_acquire(g.A, need_ab ? host_extent(g.lda, g.rows_a(), g.cols_a(), es) : 0);
+    pin_acquire(g.B, need_ab ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0);
+    pin_acquire(g.C, host_extent(g.ldc, g.M, g.N, es));
+    std::future<int> fut = r->done.get_future();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stopping) return set_error(BLASX_ERR_CLOSED, "serving loop is shutting down");
+        s->queue.push_back(rp);
+        std::lock_guard<std::mutex> lk2(s->stat_mu);
+        s->submitted += 1;
+        if (s->t_first == 0) s->t_first = r->t_submit;
+    }
+    s->cv.notify_one();
+    const int st = fut.get();
+    pin_release(g.A);
+    pin_release(g.B);
+    pin_release(g.C);
+    call_stats() = r->stats;
+    if (call_stats().path == 0) call_stats().path = 1;
+    if (st != BLASX_OK) return set_error(st, "serving: request failed");
+    return BLASX_OK;
+}
+
+}  // namespace serve
+}  // namespace bx
+
+using namespace bx::serve;
+
+extern "C" {
+
+int blasx_serve_start(size_t hbm_budget, size_t cache_bytes, int max_inflight) {
+    std::lock_guard<std::mutex> lk(g_server_mu);
+    if (g_server) return BLASX_OK;
+    bx::Context *c = bx::context();
+    if (!c) return bx::last_status();
+    auto *s = new Server;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    s->budget = hbm_budget ? hbm_budget : size_t(double(free_b) * 0.85);
+    s->cache_budget = cache_bytes ? std::min(cache_bytes, s->budget / 2) : s->budget / 4;
+    s->max_inflight = max_inflight > 0 ? std::min(max_inflight, 64) : 8;
+    s->streams.resize(size_t(s->max_inflight));
+    s->stream_busy.assign(size_t(s->max_inflight), false);
+    for (auto &st : s->streams) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&s->batch_stream, cudaStreamNonBlocking);
+    s->thread = std::thread(loop, s);
+    g_server = s;
+    g_active.store(true, std::memory_order_release);
+    return BLASX_OK;
+}
+
+int blasx_serve_stop(void) {
+    Server *s;
+    {
+        std::lock_guard<std::mutex> lk(g_server_mu);
+        s = g_server;
+        if (!s) return BLASX_OK;
+        g_active.store(false, std::memory_order_release);
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+    }
+    s->cv.notify_all();
+    s->thread.join();  // the loop drains queued and in-flight requests first
+    {
+        std::lock_guard<std::mutex> lk(s->cache_mu);
+        for (auto &kv : s->cache) {
+            cudaFree(kv.second->dev);
+            delete kv.second;
+        }
+    }
+    for (auto st : s->streams) cudaStreamDestroy(st);
+    cudaStreamDestroy(s->batch_stream);
+    std::lock_guard<std::mutex> lk(g_server_mu);
+    g_server = nullptr;
+    delete s;
+    return BLASX_OK;
+}
+
+int blasx_serve_invalidate(const void *host_ptr) {
+    std::lock_guard<std::mutex> lk(g_server_mu);
+    if (!g_server) return BLASX_OK;
+    Server &s = *g_server;
+    std::lock_guard<std::mutex> lk2(s.cache_mu);
+    int n = 0;
+    for (auto &kv : s.cache)
+        if (kv.first.ptr == host_ptr) {
+            kv.second->stale = true;
+            ++n;
+        }
+    return n;
+}
+
+void blasx_serve_get_stats(blasx_serve_stats *out) {
+    if (!out) return;
+    memset(out, 0, sizeof *out);
+    std::lock_guard<std::mutex> lk(g_server_mu);
+    if (!g_server) return;
+    Server &s = *g_server;
+    std::lock_guard<std::mutex> lk2(s.stat_mu);
+    out->submitted = s.submitted;
+    out->completed = s.completed;
+    out->failed = s.failed;
+    out->cache_hits = s.hits;
+    out->cache_misses = s.misses;
+    out->grouped_launches = s.grouped_launches;
+    out->grouped_requests = s.grouped_requests;
+    out->max_inflight_seen = s.max_seen;
+    out->flops = s.flops;
+    out->seconds = s.t_last > s.t_first ? s.t_last - s.t_first : 0;
+    out->tflops = out->seconds > 0 ? s.flops / out->seconds / 1e12 : 0;
+    if (!s.latencies.empty()) {
+        std::vector<double> l = s.latencies;
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double q) {
+            const size_t i = std::min(l.size() - 1, size_t(q * double(l.size() - 1) + 0.5));
+            return l[i] * 1e3;
+        };
+        double sum = 0;
+        for (double v : l) sum += v;
+        out->p50_ms = pct(0.50);
+        out->p99_ms = pct(0.99);
+        out->mean_ms = sum / double(l.size()) * 1e3;
+        out->max_ms = l.back() * 1e3;
+    }
+}
+
+int blasx_serve_reset_stats(void) {
+    std::lock_guard<std::mutex> lk(g_server_mu);
+    if (!g_server) return BLASX_OK;
+    Server &s = *g_server;
+    std::lock_guard<std::mutex> lk2(s.stat_mu);
+    s.latencies.clear();
+    s.flops = 0;
+    s.t_first = s.t_last = 0;
+    s.submitted = s.completed = s.hits = s.misses = s.grouped_launches = s.grouped_requests = 0;
+    s.failed = 0;
+    s.max_seen = 0;
+    return BLASX_OK;
+}
+
+}  // extern "C"

@@ -185,6 +185,36 @@ int blasx_dgemm_device_noalloc(int transa, int transb, int M, int N, int K, doub
  * threads); lets a caller count the GPU work of a region. */
 uint64_t blasx_kernel_launch_count(void);
 
+/* Serving loop (no counterpart in the reference, whose GEMM path is not
+ * re-entrant). While it runs, cblas_?gemm / ?gemm_ calls from any number of
+ * host threads are queued to one scheduler thread that owns the device: it
+ * admits requests when an in-flight slot is free and their device memory
+ * fits hbm_budget (0 = 85% of free HBM), runs several at once on their own
+ * streams (continuous batching), mixes small native FP64 / complex128
+ * requests into one grouped kernel launch, and keeps copies of B operands in
+ * an HBM operand cache of cache_bytes (0 = a quarter of the budget).
+ * Operand identity: host pointer, leading dimension, stored shape, dtype and
+ * a fingerprint of 1024 sampled elements plus the first and last column; a
+ * caller that modifies an operand in place without touching those must call
+ * blasx_serve_invalidate(ptr). max_inflight: requests on the device at once
+ * (0 = 8, at most 64). Calls block until their C is complete. */
+int blasx_serve_start(size_t hbm_budget, size_t cache_bytes, int max_inflight);
+/* Drains queued and in-flight requests, then stops; call once no thread is
+ * still submitting. */
+int blasx_serve_stop(void);
+/* Drops cached device copies of the operand at host_ptr; returns how many. */
+int blasx_serve_invalidate(const void *host_ptr);
+typedef struct blasx_serve_stats {
+    long long submitted, completed, failed;
+    long long cache_hits, cache_misses;        /* B operands reused / copied */
+    long long grouped_launches, grouped_requests;
+    int max_inflight_seen, reserved;
+    double p50_ms, p99_ms, mean_ms, max_ms;    /* submit -> completion */
+    double flops, seconds, tflops;             /* first submit -> last completion */
+} blasx_serve_stats;
+void blasx_serve_get_stats(blasx_serve_stats *out);
+int blasx_serve_reset_stats(void);
+
 /* Per-phase device timing. When enabled, every GEMM records CUDA events on
  * its own stream around its phases: 0 slicing (emulated path: statistics,
  * modulus decision, scaling, residues), 1 INT8 residue GEMMs, 2 CRT
