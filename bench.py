@@ -52,6 +52,12 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target CPU time per reference sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--serving", type=int, default=400,
+                   help="requests of the serving load (0 = skip); 10000 with --serving-dmax 16384 is the full stream")
+    p.add_argument("--serving-dmax", type=int, default=4096)
+    p.add_argument("--serving-threads", type=int, default=16)
+    p.add_argument("--serving-rate", type=float, default=0.0,
+                   help="offered requests/s over all threads (Poisson); 0 = back to back")
     return p.parse_args()
 
 
@@ -73,7 +79,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except (OSError, FileNotFoundError):
@@ -164,6 +170,93 @@ def reference_cpu_sample(n: int, seconds: float, cores: int, steps: int = 1, war
     sample = (f"C[:, :{ns}] of the {n}^3 DGEMM ({2.0 * n * n * ns / 1e12:.2f} TFLOP) as {T}-sized tile calls "
               f"through the reference's cblas_dgemm CPU path")
     return out, sample, kind, (ref.name if hasattr(ref, "name") else oracle.REF_PATH)
+
+
+def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, seed: int = 7):
+    """Serving stream through the drop-in cblas_?gemm calls with the serving
+    loop running: `threads` host threads, dtype mix 60% FP64 / 30% FP32 /
+    10% complex128, M, N, K each log-uniform in [64, dmax], random transposes,
+    30% of the calls reuse a B operand sent before (same pointer and shape),
+    inputs uniform in [-1, 1]; Poisson arrivals at `rate` requests/s (0: each
+    thread submits its next call as soon as the previous one returns).
+    Host operands are sub-matrices of pinned pools (A and B shared, read-only;
+    one C buffer per thread)."""
+    import random
+    import threading
+
+    import numpy as np
+    dts = [np.float64, np.float32, np.complex128]
+    pools = {}
+    for dt in dts:
+        t = {np.float64: torch.float64, np.float32: torch.float32, np.complex128: torch.complex128}[dt]
+        a = torch.empty(dmax * dmax, dtype=t, pin_memory=True)
+        b = torch.empty(dmax * dmax, dtype=t, pin_memory=True)
+        g = torch.Generator().manual_seed(seed)
+        if dt == np.complex128:
+            a.copy_(torch.complex(torch.rand(dmax * dmax, generator=g, dtype=torch.float64) * 2 - 1,
+                                  torch.rand(dmax * dmax, generator=g, dtype=torch.float64) * 2 - 1))
+            b.copy_(torch.complex(torch.rand(dmax * dmax, generator=g, dtype=torch.float64) * 2 - 1,
+                                  torch.rand(dmax * dmax, generator=g, dtype=torch.float64) * 2 - 1))
+        else:
+            a.copy_(torch.rand(dmax * dmax, generator=g, dtype=t) * 2 - 1)
+            b.copy_(torch.rand(dmax * dmax, generator=g, dtype=t) * 2 - 1)
+        pools[dt] = (a, b, a.element_size())
+    rng = random.Random(seed)
+    lo, hi = np.log(64), np.log(dmax)
+    reqs, sent_b = [], []
+    for _ in range(n_req):
+        dt = rng.choices(dts, weights=[60, 30, 10])[0]
+        if sent_b and rng.random() < 0.3:
+            dtb, K, N, tb = rng.choice(sent_b)
+            dt = dtb
+        else:
+            K, N = (int(np.exp(rng.uniform(lo, hi))) for _ in range(2))
+            tb = rng.choice("NTC" if dt == np.complex128 else "NT")
+            sent_b.append((dt, K, N, tb))
+        M = int(np.exp(rng.uniform(lo, hi)))
+        ta = rng.choice("NTC" if dt == np.complex128 else "NT")
+        reqs.append((dt, ta, tb, M, N, K))
+    per_thread = [reqs[t::threads] for t in range(threads)]
+    # one pinned C buffer per thread, as large as that thread's largest C
+    cbuf = []
+    for t in range(threads):
+        need = max([M * N * (16 if dt == np.complex128 else (8 if dt == np.float64 else 4))
+                    for (dt, ta, tb, M, N, K) in per_thread[t]] or [16])
+        cbuf.append(torch.empty(need, dtype=torch.uint8, pin_memory=True))
+    errors = []
+
+    def worker(t):
+        r = random.Random(seed + t)
+        for (dt, ta, tb, M, N, K) in per_thread[t]:
+            if rate > 0:
+                time.sleep(r.expovariate(rate / threads))
+            a, b, es = pools[dt]
+            lda = M if ta == "N" else K
+            ldb = K if tb == "N" else N
+            alpha = 1.0 if dt != np.complex128 else 1.0 + 0.0j
+            fn = {np.float64: bx.cblas_dgemm, np.float32: bx.cblas_sgemm, np.complex128: bx.cblas_zgemm}[dt]
+            fn(bx.CblasColMajor, bx.TRANS[ta], bx.TRANS[tb], M, N, K, alpha, a.data_ptr(), lda, b.data_ptr(), ldb,
+               0.0, cbuf[t].data_ptr(), M)
+            if bx.last_status() != 0:
+                errors.append(bx.last_error())
+
+    bx.serve_start(0, 0, 8)
+    bx.serve_reset_stats()
+    th = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
+    t0 = time.perf_counter()
+    [x.start() for x in th]
+    [x.join() for x in th]
+    wall = time.perf_counter() - t0
+    st = bx.serve_stats()
+    bx.serve_stop()
+    flops = sum((8.0 if dt == np.complex128 else 2.0) * M * N * K for (dt, ta, tb, M, N, K) in reqs)
+    return {"requests": n_req, "threads": threads, "dmax": dmax, "offered_rate_per_s": rate or None,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+            "aggregate_tflops": flops / wall / 1e12, "wall_s": wall,
+            "b_cache_hits": st["cache_hits"], "b_cache_misses": st["cache_misses"],
+            "grouped_launches": st["grouped_launches"], "grouped_requests": st["grouped_requests"],
+            "max_inflight": st["max_inflight_seen"], "failed": st["failed"] + len(errors),
+            "mix": "60% f64 / 30% f32 / 10% c128, dims log-uniform [64, dmax], 30% B reuse"}
 
 
 def traffic_for(kernel: str, n: int):
@@ -366,6 +459,10 @@ def main():
                "timing": "host wall clock around the synchronous cblas_dgemm call, median"}
         del Ah, Bh, Ch
 
+    serving = None
+    if args.serving > 0 and rank == 0:
+        serving = serving_load(bx, torch, args.serving, args.serving_dmax, args.serving_threads, args.serving_rate)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         vals, sample, kind, lib = reference_cpu_sample(n, args.cpu_seconds, cores, 1, 0)
@@ -378,7 +475,7 @@ def main():
                 "data": "synthetic", "config": config,
                 "path": path, "moduli": stats["moduli"], "phases_ms_per_step": phase_ms,
                 "fp64_equivalent": fp64_equiv, "native": native, "e2e": e2e, "roofline": roofline,
-                "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary(),
+                "cpu_baseline": cpu, "serving": serving, "gpu_launches": launches, "clocks": clk.summary(),
                 "vs_published_blasx_1gpu_16384": value * 1e3 / PUBLISHED_BLASX_1GPU_16384_GFLOPS}
         print(json.dumps(line), flush=True)
     if dist:
@@ -387,3 +484,9 @@ def main():
 
 if __name__ == "__main__":
     main()
+    # The reference library loaded for the CPU legs prints a line from its ELF
+    # destructor at exit (blas/blasx_tile_resource.c:57-80); leave without
+    # running destructors so that the JSON line stays the last line of stdout.
+    sys.stdout.flush()
+    sys.stderr.flush()
+    os._exit(0)
