@@ -58,6 +58,10 @@ def parse():
     p.add_argument("--serving-threads", type=int, default=16)
     p.add_argument("--serving-rate", type=float, default=0.0,
                    help="offered requests/s over all threads (Poisson); 0 = back to back")
+    p.add_argument("--workload", default="", choices=["", "ragged", "ooc", "c3"],
+                   help="secondary measurements (one JSON line each) instead of the headline: ragged "
+                        "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep")
+    p.add_argument("--samples", type=int, default=2000, help="entries checked against the oracle")
     return p.parse_args()
 
 
@@ -275,6 +279,168 @@ def traffic_for(kernel: str, n: int):
 
 # ---------------------------------------------------------------------------
 
+def _host(torch, shape, dtype, seed, lo=-1.0, hi=1.0, phi=None):
+    """Pinned, column-major host matrix (numpy view of a pinned torch buffer)."""
+    import numpy as np
+    rows, cols = shape
+    g = torch.Generator().manual_seed(seed)
+    if dtype == "c128":
+        t = torch.empty((cols, rows), dtype=torch.complex128, pin_memory=True)
+        t.copy_(torch.complex(torch.rand((cols, rows), generator=g, dtype=torch.float64) * (hi - lo) + lo,
+                              torch.rand((cols, rows), generator=g, dtype=torch.float64) * (hi - lo) + lo))
+    else:
+        tdt = torch.float64 if dtype == "f64" else torch.float32
+        t = torch.empty((cols, rows), dtype=tdt, pin_memory=True)
+        t.copy_(torch.rand((cols, rows), generator=g, dtype=tdt) * (hi - lo) + lo)
+        if phi:
+            t.mul_(torch.exp(phi * torch.randn((cols, rows), generator=g, dtype=tdt)))
+    return t, np.asarray(t.numpy()).T  # (rows x cols) Fortran-ordered view
+
+
+def _accuracy(C, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, dtype, n):
+    """(ratio to the (K+2)u componentwise bound, max normalised error) on n
+    sampled entries against the double-double oracle."""
+    import numpy as np
+
+    import oracle
+    rng = np.random.default_rng(11)
+    ii = rng.integers(0, M, n); jj = rng.integers(0, N, n)
+    val, bound = oracle.dd_entries(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, ii, jj)
+    dt = {"f64": np.float64, "f32": np.float32, "c128": np.complex128}[dtype]
+    return oracle.componentwise_ratio(C, ii, jj, val, bound, K, dt)
+
+
+def run_workloads(args):
+    """Secondary measurements of the configurations beside the headline."""
+    import numpy as np
+    import torch
+
+    import blasx_b200 as bx
+    fn = {"f64": bx.cblas_dgemm, "f32": bx.cblas_sgemm, "c128": bx.cblas_zgemm}
+    lines = []
+    if args.workload == "ragged":
+        # sgemm TN, dgemm NT 30001 x 17777 x 9999; zgemm CC 12001 x 8191 x 6007; U[-1,1]; alpha 1.5, beta -0.25
+        for dtype, ta, tb, M, N, K in [("f32", "T", "N", 30001, 17777, 9999), ("f64", "N", "T", 30001, 17777, 9999),
+                                       ("c128", "C", "C", 12001, 8191, 6007)]:
+            ra, ca = (M, K) if ta == "N" else (K, M)
+            rb, cb = (K, N) if tb == "N" else (N, K)
+            tA, A = _host(torch, (ra, ca), dtype, 1)
+            tB, B = _host(torch, (rb, cb), dtype, 2)
+            tC, C = _host(torch, (M, N), dtype, 3)
+            C0 = C.copy(order="F")
+            alpha, beta = (1.5, -0.25) if dtype != "c128" else (1.5 + 0j, -0.25 + 0j)
+            res = {}
+            for mode_name, mode in (("auto", bx.MODE_AUTO), ("native", bx.MODE_NATIVE)):
+                bx.set_dgemm_mode(mode)
+                times = []
+                for _ in range(2):
+                    C[:] = C0
+                    t0 = time.perf_counter()
+                    fn[dtype](bx.CblasColMajor, bx.TRANS[ta], bx.TRANS[tb], M, N, K, alpha, tA.data_ptr(), ra,
+                              tB.data_ptr(), rb, beta, tC.data_ptr(), M)
+                    times.append(time.perf_counter() - t0)
+                    assert bx.last_status() == 0, bx.last_error()
+                st = bx.call_stats()
+                ratio, err = _accuracy(C, ta, tb, M, N, K, alpha, A, ra, B, rb, beta, C0, M, dtype, args.samples)
+                fl = (8.0 if dtype == "c128" else 2.0) * M * N * K
+                res[mode_name] = {"tflops_e2e": fl / min(times) / 1e12, "seconds": min(times),
+                                  "path": st["path"], "moduli": st["moduli"], "bound_ratio": ratio,
+                                  "max_normalised_error": err}
+            bx.set_dgemm_mode(bx.MODE_AUTO)
+            lines.append({"workload": f"ragged {dtype} {ta}{tb} M={M} N={N} K={K} alpha=1.5 beta=-0.25 U[-1,1]",
+                          "host": "pinned", **res})
+            del tA, tB, tC
+    elif args.workload == "ooc":
+        n = 40960
+        tA, A = _host(torch, (n, n), "f64", 1)
+        tB, B = _host(torch, (n, n), "f64", 2)
+        tC, C = _host(torch, (n, n), "f64", 3)
+        C0 = C[:, :64].copy(order="F")  # columns checked against the oracle
+        bx.set_dgemm_mode(bx.MODE_NATIVE)
+        bx.set_hbm_budget(24 << 30)
+        peak = 35.4  # cuBLAS DGEMM TF/s measured on this pool
+        for tile in (1024, 2048, 3072, 4096):
+            C[:, :64] = C0
+            bx.set_tile(tile)
+            t0 = time.perf_counter()
+            bx.cblas_dgemm(bx.CblasColMajor, bx.CblasNoTrans, bx.CblasNoTrans, n, n, n, 1.0, tA.data_ptr(), n,
+                           tB.data_ptr(), n, 0.5, tC.data_ptr(), n)
+            dt = time.perf_counter() - t0
+            assert bx.last_status() == 0, bx.last_error()
+            st = bx.call_stats()
+            fl = 2.0 * n ** 3
+            h2d_min = 8.0 * 3 * n * n
+            roof = max(fl / (peak * 1e12), h2d_min / 55.6e9)
+            ratio, err = _accuracy(C[:, :64], "N", "N", n, 64, n, 1.0, A, n, B, n, 0.5, C0, n, "f64",
+                                   min(args.samples, 512))
+            lines.append({"workload": f"out-of-core dgemm NN {n}^3, HBM cache 24 GiB, tile {tile}",
+                          "tflops_e2e": fl / dt / 1e12, "seconds": dt, "roofline_seconds": roof,
+                          "frac_of_roofline": roof / dt, "h2d_bytes": st["h2d_bytes"], "h2d_min_bytes": h2d_min,
+                          "h2d_over_min": st["h2d_bytes"] / h2d_min, "tile_hits": st["cache_hits"],
+                          "tile_loads": st["cache_misses"], "evictions": st["evictions"],
+                          "hit_rate": st["cache_hits"] / max(1.0, st["cache_hits"] + st["cache_misses"]),
+                          "bound_ratio": ratio, "max_normalised_error": err})
+        bx.set_tile(0)
+        bx.set_hbm_budget(0)
+        bx.set_dgemm_mode(bx.MODE_AUTO)
+    elif args.workload == "c3":
+        for n in (8192, 16384):
+            for phi in (0.0, 1.0, 4.0):
+                tA, A = _host(torch, (n, n), "f64", 1, -0.5, 0.5, phi)
+                tB, B = _host(torch, (n, n), "f64", 2, -0.5, 0.5, phi)
+                dA, dB = tA.cuda(), tB.cuda()
+                dC = torch.zeros_like(dA)
+                res = {}
+                for mode_name, mode in (("auto", bx.MODE_AUTO), ("native", bx.MODE_NATIVE)):
+                    bx.set_dgemm_mode(mode)
+                    s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
+                    bx.gemm_device("N", "N", n, n, n, 1.0, dA, n, dB, n, 0.0, dC, n, stream=s)
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(s)
+                    for _ in range(2):
+                        bx.gemm_device("N", "N", n, n, n, 1.0, dA, n, dB, n, 0.0, dC, n, stream=s)
+                    e1.record(s); torch.cuda.synchronize()
+                    st = bx.call_stats()
+                    C = dC.cpu().numpy().T
+                    ratio, err = _accuracy(C, "N", "N", n, n, n, 1.0, A, n, B, n, 0.0, None, n, "f64", args.samples)
+                    ms = e0.elapsed_time(e1) / 2
+                    res[mode_name] = {"tflops": 2.0 * n ** 3 / (ms * 1e-3) / 1e12, "ms": ms, "path": st["path"],
+                                      "moduli": st["moduli"], "bound_ratio": ratio, "max_normalised_error": err}
+                bx.set_dgemm_mode(bx.MODE_AUTO)
+                lines.append({"workload": f"dgemm NN {n}^3 U[-0.5,0.5]*exp({phi} g), device-resident",
+                              "samples": args.samples, **res,
+                              "speedup": res["auto"]["tflops"] / res["native"]["tflops"]})
+                del dA, dB, dC, tA, tB
+        n = 8192
+        tA, A = _host(torch, (n, n), "c128", 1)
+        tB, B = _host(torch, (n, n), "c128", 2)
+        dA, dB = tA.cuda(), tB.cuda()
+        dC = torch.zeros_like(dA)
+        res = {}
+        for mode_name, mode in (("auto", bx.MODE_AUTO), ("native", bx.MODE_NATIVE)):
+            bx.set_dgemm_mode(mode)
+            s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
+            bx.gemm_device("N", "N", n, n, n, 1.0, dA, n, dB, n, 0.0, dC, n, stream=s, dtype="z")
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            bx.gemm_device("N", "N", n, n, n, 1.0, dA, n, dB, n, 0.0, dC, n, stream=s, dtype="z")
+            e1.record(s); torch.cuda.synchronize()
+            st = bx.call_stats()
+            C = dC.cpu().numpy().T
+            ratio, err = _accuracy(C, "N", "N", n, n, n, 1.0 + 0j, A, n, B, n, 0.0 + 0j, None, n, "c128",
+                                   min(args.samples, 1000))
+            ms = e0.elapsed_time(e1)
+            res[mode_name] = {"tflops": 8.0 * n ** 3 / (ms * 1e-3) / 1e12, "ms": ms, "path": st["path"],
+                              "moduli": st["moduli"], "bound_ratio": ratio, "max_normalised_error": err}
+        bx.set_dgemm_mode(bx.MODE_AUTO)
+        lines.append({"workload": f"zgemm NN {n}^3 complex128 U[-1,1], device-resident", **res,
+                      "speedup": res["auto"]["tflops"] / res["native"]["tflops"]})
+    for l in lines:
+        print(json.dumps(l), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -304,6 +470,10 @@ def main():
         return
 
     os.environ["BLASX_DEVICE"] = str(local)
+    if args.workload:
+        if rank == 0:
+            run_workloads(args)
+        return
     import numpy as np
     import torch
 

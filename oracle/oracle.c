@@ -225,6 +225,7 @@ void oracle_dgemm_dd_entries(int transa, int transb, int M, int N, int K, double
                              const double *C0, int ldc, int64_t n, const int64_t *ii,
                              const int64_t *jj, double *hi, double *lo, double *bound) {
     (void)M; (void)N;
+#pragma omp parallel for schedule(dynamic, 16)
     for (int64_t t = 0; t < n; ++t) {
         long i = ii[t], j = jj[t];
         dot2 d = {0, 0};
@@ -251,6 +252,7 @@ void oracle_sgemm_dd_entries(int transa, int transb, int M, int N, int K, float 
                              const float *C0, int ldc, int64_t n, const int64_t *ii,
                              const int64_t *jj, double *hi, double *lo, double *bound) {
     (void)M; (void)N;
+#pragma omp parallel for schedule(dynamic, 16)
     for (int64_t t = 0; t < n; ++t) {
         long i = ii[t], j = jj[t];
         dot2 d = {0, 0};
@@ -280,6 +282,7 @@ void oracle_zgemm_dd_entries(int transa, int transb, int M, int N, int K, const 
     (void)M; (void)N;
     int beta_zero = beta[0] == 0 && beta[1] == 0;
     double aabs = hypot(alpha[0], alpha[1]), babs = hypot(beta[0], beta[1]);
+#pragma omp parallel for schedule(dynamic, 16)
     for (int64_t t = 0; t < n; ++t) {
         long i = ii[t], j = jj[t];
         dot2 re = {0, 0}, im = {0, 0};
