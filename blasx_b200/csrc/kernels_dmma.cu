@@ -11,7 +11,7 @@
 //   * operand tiles are staged global -> shared through a 3-stage cp.async
 //     ring. Each operand keeps the contiguity it has in global memory: a
 //     k-contiguous source (A transposed, B not) lands as [m][k] rows padded
-//     by 4 doubles, an m/n-contiguous source as [k][m] rows padded by 8, so
+//     by 4 doubles, an m/n-contiguous source as [k][m] rows padded by 4, so
 //     every copy is a 16-byte cp.async along the contiguous direction and
 //     every fragment load (8 rows x 4 doubles or 4 rows x 8 doubles) falls on
 //     disjoint bank groups;
@@ -31,20 +31,31 @@ namespace bx {
 
 namespace {
 
-constexpr int kThreads = 256;
-
-template <bool CPLX> struct Tile;
-template <> struct Tile<false> {
+// CTA geometry. G selects the FP64 variant: 0 = 8 warps (2 x 4) of 64x32
+// accumulators each, 1 = 16 warps (4 x 4) of 32x32 (more warps per scheduler
+// to hide MMA latency, half the accumulator registers per thread).
+template <bool CPLX, int G = 0> struct Tile;
+template <> struct Tile<false, 0> {
+    static constexpr int THREADS = 256, WARPS_N = 4;
     static constexpr int BM = 128, BN = 128, MT = 4, NT = 4, BK = 32, STAGES = 3;
 };
-template <> struct Tile<true> {
+template <> struct Tile<false, 1> {
+    static constexpr int THREADS = 512, WARPS_N = 4;
+    static constexpr int BM = 128, BN = 128, MT = 2, NT = 4, BK = 32, STAGES = 3;
+};
+template <> struct Tile<true, 0> {
+    static constexpr int THREADS = 256, WARPS_N = 4;
     static constexpr int BM = 64, BN = 128, MT = 2, NT = 4, BK = 16, STAGES = 3;
 };
 
 // Shared-memory geometry of one operand tile (rows x k) for a given source
-// contiguity. KC: [row][k] with stride BK+4; else [k][row] with stride R+8.
+// contiguity. KC: [row][k] with stride BK+4; else [k][row] with stride R+4.
+// A 64-bit shared load is served per half-warp (lanes g < 4 or g >= 4, all
+// t): with a stride of 4 (mod 16 doubles) the 16 lanes of a fragment load,
+// at stride*t + g or stride*g + t, fall on 16 distinct bank pairs.
 template <int R, int BK, bool KC> struct SmemOp {
-    static constexpr int stride = KC ? BK + 4 : R + 8;
+    static constexpr int stride = KC ? BK + 4 : R + 4;
+    static_assert(stride % 16 == 4, "bank-conflict-free fragment loads");
     static constexpr int plane = KC ? R * stride : BK * stride;  // doubles
     __device__ static int idx(int r, int k) { return KC ? r * stride + k : k * stride + r; }
 };
@@ -124,16 +135,16 @@ template <> struct Dmma<16> {
 // Copies the R x BK operand tile at (r0, k0) of a column-major source into
 // shared memory. KC: the source is k-contiguous (element (r, k) at
 // src[k + r*ld]); else r-contiguous (src[r + k*ld]). V doubles per copy.
-template <int R, int BK, bool KC, bool CPLX, int V>
+template <int R, int BK, bool KC, bool CPLX, int V, int THREADS>
 __device__ __forceinline__ void load_tile(uint32_t sbase, const double *src, int64_t ld,
                                           int r0, int k0, int rows, int kdim, int tid) {
     using S = SmemOp<R, BK, KC>;
     constexpr int CHUNKS = R * BK / V;
-    static_assert(CHUNKS % kThreads == 0, "tile / thread mismatch");
+    static_assert(CHUNKS % THREADS == 0, "tile / thread mismatch");
     constexpr int PER_ROW = KC ? BK / V : R / V;  // chunks along the contiguous dim
 #pragma unroll
-    for (int i = 0; i < CHUNKS / kThreads; ++i) {
-        const int e = tid + i * kThreads;
+    for (int i = 0; i < CHUNKS / THREADS; ++i) {
+        const int e = tid + i * THREADS;
         const int c = (e % PER_ROW) * V, o = e / PER_ROW;  // contiguous / other coordinate
         const int r = KC ? o : c, k = KC ? c : o;
         const int gr = r0 + r, gk = k0 + k;
@@ -154,9 +165,10 @@ __device__ __forceinline__ void load_tile(uint32_t sbase, const double *src, int
 }
 
 // One C tile of one problem (`tile` in the grouped raster order below).
-template <bool CPLX, bool AKC, bool BKC, int KI>
+template <bool CPLX, bool AKC, bool BKC, int KI, int G = 0>
 __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, double *smem) {
-    using TL = Tile<CPLX>;
+    using TL = Tile<CPLX, G>;
+    constexpr int T = TL::THREADS;
     constexpr int BM = TL::BM, BN = TL::BN, MT = TL::MT, NT = TL::NT, BK = TL::BK;
     constexpr int STAGES = TL::STAGES;
     using SA = SmemOp<BM, BK, AKC>;
@@ -179,7 +191,7 @@ __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, d
     const int m0 = tm * BM, n0 = tn * BN;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp >> 2, wn = warp & 3;
+    const int wm = warp / TL::WARPS_N, wn = warp % TL::WARPS_N;
     const int g = lane >> 2, t = lane & 3;
 
     auto load_stage = [&](int stage, int kt) {
@@ -187,13 +199,13 @@ __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, d
         const uint32_t a_base = smem_u32(sA + stage * A_STAGE);
         const uint32_t b_base = smem_u32(sB + stage * B_STAGE);
         if (!CPLX && p.vec_a)
-            load_tile<BM, BK, AKC, CPLX, 2>(a_base, p.A, p.lda, m0, k0, p.M, p.K, tid);
+            load_tile<BM, BK, AKC, CPLX, 2, T>(a_base, p.A, p.lda, m0, k0, p.M, p.K, tid);
         else
-            load_tile<BM, BK, AKC, CPLX, 1>(a_base, p.A, p.lda, m0, k0, p.M, p.K, tid);
+            load_tile<BM, BK, AKC, CPLX, 1, T>(a_base, p.A, p.lda, m0, k0, p.M, p.K, tid);
         if (!CPLX && p.vec_b)
-            load_tile<BN, BK, BKC, CPLX, 2>(b_base, p.B, p.ldb, n0, k0, p.N, p.K, tid);
+            load_tile<BN, BK, BKC, CPLX, 2, T>(b_base, p.B, p.ldb, n0, k0, p.N, p.K, tid);
         else
-            load_tile<BN, BK, BKC, CPLX, 1>(b_base, p.B, p.ldb, n0, k0, p.N, p.K, tid);
+            load_tile<BN, BK, BKC, CPLX, 1, T>(b_base, p.B, p.ldb, n0, k0, p.N, p.K, tid);
     };
 
     double acc[PLANES][MT][NT][4];
@@ -311,11 +323,11 @@ __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, d
     }
 }
 
-template <bool CPLX, bool AKC, bool BKC, int KI>
-__global__ void __launch_bounds__(kThreads, 1) dmma_gemm_kernel(const DmmaParams p) {
+template <bool CPLX, bool AKC, bool BKC, int KI, int G>
+__global__ void __launch_bounds__(Tile<CPLX, G>::THREADS, 1) dmma_gemm_kernel(const DmmaParams p) {
     if (p.guard && *p.guard != 0) return;  // the emulated path produced C
     extern __shared__ __align__(16) double smem[];
-    dmma_tile<CPLX, AKC, BKC, KI>(p, blockIdx.x, smem);
+    dmma_tile<CPLX, AKC, BKC, KI, G>(p, blockIdx.x, smem);
 }
 
 // Several problems in one launch: CTA b works on tile b - start[q] of the
@@ -333,7 +345,7 @@ struct GroupTable {
 // problem q with start[q] <= b < start[q + 1]; the operand layouts of each
 // problem are chosen at run time (uniform within a CTA).
 template <bool CPLX, int KI>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(Tile<CPLX>::THREADS, 1)
     dmma_grouped_kernel(const __grid_constant__ GroupTable tab) {
     extern __shared__ __align__(16) double smem[];
     const int b = int(blockIdx.x);
@@ -355,18 +367,18 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-template <bool CPLX, bool AKC, bool BKC, int KI>
+template <bool CPLX, bool AKC, bool BKC, int KI, int G>
 int launch_cfg(const DmmaParams &p, cudaStream_t s) {
-    using TL = Tile<CPLX>;
+    using TL = Tile<CPLX, G>;
     constexpr int PLANES = CPLX ? 2 : 1;
     constexpr size_t smem = size_t(TL::STAGES) * PLANES *
                             (SmemOp<TL::BM, TL::BK, AKC>::plane + SmemOp<TL::BN, TL::BK, BKC>::plane) *
                             sizeof(double);
     static_assert(smem <= 227 * 1024, "shared memory budget");
-    auto kern = dmma_gemm_kernel<CPLX, AKC, BKC, KI>;
+    auto kern = dmma_gemm_kernel<CPLX, AKC, BKC, KI, G>;
     BX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int64_t tiles = int64_t(p.tiles_m) * p.tiles_n;
-    kern<<<unsigned(tiles), kThreads, smem, s>>>(p);
+    kern<<<unsigned(tiles), TL::THREADS, smem, s>>>(p);
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;
@@ -382,15 +394,28 @@ int dmma_k() {
     return k;
 }
 
+// FP64 CTA geometry: 0 by default (BLASX_DMMA_CFG = 0 or 1).
+int dmma_cfg() {
+    static const int c = [] {
+        const char *e = getenv("BLASX_DMMA_CFG");
+        return (e && atoi(e) == 1) ? 1 : 0;
+    }();
+    return c;
+}
+
+template <bool CPLX, bool AKC, bool BKC, int G> int launch_kg(const DmmaParams &p, cudaStream_t s) {
+    switch (dmma_k()) {
+        case 4: return launch_cfg<CPLX, AKC, BKC, 4, G>(p, s);
+        case 8: return launch_cfg<CPLX, AKC, BKC, 8, G>(p, s);
+        default: return launch_cfg<CPLX, AKC, BKC, 16, G>(p, s);
+    }
+}
+
 template <bool CPLX, bool AKC, bool BKC> int launch_k(const DmmaParams &p, cudaStream_t s) {
     if constexpr (CPLX) {
-        return launch_cfg<CPLX, AKC, BKC, 4>(p, s);  // complex: register budget
+        return launch_cfg<CPLX, AKC, BKC, 4, 0>(p, s);  // complex: register budget
     } else {
-        switch (dmma_k()) {
-            case 4: return launch_cfg<CPLX, AKC, BKC, 4>(p, s);
-            case 8: return launch_cfg<CPLX, AKC, BKC, 8>(p, s);
-            default: return launch_cfg<CPLX, AKC, BKC, 16>(p, s);
-        }
+        return dmma_cfg() == 1 ? launch_kg<CPLX, AKC, BKC, 1>(p, s) : launch_kg<CPLX, AKC, BKC, 0>(p, s);
     }
 }
 
@@ -437,7 +462,7 @@ template <bool CPLX, int KI> int launch_grouped_t(const GroupTable &tab, int til
     static_assert(smem <= 227 * 1024, "shared memory budget");
     auto kern = dmma_grouped_kernel<CPLX, KI>;
     BX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kern<<<unsigned(tiles), kThreads, smem, s>>>(tab);
+    kern<<<unsigned(tiles), TL::THREADS, smem, s>>>(tab);
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;

@@ -267,15 +267,21 @@ __device__ __forceinline__ int row_exponent(double amax, double sumsq, int Q, in
     return min(en, em);
 }
 
-__device__ __forceinline__ uint32_t modulus_of(int l) {
-    switch (l) {
-        case 0: return 256; case 1: return 255; case 2: return 253; case 3: return 251;
-        case 4: return 247; case 5: return 241; case 6: return 239; case 7: return 233;
-        case 8: return 229; case 9: return 227; case 10: return 223; case 11: return 217;
-        case 12: return 211; case 13: return 199; case 14: return 197; case 15: return 193;
-        case 16: return 191; case 17: return 181; case 18: return 179; default: return 173;
-    }
-}
+// The moduli as compile-time constants for the device code (same order as
+// kModuli). Every helper below takes the modulus index as a template
+// parameter, so the per-modulus constants fold at compile time whatever the
+// unrolling decisions of the compiler.
+template <int L> struct Mod {
+    static_assert(L >= 0 && L < kMaxModuli, "modulus index");
+    static constexpr uint32_t table[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239,
+                                                   233, 229, 227, 223, 217, 211, 199,
+                                                   197, 193, 191, 181, 179, 173};
+    static constexpr uint32_t m = table[L];
+    static constexpr uint32_t c21 = uint32_t((uint64_t(1) << 21) % m);
+    static constexpr uint32_t c42 = uint32_t((uint64_t(1) << 42) % m);
+    static constexpr uint32_t cb = uint32_t((m - (uint64_t(1) << 62) % m) % m);
+    static constexpr uint32_t magic = uint32_t(((uint64_t(1) << 39) + m - 1) / m);
+};
 
 // v + 2^62 (|v| < 2^62, so the biased value is in [0, 2^63)) split into
 // 21-bit digits, computed once per element and shared by all moduli.
@@ -287,36 +293,35 @@ __device__ __forceinline__ Digits digits_of(int64_t v) {
     return {uint32_t(a) & 0x1FFFFFu, uint32_t(a >> 21) & 0x1FFFFFu, uint32_t(a >> 42)};
 }
 
-// Residue in [0, m) of the biased value minus the bias, for the l-th modulus:
+// Residue in [0, m) of the biased value minus the bias, for the L-th modulus:
 //   t = d2 (2^42 mod m) + d1 (2^21 mod m) + d0 + (-2^62 mod m) < 2^31,
 //   t mod m = floor(t ceil(2^39/m) / 2^39), exact for t < 2^31 and m <= 256
-// (the rounding error of the magic multiplier stays below 1/m). With l a
-// compile-time constant after unrolling, every constant folds: two IMADs,
-// one multiply-high, one shift, one IMAD.
-__device__ __forceinline__ uint32_t residue_u(const Digits &x, int l) {
-    const uint32_t m = modulus_of(l);
-    const uint32_t c21 = uint32_t((uint64_t(1) << 21) % m);
-    const uint32_t c42 = uint32_t((uint64_t(1) << 42) % m);
-    const uint32_t cb = uint32_t((m - (uint64_t(1) << 62) % m) % m);
-    const uint32_t magic = uint32_t(((uint64_t(1) << 39) + m - 1) / m);
-    const uint32_t t = x.d2 * c42 + x.d1 * c21 + (x.d0 + cb);  // < 2^21 * 512 + 256 < 2^31
-    const uint32_t q = __umulhi(t, magic) >> 7;
-    return t - q * m;
+// (the rounding error of the magic multiplier stays below 1/m). Every
+// constant folds: two IMADs, one multiply-high, one shift, one IMAD.
+template <int L> __device__ __forceinline__ uint32_t residue_u(const Digits &x) {
+    using C = Mod<L>;
+    const uint32_t t = x.d2 * C::c42 + x.d1 * C::c21 + (x.d0 + C::cb);  // < 2^21 * 512 + 256 < 2^31
+    const uint32_t q = __umulhi(t, C::magic) >> 7;
+    return t - q * C::m;
 }
 
 // Four residues packed as bytes, mapped to the symmetric int8 range:
 // bytes above (m-1)/2 take m off (mod 256), 4 at a time with SIMD byte ops.
 // For m = 256 the byte already is the two's complement of the symmetric
 // residue.
+template <int L>
 __device__ __forceinline__ uint32_t pack4_sym(const Digits &a, const Digits &b, const Digits &c,
-                                              const Digits &d, int l) {
-    const uint32_t m = modulus_of(l);
-    const uint32_t w = residue_u(a, l) + (residue_u(b, l) << 8) + (residue_u(c, l) << 16) +
-                       (residue_u(d, l) << 24);
-    if (m == 256) return w;
-    const uint32_t half = ((m - 1) / 2) * 0x01010101u;
-    const uint32_t over = __vcmpgtu4(w, half);  // 0xff in every byte above (m-1)/2
-    return __vadd4(w, over & ((256 - m) * 0x01010101u));
+                                              const Digits &d) {
+    constexpr uint32_t m = Mod<L>::m;
+    const uint32_t w = residue_u<L>(a) + (residue_u<L>(b) << 8) + (residue_u<L>(c) << 16) +
+                       (residue_u<L>(d) << 24);
+    if constexpr (m == 256) {
+        return w;
+    } else {
+        constexpr uint32_t half = ((m - 1) / 2) * 0x01010101u;
+        const uint32_t over = __vcmpgtu4(w, half);  // 0xff in every byte above (m-1)/2
+        return __vadd4(w, over & ((256 - m) * 0x01010101u));
+    }
 }
 
 __device__ __forceinline__ int64_t scale_round(double x, int e) {
@@ -336,46 +341,66 @@ struct SliceOut {
     int64_t plane;   // bytes per modulus plane
 };
 
-// Packs the symmetric residues of 16 consecutive elements for modulus l.
-__device__ __forceinline__ uint4 pack16(const Digits (&x)[16], int l) {
+// Packs the symmetric residues of 16 consecutive elements for modulus L.
+template <int L> __device__ __forceinline__ uint4 pack16(const Digits (&x)[16]) {
     uint32_t w[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-        w[q] = pack4_sym(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3], l);
+        w[q] = pack4_sym<L>(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
     return make_uint4(w[0], w[1], w[2], w[3]);
 }
 __device__ __forceinline__ uint4 neg16(uint4 a) {  // residue of -x, byte-wise
     return make_uint4(__vneg4(a.x), __vneg4(a.y), __vneg4(a.z), __vneg4(a.w));
 }
 
-// Writes the residues of 16 consecutive k (k0 multiple of 16) of row r.
-template <int ROLE>
-__device__ __forceinline__ void store16(const SliceOut &o, int l, int64_t r, int64_t k0,
-                                        const Digits (&re)[16], const Digits (&im)[16]) {
-    int8_t *base = o.p + int64_t(l) * o.plane;
-    const uint4 wr = pack16(re, l);
-    *reinterpret_cast<uint4 *>(base + r * o.Kp + k0) = wr;
-    if (ROLE == 1) {
-        *reinterpret_cast<uint4 *>(base + r * o.Kp + o.Kh + k0) = pack16(im, l);
+// Writes the residues, for modulus L, of component COMP (0 re, 1 im) of 16
+// consecutive k (k0 multiple of 16) of row r, to every place the role puts
+// that component.
+template <int ROLE, int COMP, int L>
+__device__ __forceinline__ void store16(const SliceOut &o, int64_t r, int64_t k0,
+                                        const Digits (&x)[16]) {
+    int8_t *base = o.p + int64_t(L) * o.plane;
+    const uint4 w = pack16<L>(x);
+    if (COMP == 0) {
+        *reinterpret_cast<uint4 *>(base + r * o.Kp + k0) = w;
+        if (ROLE == 2) *reinterpret_cast<uint4 *>(base + (o.Rp + r) * o.Kp + o.Kh + k0) = w;
+    } else if (ROLE == 1) {
+        *reinterpret_cast<uint4 *>(base + r * o.Kp + o.Kh + k0) = w;
     } else if (ROLE == 2) {
-        const uint4 wi = pack16(im, l);
-        *reinterpret_cast<uint4 *>(base + r * o.Kp + o.Kh + k0) = neg16(wi);
-        *reinterpret_cast<uint4 *>(base + (o.Rp + r) * o.Kp + k0) = wi;
-        *reinterpret_cast<uint4 *>(base + (o.Rp + r) * o.Kp + o.Kh + k0) = wr;
+        *reinterpret_cast<uint4 *>(base + r * o.Kp + o.Kh + k0) = neg16(w);
+        *reinterpret_cast<uint4 *>(base + (o.Rp + r) * o.Kp + k0) = w;
     }
 }
 
-template <int ROLE>
+// Moduli L, L+1, ..., nmod-1 by compile-time recursion.
+template <int ROLE, int COMP, int L = 0>
 __device__ __forceinline__ void store_all(const SliceOut &o, int nmod, int64_t r, int64_t k0,
-                                          const Digits (&re)[16], const Digits (&im)[16]) {
-#pragma unroll
-    for (int l = 0; l < kMaxModuli; ++l)
-        if (l < nmod) store16<ROLE>(o, l, r, k0, re, im);
+                                          const Digits (&x)[16]) {
+    if constexpr (L < kMaxModuli) {
+        if (L < nmod) {
+            store16<ROLE, COMP, L>(o, r, k0, x);
+            store_all<ROLE, COMP, L + 1>(o, nmod, r, k0, x);
+        }
+    }
 }
 
 // k-contiguous source: a thread scales 16 consecutive k of one row and
-// writes one 16-byte word per modulus (and component).
+// writes one 16-byte word per modulus (and place), one component at a time
+// (the second pass re-reads the same 16-byte elements, from L1).
 // grid (Kc/64, Rp/64), block 256: row = tid / 4, k = 16 (tid % 4).
+template <typename T, int ROLE, int COMP>
+__device__ __forceinline__ void slice_kc_comp(const View &v, int nmod, int e, int64_t r, int64_t k0,
+                                              const SliceOut &o) {
+    Digits d[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        double re = 0, im = 0;
+        if (r < v.R && k0 + q < v.K) load_elem<T>(v, r, k0 + q, true, re, im);
+        d[q] = digits_of(scale_round(COMP ? im : re, e));
+    }
+    store_all<ROLE, COMP>(o, nmod, r, k0, d);
+}
+
 template <typename T, int ROLE>
 __global__ void __launch_bounds__(256) slice_kc_kernel(View v, RowStats st, const Decision *dec,
                                                        int *expo, SliceOut o) {
@@ -387,20 +412,14 @@ __global__ void __launch_bounds__(256) slice_kc_kernel(View v, RowStats st, cons
     int e = 0;
     if (r < v.R) e = row_exponent(st.amax[r], st.sumsq[r], Q, v.K);
     if (blockIdx.x == 0 && (threadIdx.x & 3) == 0 && r < v.R) expo[r] = e;
-    Digits dr[16], di[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        double re = 0, im = 0;
-        if (r < v.R && k0 + q < v.K) load_elem<T>(v, r, k0 + q, true, re, im);
-        dr[q] = digits_of(scale_round(re, e));
-        di[q] = digits_of(scale_round(im, e));
-    }
-    store_all<ROLE>(o, nmod, r, k0, dr, di);
+    slice_kc_comp<T, ROLE, 0>(v, nmod, e, r, k0, o);
+    if (ROLE) slice_kc_comp<T, ROLE, 1>(v, nmod, e, r, k0, o);
 }
 
 // row-contiguous source: a 64-row x KT-k tile is read along rows, scaled,
 // and its integers are transposed once through shared memory; then a thread
-// owns 16 consecutive k of one row, as in the k-contiguous kernel.
+// owns 16 consecutive k of one row and one component, as in the
+// k-contiguous kernel (complex: warps 0-3 the real parts, 4-7 the imaginary).
 // grid (Kc/KT, Rp/64), block 256.
 template <typename T, int ROLE>
 __global__ void __launch_bounds__(256) slice_rc_kernel(View v, RowStats st, const Decision *dec,
@@ -436,17 +455,15 @@ __global__ void __launch_bounds__(256) slice_rc_kernel(View v, RowStats st, cons
         }
     }
     __syncthreads();
-    constexpr int TPR = KT / 16;  // threads per row in the residue phase
-    if (tid < 64 * TPR) {
-        const int wr = tid / TPR, wk = (tid % TPR) * 16;
-        Digits dr[16], di[16];
+    constexpr int TPR = KT / 16;  // threads per row and component
+    static_assert(64 * TPR * CPL == 256, "one 16-k word per thread");
+    const int comp = tid / (64 * TPR), idx = tid % (64 * TPR);
+    const int wr = idx / TPR, wk = (idx % TPR) * 16;
+    Digits d[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            dr[q] = digits_of(tile[0][wk + q][wr]);
-            di[q] = ROLE ? digits_of(tile[CPL - 1][wk + q][wr]) : digits_of(0);
-        }
-        store_all<ROLE>(o, nmod, r0 + wr, k0 + wk, dr, di);
-    }
+    for (int q = 0; q < 16; ++q) d[q] = digits_of(tile[comp][wk + q][wr]);
+    if (comp == 0) store_all<ROLE, 0>(o, nmod, r0 + wr, k0 + wk, d);
+    else if (ROLE) store_all<ROLE, 1>(o, nmod, r0 + wr, k0 + wk, d);
 }
 
 // ---- reconstruction -----------------------------------------------------------
@@ -823,7 +840,7 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
 
     oz::SliceOut oy{Y, Ip, Kp, Kh, Ip * Kp};
     oz::SliceOut ox{X, Jp, Kp, Kh, Jx * Kp};
-    if (CPLX) {
+    if constexpr (CPLX) {
         BX_TRY((launch_slice<T, 1>(va, akc, sa, dec, ea, oy, Kc, s)));
         BX_TRY((launch_slice<T, 2>(vb, bkc, sb, dec, fb, ox, Kc, s)));
     } else {
