@@ -310,6 +310,28 @@ def _accuracy(C, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, dtype, n
     return oracle.componentwise_ratio(C, ii, jj, val, bound, K, dt)
 
 
+def measure_peaks(torch):
+    """cuBLAS DGEMM and cuBLASLt INT8 GEMM rates at 8192^3 on this GPU (TFLOP/s, TOP/s)."""
+    def lib_rate(fn, ops, reps=3):
+        fn(); torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record(); torch.cuda.synchronize()
+        return reps * ops / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+    x = torch.rand((8192, 8192), dtype=torch.float64, device="cuda")
+    fp64_peak = lib_rate(lambda: torch.matmul(x, x), 2.0 * 8192 ** 3)
+    del x
+    xi = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+    yi = xi.t().contiguous().t()
+    int8_peak = lib_rate(lambda: torch._int_mm(xi, yi), 2.0 * 8192 ** 3)
+    del xi, yi
+    torch.cuda.empty_cache()
+    return fp64_peak, int8_peak
+
+
 def run_workloads(args):
     """Secondary measurements of the configurations beside the headline."""
     import numpy as np
@@ -352,15 +374,20 @@ def run_workloads(args):
             del tA, tB, tC
     elif args.workload == "ooc":
         n = 40960
+        fp64_peak, int8_peak = measure_peaks(torch)
         tA, A = _host(torch, (n, n), "f64", 1)
         tB, B = _host(torch, (n, n), "f64", 2)
         tC, C = _host(torch, (n, n), "f64", 3)
         C0 = C[:, :64].copy(order="F")  # columns checked against the oracle
-        bx.set_dgemm_mode(bx.MODE_NATIVE)
         bx.set_hbm_budget(24 << 30)
-        peak = 35.4  # cuBLAS DGEMM TF/s measured on this pool
-        for tile in (1024, 2048, 3072, 4096):
+        fl = 2.0 * n ** 3
+        h2d_min = 8.0 * 3 * n * n
+        link = h2d_min / 55.6e9  # measured pinned H2D rate on this pool
+        sweep = [("native", bx.MODE_NATIVE, t) for t in (1024, 2048, 3072, 4096)]
+        sweep += [("auto", bx.MODE_AUTO, t) for t in (2048, 4096, 8192)]
+        for mode_name, mode, tile in sweep:
             C[:, :64] = C0
+            bx.set_dgemm_mode(mode)
             bx.set_tile(tile)
             t0 = time.perf_counter()
             bx.cblas_dgemm(bx.CblasColMajor, bx.CblasNoTrans, bx.CblasNoTrans, n, n, n, 1.0, tA.data_ptr(), n,
@@ -368,18 +395,27 @@ def run_workloads(args):
             dt = time.perf_counter() - t0
             assert bx.last_status() == 0, bx.last_error()
             st = bx.call_stats()
-            fl = 2.0 * n ** 3
-            h2d_min = 8.0 * 3 * n * n
-            roof = max(fl / (peak * 1e12), h2d_min / 55.6e9)
+            # roofline: the slower of the pipe bound and the host-link bytes; the
+            # pipe is FP64 for native K-steps, INT8 (moduli x 2n^3 ops) for emulated ones
+            emulated = st["path"] == 2
+            pipe = (st["moduli"] * fl / (int8_peak * 1e12)) if emulated else fl / (fp64_peak * 1e12)
+            roof = max(pipe, link)
             ratio, err = _accuracy(C[:, :64], "N", "N", n, 64, n, 1.0, A, n, B, n, 0.5, C0, n, "f64",
                                    min(args.samples, 512))
-            lines.append({"workload": f"out-of-core dgemm NN {n}^3, HBM cache 24 GiB, tile {tile}",
-                          "tflops_e2e": fl / dt / 1e12, "seconds": dt, "roofline_seconds": roof,
-                          "frac_of_roofline": roof / dt, "h2d_bytes": st["h2d_bytes"], "h2d_min_bytes": h2d_min,
+            lines.append({"workload": f"out-of-core dgemm NN {n}^3, HBM cache 24 GiB, tile {tile}, {mode_name}",
+                          "path": {1: "native", 2: "emulated", 4: "native (device fallback)"}.get(st["path"], "?"),
+                          "moduli": st["moduli"], "tflops_e2e": fl / dt / 1e12, "seconds": dt,
+                          "roofline_seconds": roof, "roofline_bound": "link" if link >= pipe else
+                          ("int8" if emulated else "fp64"), "frac_of_roofline": roof / dt,
+                          "fp64_roofline_seconds": max(fl / (fp64_peak * 1e12), link),
+                          "frac_of_fp64_roofline": max(fl / (fp64_peak * 1e12), link) / dt,
+                          "fp64_peak": fp64_peak, "int8_peak": int8_peak,
+                          "h2d_bytes": st["h2d_bytes"], "h2d_min_bytes": h2d_min,
                           "h2d_over_min": st["h2d_bytes"] / h2d_min, "tile_hits": st["cache_hits"],
                           "tile_loads": st["cache_misses"], "evictions": st["evictions"],
                           "hit_rate": st["cache_hits"] / max(1.0, st["cache_hits"] + st["cache_misses"]),
                           "bound_ratio": ratio, "max_normalised_error": err})
+            print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
         bx.set_tile(0)
         bx.set_hbm_budget(0)
         bx.set_dgemm_mode(bx.MODE_AUTO)
@@ -561,22 +597,7 @@ def main():
         bx.set_dgemm_mode(mode)
 
     # --- pipe peaks on this box, measured now with the vendor library ---
-    def lib_rate(fn, ops, reps=3):
-        fn(); torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(reps):
-            fn()
-        e1.record(); torch.cuda.synchronize()
-        return reps * ops / (e0.elapsed_time(e1) * 1e-3) / 1e12
-
-    x = torch.rand((8192, 8192), dtype=torch.float64, device="cuda")
-    fp64_peak = lib_rate(lambda: torch.matmul(x, x), 2.0 * 8192 ** 3)
-    del x
-    xi = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
-    yi = xi.t().contiguous().t()
-    int8_peak = lib_rate(lambda: torch._int_mm(xi, yi), 2.0 * 8192 ** 3)
-    del xi, yi
+    fp64_peak, int8_peak = measure_peaks(torch)
 
     per_gpu = flops / (ms * 1e-3) / 1e12
     path = {1: "native", 2: "ozaki", 3: "scale", 4: "native (device fallback)"}.get(stats["path"], "?")

@@ -260,8 +260,16 @@ int host_gemm(const Gemm &g) {
 
     HostPin pins;
     if (bytes_a + bytes_b + bytes_c + bytes_ws > budget && need_ab) {
-        // out-of-core: HBM tile cache under the byte budget, native kernels
-        const int st_code = tiled_host_gemm(g, c, budget, pick_tile(g), 0);
+        // out-of-core: HBM tile cache under the byte budget; each K-step on
+        // the emulated path when the precision mode picks it for a step's shape
+        const int T = pick_tile(g);
+        Gemm step = g;
+        step.M = std::min<int64_t>(g.M, T);
+        step.N = std::min<int64_t>(g.N, T);
+        step.K = std::min<int64_t>(g.K, T);
+        step.lda = step.ldb = step.ldc = T;
+        const size_t step_ws = want_ozaki(step, mode) ? ozaki_scratch_bytes(step) : 0;
+        const int st_code = tiled_host_gemm(g, c, budget, T, 0, step_ws, mode);
         st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return st_code;
     }

@@ -807,25 +807,27 @@ Plan make_plan(const Gemm &g) {
 // flag are copied to the given host slots when they are not null.
 template <typename T>
 int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, void *dec_host,
-              int *err_host, const PanelHooks *hooks = nullptr) {
+              int *err_host, const PanelHooks *hooks = nullptr, bool clear_err = true) {
     constexpr bool CPLX = oz::Elem<T>::cplx;
     const Plan pl = make_plan(g);
     const int64_t M = pl.M, N = pl.N, K = pl.K, Kh = pl.Kh, Kp = pl.Kp, Kc = pl.Kc;
     const int64_t Ip = pl.Ip, Jp = pl.Jp, Jx = pl.Jx;
     const int64_t L = oz::kMaxModuli;
     Carve cv{static_cast<char *>(ws)};
+    // the error word first: the same offset for every shape, so a sequence of
+    // steps on one scratch accumulates into one word
+    int *err = cv.take<int>(1);
+    oz::Decision *dec = cv.take<oz::Decision>(1);
     oz::RowStats sa{cv.take<double>(M), cv.take<double>(M), cv.take<double>(M), cv.take<int>(M)};
     oz::RowStats sb{cv.take<double>(N), cv.take<double>(N), cv.take<double>(N), cv.take<int>(N)};
     int *ea = cv.take<int>(M), *fb = cv.take<int>(N);
-    oz::Decision *dec = cv.take<oz::Decision>(1);
-    int *err = cv.take<int>(1);
     int8_t *Y = cv.take<int8_t>(size_t(L) * Ip * Kp);
     int8_t *X = cv.take<int8_t>(size_t(L) * Jx * Kp);
     uint8_t *U = cv.take<uint8_t>(size_t(L) * Jx * Ip);
-    const size_t stats_bytes = reinterpret_cast<char *>(ea) - static_cast<char *>(ws);
+    const size_t stats_bytes = reinterpret_cast<char *>(ea) - reinterpret_cast<char *>(sa.amax);
     cudaEvent_t ev0 = prof::mark(s);
-    BX_CUDA(cudaMemsetAsync(ws, 0, stats_bytes, s));
-    BX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    BX_CUDA(cudaMemsetAsync(sa.amax, 0, stats_bytes, s));
+    if (clear_err) BX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
 
     // op(A) rows i over k; op(B) columns j over k
     oz::View va{g.A, g.lda, M, K, g.ta == ConjT};
@@ -949,6 +951,20 @@ int ozaki_gemm_panels(const Gemm &g, cudaStream_t s, int mode, void *ws, int num
         default:
             return ozaki_run<oz::zpair>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag,
                                         &hooks);
+    }
+}
+
+int ozaki_gemm_step(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, bool first,
+                    bool last) {
+    Context *ctx = context();
+    if (!ctx) return last_status();
+    BX_TRY(oz::upload_crt_tables());
+    void *dec_host = last ? ctx->last_decision : nullptr;
+    int *err_host = last ? ctx->last_error_flag : nullptr;
+    switch (g.dt) {
+        case DType::F64: return ozaki_run<double>(g, s, mode, ws, num_sms, dec_host, err_host, nullptr, first);
+        case DType::F32: return ozaki_run<float>(g, s, mode, ws, num_sms, dec_host, err_host, nullptr, first);
+        default: return ozaki_run<oz::zpair>(g, s, mode, ws, num_sms, dec_host, err_host, nullptr, first);
     }
 }
 

@@ -90,6 +90,14 @@ int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode);
 size_t ozaki_scratch_bytes(const Gemm &g);
 int ozaki_gemm_in(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms);
 
+// One K-step of a sequence of emulated GEMMs that share the scratch `ws` in
+// stream order (the out-of-core tile steps). The device error flag in the
+// scratch is cleared by the first step only, so a bounded-wait failure of
+// any step survives to the last one, which copies the flag and the modulus
+// decision to the context's host words.
+int ozaki_gemm_step(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, bool first,
+                    bool last);
+
 // Column panels of C for the host pipeline: the residue GEMMs and the
 // reconstruction run panel by panel (real types; complex runs one panel).
 // before_reconstruct(ctx, j0, j1) is called before panel [j0, j1) reads C

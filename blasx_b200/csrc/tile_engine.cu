@@ -1,5 +1,6 @@
 // tile_engine.cu -- executes a TilePlan for a host GEMM larger than the HBM
-// budget (out-of-core), on the native kernels.
+// budget (out-of-core), on the native kernels or, K-step by K-step, on the
+// emulated (Ozaki) path.
 //
 // Replaces the reference's worker loop (blas/blasx_dgemm.c:98-248: batches
 // of 4 tasks, a host busy-wait on an event, cudaStreamSynchronize after the
@@ -10,6 +11,9 @@
 //   compute stream  waits for the tile's ready event, runs the K-step GEMM
 //                   (beta on the first K-step, 1 afterwards as in
 //                   blas/blasx_dgemm.c:82), records the slot's last use;
+//                   an emulated K-step slices both tiles, runs the residue
+//                   GEMMs and adds alpha X into the C tile in FP64, with its
+//                   own modulus decision (native fallback on the device);
 //   D2H stream      writes a finished C tile back to the host.
 // The host thread never blocks until the final synchronisation, so copies
 // run ahead of compute as far as slot reuse allows. Host operands that are
@@ -21,6 +25,7 @@
 #include <vector>
 
 #include "kernels.h"
+#include "ozaki.h"
 #include "tile_engine.h"
 #include "tile_plan.h"
 
@@ -83,11 +88,13 @@ size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es) {
     return (size_t(ld) * size_t(cols - 1) + size_t(rows)) * es;
 }
 
-int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy) {
+int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy, size_t ws_bytes,
+                    int mode) {
     blasx_call_stats &st = call_stats();
     const size_t es = elem_size(g.dt);
     const size_t slot_bytes = size_t(T) * T * es;
-    const int64_t total_slots = int64_t(budget / slot_bytes);
+    const size_t ws_reserve = ws_bytes ? ((ws_bytes + 255) & ~size_t(255)) + 256 : 0;
+    const int64_t total_slots = int64_t((budget > ws_reserve ? budget - ws_reserve : 0) / slot_bytes);
     const int op_slots = int(total_slots - kCSlots);
     if (op_slots < 2)
         return set_error(BLASX_ERR_NOMEM, "HBM budget %zu B holds fewer than %d tiles of %d^2",
@@ -97,11 +104,17 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy)
         return set_error(BLASX_ERR_ARG, "tile plan failed");
     {
         std::lock_guard<std::mutex> lk(g_arena_mu);
-        BX_TRY(ensure_arena(size_t(op_slots + kCSlots) * slot_bytes));
+        BX_TRY(ensure_arena(size_t(op_slots + kCSlots) * slot_bytes + ws_reserve));
     }
     char *arena = static_cast<char *>(g_arena);
     auto op_ptr = [&](int s) { return arena + size_t(s) * slot_bytes; };
     auto c_ptr = [&](int s) { return arena + size_t(op_slots + s) * slot_bytes; };
+    // emulated K-steps: scratch after the C slots, 256-byte aligned
+    void *ws = nullptr;
+    if (ws_bytes) {
+        const size_t off = (size_t(op_slots + kCSlots) * slot_bytes + 255) & ~size_t(255);
+        ws = arena + off;
+    }
 
     HostPin pins;
     BX_TRY(pins.pin(g.A, host_extent(g.lda, g.rows_a(), g.cols_a(), es)));
@@ -153,7 +166,9 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy)
     };
 
     int ctile = -1;
+    size_t step_no = 0;
     for (const TileStep &s : plan.steps) {
+        ++step_no;
         if (s.a.load) BX_TRY(load_tile(s.a, s));
         if (s.b.load) BX_TRY(load_tile(s.b, s));
         const int64_t m = ext(s.i, g.M), n = ext(s.j, g.N), k = ext(s.k, g.K);
@@ -184,7 +199,11 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy)
         d.C = c_ptr(cs); d.ldc = T;
         if (!s.first_k) d.beta = cplx{1.0, 0.0};
         d.guard = nullptr;
-        BX_TRY(dmma_supported(d) ? launch_gemm_dmma(d, c->compute) : launch_gemm_simt(d, c->compute));
+        if (ws)
+            BX_TRY(ozaki_gemm_step(d, c->compute, mode, ws, c->num_sms, step_no == 1,
+                                   step_no == plan.steps.size()));
+        else
+            BX_TRY(dmma_supported(d) ? launch_gemm_dmma(d, c->compute) : launch_gemm_simt(d, c->compute));
         BX_CUDA(cudaEventRecord(lastuse[size_t(s.a.slot)], c->compute));
         BX_CUDA(cudaEventRecord(lastuse[size_t(s.b.slot)], c->compute));
         used[size_t(s.a.slot)] = used[size_t(s.b.slot)] = true;
@@ -205,7 +224,13 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy)
     st.cache_misses = double(plan.loads);
     st.evictions = double(plan.evictions);
     st.tile = T;
-    st.path = 1;
+    st.path = ws ? 2 : 1;
+    if (ws) {
+        resolve_decision(st);  // the last K-step's modulus count
+        if (*c->last_error_flag)
+            return set_error(BLASX_ERR_TIMEOUT, "emulated tile step: bounded device wait expired (flag %d)",
+                             *c->last_error_flag);
+    }
     return BLASX_OK;
 }
 

@@ -20,8 +20,12 @@ struct HostPin {
 size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es);
 
 // Host GEMM through tile x tile operand tiles cached in an HBM arena of
-// `budget` bytes (policy: 0 Belady, 1 LRU). Synchronous.
-int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int tile, int policy);
+// `budget` bytes (policy: 0 Belady, 1 LRU). Synchronous. With ws_bytes > 0
+// every K-step runs on the emulated (Ozaki) path in precision mode `mode`,
+// on a scratch of ws_bytes carved from the same budget; otherwise on the
+// native kernels.
+int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int tile, int policy,
+                    size_t ws_bytes = 0, int mode = 0);
 
 // Frees the arena (blasx_finalize).
 void release_tile_arena();
