@@ -58,9 +58,10 @@ def parse():
     p.add_argument("--serving-threads", type=int, default=16)
     p.add_argument("--serving-rate", type=float, default=0.0,
                    help="offered requests/s over all threads (Poisson); 0 = back to back")
-    p.add_argument("--workload", default="", choices=["", "ragged", "ooc", "c3"],
+    p.add_argument("--workload", default="", choices=["", "ragged", "ooc", "c3", "serving"],
                    help="secondary measurements (one JSON line each) instead of the headline: ragged "
-                        "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep")
+                        "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep, "
+                        "the full serving stream (10,000 calls, dims to 16384)")
     p.add_argument("--samples", type=int, default=2000, help="entries checked against the oracle")
     return p.parse_args()
 
@@ -176,7 +177,8 @@ def reference_cpu_sample(n: int, seconds: float, cores: int, steps: int = 1, war
     return out, sample, kind, (ref.name if hasattr(ref, "name") else oracle.REF_PATH)
 
 
-def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, seed: int = 7):
+def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, seed: int = 7,
+                 budget: int = 0, inflight: int = 8):
     """Serving stream through the drop-in cblas_?gemm calls with the serving
     loop running: `threads` host threads, dtype mix 60% FP64 / 30% FP32 /
     10% complex128, M, N, K each log-uniform in [64, dmax], random transposes,
@@ -184,7 +186,8 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
     inputs uniform in [-1, 1]; Poisson arrivals at `rate` requests/s (0: each
     thread submits its next call as soon as the previous one returns).
     Host operands are sub-matrices of pinned pools (A and B shared, read-only;
-    one C buffer per thread)."""
+    one C buffer per thread). budget: HBM admission budget in bytes (0: the
+    library default); inflight: requests on the GPU at once."""
     import random
     import threading
 
@@ -231,9 +234,13 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
 
     def worker(t):
         r = random.Random(seed + t)
+        t_next = time.perf_counter()
         for (dt, ta, tb, M, N, K) in per_thread[t]:
-            if rate > 0:
-                time.sleep(r.expovariate(rate / threads))
+            if rate > 0:  # arrival times fixed in advance; a thread still busy submits late
+                t_next += r.expovariate(rate / threads)
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
             a, b, es = pools[dt]
             lda = M if ta == "N" else K
             ldb = K if tb == "N" else N
@@ -244,7 +251,7 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
             if bx.last_status() != 0:
                 errors.append(bx.last_error())
 
-    bx.serve_start(0, 0, 8)
+    bx.serve_start(budget, 0, inflight)
     bx.serve_reset_stats()
     th = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
     t0 = time.perf_counter()
@@ -255,6 +262,7 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
     bx.serve_stop()
     flops = sum((8.0 if dt == np.complex128 else 2.0) * M * N * K for (dt, ta, tb, M, N, K) in reqs)
     return {"requests": n_req, "threads": threads, "dmax": dmax, "offered_rate_per_s": rate or None,
+            "achieved_rate_per_s": n_req / wall, "hbm_budget_bytes": budget or None, "max_inflight_cfg": inflight,
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
             "aggregate_tflops": flops / wall / 1e12, "wall_s": wall,
             "b_cache_hits": st["cache_hits"], "b_cache_misses": st["cache_misses"],
@@ -418,6 +426,17 @@ def run_workloads(args):
             print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
         bx.set_tile(0)
         bx.set_hbm_budget(0)
+        bx.set_dgemm_mode(bx.MODE_AUTO)
+    elif args.workload == "serving":
+        # the serving stream at full size: 10,000 calls from 16 threads, Poisson
+        # arrivals, dims log-uniform in [64, 16384], 120 GB admission budget;
+        # once with FP64 on the emulated path (auto) and once native
+        rate = args.serving_rate or 200.0
+        for mode_name, mode in (("auto", bx.MODE_AUTO), ("native", bx.MODE_NATIVE)):
+            bx.set_dgemm_mode(mode)
+            res = serving_load(bx, torch, 10000, 16384, 16, rate, seed=11, budget=120 * 10 ** 9, inflight=16)
+            lines.append({"workload": f"serving stream, FP64/complex on the {mode_name} path", **res})
+            print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
         bx.set_dgemm_mode(bx.MODE_AUTO)
     elif args.workload == "c3":
         for n in (8192, 16384):

@@ -11,6 +11,9 @@
 //             compute. The emulated path slices A and B once (its statistics
 //             need the whole operands), then runs the residue GEMMs and the
 //             reconstruction panel by panel with the same write-back overlap.
+//             With K >= 4096 it works in two K-blocks: block 1 is sliced and
+//             multiplied while block 2's A and B are still on the host link,
+//             C0 comes last and is added panel by panel (beta C0).
 //   tiled     otherwise: the HBM tile cache with an explicit byte budget
 //             (tile_engine.cu), native kernels.
 //
@@ -46,10 +49,11 @@ struct Events {
 // Device copies of the operands, laid out column-major with ld padded to 32.
 struct DeviceOps {
     void *A = nullptr, *B = nullptr, *C = nullptr, *ws = nullptr;
+    void *C0 = nullptr;  // input C, when the emulated path accumulates K-blocks into C
     int64_t lda = 0, ldb = 0, ldc = 0;
     cudaStream_t s = nullptr;
     ~DeviceOps() {
-        for (void *p : {A, B, C, ws})
+        for (void *p : {A, B, C, ws, C0})
             if (p) cudaFreeAsync(p, s);
     }
 };
@@ -106,8 +110,9 @@ int copy_panel_out(const Gemm &g, const DeviceOps &d, int64_t j0, int64_t j1, cu
 }
 
 int panel_count(const Gemm &g) {
-    // panels of >= 1024 columns, at most 8
-    return int(std::max<int64_t>(1, std::min<int64_t>(8, g.N / 1024)));
+    // panels of >= 1024 columns, at most 16: the last panel's copies are
+    // the pipeline's exposed tail
+    return int(std::max<int64_t>(1, std::min<int64_t>(16, g.N / 1024)));
 }
 
 // ---- in-core, native kernels ----------------------------------------------
@@ -184,8 +189,120 @@ int oz_before_reconstruct(void *vctx, int64_t j0, int64_t j1) {
     return BLASX_OK;
 }
 
+// K-blocks of the emulated in-core path: op(A)(:, k0:k1) and op(B)(k0:k1, :)
+// are copied block by block, so that block b computes while block b + 1 is
+// on the host link. Two blocks once K >= 4096 (each block's slicing and
+// residue GEMMs are independent; the blocks' results are summed in FP64).
+int kblock_count(const Gemm &g) { return g.K >= 4096 ? 2 : 1; }
+
+int64_t kblock_edge(const Gemm &g, int b, int blocks) {
+    return b == blocks ? g.K : (g.K * b / blocks) / 128 * 128;
+}
+
+// The block's view of a GEMM whose A and B start at a, b with leading
+// dimensions lda, ldb (host or device copies alike).
+Gemm kblock_of(const Gemm &g, const void *a, int64_t lda, const void *b, int64_t ldb, int64_t k0,
+               int64_t k1) {
+    const size_t es = elem_size(g.dt);
+    Gemm k = g;
+    k.K = k1 - k0;
+    k.A = static_cast<const char *>(a) + (g.ta == NoTrans ? k0 * lda : k0) * int64_t(es);
+    k.lda = lda;
+    k.B = static_cast<const char *>(b) + (g.tb == NoTrans ? k0 : k0 * ldb) * int64_t(es);
+    k.ldb = ldb;
+    return k;
+}
+
+int copy_kblock_in(const Gemm &g, const DeviceOps &d, int64_t k0, int64_t k1, cudaStream_t s,
+                   blasx_call_stats &st) {
+    const size_t es = elem_size(g.dt);
+    const Gemm h = kblock_of(g, g.A, g.lda, g.B, g.ldb, k0, k1);
+    const Gemm v = kblock_of(g, d.A, d.lda, d.B, d.ldb, k0, k1);
+    BX_CUDA(cudaMemcpy2DAsync(const_cast<void *>(v.A), d.lda * es, h.A, g.lda * es, h.rows_a() * es,
+                              h.cols_a(), cudaMemcpyHostToDevice, s));
+    BX_CUDA(cudaMemcpy2DAsync(const_cast<void *>(v.B), d.ldb * es, h.B, g.ldb * es, h.rows_b() * es,
+                              h.cols_b(), cudaMemcpyHostToDevice, s));
+    st.h2d_bytes += double(es) * (h.rows_a() * h.cols_a() + h.rows_b() * h.cols_b());
+    return BLASX_OK;
+}
+
+// Last K-block, per C panel: C0 panel in (beta != 0), C += beta C0, write-back.
+int oz_after_panel_kblocks(void *vctx, int64_t j0, int64_t j1) {
+    auto *x = static_cast<OzPanelCtx *>(vctx);
+    const Gemm &g = *x->g;
+    const DeviceOps &d = *x->d;
+    const size_t es = elem_size(g.dt);
+    if (!g.beta_zero()) {
+        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.C0) + j0 * d.ldc * es, d.ldc * es,
+                                  static_cast<const char *>(g.C) + j0 * g.ldc * es, g.ldc * es,
+                                  g.M * es, j1 - j0, cudaMemcpyHostToDevice, x->c->h2d));
+        x->st->h2d_bytes += double(j1 - j0) * g.M * es;
+        cudaEvent_t in = x->ev->make();
+        BX_CUDA(cudaEventRecord(in, x->c->h2d));
+        BX_CUDA(cudaStreamWaitEvent(x->c->compute, in, 0));
+        Gemm p = g;
+        p.N = j1 - j0;
+        p.C = static_cast<char *>(d.C) + j0 * d.ldc * es;
+        p.ldc = d.ldc;
+        BX_TRY(launch_add_scaled(p, static_cast<const char *>(d.C0) + j0 * d.ldc * es, d.ldc,
+                                 x->c->compute));
+    }
+    return oz_after_panel(vctx, j0, j1);
+}
+
+int finish_ozaki(Context *c, blasx_call_stats &st) {
+    BX_CUDA(cudaStreamSynchronize(c->h2d));
+    BX_CUDA(cudaStreamSynchronize(c->compute));
+    BX_CUDA(cudaStreamSynchronize(c->d2h));
+    st.path = 2;
+    resolve_decision(st);
+    if (*c->last_error_flag)
+        return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
+                         *c->last_error_flag);
+    return BLASX_OK;
+}
+
+// Emulated path in K-blocks: every block's A and B columns / rows go first on
+// the H2D stream, C0 (beta != 0) after all of them. Block b computes
+// C = alpha op(A_b) op(B_b) + (b ? C : 0) as soon as its operands landed,
+// each with its own modulus decision (or native fallback); the last block
+// runs in C panels, and each panel gets beta C0 added and is written back
+// while later panels compute.
+int incore_ozaki_kblocks(const Gemm &g, Context *c, DeviceOps &d, int mode, blasx_call_stats &st) {
+    Events ev;
+    const int blocks = kblock_count(g);
+    cudaEvent_t start = ev.make();
+    BX_CUDA(cudaEventRecord(start, c->compute));
+    BX_CUDA(cudaStreamWaitEvent(c->h2d, start, 0));
+    BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
+    std::vector<cudaEvent_t> in(static_cast<size_t>(blocks));
+    for (int b = 0; b < blocks; ++b) {
+        BX_TRY(copy_kblock_in(g, d, kblock_edge(g, b, blocks), kblock_edge(g, b + 1, blocks), c->h2d, st));
+        in[size_t(b)] = ev.make();
+        BX_CUDA(cudaEventRecord(in[size_t(b)], c->h2d));
+    }
+    Gemm dg = g;
+    dg.C = d.C;
+    dg.ldc = d.ldc;
+    OzPanelCtx pctx{&g, &d, c, &ev, &st};
+    for (int b = 0; b < blocks; ++b) {
+        BX_CUDA(cudaStreamWaitEvent(c->compute, in[size_t(b)], 0));
+        Gemm kb = kblock_of(dg, d.A, d.lda, d.B, d.ldb, kblock_edge(g, b, blocks),
+                            kblock_edge(g, b + 1, blocks));
+        kb.beta = b == 0 ? cplx{0.0, 0.0} : cplx{1.0, 0.0};
+        if (b + 1 < blocks) {
+            BX_TRY(ozaki_gemm_step(kb, c->compute, mode, d.ws, c->num_sms, b == 0, false));
+        } else {
+            PanelHooks hooks{panel_count(g), nullptr, &oz_after_panel_kblocks, &pctx};
+            BX_TRY(ozaki_gemm_panels(kb, c->compute, mode, d.ws, c->num_sms, hooks, false));
+        }
+    }
+    return finish_ozaki(c, st);
+}
+
 int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
                  blasx_call_stats &st) {
+    if (kblock_count(g) > 1) return incore_ozaki_kblocks(g, c, d, mode, st);
     Events ev;
     const size_t es = elem_size(g.dt);
     cudaEvent_t start = ev.make();
@@ -210,24 +327,10 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
     PanelHooks hooks{panel_count(g), read_c ? &oz_before_reconstruct : nullptr, &oz_after_panel,
                      &pctx};
     BX_TRY(ozaki_gemm_panels(dg, c->compute, mode, d.ws, c->num_sms, hooks));
-    BX_CUDA(cudaStreamSynchronize(c->h2d));
-    BX_CUDA(cudaStreamSynchronize(c->compute));
-    BX_CUDA(cudaStreamSynchronize(c->d2h));
-    st.path = 2;
-    resolve_decision(st);
-    if (*c->last_error_flag)
-        return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
-                         *c->last_error_flag);
-    return BLASX_OK;
+    return finish_ozaki(c, st);
 }
 
-bool want_ozaki(const Gemm &g, int mode) {
-    const int64_t kmax = g.dt == DType::C128 ? oz::kMaxK / 2 : oz::kMaxK;
-    if (g.K > kmax) return false;
-    const double work = double(g.M) * double(g.N) * double(g.K);
-    const bool worth = work >= double(1 << 27) && g.M >= 64 && g.N >= 64 && g.K >= 32;
-    return mode == 2 || (mode == 0 && worth);
-}
+bool want_ozaki(const Gemm &g, int mode) { return ozaki_selected(g, mode); }
 
 }  // namespace
 
@@ -256,10 +359,11 @@ int host_gemm(const Gemm &g) {
     Gemm probe = g;
     probe.lda = d.lda; probe.ldb = d.ldb; probe.ldc = d.ldc;
     const size_t bytes_ws = oz ? ozaki_scratch_bytes(probe) : 0;
+    const size_t bytes_c0 = (oz && read_c && kblock_count(g) > 1) ? bytes_c : 0;
     const size_t budget = default_budget(c);
 
     HostPin pins;
-    if (bytes_a + bytes_b + bytes_c + bytes_ws > budget && need_ab) {
+    if (bytes_a + bytes_b + bytes_c + bytes_c0 + bytes_ws > budget && need_ab) {
         // out-of-core: HBM tile cache under the byte budget; each K-step on
         // the emulated path when the precision mode picks it for a step's shape
         const int T = pick_tile(g);
@@ -282,6 +386,7 @@ int host_gemm(const Gemm &g) {
     }
     BX_CUDA(cudaMallocAsync(&d.C, bytes_c, c->compute));
     if (oz) BX_CUDA(cudaMallocAsync(&d.ws, bytes_ws, c->compute));
+    if (bytes_c0) BX_CUDA(cudaMallocAsync(&d.C0, bytes_c0, c->compute));
     const int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
                       : incore_native(g, c, d, need_ab, read_c, st);
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -8,6 +8,8 @@ namespace bx {
 
 // C = beta * C (alpha == 0 or K == 0); C is not read when beta == 0.
 int launch_scale(const Gemm &g, cudaStream_t s);
+// g.C (g.M x g.N, ld g.ldc) += g.beta * X (ld ldx); nothing when beta == 0.
+int launch_add_scaled(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s);
 
 // Portable SIMT tiled kernel (all dtypes, transposes, ragged edges). Used for
 // small problems and as the first correct path.

@@ -31,17 +31,18 @@ namespace bx {
 
 namespace {
 
-// CTA geometry. G selects the FP64 variant: 0 = 8 warps (2 x 4) of 64x32
-// accumulators each, 1 = 16 warps (4 x 4) of 32x32 (more warps per scheduler
-// to hide MMA latency, half the accumulator registers per thread).
+// CTA geometry. G selects the FP64 variant: 0 = a 128x128 C tile, 8 warps
+// (2 x 4) of 64x32 accumulators each; 1 = a 64x64 C tile, 4 warps (2 x 2) of
+// 32x32, two CTAs per SM, for problems with too few 128x128 tiles to occupy
+// every SM (one CTA computes its whole K extent, at one SM's FP64 rate).
 template <bool CPLX, int G = 0> struct Tile;
 template <> struct Tile<false, 0> {
     static constexpr int THREADS = 256, WARPS_N = 4;
     static constexpr int BM = 128, BN = 128, MT = 4, NT = 4, BK = 32, STAGES = 3;
 };
 template <> struct Tile<false, 1> {
-    static constexpr int THREADS = 512, WARPS_N = 4;
-    static constexpr int BM = 128, BN = 128, MT = 2, NT = 4, BK = 32, STAGES = 3;
+    static constexpr int THREADS = 128, WARPS_N = 2;
+    static constexpr int BM = 64, BN = 64, MT = 2, NT = 4, BK = 32, STAGES = 3;
 };
 template <> struct Tile<true, 0> {
     static constexpr int THREADS = 256, WARPS_N = 4;
@@ -394,13 +395,34 @@ int dmma_k() {
     return k;
 }
 
-// FP64 CTA geometry: 0 by default (BLASX_DMMA_CFG = 0 or 1).
-int dmma_cfg() {
-    static const int c = [] {
-        const char *e = getenv("BLASX_DMMA_CFG");
-        return (e && atoi(e) == 1) ? 1 : 0;
+// FP64 CTA geometry, by the estimated fraction of the SMs' FP64 pipes kept
+// busy: a grid of t CTAs, r resident per SM, runs in ceil(t / (r S)) waves,
+// so the busy fraction is t / (ceil(t / (r S)) r S). The 128x128 tile runs
+// one CTA per SM; the 64x64 tile two, at an assumed 85% of the larger
+// tile's per-SM rate (more shared-memory traffic per flop). BLASX_DMMA_TILE
+// = 64 or 128 forces one.
+int dmma_geometry(int64_t M, int64_t N) {
+    static const int forced = [] {
+        const char *e = getenv("BLASX_DMMA_TILE");
+        const int v = e ? atoi(e) : 0;
+        return v == 64 ? 1 : (v == 128 ? 0 : -1);
     }();
-    return c;
+    if (forced >= 0) return forced;
+    static const int sms = [] {
+        int dev = 0, n = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            n = 148;
+        return n;
+    }();
+    auto busy = [&](int64_t tiles, int per_sm) {
+        const int64_t slots = int64_t(sms) * per_sm;
+        const int64_t waves = (tiles + slots - 1) / slots;
+        return double(tiles) / double(waves * slots);
+    };
+    const double big = busy(((M + 127) / 128) * ((N + 127) / 128), 1);
+    const double small = 0.85 * busy(((M + 63) / 64) * ((N + 63) / 64), 2);
+    return small > big ? 1 : 0;
 }
 
 template <bool CPLX, bool AKC, bool BKC, int G> int launch_kg(const DmmaParams &p, cudaStream_t s) {
@@ -411,16 +433,16 @@ template <bool CPLX, bool AKC, bool BKC, int G> int launch_kg(const DmmaParams &
     }
 }
 
-template <bool CPLX, bool AKC, bool BKC> int launch_k(const DmmaParams &p, cudaStream_t s) {
+template <bool CPLX, bool AKC, bool BKC, int G> int launch_k(const DmmaParams &p, cudaStream_t s) {
     if constexpr (CPLX) {
         return launch_cfg<CPLX, AKC, BKC, 4, 0>(p, s);  // complex: register budget
     } else {
-        return dmma_cfg() == 1 ? launch_kg<CPLX, AKC, BKC, 1>(p, s) : launch_kg<CPLX, AKC, BKC, 0>(p, s);
+        return launch_kg<CPLX, AKC, BKC, G>(p, s);
     }
 }
 
-template <bool CPLX> DmmaParams make_params(const Gemm &g) {
-    using TL = Tile<CPLX>;
+template <bool CPLX, int G = 0> DmmaParams make_params(const Gemm &g) {
+    using TL = Tile<CPLX, G>;
     DmmaParams p;
     p.M = int(g.M); p.N = int(g.N); p.K = int(g.K);
     p.ta = g.ta; p.tb = g.tb;
@@ -438,14 +460,19 @@ template <bool CPLX> DmmaParams make_params(const Gemm &g) {
     return p;
 }
 
-template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
-    const DmmaParams p = make_params<CPLX>(g);
+template <bool CPLX, int G> int launch_g(const Gemm &g, cudaStream_t s) {
+    const DmmaParams p = make_params<CPLX, G>(g);
     if (int64_t(p.tiles_m) * p.tiles_n > INT32_MAX)
         return set_error(BLASX_ERR_UNSUPPORTED, "DMMA grid too large");
     const bool akc = g.ta != NoTrans;  // op(A) = A^T: stored K x M, k contiguous
     const bool bkc = g.tb == NoTrans;  // op(B) = B: stored K x N, k contiguous
-    if (akc) return bkc ? launch_k<CPLX, true, true>(p, s) : launch_k<CPLX, true, false>(p, s);
-    return bkc ? launch_k<CPLX, false, true>(p, s) : launch_k<CPLX, false, false>(p, s);
+    if (akc) return bkc ? launch_k<CPLX, true, true, G>(p, s) : launch_k<CPLX, true, false, G>(p, s);
+    return bkc ? launch_k<CPLX, false, true, G>(p, s) : launch_k<CPLX, false, false, G>(p, s);
+}
+
+template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
+    if constexpr (CPLX) return launch_g<CPLX, 0>(g, s);
+    else return dmma_geometry(g.M, g.N) == 1 ? launch_g<CPLX, 1>(g, s) : launch_g<CPLX, 0>(g, s);
 }
 
 template <bool CPLX, int KI> int launch_grouped_t(const GroupTable &tab, int tiles, cudaStream_t s) {

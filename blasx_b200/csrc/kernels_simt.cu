@@ -1,9 +1,12 @@
-// kernels_simt.cu -- portable SIMT GEMM kernel and the beta-scale kernel.
+// kernels_simt.cu -- portable SIMT GEMM kernel, the beta-scale kernel and the
+// scaled-add kernel of the host pipeline.
 //
 // The SIMT kernel is the correctness baseline of the device path: any dtype,
 // any transpose, ragged edges, BLAS alpha/beta semantics (C not read when
 // beta == 0). Fast paths live in kernels_dmma.cu (FP64 pipe) and the Ozaki
 // INT8 tensor-core path.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace bx {
@@ -142,6 +145,28 @@ __global__ void scale_kernel(int M, int N, T beta, T *__restrict__ C, int64_t ld
     }
 }
 
+// C(i, j) += beta X(i, j): blockIdx.y strides over columns, threads over rows.
+template <typename T>
+__global__ void add_scaled_kernel(int M, int N, T beta, const T *__restrict__ X, int64_t ldx,
+                                  T *__restrict__ C, int64_t ldc) {
+    using Ar = Arith<T>;
+    for (int64_t j = blockIdx.y; j < N; j += gridDim.y)
+        for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < M;
+             i += int64_t(gridDim.x) * blockDim.x) {
+            T *cp = &C[i + j * ldc];
+            *cp = Ar::add(*cp, Ar::mul(beta, X[i + j * ldx]));
+        }
+}
+
+template <typename T> int launch_add_scaled_t(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s) {
+    dim3 grid(unsigned(std::min<int64_t>(8, (g.M + 255) / 256)), unsigned(std::min<int64_t>(g.N, 65535)));
+    add_scaled_kernel<T><<<grid, 256, 0, s>>>(int(g.M), int(g.N), from_cplx<T>(g.beta),
+                                              static_cast<const T *>(X), ldx, static_cast<T *>(g.C), g.ldc);
+    BX_CUDA(cudaGetLastError());
+    count_launch();
+    return BLASX_OK;
+}
+
 template <typename T> int launch_simt_t(const Gemm &g, cudaStream_t s) {
     dim3 grid(unsigned((g.M + BM - 1) / BM), unsigned((g.N + BN - 1) / BN));
     if (grid.y > 65535) return set_error(BLASX_ERR_UNSUPPORTED, "N too large for SIMT grid");
@@ -173,6 +198,15 @@ int launch_gemm_simt(const Gemm &g, cudaStream_t s) {
         case DType::F32: return launch_simt_t<float>(g, s);
         case DType::F64: return launch_simt_t<double>(g, s);
         default: return launch_simt_t<z2>(g, s);
+    }
+}
+
+int launch_add_scaled(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s) {
+    if (g.M == 0 || g.N == 0 || g.beta_zero()) return BLASX_OK;
+    switch (g.dt) {
+        case DType::F32: return launch_add_scaled_t<float>(g, X, ldx, s);
+        case DType::F64: return launch_add_scaled_t<double>(g, X, ldx, s);
+        default: return launch_add_scaled_t<z2>(g, X, ldx, s);
     }
 }
 

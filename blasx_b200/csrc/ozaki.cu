@@ -849,7 +849,10 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         BX_TRY((launch_slice<T, 0>(va, akc, sa, dec, ea, oy, Kc, s)));
         BX_TRY((launch_slice<T, 0>(vb, bkc, sb, dec, fb, ox, Kc, s)));
     }
-    // residue GEMMs and reconstruction, in column panels of C when asked
+    // residue GEMMs and reconstruction, in column panels of C when asked.
+    // (Running a panel's reconstruction on a second stream beside the next
+    // panel's residue GEMM was measured slower: under the power cap the
+    // concurrent integer work lowers the clock of the tensor work.)
     const int64_t tiles_j = Jp / oz::kTileJ;
     const int panels = (CPLX || !hooks) ? 1 : int(std::max<int64_t>(1, std::min<int64_t>(hooks->panels, tiles_j)));
     cudaEvent_t ev1 = prof::mark(s), ev2 = nullptr;
@@ -857,17 +860,20 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         const int64_t tj0 = tiles_j * pnl / panels, tj1 = tiles_j * (pnl + 1) / panels;
         const int64_t j0 = tj0 * oz::kTileJ, j1 = std::min<int64_t>(N, tj1 * oz::kTileJ);
         if (panels == 1) {
-            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s));
+            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s, 0, -1, g.max_cta_tiles));
         } else {
-            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s, tj0, tj1 - tj0));
+            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s, tj0, tj1 - tj0,
+                                           g.max_cta_tiles));
         }
         if (pnl == 0) ev2 = prof::mark(s);
         if (hooks && hooks->before_reconstruct && j1 > j0)
             BX_TRY(hooks->before_reconstruct(hooks->ctx, j0, j1));
-        if (j1 > j0) {
-            dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(j1 - j0));
+        // grid.y is limited to 65535 columns per launch
+        for (int64_t c0 = j0; c0 < j1; c0 += 65535) {
+            const int64_t c1 = std::min<int64_t>(j1, c0 + 65535);
+            dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(c1 - c0));
             oz::ReconArgs ra{U, Jp, Ip, M, N, ea, fb, g.alpha.re, g.alpha.im, g.beta.re, g.beta.im,
-                             g.beta_zero() ? 1 : 0, g.C, g.ldc, j0};
+                             g.beta_zero() ? 1 : 0, g.C, g.ldc, c0};
             oz::reconstruct_kernel<T, CPLX><<<rgrid, 128, 0, s>>>(ra, dec);
             BX_CUDA(cudaGetLastError());
             count_launch();
@@ -886,7 +892,6 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         }
         if (hooks && hooks->after_panel) BX_TRY(hooks->after_panel(hooks->ctx, j0, j1));
     }
-
     cudaEvent_t ev3 = prof::mark(s);
 
     // native fallback, decided on the device (runs only when nmod == 0);
@@ -939,18 +944,20 @@ int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode) {
 size_t ozaki_scratch_bytes(const Gemm &g) { return make_plan(g).bytes; }
 
 int ozaki_gemm_panels(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms,
-                      const PanelHooks &hooks) {
+                      const PanelHooks &hooks, bool clear_err) {
     Context *ctx = context();
     if (!ctx) return last_status();
     BX_TRY(oz::upload_crt_tables());
     switch (g.dt) {
         case DType::F64:
-            return ozaki_run<double>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks);
+            return ozaki_run<double>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks,
+                                     clear_err);
         case DType::F32:
-            return ozaki_run<float>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks);
+            return ozaki_run<float>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks,
+                                    clear_err);
         default:
             return ozaki_run<oz::zpair>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag,
-                                        &hooks);
+                                        &hooks, clear_err);
     }
 }
 

@@ -62,10 +62,13 @@ struct RowStats {
 // X: [kMaxModuli][Jp][Kp] int8, Y: [kMaxModuli][Ip][Kp] int8 (K-major).
 // Kp multiple of 128, Jp of 128, Ip of 256. Returns a blasx status.
 // tj_begin / tj_count: the range of 128-row X tiles (columns of C) to
-// compute; tj_count < 0 covers all of them.
+// compute; tj_count < 0 covers all of them. max_cta_tiles > 0 bounds the
+// tiles one CTA computes (more CTAs than SMs, each retiring after a few
+// milliseconds); 0 launches one persistent CTA per SM.
 int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
                         int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
-                        cudaStream_t s, int64_t tj_begin = 0, int64_t tj_count = -1);
+                        cudaStream_t s, int64_t tj_begin = 0, int64_t tj_count = -1,
+                        int max_cta_tiles = 0);
 
 // Host-side CRT constant tables (uploaded once to constant memory).
 int upload_crt_tables();
@@ -79,6 +82,15 @@ int prepare_residue_gemm_current_device();
 extern const int kModuli[kMaxModuli];
 
 }  // namespace oz
+
+// Whether precision mode `mode` runs g on the emulated path. Mode 2 (ozaki)
+// always does when K is within the exact range; mode 1 (native) never; mode
+// 0 (auto) where the emulated path measured faster than the native kernels
+// on one B200 (device-resident n^3 sweep, 256 <= n <= 4096): FP64 from
+// about 1800^3, FP32 from about 640^3, complex128 from about 1200^3. Small K
+// also loses: reconstruction costs about as much per C entry as ~350 native
+// FP64 multiply-adds, whatever K is.
+bool ozaki_selected(const Gemm &g, int mode);
 
 // Emulated GEMM on device-resident operands. Chooses the modulus count on
 // the device; falls back to the native kernel on the device when needed.
@@ -110,7 +122,9 @@ struct PanelHooks {
     int (*after_panel)(void *ctx, int64_t j0, int64_t j1);
     void *ctx;
 };
+// clear_err = false keeps the device error word of earlier calls on the
+// same scratch (a sequence of K-blocks accumulating into one C).
 int ozaki_gemm_panels(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms,
-                      const PanelHooks &hooks);
+                      const PanelHooks &hooks, bool clear_err = true);
 
 }  // namespace bx

@@ -23,6 +23,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -379,7 +380,7 @@ int prepare_residue_gemm_current_device() {
 
 int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
                         int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
-                        cudaStream_t s, int64_t tj_begin, int64_t tj_count) {
+                        cudaStream_t s, int64_t tj_begin, int64_t tj_count, int max_cta_tiles) {
     if (Jp % kTileJ || Ip % kTileI || Kp % kTileK || Kp > int64_t(kMaxK) * 2)
         return set_error(BLASX_ERR_UNSUPPORTED, "residue GEMM: bad padded extents");
     static std::once_flag once;
@@ -403,8 +404,10 @@ int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp
     TcArgs a{Jp, Ip, Kp, U, dec, err_flag, int(tj_begin), int(tj_count)};
     const int64_t tiles_upper = int64_t(kMaxModuli) * tj_count * (Ip / kTileI);
     if (tiles_upper == 0) return BLASX_OK;
-    const int grid = int(tiles_upper < num_sms ? tiles_upper : num_sms);
-    residue_gemm_kernel<<<grid, kThreadsTC, kSmemBytes, s>>>(mx, my, a);
+    int64_t grid = tiles_upper < num_sms ? tiles_upper : num_sms;
+    if (max_cta_tiles > 0) grid = std::max<int64_t>(grid, (tiles_upper + max_cta_tiles - 1) / max_cta_tiles);
+    grid = std::min<int64_t>(grid, INT32_MAX);
+    residue_gemm_kernel<<<unsigned(grid), kThreadsTC, kSmemBytes, s>>>(mx, my, a);
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;

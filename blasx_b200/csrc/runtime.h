@@ -42,6 +42,10 @@ struct Gemm {
     // Device pointer; when set, the native kernels return at once unless
     // *guard == 0 (the emulated path chose its native fallback on the device).
     const int *guard = nullptr;
+    // Emulated path: at most this many residue-GEMM tiles per CTA (0: one
+    // persistent CTA per SM). A bound makes its CTAs retire every few
+    // milliseconds, so that kernels of other streams get SMs in between.
+    int max_cta_tiles = 0;
 
     bool alpha_zero() const { return alpha.re == 0 && alpha.im == 0; }
     bool beta_zero() const { return beta.re == 0 && beta.im == 0; }

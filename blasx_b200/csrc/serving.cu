@@ -4,17 +4,22 @@
 // from any number of host threads become requests in one queue, served by a
 // single scheduler thread that owns the device:
 //
-//   admission   FIFO; a request is admitted when an in-flight slot is free and
-//               its device bytes (A, B, C copies and the emulated path's
-//               scratch) fit the HBM budget; a B operand found in the operand
-//               cache is not copied again and not charged again;
+//   admission   in arrival order; a request is admitted when an in-flight slot
+//               is free and its device bytes (A, B, C copies and the emulated
+//               path's scratch) fit the HBM budget; a B operand found in the
+//               operand cache is not copied again and not charged again.
+//               Requests behind one that waits for memory may pass it if they
+//               fit, until it has waited 50 ms (then its memory is kept free);
 //   in flight   every admitted request gets its own stream: its copies in,
 //               compute and copy out overlap with other requests' on the
 //               device, and requests that arrive meanwhile are admitted as
 //               slots and memory free up;
 //   mixing      small native FP64 / complex128 requests wait for their
 //               operands and are then run together by ONE grouped kernel
-//               launch whose grid holds the tiles of all of them;
+//               launch whose grid holds the tiles of all of them, on the
+//               highest-priority stream; an emulated request's residue GEMM
+//               runs CTAs of bounded life (not one persistent CTA per SM),
+//               so that small requests' CTAs are scheduled in between;
 //   completion  detected by polling each request's last event; device memory
 //               is released, the B copy is kept in the operand cache (LRU,
 //               byte budget, pinned while in use) and the caller wakes up.
@@ -61,6 +66,14 @@ double now_s() {
 }
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Admission: how many pending requests one pass examines, and how long (s)
+// the oldest one may be passed by later requests that fit in memory.
+constexpr int kLookahead = 64;
+constexpr double kHeadWait = 0.05;
+// Residue-GEMM tiles per CTA on the emulated path: ~2 ms of one SM at
+// K = 16384, after which the SM can take a CTA of another request.
+constexpr int kResidueTilesPerCta = 32;
 
 // ---- host-buffer pinning shared by all requests --------------------------------
 std::mutex g_pin_mu;
@@ -209,11 +222,7 @@ size_t device_bytes(const Request &r, bool need_b) {
     if (need_ab) {
         b += size_t(round_up(g.rows_a(), 32)) * g.cols_a() * es;
         if (need_b) b += size_t(round_up(g.rows_b(), 32)) * g.cols_b() * es;
-        const int mode = config().dgemm_mode.load();
-        const int64_t kmax = g.dt == DType::C128 ? oz::kMaxK / 2 : oz::kMaxK;
-        const double work = double(g.M) * double(g.N) * double(g.K);
-        const bool worth = work >= double(1 << 27) && g.M >= 64 && g.N >= 64 && g.K >= 32;
-        if (g.K <= kmax && (mode == 2 || (mode == 0 && worth))) {
+        if (ozaki_selected(g, config().dgemm_mode.load())) {
             Gemm probe = g;
             b += ozaki_scratch_bytes(probe);
         }
@@ -287,6 +296,7 @@ int admit(Server &s, Request *r, int slot) {
     d.A = r->dA; d.lda = r->lda;
     d.B = r->dB; d.ldb = r->ldb;
     d.C = r->dC; d.ldc = r->ldc;
+    d.max_cta_tiles = kResidueTilesPerCta;  // emulated path: let other requests' kernels in
     BX_TRY(device_gemm(d, st));
     r->stats.path = call_stats().path;
     r->stats.moduli = 0;
@@ -432,10 +442,19 @@ void loop(Server *sp) {
         }
         // grouped launches of small native requests whose operands landed
         launch_groups(s);
-        // admission (FIFO)
-        while (!s.pending.empty() && int(s.inflight.size()) < s.max_inflight) {
-            std::shared_ptr<Request> rp = s.pending.front();
+        // admission: arrival order, except that while the oldest pending
+        // request waits for memory, up to kLookahead requests behind it that
+        // fit may pass it -- until it has waited kHeadWait; from then on
+        // nothing passes it, so the memory that finishing requests free
+        // goes to it
+        size_t idx = 0;
+        int scanned = 0;
+        const double now = now_s();
+        while (idx < s.pending.size() && int(s.inflight.size()) < s.max_inflight &&
+               scanned < kLookahead) {
+            std::shared_ptr<Request> rp = s.pending[idx];
             Request *r = rp.get();
+            ++scanned;
             // operand cache lookup for B
             Entry *hit = nullptr;
             {
@@ -456,7 +475,9 @@ void loop(Server *sp) {
                     std::lock_guard<std::mutex> lk(s.cache_mu);
                     hit->users--;
                 }
-                break;  // wait for memory to free up
+                if (idx == 0 && now - r->t_submit > kHeadWait) break;  // memory is kept for it
+                ++idx;  // does not fit yet: look further back
+                continue;
             }
             int slot = -1;
             for (size_t k = 0; k < s.stream_busy.size(); ++k)
@@ -468,7 +489,7 @@ void loop(Server *sp) {
                 }
                 break;
             }
-            s.pending.erase(s.pending.begin());
+            s.pending.erase(s.pending.begin() + long(idx));
             s.stream_busy[size_t(slot)] = true;
             r->bcache = hit;
             r->charged = need;
@@ -512,10 +533,7 @@ int submit(const Gemm &g) {
     r->flops = 0;
     r->grouped = false;
     if (g.dt != DType::F32 && need_ab) {
-        const int mode = config().dgemm_mode.load();
-        const double work = double(g.M) * double(g.N) * double(g.K);
-        const bool emulated = mode == 2 || (mode == 0 && work >= double(1 << 27) && g.M >= 64 &&
-                                            g.N >= 64 && g.K >= 32);
+        const bool emulated = ozaki_selected(g, config().dgemm_mode.load());
         r->grouped = !emulated && g.flops() <= s->group_flops;
     }
     if (need_ab) {
@@ -566,8 +584,12 @@ int blasx_serve_start(size_t hbm_budget, size_t cache_bytes, int max_inflight) {
     s->max_inflight = max_inflight > 0 ? std::min(max_inflight, 64) : 8;
     s->streams.resize(size_t(s->max_inflight));
     s->stream_busy.assign(size_t(s->max_inflight), false);
-    for (auto &st : s->streams) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&s->batch_stream, cudaStreamNonBlocking);
+    // the grouped launches of small requests get the highest stream priority:
+    // when CTAs of a large request's kernel retire, theirs are scheduled first
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    for (auto &st : s->streams) cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_low);
+    cudaStreamCreateWithPriority(&s->batch_stream, cudaStreamNonBlocking, prio_high);
     s->thread = std::thread(loop, s);
     g_server = s;
     g_active.store(true, std::memory_order_release);

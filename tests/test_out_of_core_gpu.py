@@ -104,13 +104,14 @@ def test_out_of_core_zgemm_emulated_steps(small_cache_emulated):
 
 
 def test_out_of_core_auto_falls_back_per_step(blx):
-    """Auto mode on a wide exponent spread: each K-step's device decision
-    picks the native kernel; the result is still the FP64 one."""
-    blx.set_hbm_budget(64 << 20)
-    blx.set_tile(512)
+    """Auto mode on a wide exponent spread: the K-steps (2048^3, large enough
+    for auto mode to pick the emulated path) each decide on the device to
+    run the native kernel; the result is still the FP64 one."""
+    blx.set_hbm_budget(600 << 20)
+    blx.set_tile(2048)
     prev = blx.set_dgemm_mode(blx.MODE_AUTO)
     try:
-        M, N, K = 1800, 1700, 1536  # every K-step 512 deep
+        M, N, K = 6144, 6000, 6144  # every K-step 2048 deep
         A = oracle.spread((M, K), 21, 6.0)
         B = oracle.spread((K, N), 22, 6.0)
         C0 = oracle.uniform((M, N), np.float64, 23)

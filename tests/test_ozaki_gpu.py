@@ -101,7 +101,7 @@ def test_spread_inputs_at_least_native_accuracy(ozaki, blx, phi):
 def test_auto_mode_falls_back_to_native_for_wide_spread(blx):
     prev = blx.set_dgemm_mode(blx.MODE_AUTO)
     try:
-        M = N = K = 1024
+        M = N = K = 2048  # large enough for auto mode to pick the emulated path
         A = oracle.spread((M, K), 51, 4.0); B = oracle.spread((K, N), 52, 4.0)
         C = np.zeros((M, N), order="F")
         st = run(blx, np.float64, "N", "N", M, N, K, 1.0, A, M, B, K, 0.0, C, M)
@@ -174,3 +174,76 @@ def test_device_entry_emulated_matches_host(ozaki, blx):
     torch.cuda.synchronize()
     # same inputs, same deterministic pipeline: bitwise equal
     np.testing.assert_array_equal(dC.cpu().numpy().T, Ch)
+
+
+def test_device_entry_emulated_wide_c(ozaki, blx):
+    """N above 65535: the reconstruction is launched in column chunks."""
+    torch = pytest.importorskip("torch")
+    M, N, K = 64, 70001, 96
+    A = oracle.uniform((M, K), np.float64, 94); B = oracle.uniform((K, N), np.float64, 95)
+    C0 = oracle.uniform((M, N), np.float64, 96)
+    dA = torch.from_numpy(A.T.copy()).cuda(); dB = torch.from_numpy(B.T.copy()).cuda()
+    dC = torch.from_numpy(C0.T.copy()).cuda()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    assert blx.gemm_device("N", "N", M, N, K, 0.75, dA, M, dB, K, 0.5, dC, M, stream=s, dtype="d") == 0
+    torch.cuda.synchronize()
+    st = blx.call_stats()
+    assert st["path"] == 2 and st["moduli"] > 0
+    C = dC.cpu().numpy().T
+    rng = np.random.default_rng(4)
+    ii = rng.integers(0, M, 3000); jj = np.concatenate([rng.integers(65535, N, 1500), rng.integers(0, N, 1500)])
+    val, bound = oracle.dd_entries("N", "N", M, N, K, 0.75, A, M, B, K, 0.5, C0, M, ii, jj)
+    ratio, _ = oracle.componentwise_ratio(C, ii, jj, val, bound, K, np.float64)
+    assert ratio <= 1.0
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+def test_host_emulated_k_blocks(ozaki, blx, ta, tb):
+    """K >= 4096: the host pipeline copies and computes K in two blocks
+    (summed in FP64); beta C0 is added per C panel at the end."""
+    M, N, K = 700, 2100, 5000
+    A, lda, B, ldb, C0 = make(np.float64, ta, tb, M, N, K, 61)
+    C = C0.copy(order="F")
+    st = run(blx, np.float64, ta, tb, M, N, K, 1.5, A, lda, B, ldb, -0.25, C, M)
+    assert st["path"] == 2 and st["moduli"] >= 12, st
+    assert st["h2d_bytes"] == 8.0 * (M * K + K * N + M * N)
+    ratio, err = sampled_error(C, ta, tb, M, N, K, 1.5, A, lda, B, ldb, -0.25, C0, M, np.float64)
+    assert ratio <= 1.0
+    blx.set_dgemm_mode(blx.MODE_NATIVE)
+    Cn = C0.copy(order="F")
+    run(blx, np.float64, ta, tb, M, N, K, 1.5, A, lda, B, ldb, -0.25, Cn, M)
+    blx.set_dgemm_mode(blx.MODE_OZAKI)
+    _, err_n = sampled_error(Cn, ta, tb, M, N, K, 1.5, A, lda, B, ldb, -0.25, C0, M, np.float64)
+    assert err <= max(err_n, 2.0 ** -53), (err, err_n)
+
+
+def test_host_emulated_k_blocks_zgemm_beta_zero(ozaki, blx):
+    M, N, K = 600, 500, 4500
+    A = oracle.uniform((K, M), np.complex128, 64)
+    B = oracle.uniform((N, K), np.complex128, 65)
+    C = np.full((M, N), np.nan, dtype=np.complex128, order="F")  # beta = 0: C never read
+    st = run(blx, np.complex128, "C", "C", M, N, K, 1 - 0.5j, A, K, B, N, 0, C, M)
+    assert st["path"] == 2 and st["h2d_bytes"] == 16.0 * (M * K + K * N)
+    want = (1 - 0.5j) * (A.conj().T @ B.conj().T)
+    np.testing.assert_allclose(C, want, rtol=1e-12, atol=1e-11)
+
+
+def test_host_k_blocks_second_block_falls_back(blx):
+    """The K-blocks decide separately: uniform first half (emulated), a wide
+    exponent spread in the second half (native on the device)."""
+    prev = blx.set_dgemm_mode(blx.MODE_AUTO)
+    try:
+        M, N, K = 2048, 2048, 8192
+        A = oracle.uniform((M, K), np.float64, 71)
+        B = oracle.uniform((K, N), np.float64, 72)
+        A[:, K // 2:] = oracle.spread((M, K // 2), 73, 6.0)
+        B[K // 2:, :] = oracle.spread((K // 2, N), 74, 6.0)
+        C0 = oracle.uniform((M, N), np.float64, 75)
+        C = C0.copy(order="F")
+        st = run(blx, np.float64, "N", "N", M, N, K, 1.0, A, M, B, K, 0.5, C, M)
+        assert st["path"] == 4 and st["moduli"] == 0, st  # the last block's decision
+        ratio, _ = sampled_error(C, "N", "N", M, N, K, 1.0, A, M, B, K, 0.5, C0, M, np.float64)
+        assert ratio <= 1.0
+    finally:
+        blx.set_dgemm_mode(prev)
