@@ -58,10 +58,13 @@ def parse():
     p.add_argument("--serving-threads", type=int, default=16)
     p.add_argument("--serving-rate", type=float, default=0.0,
                    help="offered requests/s over all threads (Poisson); 0 = back to back")
-    p.add_argument("--workload", default="", choices=["", "ragged", "ooc", "c3", "serving"],
+    p.add_argument("--dtype", default="d", choices=["d", "s", "z"],
+                   help="--workload device: FP64, FP32 or complex128")
+    p.add_argument("--workload", default="", choices=["", "ragged", "ooc", "c3", "serving", "device"],
                    help="secondary measurements (one JSON line each) instead of the headline: ragged "
                         "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep, "
-                        "the full serving stream (10,000 calls, dims to 16384)")
+                        "the full serving stream (10,000 calls, dims to 16384), or a device-resident "
+                        "loop (--size, --dtype, --mode, --warmup, --steps) for profiling one kernel")
     p.add_argument("--samples", type=int, default=2000, help="entries checked against the oracle")
     return p.parse_args()
 
@@ -426,6 +429,38 @@ def run_workloads(args):
             print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
         bx.set_tile(0)
         bx.set_hbm_budget(0)
+        bx.set_dgemm_mode(bx.MODE_AUTO)
+    elif args.workload == "device":
+        # device-resident n^3 NN calls through blasx_?gemm_device (for ncu captures of one kernel)
+        n = args.size
+        dt = {"d": torch.float64, "s": torch.float32, "z": torch.complex128}[args.dtype]
+        g = torch.Generator(device="cuda").manual_seed(5)
+        A = (torch.rand(n, n, dtype=dt, device="cuda", generator=g) - 0.5)
+        B = (torch.rand(n, n, dtype=dt, device="cuda", generator=g) - 0.5)
+        C = torch.zeros(n, n, dtype=dt, device="cuda")
+        bx.set_dgemm_mode({"auto": bx.MODE_AUTO, "native": bx.MODE_NATIVE, "ozaki": bx.MODE_OZAKI}[args.mode])
+        s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
+        call = lambda: bx.gemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, stream=s, dtype=args.dtype)
+        for _ in range(args.warmup):
+            assert call() == 0, bx.last_error()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            assert call() == 0, bx.last_error()
+        e1.record(s); torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(1, args.steps)
+        st = bx.call_stats()
+        # per-phase device time, one more call with the library's phase events on
+        bx.profile_enable(True)
+        assert call() == 0, bx.last_error()
+        torch.cuda.synchronize()
+        phases = {k: v["ms"] for k, v in bx.profile_read().items() if v["count"]}
+        bx.profile_enable(False)
+        fl = (8.0 if args.dtype == "z" else 2.0) * n ** 3
+        lines.append({"workload": f"device-resident {args.dtype}gemm NN {n}^3, mode {args.mode}",
+                      "tflops": fl / (ms * 1e-3) / 1e12, "ms": ms, "path": st["path"], "moduli": st["moduli"],
+                      "phases_ms": phases})
         bx.set_dgemm_mode(bx.MODE_AUTO)
     elif args.workload == "serving":
         # the serving stream at full size: 10,000 calls from 16 threads, Poisson

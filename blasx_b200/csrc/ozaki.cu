@@ -481,9 +481,14 @@ __device__ __forceinline__ double scale_pow2(double x, int e) {
 }
 
 // CRT value of the residues u[0..N) times 2^scale as a double, correctly
-// rounded from the exact symmetric integer X in (-M/2, M/2] (the scaling by
-// a power of two is exact unless the result leaves the normal range):
-//   S = sum_l u_l w_l (multi-limb), X = S mod M, X -= M if 2X >= M.
+// rounded from the exact integer X (the scaling by a power of two is exact
+// unless the result leaves the normal range):
+//   S = sum_l u_l w_l (multi-limb) is congruent to X mod M, and the row and
+//   column scaling guarantees |X| < 2^(2Q) <= M/4. So X = S - q M with
+//   q = rint(S / M): S / M lies within 1/4 of an integer, and its double
+//   estimate (S < N 2^8 M, a few roundings of 2^-53) is off by far less, so
+//   the rounding is never ambiguous. X comes out in two's complement; its
+//   magnitude is converted with one rounding.
 template <int N>
 __device__ __forceinline__ double crt_to_double(const uint32_t (&u)[N], int scale) {
     constexpr int L = limbs_for(N);
@@ -503,70 +508,32 @@ __device__ __forceinline__ double crt_to_double(const uint32_t (&u)[N], int scal
         s[t] = uint32_t(v);
         carry = v >> 32;
     }
-    // q = floor(S / M) estimated in double (S / M < N 2^8, so the estimate is
-    // off by at most one), then corrected exactly
     double sd = 0;
 #pragma unroll
     for (int t = L - 1; t >= 0; --t) sd = sd * 4294967296.0 + double(s[t]);
-    const uint32_t q = uint32_t(fmax(0.0, floor(sd * c_crt.invMd[ni])));
+    const uint32_t q = uint32_t(rint(sd * c_crt.invMd[ni]));
+    // x = s - q M, L-limb two's complement
     uint32_t x[L];
-    int64_t borrow = 0;
-    uint64_t qc = 0;
-#pragma unroll
-    for (int t = 0; t < L; ++t) {
-        const uint64_t qm = uint64_t(q) * c_crt.M[ni][t] + qc;
-        qc = qm >> 32;
-        const int64_t d = int64_t(s[t]) - int64_t(uint32_t(qm)) - borrow;
-        x[t] = uint32_t(d);
-        borrow = d < 0 ? 1 : 0;
-    }
-    if (borrow + int64_t(qc) > 0) {  // X < 0: add M
-        uint64_t c = 0;
-#pragma unroll
-        for (int t = 0; t < L; ++t) {
-            const uint64_t v = uint64_t(x[t]) + c_crt.M[ni][t] + c;
-            x[t] = uint32_t(v);
-            c = v >> 32;
-        }
-    }
-    auto cmp_ge_M = [&](const uint32_t (&y)[L]) {
-        bool ge = true, decided = false;
-#pragma unroll
-        for (int t = L - 1; t >= 0; --t) {
-            if (!decided && y[t] != c_crt.M[ni][t]) {
-                ge = y[t] > c_crt.M[ni][t];
-                decided = true;
-            }
-        }
-        return ge;
-    };
-    if (cmp_ge_M(x)) {  // X >= M: subtract M
-        int64_t b = 0;
-#pragma unroll
-        for (int t = 0; t < L; ++t) {
-            const int64_t d = int64_t(x[t]) - int64_t(c_crt.M[ni][t]) - b;
-            x[t] = uint32_t(d);
-            b = d < 0 ? 1 : 0;
-        }
-    }
-    // symmetric representative: 2X >= M -> magnitude M - X, negative
-    uint32_t x2[L];
     {
-        uint32_t c = 0;
+        uint64_t qc = 0;
+        int64_t borrow = 0;
 #pragma unroll
         for (int t = 0; t < L; ++t) {
-            x2[t] = (x[t] << 1) | c;
-            c = x[t] >> 31;
+            const uint64_t qm = uint64_t(q) * c_crt.M[ni][t] + qc;
+            qc = qm >> 32;
+            const int64_t d = int64_t(s[t]) - int64_t(uint32_t(qm)) - borrow;
+            x[t] = uint32_t(d);
+            borrow = d < 0 ? 1 : 0;
         }
     }
-    const bool neg = cmp_ge_M(x2);
-    if (neg) {
-        int64_t b = 0;
+    const bool neg = int32_t(x[L - 1]) < 0;
+    if (neg) {  // magnitude: ~x + 1
+        uint32_t c = 1;
 #pragma unroll
         for (int t = 0; t < L; ++t) {
-            const int64_t d = int64_t(c_crt.M[ni][t]) - int64_t(x[t]) - b;
-            x[t] = uint32_t(d);
-            b = d < 0 ? 1 : 0;
+            const uint64_t v = uint64_t(~x[t]) + c;
+            x[t] = uint32_t(v);
+            c = uint32_t(v >> 32);
         }
     }
     // magnitude -> double, correctly rounded: a 64-bit window whose bit 63 is
