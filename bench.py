@@ -60,12 +60,15 @@ def parse():
                    help="offered requests/s over all threads (Poisson); 0 = back to back")
     p.add_argument("--dtype", default="d", choices=["d", "s", "z"],
                    help="--workload device: FP64, FP32 or complex128")
-    p.add_argument("--workload", default="", choices=["", "ragged", "ooc", "c3", "serving", "device"],
+    p.add_argument("--rates", default="100,200,400",
+                   help="--workload serving: offered Poisson rates (requests/s) to sweep")
+    p.add_argument("--workload", default="", choices=["", "c0", "ragged", "ooc", "c3", "serving", "device"],
                    help="secondary measurements (one JSON line each) instead of the headline: ragged "
                         "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep, "
                         "the full serving stream (10,000 calls, dims to 16384), or a device-resident "
                         "loop (--size, --dtype, --mode, --warmup, --steps) for profiling one kernel")
-    p.add_argument("--samples", type=int, default=2000, help="entries checked against the oracle")
+    p.add_argument("--samples", type=int, default=100000,
+                   help="entries checked against the double-double oracle (--workload lines)")
     return p.parse_args()
 
 
@@ -234,6 +237,7 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
                     for (dt, ta, tb, M, N, K) in per_thread[t]] or [16])
         cbuf.append(torch.empty(need, dtype=torch.uint8, pin_memory=True))
     errors = []
+    lat = []  # (flops, seconds) per call, measured around the blocking call
 
     def worker(t):
         r = random.Random(seed + t)
@@ -249,8 +253,10 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
             ldb = K if tb == "N" else N
             alpha = 1.0 if dt != np.complex128 else 1.0 + 0.0j
             fn = {np.float64: bx.cblas_dgemm, np.float32: bx.cblas_sgemm, np.complex128: bx.cblas_zgemm}[dt]
+            c0 = time.perf_counter()
             fn(bx.CblasColMajor, bx.TRANS[ta], bx.TRANS[tb], M, N, K, alpha, a.data_ptr(), lda, b.data_ptr(), ldb,
                0.0, cbuf[t].data_ptr(), M)
+            lat.append(((8.0 if dt == np.complex128 else 2.0) * M * N * K, time.perf_counter() - c0))
             if bx.last_status() != 0:
                 errors.append(bx.last_error())
 
@@ -264,6 +270,12 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
     st = bx.serve_stats()
     bx.serve_stop()
     flops = sum((8.0 if dt == np.complex128 else 2.0) * M * N * K for (dt, ta, tb, M, N, K) in reqs)
+    classes = {}
+    for name, lo_f, hi_f in (("below 1 GFLOP", 0, 1e9), ("1-100 GFLOP", 1e9, 1e11), ("above 100 GFLOP", 1e11, 1e30)):
+        xs = sorted(v for f, v in lat if lo_f <= f < hi_f)
+        if xs:
+            classes[name] = {"calls": len(xs), "p50_ms": 1e3 * xs[len(xs) // 2],
+                             "p99_ms": 1e3 * xs[min(len(xs) - 1, int(0.99 * len(xs)))]}
     return {"requests": n_req, "threads": threads, "dmax": dmax, "offered_rate_per_s": rate or None,
             "achieved_rate_per_s": n_req / wall, "hbm_budget_bytes": budget or None, "max_inflight_cfg": inflight,
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
@@ -271,6 +283,11 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
             "b_cache_hits": st["cache_hits"], "b_cache_misses": st["cache_misses"],
             "grouped_launches": st["grouped_launches"], "grouped_requests": st["grouped_requests"],
             "max_inflight": st["max_inflight_seen"], "failed": st["failed"] + len(errors),
+            "by_size_call_latency": classes,
+            "scheduler": {"admit_seconds": st["admit_seconds"], "admit_max_ms": st["admit_max_ms"],
+                          "memory_waits": st["memory_waits"], "head_holds": st["head_holds"],
+                          "alloc_seconds": st["alloc_seconds"], "copy_seconds": st["copy_seconds"],
+                          "compute_enqueue_seconds": st["compute_enqueue_seconds"]},
             "mix": "60% f64 / 30% f32 / 10% c128, dims log-uniform [64, dmax], 30% B reuse"}
 
 
@@ -394,7 +411,7 @@ def run_workloads(args):
         fl = 2.0 * n ** 3
         h2d_min = 8.0 * 3 * n * n
         link = h2d_min / 55.6e9  # measured pinned H2D rate on this pool
-        sweep = [("native", bx.MODE_NATIVE, t) for t in (1024, 2048, 3072, 4096)]
+        sweep = [("native", bx.MODE_NATIVE, t) for t in (1024, 1536, 2048, 3072, 4096)]
         sweep += [("auto", bx.MODE_AUTO, t) for t in (2048, 4096, 8192)]
         for mode_name, mode, tile in sweep:
             C[:, :64] = C0
@@ -430,6 +447,39 @@ def run_workloads(args):
         bx.set_tile(0)
         bx.set_hbm_budget(0)
         bx.set_dgemm_mode(bx.MODE_AUTO)
+    elif args.workload == "c0":
+        # cblas_dgemm NN 4096^3 on the native path, U[-1,1], alpha = 1, beta = 0.5, pinned host arrays;
+        # checked against OpenBLAS (full matrix) and the double-double oracle (sampled)
+        import oracle
+        n = 4096
+        tA, A = _host(torch, (n, n), "f64", 1)
+        tB, B = _host(torch, (n, n), "f64", 2)
+        tC, C = _host(torch, (n, n), "f64", 3)
+        C0 = C.copy(order="F")
+        bx.set_dgemm_mode(bx.MODE_NATIVE)
+        times = []
+        for _ in range(max(3, args.steps)):
+            C[:] = C0
+            t0 = time.perf_counter()
+            bx.cblas_dgemm(bx.CblasColMajor, bx.CblasNoTrans, bx.CblasNoTrans, n, n, n, 1.0, tA.data_ptr(), n,
+                           tB.data_ptr(), n, 0.5, tC.data_ptr(), n)
+            times.append(time.perf_counter() - t0)
+            assert bx.last_status() == 0, bx.last_error()
+        bx.set_dgemm_mode(bx.MODE_AUTO)
+        st = bx.call_stats()
+        ob = oracle.OpenBLAS()
+        Co = C0.copy(order="F")
+        ob.gemm("N", "N", n, n, n, 1.0, A, n, B, n, 0.5, Co, n)
+        u = 2.0 ** -53
+        bound = (n + 2) * u * (np.abs(A) @ np.abs(B) + 0.5 * np.abs(C0))
+        ratio_ob = float(np.max(np.abs(C - Co) / (2 * bound)))
+        ratio, err = _accuracy(C, "N", "N", n, n, n, 1.0, A, n, B, n, 0.5, C0, n, "f64", args.samples)
+        dt = statistics.median(times)
+        lines.append({"workload": f"cblas_dgemm NN {n}^3 native, pinned host, U[-1,1], alpha 1, beta 0.5",
+                      "tflops_e2e": 2.0 * n ** 3 / dt / 1e12, "seconds_median": dt, "path": st["path"],
+                      "h2d_bytes": st["h2d_bytes"], "d2h_bytes": st["d2h_bytes"],
+                      "vs_openblas_max_ratio_to_2x_bound": ratio_ob, "openblas": ob.name,
+                      "oracle_samples": args.samples, "bound_ratio": ratio, "max_normalised_error": err})
     elif args.workload == "device":
         # device-resident n^3 NN calls through blasx_?gemm_device (for ncu captures of one kernel)
         n = args.size
@@ -466,12 +516,13 @@ def run_workloads(args):
         # the serving stream at full size: 10,000 calls from 16 threads, Poisson
         # arrivals, dims log-uniform in [64, 16384], 120 GB admission budget;
         # once with FP64 on the emulated path (auto) and once native
-        rate = args.serving_rate or 200.0
-        for mode_name, mode in (("auto", bx.MODE_AUTO), ("native", bx.MODE_NATIVE)):
-            bx.set_dgemm_mode(mode)
-            res = serving_load(bx, torch, 10000, 16384, 16, rate, seed=11, budget=120 * 10 ** 9, inflight=16)
-            lines.append({"workload": f"serving stream, FP64/complex on the {mode_name} path", **res})
-            print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
+        rates = [float(r) for r in args.rates.split(",") if r.strip()]
+        for rate in rates:
+            for mode_name, mode in (("auto", bx.MODE_AUTO), ("native", bx.MODE_NATIVE)):
+                bx.set_dgemm_mode(mode)
+                res = serving_load(bx, torch, 10000, 16384, 16, rate, seed=11, budget=120 * 10 ** 9, inflight=16)
+                lines.append({"workload": f"serving stream, FP64/complex on the {mode_name} path", **res})
+                print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
         bx.set_dgemm_mode(bx.MODE_AUTO)
     elif args.workload == "c3":
         for n in (8192, 16384):
@@ -520,7 +571,7 @@ def run_workloads(args):
             st = bx.call_stats()
             C = dC.cpu().numpy().T
             ratio, err = _accuracy(C, "N", "N", n, n, n, 1.0 + 0j, A, n, B, n, 0.0 + 0j, None, n, "c128",
-                                   min(args.samples, 1000))
+                                   args.samples)
             ms = e0.elapsed_time(e1)
             res[mode_name] = {"tflops": 8.0 * n ** 3 / (ms * 1e-3) / 1e12, "ms": ms, "path": st["path"],
                               "moduli": st["moduli"], "bound_ratio": ratio, "max_normalised_error": err}

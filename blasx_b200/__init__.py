@@ -53,7 +53,10 @@ class ServeStats(ctypes.Structure):
                 ("cache_misses", ctypes.c_longlong), ("grouped_launches", ctypes.c_longlong),
                 ("grouped_requests", ctypes.c_longlong), ("max_inflight_seen", _I), ("reserved", _I),
                 ("p50_ms", _D), ("p99_ms", _D), ("mean_ms", _D), ("max_ms", _D),
-                ("flops", _D), ("seconds", _D), ("tflops", _D)]
+                ("flops", _D), ("seconds", _D), ("tflops", _D),
+                ("admit_seconds", _D), ("admit_max_ms", _D), ("memory_waits", ctypes.c_longlong),
+                ("head_holds", ctypes.c_longlong), ("alloc_seconds", _D), ("copy_seconds", _D),
+                ("compute_enqueue_seconds", _D)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -49,6 +49,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "host_pipeline.h"
 #include "kernels.h"
 #include "ozaki.h"
 #include "serving.h"
@@ -157,6 +158,76 @@ uint64_t fingerprint(const void *p, int64_t ld, int64_t rows, int64_t cols, size
     return h;
 }
 
+// ---- device memory ---------------------------------------------------------------------
+// The serving loop's device memory: one allocation of the HBM budget, made at
+// start, cut into 256-byte-aligned blocks first-fit by the scheduler thread
+// (the only thread that takes or returns blocks); a returned block merges
+// with free neighbours. A request's blocks are returned only after its last
+// event has completed, so a block can be reused at once, by any stream.
+// Requests never call the stream-ordered allocator, whose pool growth and
+// reclaim block the calling thread (they stalled the whole queue).
+class Arena {
+public:
+    int init(size_t bytes) {
+        size_ = bytes & ~size_t(255);
+        if (size_ == 0) return set_error(BLASX_ERR_ARG, "serving: HBM budget of %zu bytes", bytes);
+        if (cudaMalloc(&base_, size_) != cudaSuccess) {
+            cudaGetLastError();
+            base_ = nullptr;
+            return set_error(BLASX_ERR_NOMEM, "serving: cannot reserve the HBM budget of %zu bytes", size_);
+        }
+        free_[0] = size_;
+        return BLASX_OK;
+    }
+    void release() {
+        if (base_) cudaFree(base_);
+        base_ = nullptr;
+        free_.clear();
+        used_.clear();
+    }
+    size_t size() const { return size_; }
+    void *alloc(size_t bytes) {
+        bytes = (std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            const size_t off = it->first, len = it->second;
+            free_.erase(it);
+            if (len > bytes) free_[off + bytes] = len - bytes;
+            used_[off] = bytes;
+            return base_ + off;
+        }
+        return nullptr;
+    }
+    void release_block(void *p) {
+        if (!p) return;
+        const size_t off = size_t(static_cast<char *>(p) - base_);
+        auto u = used_.find(off);
+        if (u == used_.end()) return;
+        size_t start = off, len = u->second;
+        used_.erase(u);
+        auto next = free_.lower_bound(start);
+        if (next != free_.end() && next->first == start + len) {
+            len += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == start) {
+                start = prev->first;
+                len += prev->second;
+                free_.erase(prev);
+            }
+        }
+        free_[start] = len;
+    }
+
+private:
+    char *base_ = nullptr;
+    size_t size_ = 0;
+    std::map<size_t, size_t> free_;            // offset -> length
+    std::unordered_map<size_t, size_t> used_;  // offset -> length
+};
+
 // ---- requests -----------------------------------------------------------------------
 struct Request {
     Gemm g;
@@ -165,11 +236,12 @@ struct Request {
     int status = BLASX_OK;
     // device side
     void *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    void *ws = nullptr;     // emulated path: its scratch
+    bool emulated = false;  // chosen at submission
     int64_t lda = 0, ldb = 0, ldc = 0;
     Entry *bcache = nullptr;  // cached B in use
     Key bkey{};
     bool bkey_valid = false;
-    size_t charged = 0;        // bytes counted against the budget
     bool grouped = false;
     int stream_slot = -1;
     cudaEvent_t ev_in = nullptr, ev_done = nullptr;
@@ -194,7 +266,8 @@ struct Server {
     std::vector<bool> stream_busy;
     cudaStream_t batch_stream = nullptr;
     std::vector<std::shared_ptr<Request>> pending, inflight;
-    size_t used = 0;  // bytes of in-flight device copies (excluding cached operands)
+    Arena arena;
+    int *err_words = nullptr;  // pinned, one per stream slot: the emulated path's device error word
 
     std::mutex cache_mu;
     std::unordered_map<Key, Entry *, KeyHash> cache;
@@ -206,34 +279,20 @@ struct Server {
     std::vector<double> latencies;
     double flops = 0, t_first = 0, t_last = 0;
     long long submitted = 0, completed = 0, hits = 0, misses = 0, grouped_launches = 0,
-              grouped_requests = 0, failed = 0;
+              grouped_requests = 0, failed = 0, memory_waits = 0, head_holds = 0;
     int max_seen = 0;
+    double admit_s = 0, admit_max_s = 0;
+    double alloc_s = 0, copy_s = 0, enqueue_s = 0;  // parts of admit_s
 };
 
 std::mutex g_server_mu;
 Server *g_server = nullptr;
 std::atomic<bool> g_active{false};
 
-size_t device_bytes(const Request &r, bool need_b) {
-    const Gemm &g = r.g;
-    const size_t es = elem_size(g.dt);
-    const bool need_ab = !(g.alpha_zero() || g.K == 0);
-    size_t b = size_t(round_up(g.M, 32)) * g.N * es;
-    if (need_ab) {
-        b += size_t(round_up(g.rows_a(), 32)) * g.cols_a() * es;
-        if (need_b) b += size_t(round_up(g.rows_b(), 32)) * g.cols_b() * es;
-        if (ozaki_selected(g, config().dgemm_mode.load())) {
-            Gemm probe = g;
-            b += ozaki_scratch_bytes(probe);
-        }
-    }
-    return b;
-}
-
-// Evicts unused cache entries (LRU first) until `need` more bytes fit.
 // Drops unused cache entries from the least recently used end while `over`
-// holds (caller holds cache_mu).
-template <typename Pred> void evict_lru(Server &s, cudaStream_t st, Pred over) {
+// holds (caller holds cache_mu; scheduler thread). Returns how many.
+template <typename Pred> int evict_lru(Server &s, Pred over) {
+    int n = 0;
     auto it = s.lru.end();
     while (it != s.lru.begin() && over()) {
         --it;
@@ -242,15 +301,61 @@ template <typename Pred> void evict_lru(Server &s, cudaStream_t st, Pred over) {
         it = s.lru.erase(it);  // next element: already visited going backwards
         s.cache.erase(e->key);
         s.cache_bytes -= e->bytes;
-        cudaFreeAsync(e->dev, st);
+        s.arena.release_block(e->dev);
         delete e;
+        ++n;
     }
+    return n;
 }
 
-void cache_make_room(Server &s, size_t need, cudaStream_t st) {
-    std::lock_guard<std::mutex> lk(s.cache_mu);
-    evict_lru(s, st, [&] { return s.used + s.cache_bytes + need > s.budget; });
+// Takes a request's device blocks from the arena: A, B (unless a cached copy
+// is used), C and the emulated path's scratch, evicting unused cached
+// operands (least recently used first) while a block does not fit. Returns
+// false, holding nothing, when they still do not fit.
+bool reserve(Server &s, Request *r, bool need_b) {
+    const Gemm &g = r->g;
+    const size_t es = elem_size(g.dt);
+    const bool need_ab = !(g.alpha_zero() || g.K == 0);
+    r->lda = round_up(g.rows_a(), 32);
+    r->ldb = round_up(g.rows_b(), 32);
+    r->ldc = round_up(g.M, 32);
+    void **dst[4] = {&r->dA, &r->dB, &r->dC, &r->ws};
+    const size_t bytes[4] = {need_ab ? size_t(r->lda) * g.cols_a() * es : 0,
+                             need_ab && need_b ? size_t(r->ldb) * g.cols_b() * es : 0,
+                             size_t(r->ldc) * g.N * es,
+                             need_ab && r->emulated ? ozaki_scratch_bytes(g) : 0};
+    for (int k = 0; k < 4; ++k) {
+        if (!bytes[k]) continue;
+        void *p = s.arena.alloc(bytes[k]);
+        while (!p) {
+            int freed;
+            {
+                std::lock_guard<std::mutex> lk(s.cache_mu);
+                bool once = true;
+                freed = evict_lru(s, [&] { const bool o = once; once = false; return o; });
+            }
+            if (!freed) break;
+            p = s.arena.alloc(bytes[k]);
+        }
+        if (!p) {
+            for (int j = 0; j < k; ++j) {
+                s.arena.release_block(*dst[j]);
+                *dst[j] = nullptr;
+            }
+            return false;
+        }
+        *dst[k] = p;
+    }
+    return true;
 }
+
+// Adds the host time of one enqueue call to a scheduler counter.
+struct HostTimer {
+    double &acc;
+    double t0;
+    explicit HostTimer(double &a) : acc(a), t0(now_s()) {}
+    ~HostTimer() { acc += now_s() - t0; }
+};
 
 int admit(Server &s, Request *r, int slot) {
     Gemm &g = r->g;
@@ -259,30 +364,29 @@ int admit(Server &s, Request *r, int slot) {
     r->stream_slot = slot;
     const bool need_ab = !(g.alpha_zero() || g.K == 0);
     const bool read_c = !g.beta_zero();
-    r->lda = round_up(g.rows_a(), 32);
-    r->ldb = round_up(g.rows_b(), 32);
-    r->ldc = round_up(g.M, 32);
     BX_CUDA(cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming));
     BX_CUDA(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
     if (need_ab) {
-        BX_CUDA(cudaMallocAsync(&r->dA, size_t(r->lda) * g.cols_a() * es, st));
-        BX_CUDA(cudaMemcpy2DAsync(r->dA, r->lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
-                                  cudaMemcpyHostToDevice, st));
+        {
+            HostTimer t(s.copy_s);
+            BX_CUDA(cudaMemcpy2DAsync(r->dA, r->lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
+                                      cudaMemcpyHostToDevice, st));
+        }
         r->stats.h2d_bytes += double(es) * g.rows_a() * g.cols_a();
         if (r->bcache) {
             r->dB = r->bcache->dev;
             r->ldb = r->bcache->dld;
             r->stats.cache_hits += 1;
         } else {
-            BX_CUDA(cudaMallocAsync(&r->dB, size_t(r->ldb) * g.cols_b() * es, st));
+            HostTimer t(s.copy_s);
             BX_CUDA(cudaMemcpy2DAsync(r->dB, r->ldb * es, g.B, g.ldb * es, g.rows_b() * es,
                                       g.cols_b(), cudaMemcpyHostToDevice, st));
             r->stats.h2d_bytes += double(es) * g.rows_b() * g.cols_b();
             r->stats.cache_misses += 1;
         }
     }
-    BX_CUDA(cudaMallocAsync(&r->dC, size_t(r->ldc) * g.N * es, st));
     if (read_c) {
+        HostTimer t(s.copy_s);
         BX_CUDA(cudaMemcpy2DAsync(r->dC, r->ldc * es, g.C, g.ldc * es, g.M * es, g.N,
                                   cudaMemcpyHostToDevice, st));
         r->stats.h2d_bytes += double(es) * g.M * g.N;
@@ -297,8 +401,19 @@ int admit(Server &s, Request *r, int slot) {
     d.B = r->dB; d.ldb = r->ldb;
     d.C = r->dC; d.ldc = r->ldc;
     d.max_cta_tiles = kResidueTilesPerCta;  // emulated path: let other requests' kernels in
-    BX_TRY(device_gemm(d, st));
-    r->stats.path = call_stats().path;
+    {
+        HostTimer t(s.enqueue_s);
+        if (need_ab && r->emulated) {
+            // on the request's own scratch; its device error word (the scratch's
+            // first word) comes back with the request
+            BX_TRY(ozaki_gemm_in(d, st, config().dgemm_mode.load(), r->ws, context()->num_sms));
+            BX_CUDA(cudaMemcpyAsync(&s.err_words[slot], r->ws, sizeof(int), cudaMemcpyDeviceToHost, st));
+            r->stats.path = 2;
+        } else {
+            BX_TRY(device_gemm(d, st));
+            r->stats.path = call_stats().path;
+        }
+    }
     r->stats.moduli = 0;
     BX_CUDA(cudaMemcpy2DAsync(g.C, g.ldc * es, r->dC, r->ldc * es, g.M * es, g.N,
                               cudaMemcpyDeviceToHost, st));
@@ -356,8 +471,14 @@ void finish(Server &s, Request *r, int status) {
     cudaStream_t st = s.streams[size_t(r->stream_slot)];
     const Gemm &g = r->g;
     const size_t es = elem_size(g.dt);
-    if (r->dA) cudaFreeAsync(r->dA, st);
-    if (r->dC) cudaFreeAsync(r->dC, st);
+    if (r->emulated && r->ws && status == BLASX_OK && s.err_words[r->stream_slot] != 0) {
+        set_error(BLASX_ERR_TIMEOUT, "serving: emulated GEMM's bounded device wait expired (flag %d)",
+                  s.err_words[r->stream_slot]);
+        status = BLASX_ERR_TIMEOUT;
+    }
+    s.arena.release_block(r->dA);
+    s.arena.release_block(r->dC);
+    s.arena.release_block(r->ws);
     {
         std::lock_guard<std::mutex> lk(s.cache_mu);
         if (r->bcache) {
@@ -366,7 +487,7 @@ void finish(Server &s, Request *r, int status) {
                 s.lru.erase(r->bcache->lru);
                 s.cache.erase(r->bcache->key);
                 s.cache_bytes -= r->bcache->bytes;
-                cudaFreeAsync(r->bcache->dev, st);
+                s.arena.release_block(r->bcache->dev);
                 delete r->bcache;
             }
         } else if (r->dB) {
@@ -374,7 +495,7 @@ void finish(Server &s, Request *r, int status) {
             const bool keep = status == BLASX_OK && r->bkey_valid && bytes <= s.cache_budget &&
                               s.cache.find(r->bkey) == s.cache.end();
             if (keep)  // make room inside the cache budget (least recently used, unused first)
-                evict_lru(s, st, [&] { return s.cache_bytes + bytes > s.cache_budget; });
+                evict_lru(s, [&] { return s.cache_bytes + bytes > s.cache_budget; });
             if (keep && s.cache_bytes + bytes <= s.cache_budget) {
                 Entry *e = new Entry;
                 e->key = r->bkey;
@@ -386,11 +507,10 @@ void finish(Server &s, Request *r, int status) {
                 s.cache[e->key] = e;
                 s.cache_bytes += bytes;
             } else {
-                cudaFreeAsync(r->dB, st);
+                s.arena.release_block(r->dB);
             }
         }
     }
-    s.used -= r->charged;
     s.stream_busy[size_t(r->stream_slot)] = false;
     if (r->ev_in) cudaEventDestroy(r->ev_in);
     if (r->ev_done) cudaEventDestroy(r->ev_done);
@@ -406,6 +526,25 @@ void finish(Server &s, Request *r, int status) {
     }
     r->status = status;
     r->done.set_value(status);
+}
+
+// A request larger than the whole budget: the library's own host path (in
+// core, or out of core through the tile cache, with its own device memory)
+// runs it on the scheduler thread while nothing else is in flight.
+void run_alone(Server &s, Request *r) {
+    const int st = host_gemm(r->g);
+    r->stats = call_stats();
+    r->t_done = now_s();
+    {
+        std::lock_guard<std::mutex> lk(s.stat_mu);
+        s.completed += 1;
+        if (st != BLASX_OK) s.failed += 1;
+        s.latencies.push_back(r->t_done - r->t_submit);
+        s.flops += r->g.flops();
+        s.t_last = r->t_done;
+    }
+    r->status = st;
+    r->done.set_value(st);
 }
 
 void loop(Server *sp) {
@@ -468,17 +607,6 @@ void loop(Server *sp) {
                     }
                 }
             }
-            const size_t need = device_bytes(*r, hit == nullptr);
-            if (s.used + s.cache_bytes + need > s.budget) cache_make_room(s, need, s.batch_stream);
-            if (s.used + need > s.budget && !s.inflight.empty()) {
-                if (hit) {
-                    std::lock_guard<std::mutex> lk(s.cache_mu);
-                    hit->users--;
-                }
-                if (idx == 0 && now - r->t_submit > kHeadWait) break;  // memory is kept for it
-                ++idx;  // does not fit yet: look further back
-                continue;
-            }
             int slot = -1;
             for (size_t k = 0; k < s.stream_busy.size(); ++k)
                 if (!s.stream_busy[k]) { slot = int(k); break; }
@@ -489,16 +617,46 @@ void loop(Server *sp) {
                 }
                 break;
             }
+            bool fits;
+            {
+                HostTimer t(s.alloc_s);
+                fits = reserve(s, r, hit == nullptr);
+            }
+            if (!fits) {
+                if (hit) {
+                    std::lock_guard<std::mutex> lk(s.cache_mu);
+                    hit->users--;
+                }
+                if (s.inflight.empty()) {  // larger than the whole budget
+                    s.pending.erase(s.pending.begin() + long(idx));
+                    run_alone(s, r);
+                    progress = true;
+                    continue;
+                }
+                {
+                    std::lock_guard<std::mutex> lk(s.stat_mu);
+                    ++s.memory_waits;
+                    if (idx == 0 && now - r->t_submit > kHeadWait) ++s.head_holds;
+                }
+                if (idx == 0 && now - r->t_submit > kHeadWait) break;  // memory is kept for it
+                ++idx;  // does not fit yet: look further back
+                continue;
+            }
             s.pending.erase(s.pending.begin() + long(idx));
             s.stream_busy[size_t(slot)] = true;
             r->bcache = hit;
-            r->charged = need;
-            s.used += need;
             {
                 std::lock_guard<std::mutex> lk(s.stat_mu);
                 if (r->bkey_valid && !(r->g.alpha_zero() || r->g.K == 0)) (hit ? s.hits : s.misses) += 1;
             }
+            const double a0 = now_s();
             const int st = admit(s, r, slot);
+            {
+                const double da = now_s() - a0;
+                std::lock_guard<std::mutex> lk(s.stat_mu);
+                s.admit_s += da;
+                s.admit_max_s = std::max(s.admit_max_s, da);
+            }
             s.inflight.push_back(rp);
             s.max_seen = std::max(s.max_seen, int(s.inflight.size()));
             if (st != BLASX_OK) {
@@ -531,11 +689,8 @@ int submit(const Gemm &g) {
     r->t_submit = now_s();
     // small native requests are mixed into grouped launches
     r->flops = 0;
-    r->grouped = false;
-    if (g.dt != DType::F32 && need_ab) {
-        const bool emulated = ozaki_selected(g, config().dgemm_mode.load());
-        r->grouped = !emulated && g.flops() <= s->group_flops;
-    }
+    r->emulated = need_ab && ozaki_selected(g, config().dgemm_mode.load());
+    r->grouped = need_ab && !r->emulated && g.dt != DType::F32 && g.flops() <= s->group_flops;
     if (need_ab) {
         r->bkey = Key{g.B, g.ldb, g.rows_b(), g.cols_b(), int(g.dt),
                       fingerprint(g.B, g.ldb, g.rows_b(), g.cols_b(), es)};
@@ -582,6 +737,17 @@ int blasx_serve_start(size_t hbm_budget, size_t cache_bytes, int max_inflight) {
     s->budget = hbm_budget ? hbm_budget : size_t(double(free_b) * 0.85);
     s->cache_budget = cache_bytes ? std::min(cache_bytes, s->budget / 2) : s->budget / 4;
     s->max_inflight = max_inflight > 0 ? std::min(max_inflight, 64) : 8;
+    int rc = s->arena.init(s->budget);
+    if (rc == BLASX_OK) rc = bx::oz::upload_crt_tables();
+    if (rc == BLASX_OK && cudaHostAlloc(reinterpret_cast<void **>(&s->err_words),
+                                        sizeof(int) * size_t(s->max_inflight), cudaHostAllocDefault) != cudaSuccess)
+        rc = bx::set_error(BLASX_ERR_NOMEM, "serving: pinned error words");
+    if (rc != BLASX_OK) {
+        s->arena.release();
+        delete s;
+        return rc;
+    }
+    memset(s->err_words, 0, sizeof(int) * size_t(s->max_inflight));
     s->streams.resize(size_t(s->max_inflight));
     s->stream_busy.assign(size_t(s->max_inflight), false);
     // the grouped launches of small requests get the highest stream priority:
@@ -612,13 +778,12 @@ int blasx_serve_stop(void) {
     s->thread.join();  // the loop drains queued and in-flight requests first
     {
         std::lock_guard<std::mutex> lk(s->cache_mu);
-        for (auto &kv : s->cache) {
-            cudaFree(kv.second->dev);
-            delete kv.second;
-        }
+        for (auto &kv : s->cache) delete kv.second;
     }
     for (auto st : s->streams) cudaStreamDestroy(st);
     cudaStreamDestroy(s->batch_stream);
+    s->arena.release();
+    cudaFreeHost(s->err_words);
     std::lock_guard<std::mutex> lk(g_server_mu);
     g_server = nullptr;
     delete s;
@@ -657,6 +822,13 @@ void blasx_serve_get_stats(blasx_serve_stats *out) {
     out->flops = s.flops;
     out->seconds = s.t_last > s.t_first ? s.t_last - s.t_first : 0;
     out->tflops = out->seconds > 0 ? s.flops / out->seconds / 1e12 : 0;
+    out->admit_seconds = s.admit_s;
+    out->admit_max_ms = s.admit_max_s * 1e3;
+    out->memory_waits = s.memory_waits;
+    out->head_holds = s.head_holds;
+    out->alloc_seconds = s.alloc_s;
+    out->copy_seconds = s.copy_s;
+    out->compute_enqueue_seconds = s.enqueue_s;
     if (!s.latencies.empty()) {
         std::vector<double> l = s.latencies;
         std::sort(l.begin(), l.end());
@@ -684,6 +856,9 @@ int blasx_serve_reset_stats(void) {
     s.submitted = s.completed = s.hits = s.misses = s.grouped_launches = s.grouped_requests = 0;
     s.failed = 0;
     s.max_seen = 0;
+    s.memory_waits = s.head_holds = 0;
+    s.admit_s = s.admit_max_s = 0;
+    s.alloc_s = s.copy_s = s.enqueue_s = 0;
     return BLASX_OK;
 }
 

@@ -211,6 +211,11 @@ typedef struct blasx_serve_stats {
     int max_inflight_seen, reserved;
     double p50_ms, p99_ms, mean_ms, max_ms;    /* submit -> completion */
     double flops, seconds, tflops;             /* first submit -> last completion */
+    double admit_seconds, admit_max_ms;        /* scheduler time spent enqueueing requests */
+    long long memory_waits;                    /* admission passes over a request that did not fit */
+    long long head_holds;                      /* passes stopped to keep memory for the oldest request */
+    double alloc_seconds, copy_seconds;        /* parts of admit_seconds: device allocation, copy calls */
+    double compute_enqueue_seconds;            /* part of admit_seconds: enqueueing the GEMM kernels */
 } blasx_serve_stats;
 void blasx_serve_get_stats(blasx_serve_stats *out);
 int blasx_serve_reset_stats(void);
