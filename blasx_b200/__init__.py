@@ -87,6 +87,17 @@ def lib() -> ctypes.CDLL:
         L.cblas_sgemm.argtypes = [_I] * 6 + [_F, _P, _I, _P, _I, _F, _P, _I]
         L.cblas_dgemm.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _D, _P, _I]
         L.cblas_zgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
+        L.cblas_ssyrk.argtypes = [_I] * 5 + [_F, _P, _I, _F, _P, _I]
+        L.cblas_dsyrk.argtypes = [_I] * 5 + [_D, _P, _I, _D, _P, _I]
+        L.cblas_zsyrk.argtypes = [_I] * 5 + [_P, _P, _I, _P, _P, _I]
+        L.cblas_ssyr2k.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I]
+        L.cblas_dsyr2k.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I]
+        L.cblas_zsyr2k.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I]
+        for f in ("ssyrk_", "dsyrk_", "zsyrk_"):
+            getattr(L, f).argtypes = [_P] * 10
+        for f in ("ssyr2k_", "dsyr2k_", "zsyr2k_"):
+            getattr(L, f).argtypes = [_P] * 12
+        L.blasx_dsyrk_device.argtypes = [_I] * 4 + [_D, _P, _I, _D, _P, _I, _P]
         for f in ("sgemm_", "dgemm_", "zgemm_"):
             getattr(L, f).argtypes = [_P] * 13
         L.xerbla_.argtypes = [ctypes.c_char_p, _P]
@@ -159,6 +170,79 @@ def cblas_zgemm(Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, beta, C, 
     al, be = _cpair(alpha), _cpair(beta)
     lib().cblas_zgemm(Order, TransA, TransB, M, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb,
                       be.ctypes.data, _addr(C), ldc)
+
+
+UPLO = {"U": 121, "L": 122}
+CblasUpper, CblasLower = 121, 122
+
+
+def cblas_ssyrk(Order, Uplo, Trans, N, K, alpha, A, lda, beta, C, ldc):
+    lib().cblas_ssyrk(Order, Uplo, Trans, N, K, alpha, _addr(A), lda, beta, _addr(C), ldc)
+
+
+def cblas_dsyrk(Order, Uplo, Trans, N, K, alpha, A, lda, beta, C, ldc):
+    lib().cblas_dsyrk(Order, Uplo, Trans, N, K, alpha, _addr(A), lda, beta, _addr(C), ldc)
+
+
+def cblas_zsyrk(Order, Uplo, Trans, N, K, alpha, A, lda, beta, C, ldc):
+    al, be = _cpair(alpha), _cpair(beta)
+    lib().cblas_zsyrk(Order, Uplo, Trans, N, K, al.ctypes.data, _addr(A), lda, be.ctypes.data, _addr(C), ldc)
+
+
+def cblas_ssyr2k(Order, Uplo, Trans, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    lib().cblas_ssyr2k(Order, Uplo, Trans, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta, _addr(C), ldc)
+
+
+def cblas_dsyr2k(Order, Uplo, Trans, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    lib().cblas_dsyr2k(Order, Uplo, Trans, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta, _addr(C), ldc)
+
+
+def cblas_zsyr2k(Order, Uplo, Trans, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    al, be = _cpair(alpha), _cpair(beta)
+    lib().cblas_zsyr2k(Order, Uplo, Trans, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb,
+                       be.ctypes.data, _addr(C), ldc)
+
+
+def _f77_syr(fn, ctype, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, B=None, ldb=None, cplx=False):
+    u = ctypes.c_char(uplo.encode() if isinstance(uplo, str) else uplo)
+    t = ctypes.c_char(trans.encode() if isinstance(trans, str) else trans)
+    ints = [ctypes.c_int(v) for v in (n, k, lda, ldc, ldb or 1)]
+    if cplx:
+        al, be = _cpair(alpha), _cpair(beta)
+        pa, pb = al.ctypes.data, be.ctypes.data
+    else:
+        al, be = ctype(alpha), ctype(beta)
+        pa, pb = ctypes.addressof(al), ctypes.addressof(be)
+    r = ctypes.byref
+    if B is None:
+        fn(r(u), r(t), r(ints[0]), r(ints[1]), pa, _addr(A), r(ints[2]), pb, _addr(C), r(ints[3]))
+    else:
+        fn(r(u), r(t), r(ints[0]), r(ints[1]), pa, _addr(A), r(ints[2]), _addr(B), r(ints[4]), pb, _addr(C),
+           r(ints[3]))
+
+
+def ssyrk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
+    _f77_syr(lib().ssyrk_, ctypes.c_float, uplo, trans, n, k, alpha, A, lda, beta, C, ldc)
+
+
+def dsyrk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
+    _f77_syr(lib().dsyrk_, ctypes.c_double, uplo, trans, n, k, alpha, A, lda, beta, C, ldc)
+
+
+def zsyrk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
+    _f77_syr(lib().zsyrk_, None, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, cplx=True)
+
+
+def dsyr2k_(uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    _f77_syr(lib().dsyr2k_, ctypes.c_double, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, B=B, ldb=ldb)
+
+
+def dsyrk_device(uplo, trans, N, K, alpha, A, lda, beta, C, ldc, stream=None):
+    """Device-resident DSYRK on device pointers (ints or tensors with data_ptr)."""
+    s = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else _addr(stream))
+    u = UPLO[uplo] if isinstance(uplo, str) else uplo
+    t = TRANS[trans] if isinstance(trans, str) else trans
+    return lib().blasx_dsyrk_device(u, t, N, K, alpha, _addr(A), lda, beta, _addr(C), ldc, s)
 
 
 def _f77(fn, ctype, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cplx=False):

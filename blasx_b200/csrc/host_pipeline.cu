@@ -50,13 +50,19 @@ struct Events {
 struct DeviceOps {
     void *A = nullptr, *B = nullptr, *C = nullptr, *ws = nullptr;
     void *C0 = nullptr;  // input C, when the emulated path accumulates K-blocks into C
+    bool b_is_a = false;  // B is the same host buffer as A (SYRK): one device copy
     int64_t lda = 0, ldb = 0, ldc = 0;
     cudaStream_t s = nullptr;
     ~DeviceOps() {
-        for (void *p : {A, B, C, ws, C0})
+        for (void *p : {A, b_is_a ? nullptr : B, C, ws, C0})
             if (p) cudaFreeAsync(p, s);
     }
 };
+
+// B read from A's host buffer with the same stored shape (SYRK's op(A) op(A)^T).
+bool b_is_a(const Gemm &g) {
+    return g.A == g.B && g.lda == g.ldb && g.rows_a() == g.rows_b() && g.cols_a() == g.cols_b();
+}
 
 size_t default_budget(const Context *c) {
     size_t b = config().hbm_budget.load();
@@ -78,7 +84,7 @@ int copy_panel_in(const Gemm &g, const DeviceOps &d, int64_t j0, int64_t j1, boo
                   bool read_c, cudaStream_t s, blasx_call_stats &st) {
     const size_t es = elem_size(g.dt);
     const int64_t w = j1 - j0;
-    if (need_b) {
+    if (need_b && !d.b_is_a) {
         const char *hb = static_cast<const char *>(g.B);
         char *db = static_cast<char *>(d.B);
         if (g.tb == NoTrans) {  // K x N stored: columns j0..j1
@@ -143,6 +149,7 @@ int incore_native(const Gemm &g, Context *c, DeviceOps &d, bool need_ab, bool re
         p_g.ldb = d.ldb;
         p_g.C = static_cast<char *>(d.C) + j0 * d.ldc * es;
         p_g.ldc = d.ldc;
+        p_g.diag = g.diag + j0;  // triangular output: this panel's columns start at j0
         if (need_ab) {
             BX_TRY(dmma_supported(p_g) ? launch_gemm_dmma(p_g, c->compute)
                                        : launch_gemm_simt(p_g, c->compute));
@@ -193,7 +200,11 @@ int oz_before_reconstruct(void *vctx, int64_t j0, int64_t j1) {
 // are copied block by block, so that block b computes while block b + 1 is
 // on the host link. Two blocks once K >= 4096 (each block's slicing and
 // residue GEMMs are independent; the blocks' results are summed in FP64).
-int kblock_count(const Gemm &g) { return g.K >= 4096 ? 2 : 1; }
+int kblock_count(const Gemm &g) {
+    // a triangular output keeps one block: its panels read C whole before
+    // reconstructing into it, so the other triangle goes back unchanged
+    return g.K >= 4096 && g.uplo == 0 ? 2 : 1;
+}
 
 int64_t kblock_edge(const Gemm &g, int b, int blocks) {
     return b == blocks ? g.K : (g.K * b / blocks) / 128 * 128;
@@ -220,9 +231,10 @@ int copy_kblock_in(const Gemm &g, const DeviceOps &d, int64_t k0, int64_t k1, cu
     const Gemm v = kblock_of(g, d.A, d.lda, d.B, d.ldb, k0, k1);
     BX_CUDA(cudaMemcpy2DAsync(const_cast<void *>(v.A), d.lda * es, h.A, g.lda * es, h.rows_a() * es,
                               h.cols_a(), cudaMemcpyHostToDevice, s));
-    BX_CUDA(cudaMemcpy2DAsync(const_cast<void *>(v.B), d.ldb * es, h.B, g.ldb * es, h.rows_b() * es,
-                              h.cols_b(), cudaMemcpyHostToDevice, s));
-    st.h2d_bytes += double(es) * (h.rows_a() * h.cols_a() + h.rows_b() * h.cols_b());
+    if (!d.b_is_a)
+        BX_CUDA(cudaMemcpy2DAsync(const_cast<void *>(v.B), d.ldb * es, h.B, g.ldb * es, h.rows_b() * es,
+                                  h.cols_b(), cudaMemcpyHostToDevice, s));
+    st.h2d_bytes += double(es) * (h.rows_a() * h.cols_a() + (d.b_is_a ? 0 : h.rows_b() * h.cols_b()));
     return BLASX_OK;
 }
 
@@ -244,6 +256,7 @@ int oz_after_panel_kblocks(void *vctx, int64_t j0, int64_t j1) {
         p.N = j1 - j0;
         p.C = static_cast<char *>(d.C) + j0 * d.ldc * es;
         p.ldc = d.ldc;
+        p.diag = g.diag + j0;
         BX_TRY(launch_add_scaled(p, static_cast<const char *>(d.C0) + j0 * d.ldc * es, d.ldc,
                                  x->c->compute));
     }
@@ -313,9 +326,10 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
     // each reconstruction waiting only for its own panel
     BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
                               cudaMemcpyHostToDevice, c->h2d));
-    BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
-                              cudaMemcpyHostToDevice, c->h2d));
-    st.h2d_bytes += double(es) * (g.rows_a() * g.cols_a() + g.rows_b() * g.cols_b());
+    if (!d.b_is_a)
+        BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
+                                  cudaMemcpyHostToDevice, c->h2d));
+    st.h2d_bytes += double(es) * (g.rows_a() * g.cols_a() + (d.b_is_a ? 0 : g.rows_b() * g.cols_b()));
     cudaEvent_t ab = ev.make();
     BX_CUDA(cudaEventRecord(ab, c->h2d));
     BX_CUDA(cudaStreamWaitEvent(c->compute, ab, 0));
@@ -344,20 +358,23 @@ int host_gemm(const Gemm &g) {
     std::lock_guard<std::mutex> lk(c->host_mu);
     const size_t es = elem_size(g.dt);
     const bool need_ab = !(g.alpha_zero() || g.K == 0);
-    const bool read_c = !g.beta_zero();
+    // a triangular output keeps the other triangle: C always makes the round trip
+    const bool read_c = !g.beta_zero() || g.uplo != 0;
     const int mode = config().dgemm_mode.load();
     const bool oz = need_ab && want_ozaki(g, mode);
 
     DeviceOps d;
     d.s = c->compute;
+    d.b_is_a = need_ab && b_is_a(g);
     d.lda = round_up(g.rows_a(), 32);
     d.ldb = round_up(g.rows_b(), 32);
     d.ldc = round_up(g.M, 32);
     const size_t bytes_a = need_ab ? size_t(d.lda) * g.cols_a() * es : 0;
-    const size_t bytes_b = need_ab ? size_t(d.ldb) * g.cols_b() * es : 0;
+    const size_t bytes_b = need_ab && !d.b_is_a ? size_t(d.ldb) * g.cols_b() * es : 0;
     const size_t bytes_c = size_t(d.ldc) * g.N * es;
     Gemm probe = g;
     probe.lda = d.lda; probe.ldb = d.ldb; probe.ldc = d.ldc;
+    if (!d.b_is_a) probe.B = nullptr;  // the scratch shares slices only when the device copy is shared
     const size_t bytes_ws = oz ? ozaki_scratch_bytes(probe) : 0;
     const size_t bytes_c0 = (oz && read_c && kblock_count(g) > 1) ? bytes_c : 0;
     const size_t budget = default_budget(c);
@@ -372,17 +389,19 @@ int host_gemm(const Gemm &g) {
         step.N = std::min<int64_t>(g.N, T);
         step.K = std::min<int64_t>(g.K, T);
         step.lda = step.ldb = step.ldc = T;
+        step.B = nullptr;  // a step's A and B tiles sit in separate slots, even for SYRK
         const size_t step_ws = want_ozaki(step, mode) ? ozaki_scratch_bytes(step) : 0;
         const int st_code = tiled_host_gemm(g, c, budget, T, 0, step_ws, mode);
         st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return st_code;
     }
     BX_TRY(pins.pin(g.A, need_ab ? host_extent(g.lda, g.rows_a(), g.cols_a(), es) : 0));
-    BX_TRY(pins.pin(g.B, need_ab ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
+    BX_TRY(pins.pin(g.B, need_ab && !d.b_is_a ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
     BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
     if (need_ab) {
         BX_CUDA(cudaMallocAsync(&d.A, bytes_a ? bytes_a : 256, c->compute));
-        BX_CUDA(cudaMallocAsync(&d.B, bytes_b ? bytes_b : 256, c->compute));
+        if (d.b_is_a) d.B = d.A;
+        else BX_CUDA(cudaMallocAsync(&d.B, bytes_b ? bytes_b : 256, c->compute));
     }
     BX_CUDA(cudaMallocAsync(&d.C, bytes_c, c->compute));
     if (oz) BX_CUDA(cudaMallocAsync(&d.ws, bytes_ws, c->compute));

@@ -74,7 +74,13 @@ struct DmmaParams {
     int tiles_m, tiles_n;
     int vec_a, vec_b;  // 16-byte copies allowed (ld even, base 16-byte aligned)
     const int *guard;  // when set, run only if *guard == 0
+    int uplo;          // triangular output: 0 all, 1 row - col <= diag, 2 row - col >= diag
+    int64_t diag;
 };
+
+__device__ __forceinline__ bool tri_keep(int uplo, int64_t diag, int64_t r, int64_t c) {
+    return uplo == 0 || (uplo == 1 ? r - c <= diag : r - c >= diag);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -190,6 +196,9 @@ __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, d
     const int tm = first_m + (tile % per_group) % gsize;
     const int tn = (tile % per_group) / gsize;
     const int m0 = tm * BM, n0 = tn * BN;
+    // triangular output: a tile with no entry inside computes nothing (uniform per CTA)
+    if (p.uplo == 1 && int64_t(m0) - (n0 + BN - 1) > p.diag) return;
+    if (p.uplo == 2 && int64_t(m0 + BM - 1) - n0 < p.diag) return;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp / TL::WARPS_N, wn = warp % TL::WARPS_N;
@@ -301,7 +310,7 @@ __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, d
             for (int r = 0; r < 4; ++r) {
                 const int row = m0 + wm * (MT * 16) + i * 16 + g + (r >= 2 ? 8 : 0);
                 const int col = n0 + wn * (NT * 8) + j * 8 + 2 * t + (r & 1);
-                if (row >= p.M || col >= p.N) continue;
+                if (row >= p.M || col >= p.N || !tri_keep(p.uplo, p.diag, row, col)) continue;
                 double *cp = p.C + (row + int64_t(col) * p.ldc) * es;
                 if (!CPLX) {
                     double v = p.alpha_re * acc[0][i][j][r];
@@ -457,6 +466,8 @@ template <bool CPLX, int G = 0> DmmaParams make_params(const Gemm &g) {
     p.vec_a = (g.lda % 2 == 0) && (reinterpret_cast<uintptr_t>(g.A) % 16 == 0);
     p.vec_b = (g.ldb % 2 == 0) && (reinterpret_cast<uintptr_t>(g.B) % 16 == 0);
     p.guard = g.guard;
+    p.uplo = g.uplo;
+    p.diag = g.diag;
     return p;
 }
 

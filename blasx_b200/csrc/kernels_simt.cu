@@ -63,7 +63,7 @@ template <typename T>
 __global__ void __launch_bounds__(NT)
     gemm_simt_kernel(int ta, int tb, int M, int N, int K, T alpha, const T *__restrict__ A,
                      int64_t lda, const T *__restrict__ B, int64_t ldb, T beta, T *__restrict__ C,
-                     int64_t ldc, int beta_zero, const int *guard) {
+                     int64_t ldc, int beta_zero, const int *guard, int uplo, int64_t diag) {
     using Ar = Arith<T>;
     if (guard && *guard != 0) return;  // the emulated path produced C
     __shared__ T As[BK][BM + 1];
@@ -71,6 +71,9 @@ __global__ void __launch_bounds__(NT)
     const int tid = threadIdx.x;
     const int tx = tid % 16, ty = tid / 16;
     const int64_t m0 = int64_t(blockIdx.x) * BM, n0 = int64_t(blockIdx.y) * BN;
+    // triangular output: a tile with no entry inside computes nothing
+    if (uplo == 1 && m0 - (n0 + BN - 1) > diag) return;
+    if (uplo == 2 && (m0 + BM - 1) - n0 < diag) return;
     T acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -125,6 +128,7 @@ __global__ void __launch_bounds__(NT)
         for (int i = 0; i < 4; ++i) {
             const int64_t gm = m0 + tx + 16 * i;
             if (gm >= M) continue;
+            if (uplo && (uplo == 1 ? gm - gn > diag : gm - gn < diag)) continue;
             T *cp = &C[gm + gn * ldc];
             T v = Ar::mul(alpha, acc[i][j]);
             if (!beta_zero) v = Ar::add(v, Ar::mul(beta, *cp));
@@ -134,12 +138,14 @@ __global__ void __launch_bounds__(NT)
 }
 
 template <typename T>
-__global__ void scale_kernel(int M, int N, T beta, T *__restrict__ C, int64_t ldc, int beta_zero) {
+__global__ void scale_kernel(int M, int N, T beta, T *__restrict__ C, int64_t ldc, int beta_zero,
+                             int uplo, int64_t diag) {
     using Ar = Arith<T>;
     const int64_t total = int64_t(M) * N;
     for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total;
          t += int64_t(gridDim.x) * blockDim.x) {
         const int64_t i = t % M, j = t / M;
+        if (uplo && (uplo == 1 ? i - j > diag : i - j < diag)) continue;
         T *cp = &C[i + j * ldc];
         *cp = beta_zero ? Ar::zero() : Ar::mul(beta, *cp);
     }
@@ -148,11 +154,12 @@ __global__ void scale_kernel(int M, int N, T beta, T *__restrict__ C, int64_t ld
 // C(i, j) += beta X(i, j): blockIdx.y strides over columns, threads over rows.
 template <typename T>
 __global__ void add_scaled_kernel(int M, int N, T beta, const T *__restrict__ X, int64_t ldx,
-                                  T *__restrict__ C, int64_t ldc) {
+                                  T *__restrict__ C, int64_t ldc, int uplo, int64_t diag) {
     using Ar = Arith<T>;
     for (int64_t j = blockIdx.y; j < N; j += gridDim.y)
         for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < M;
              i += int64_t(gridDim.x) * blockDim.x) {
+            if (uplo && (uplo == 1 ? i - j > diag : i - j < diag)) continue;
             T *cp = &C[i + j * ldc];
             *cp = Ar::add(*cp, Ar::mul(beta, X[i + j * ldx]));
         }
@@ -161,7 +168,8 @@ __global__ void add_scaled_kernel(int M, int N, T beta, const T *__restrict__ X,
 template <typename T> int launch_add_scaled_t(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s) {
     dim3 grid(unsigned(std::min<int64_t>(8, (g.M + 255) / 256)), unsigned(std::min<int64_t>(g.N, 65535)));
     add_scaled_kernel<T><<<grid, 256, 0, s>>>(int(g.M), int(g.N), from_cplx<T>(g.beta),
-                                              static_cast<const T *>(X), ldx, static_cast<T *>(g.C), g.ldc);
+                                              static_cast<const T *>(X), ldx, static_cast<T *>(g.C), g.ldc,
+                                              g.uplo, g.diag);
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;
@@ -173,7 +181,7 @@ template <typename T> int launch_simt_t(const Gemm &g, cudaStream_t s) {
     gemm_simt_kernel<T><<<grid, NT, 0, s>>>(
         g.ta, g.tb, int(g.M), int(g.N), int(g.K), from_cplx<T>(g.alpha),
         static_cast<const T *>(g.A), g.lda, static_cast<const T *>(g.B), g.ldb,
-        from_cplx<T>(g.beta), static_cast<T *>(g.C), g.ldc, g.beta_zero() ? 1 : 0, g.guard);
+        from_cplx<T>(g.beta), static_cast<T *>(g.C), g.ldc, g.beta_zero() ? 1 : 0, g.guard, g.uplo, g.diag);
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;
@@ -185,7 +193,8 @@ template <typename T> int launch_scale_t(const Gemm &g, cudaStream_t s) {
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;
     scale_kernel<T><<<blocks, 256, 0, s>>>(int(g.M), int(g.N), from_cplx<T>(g.beta),
-                                            static_cast<T *>(g.C), g.ldc, g.beta_zero() ? 1 : 0);
+                                            static_cast<T *>(g.C), g.ldc, g.beta_zero() ? 1 : 0, g.uplo,
+                                            g.diag);
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;

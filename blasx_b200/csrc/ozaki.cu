@@ -589,7 +589,13 @@ struct ReconArgs {
     void *C;
     int64_t ldc;
     int64_t j0;  // first column of this launch
+    int uplo;    // triangular output: 0 all, 1 i - j <= diag, 2 i - j >= diag
+    int64_t diag;
 };
+
+__device__ __forceinline__ bool recon_keep(const ReconArgs &a, int64_t i, int64_t j) {
+    return a.uplo == 0 || (a.uplo == 1 ? i - j <= a.diag : i - j >= a.diag);
+}
 
 template <typename T, int N>
 __device__ __forceinline__ void recon_real(const ReconArgs &a, int64_t i0, int64_t j) {
@@ -601,6 +607,7 @@ __device__ __forceinline__ void recon_real(const ReconArgs &a, int64_t i0, int64
     for (int q = 0; q < 4; ++q) {
         const int64_t i = i0 + q;
         if (i >= a.M) break;
+        if (!recon_keep(a, i, j)) continue;
         uint32_t u[N];
         unpack<N>(w, q, u);
         const double val = crt_to_double<N>(u, -(a.ea[i] + fj));
@@ -625,6 +632,7 @@ __device__ __forceinline__ void recon_cplx(const ReconArgs &a, int64_t i0, int64
     for (int q = 0; q < 4; ++q) {
         const int64_t i = i0 + q;
         if (i >= a.M) break;
+        if (!recon_keep(a, i, j)) continue;
         uint32_t u[N];
         const int sc = -(a.ea[i] + fj);
         unpack<N>(wr, q, u);
@@ -749,8 +757,16 @@ int forced_moduli() {
 // Padded extents and scratch size of one emulated GEMM.
 struct Plan {
     int64_t M, N, K, Kh, Kp, Kc, Ip, Jp, Jx;
+    bool alias;  // op(B) = op(A)^T on the same buffer (SYRK): X is Y, sliced once
     size_t bytes;
 };
+
+// op(B) = op(A)^T read from the same buffer (real types): the rows of op(A)
+// are the columns of op(B), so their statistics, exponents and slices agree.
+bool aliased(const Gemm &g) {
+    return g.dt != DType::C128 && g.A == g.B && g.lda == g.ldb && g.M == g.N &&
+           (g.ta == NoTrans) != (g.tb == NoTrans);
+}
 
 Plan make_plan(const Gemm &g) {
     const bool cplx = g.dt == DType::C128;
@@ -761,11 +777,12 @@ Plan make_plan(const Gemm &g) {
     p.Kp = cplx ? 2 * p.Kh : oz::pad(p.K, oz::kTileK);
     p.Kc = cplx ? p.Kh : p.Kp;  // k extent covered by the slice kernels
     p.Ip = oz::pad(p.M, oz::kTileI);
-    p.Jp = oz::pad(p.N, oz::kTileJ);
+    p.alias = aliased(g);
+    p.Jp = p.alias ? p.Ip : oz::pad(p.N, oz::kTileJ);
     p.Jx = cplx ? 2 * p.Jp : p.Jp;  // X rows (Re block + Im block)
     p.bytes = 256 * 16 + (3 * sizeof(double) + 2 * sizeof(int)) * size_t(p.M + p.N) +
               sizeof(oz::Decision) + sizeof(int) + size_t(L) * p.Ip * p.Kp +
-              size_t(L) * p.Jx * p.Kp + size_t(L) * p.Jx * p.Ip;
+              (p.alias ? 0 : size_t(L) * p.Jx * p.Kp) + size_t(L) * p.Jx * p.Ip;
     return p;
 }
 
@@ -789,7 +806,7 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
     oz::RowStats sb{cv.take<double>(N), cv.take<double>(N), cv.take<double>(N), cv.take<int>(N)};
     int *ea = cv.take<int>(M), *fb = cv.take<int>(N);
     int8_t *Y = cv.take<int8_t>(size_t(L) * Ip * Kp);
-    int8_t *X = cv.take<int8_t>(size_t(L) * Jx * Kp);
+    int8_t *X = pl.alias ? Y : cv.take<int8_t>(size_t(L) * Jx * Kp);
     uint8_t *U = cv.take<uint8_t>(size_t(L) * Jx * Ip);
     const size_t stats_bytes = reinterpret_cast<char *>(ea) - reinterpret_cast<char *>(sa.amax);
     cudaEvent_t ev0 = prof::mark(s);
@@ -801,9 +818,11 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
     oz::View vb{g.B, g.ldb, N, K, g.tb == ConjT};
     const bool akc = g.ta != NoTrans, bkc = g.tb == NoTrans;
     BX_TRY(launch_stats<T>(va, akc, sa, s));
-    BX_TRY(launch_stats<T>(vb, bkc, sb, s));
+    if (!pl.alias) BX_TRY(launch_stats<T>(vb, bkc, sb, s));
+    const oz::RowStats sbd = pl.alias ? sa : sb;  // aliased: the columns of op(B) are the rows of op(A)
+    int *fbd = pl.alias ? ea : fb;
     const double unit = std::is_same<T, float>::value ? std::ldexp(1.0, -24) : std::ldexp(1.0, -53);
-    oz::decide_kernel<<<1, 1024, 0, s>>>(sa, M, sb, N, K, unit, mode, forced_moduli(), dec);
+    oz::decide_kernel<<<1, 1024, 0, s>>>(sa, M, sbd, N, K, unit, mode, forced_moduli(), dec);
     BX_CUDA(cudaGetLastError());
     count_launch();
 
@@ -814,7 +833,7 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         BX_TRY((launch_slice<T, 2>(vb, bkc, sb, dec, fb, ox, Kc, s)));
     } else {
         BX_TRY((launch_slice<T, 0>(va, akc, sa, dec, ea, oy, Kc, s)));
-        BX_TRY((launch_slice<T, 0>(vb, bkc, sb, dec, fb, ox, Kc, s)));
+        if (!pl.alias) BX_TRY((launch_slice<T, 0>(vb, bkc, sb, dec, fb, ox, Kc, s)));
     }
     // residue GEMMs and reconstruction, in column panels of C when asked.
     // (Running a panel's reconstruction on a second stream beside the next
@@ -827,10 +846,11 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         const int64_t tj0 = tiles_j * pnl / panels, tj1 = tiles_j * (pnl + 1) / panels;
         const int64_t j0 = tj0 * oz::kTileJ, j1 = std::min<int64_t>(N, tj1 * oz::kTileJ);
         if (panels == 1) {
-            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s, 0, -1, g.max_cta_tiles));
+            BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s, 0, -1, g.max_cta_tiles,
+                                           g.uplo, g.diag, Jp));
         } else {
             BX_TRY(oz::launch_residue_gemm(X, Y, U, Jx, Ip, Kp, dec, err, num_sms, s, tj0, tj1 - tj0,
-                                           g.max_cta_tiles));
+                                           g.max_cta_tiles, g.uplo, g.diag, Jp));
         }
         if (pnl == 0) ev2 = prof::mark(s);
         if (hooks && hooks->before_reconstruct && j1 > j0)
@@ -839,8 +859,8 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         for (int64_t c0 = j0; c0 < j1; c0 += 65535) {
             const int64_t c1 = std::min<int64_t>(j1, c0 + 65535);
             dim3 rgrid(unsigned((M + 4 * 128 - 1) / (4 * 128)), unsigned(c1 - c0));
-            oz::ReconArgs ra{U, Jp, Ip, M, N, ea, fb, g.alpha.re, g.alpha.im, g.beta.re, g.beta.im,
-                             g.beta_zero() ? 1 : 0, g.C, g.ldc, c0};
+            oz::ReconArgs ra{U, Jp, Ip, M, N, ea, fbd, g.alpha.re, g.alpha.im, g.beta.re, g.beta.im,
+                             g.beta_zero() ? 1 : 0, g.C, g.ldc, c0, g.uplo, g.diag};
             oz::reconstruct_kernel<T, CPLX><<<rgrid, 128, 0, s>>>(ra, dec);
             BX_CUDA(cudaGetLastError());
             count_launch();
@@ -853,6 +873,7 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
             gp.B = static_cast<const char *>(g.B) +
                    (g.tb == NoTrans ? j0 * g.ldb : j0) * int64_t(elem_size(g.dt));
             gp.C = static_cast<char *>(g.C) + j0 * g.ldc * int64_t(elem_size(g.dt));
+            gp.diag = g.diag + j0;
             gp.guard = &dec->nmod;
             if (g.dt == DType::F32) BX_TRY(launch_gemm_simt(gp, s));
             else BX_TRY(launch_gemm_dmma(gp, s));

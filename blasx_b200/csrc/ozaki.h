@@ -64,11 +64,14 @@ struct RowStats {
 // tj_begin / tj_count: the range of 128-row X tiles (columns of C) to
 // compute; tj_count < 0 covers all of them. max_cta_tiles > 0 bounds the
 // tiles one CTA computes (more CTAs than SMs, each retiring after a few
-// milliseconds); 0 launches one persistent CTA per SM.
+// milliseconds); 0 launches one persistent CTA per SM. uplo / diag: only C
+// tiles with an entry inside the triangle are computed (row - col <= diag
+// for uplo 1, >= diag for 2); jblock: rows of X per column block (Jp for
+// real types, half of the stacked complex X).
 int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
                         int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
                         cudaStream_t s, int64_t tj_begin = 0, int64_t tj_count = -1,
-                        int max_cta_tiles = 0);
+                        int max_cta_tiles = 0, int uplo = 0, int64_t diag = 0, int64_t jblock = 0);
 
 // Host-side CRT constant tables (uploaded once to constant memory).
 int upload_crt_tables();

@@ -52,6 +52,9 @@ struct TcArgs {
     const Decision *dec;
     int *err;
     int tj0, tjn;  // range of j-tiles (128 columns of C each) this launch covers
+    int uplo;      // triangular output: 0 all, 1 row - col <= diag, 2 row - col >= diag
+    int jtiles;    // j-tiles per column block of X (complex X stacks two blocks)
+    int64_t diag;
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
@@ -179,6 +182,15 @@ __device__ __forceinline__ TileCoord decode(int64_t tile, int tiles_j, int tiles
     return c;
 }
 
+// Triangular output: whether the C tile (rows ti*256.., columns tj*128..) has
+// an entry inside the triangle. Every role of the kernel skips the same tiles.
+__device__ __forceinline__ bool tile_needed(const TileCoord &c, const TcArgs &a) {
+    if (a.uplo == 0) return true;
+    const int64_t r0 = int64_t(c.ti) * kTileI, c0 = int64_t(c.tj % a.jtiles) * kTileJ;
+    if (a.uplo == 1) return r0 - (c0 + kTileJ - 1) <= a.diag;
+    return (r0 + kTileI - 1) - c0 >= a.diag;
+}
+
 __global__ void __launch_bounds__(kThreadsTC, 1)
     residue_gemm_kernel(const __grid_constant__ CUtensorMap mapX,
                         const __grid_constant__ CUtensorMap mapY, const TcArgs a) {
@@ -233,6 +245,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
                 const TileCoord c = decode(tile, tiles_j, tiles_i, a.tj0);
+                if (!tile_needed(c, a)) continue;
                 for (int kb = 0; kb < num_kb; ++kb) {
                     if (!mbar_wait(empty0 + 8 * stage, phase ^ 1, abort_flag)) { ok = false; break; }
                     const uint32_t fb = full0 + 8 * stage;
@@ -263,6 +276,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             uint32_t acc_phase = 0;
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
+                if (!tile_needed(decode(tile, tiles_j, tiles_i, a.tj0), a)) continue;
                 if (!mbar_wait(tempty0 + 8 * acc, acc_phase ^ 1, abort_flag)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t d = tmem + uint32_t(acc * kAccCols);
@@ -297,6 +311,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         uint32_t acc_phase = 0;
         for (int64_t tile = blockIdx.x; tile < total; tile += gridDim.x) {
             const TileCoord c = decode(tile, tiles_j, tiles_i, a.tj0);
+            if (!tile_needed(c, a)) continue;
             const int32_t m = c_mod[c.l];
             const float inv_m = 1.0f / float(m);
             if (!mbar_wait(tfull0 + 8 * acc, acc_phase, abort_flag)) {
@@ -380,7 +395,8 @@ int prepare_residue_gemm_current_device() {
 
 int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp, int64_t Ip,
                         int64_t Kp, const Decision *dec, int *err_flag, int num_sms,
-                        cudaStream_t s, int64_t tj_begin, int64_t tj_count, int max_cta_tiles) {
+                        cudaStream_t s, int64_t tj_begin, int64_t tj_count, int max_cta_tiles, int uplo,
+                        int64_t diag, int64_t jblock) {
     if (Jp % kTileJ || Ip % kTileI || Kp % kTileK || Kp > int64_t(kMaxK) * 2)
         return set_error(BLASX_ERR_UNSUPPORTED, "residue GEMM: bad padded extents");
     static std::once_flag once;
@@ -401,7 +417,10 @@ int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp
     }
     if (tj_begin < 0 || tj_begin + tj_count > Jp / kTileJ)
         return set_error(BLASX_ERR_ARG, "residue GEMM: j-tile range out of bounds");
-    TcArgs a{Jp, Ip, Kp, U, dec, err_flag, int(tj_begin), int(tj_count)};
+    if (uplo && (jblock <= 0 || jblock % kTileJ || Jp % jblock))
+        return set_error(BLASX_ERR_ARG, "residue GEMM: bad column block for a triangular output");
+    TcArgs a{Jp, Ip, Kp, U, dec, err_flag, int(tj_begin), int(tj_count), uplo,
+             uplo ? int(jblock / kTileJ) : 1, diag};
     const int64_t tiles_upper = int64_t(kMaxModuli) * tj_count * (Ip / kTileI);
     if (tiles_upper == 0) return BLASX_OK;
     int64_t grid = tiles_upper < num_sms ? tiles_upper : num_sms;

@@ -46,6 +46,12 @@ struct Gemm {
     // persistent CTA per SM). A bound makes its CTAs retire every few
     // milliseconds, so that kernels of other streams get SMs in between.
     int max_cta_tiles = 0;
+    // Triangular output (SYRK): 0 every entry of C; 1 (upper) only entries
+    // with row - col <= diag; 2 (lower) only entries with row - col >= diag.
+    // Row and column are this GEMM's own C coordinates; diag shifts the
+    // diagonal for a block of a larger C. Entries outside are not touched.
+    int uplo = 0;
+    int64_t diag = 0;
 
     bool alpha_zero() const { return alpha.re == 0 && alpha.im == 0; }
     bool beta_zero() const { return beta.re == 0 && beta.im == 0; }
@@ -55,6 +61,10 @@ struct Gemm {
     int64_t cols_a() const { return ta == NoTrans ? K : M; }
     int64_t rows_b() const { return tb == NoTrans ? K : N; }
     int64_t cols_b() const { return tb == NoTrans ? N : K; }
+    // whether C entry (r, c) is written
+    __host__ __device__ bool in_tri(int64_t r, int64_t c) const {
+        return uplo == 0 || (uplo == 1 ? r - c <= diag : r - c >= diag);
+    }
     double flops() const {
         return (dt == DType::C128 ? 8.0 : 2.0) * double(M) * double(N) * double(K);
     }

@@ -308,6 +308,15 @@ template <typename Pred> int evict_lru(Server &s, Pred over) {
     return n;
 }
 
+// The emulated scratch for g when its device A and B are separate buffers
+// (the loop copies B on its own, or takes it from the operand cache, even
+// when the caller passed the same host buffer twice, as SYRK does).
+size_t scratch_bytes_separate_b(const Gemm &g) {
+    Gemm probe = g;
+    probe.B = nullptr;
+    return ozaki_scratch_bytes(probe);
+}
+
 // Takes a request's device blocks from the arena: A, B (unless a cached copy
 // is used), C and the emulated path's scratch, evicting unused cached
 // operands (least recently used first) while a block does not fit. Returns
@@ -323,7 +332,7 @@ bool reserve(Server &s, Request *r, bool need_b) {
     const size_t bytes[4] = {need_ab ? size_t(r->lda) * g.cols_a() * es : 0,
                              need_ab && need_b ? size_t(r->ldb) * g.cols_b() * es : 0,
                              size_t(r->ldc) * g.N * es,
-                             need_ab && r->emulated ? ozaki_scratch_bytes(g) : 0};
+                             need_ab && r->emulated ? scratch_bytes_separate_b(g) : 0};
     for (int k = 0; k < 4; ++k) {
         if (!bytes[k]) continue;
         void *p = s.arena.alloc(bytes[k]);
@@ -363,7 +372,7 @@ int admit(Server &s, Request *r, int slot) {
     cudaStream_t st = s.streams[size_t(slot)];
     r->stream_slot = slot;
     const bool need_ab = !(g.alpha_zero() || g.K == 0);
-    const bool read_c = !g.beta_zero();
+    const bool read_c = !g.beta_zero() || g.uplo != 0;  // a triangular output keeps the rest of C
     BX_CUDA(cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming));
     BX_CUDA(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
     if (need_ab) {
@@ -690,7 +699,8 @@ int submit(const Gemm &g) {
     // small native requests are mixed into grouped launches
     r->flops = 0;
     r->emulated = need_ab && ozaki_selected(g, config().dgemm_mode.load());
-    r->grouped = need_ab && !r->emulated && g.dt != DType::F32 && g.flops() <= s->group_flops;
+    r->grouped = need_ab && !r->emulated && g.dt != DType::F32 && g.uplo == 0 &&
+                 g.flops() <= s->group_flops;
     if (need_ab) {
         r->bkey = Key{g.B, g.ldb, g.rows_b(), g.cols_b(), int(g.dt),
                       fingerprint(g.B, g.ldb, g.rows_b(), g.cols_b(), es)};

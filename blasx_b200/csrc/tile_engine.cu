@@ -165,22 +165,37 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
         return BLASX_OK;
     };
 
+    // triangular output: C tiles with no entry inside the triangle are
+    // skipped (no C copies, no compute); the others compute with the
+    // diagonal shifted to the tile's origin
+    auto c_needed = [&](const TileStep &s) {
+        if (g.uplo == 0) return true;
+        const int64_t i0 = int64_t(s.i) * T, j0 = int64_t(s.j) * T;
+        const int64_t m = ext(s.i, g.M), n = ext(s.j, g.N);
+        return g.uplo == 1 ? i0 - (j0 + n - 1) <= g.diag : (i0 + m - 1) - j0 >= g.diag;
+    };
+    size_t last_needed = 0;
+    for (size_t i = 0; i < plan.steps.size(); ++i)
+        if (c_needed(plan.steps[i])) last_needed = i + 1;
     int ctile = -1;
     size_t step_no = 0;
+    bool first_emulated = true;
     for (const TileStep &s : plan.steps) {
         ++step_no;
         if (s.a.load) BX_TRY(load_tile(s.a, s));
         if (s.b.load) BX_TRY(load_tile(s.b, s));
         const int64_t m = ext(s.i, g.M), n = ext(s.j, g.N), k = ext(s.k, g.K);
+        const bool needed = c_needed(s);
+        if (s.first_k) ++ctile;
+        if (!needed) continue;
         if (s.first_k) {
-            ++ctile;
             const int cs = ctile % kCSlots;
             if (c_used[cs]) {  // previous occupant written back before reuse
                 BX_CUDA(cudaStreamWaitEvent(c->h2d, c_out[cs], 0));
                 BX_CUDA(cudaStreamWaitEvent(c->compute, c_out[cs], 0));
             }
             c_used[cs] = true;
-            if (!g.beta_zero()) {
+            if (!g.beta_zero() || g.uplo != 0) {  // a triangular tile keeps its other entries
                 char *src = hC + (int64_t(s.i) * T + int64_t(s.j) * T * g.ldc) * int64_t(es);
                 BX_CUDA(cudaMemcpy2DAsync(c_ptr(cs), size_t(T) * es, src, size_t(g.ldc) * es,
                                           size_t(m) * es, size_t(n), cudaMemcpyHostToDevice, c->h2d));
@@ -199,10 +214,12 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
         d.C = c_ptr(cs); d.ldc = T;
         if (!s.first_k) d.beta = cplx{1.0, 0.0};
         d.guard = nullptr;
-        if (ws)
-            BX_TRY(ozaki_gemm_step(d, c->compute, mode, ws, c->num_sms, step_no == 1,
-                                   step_no == plan.steps.size()));
-        else
+        d.diag = g.diag + (int64_t(s.j) - int64_t(s.i)) * T;
+        if (ws) {
+            BX_TRY(ozaki_gemm_step(d, c->compute, mode, ws, c->num_sms, first_emulated,
+                                   step_no == last_needed));
+            first_emulated = false;
+        } else
             BX_TRY(dmma_supported(d) ? launch_gemm_dmma(d, c->compute) : launch_gemm_simt(d, c->compute));
         BX_CUDA(cudaEventRecord(lastuse[size_t(s.a.slot)], c->compute));
         BX_CUDA(cudaEventRecord(lastuse[size_t(s.b.slot)], c->compute));

@@ -33,6 +33,7 @@ extern "C" {
 #define CBLAS_ENUM_DEFINED_H
 enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
 enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 };
+enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 };
 #endif
 
 /* ------------------------------------------------------------------------ */
@@ -67,6 +68,53 @@ void dgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, d
             int *lda, double *B, int *ldb, double *beta, double *C, int *ldc);
 void zgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, double *A,
             int *lda, double *B, int *ldb, double *beta, double *C, int *ldc);
+
+/* Replace cblas_ssyrk / cblas_dsyrk / cblas_zsyrk (include/cblas.h:434,464,524;
+ * implementations blas/ssyrk.c, blas/dsyrk.c:15-77, blas/zsyrk.c, which always
+ * run on the host BLAS): C = alpha op(A) op(A)^T + beta C on the uplo
+ * triangle only, on the GPU. ConjTrans is Trans for the real routines and
+ * illegal (info 2) for ZSYRK. */
+void cblas_ssyrk(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                 const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const float alpha,
+                 const float *A, const int lda, const float beta, float *C, const int ldc);
+void cblas_dsyrk(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                 const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const double alpha,
+                 const double *A, const int lda, const double beta, double *C, const int ldc);
+void cblas_zsyrk(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                 const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const void *alpha,
+                 const void *A, const int lda, const void *beta, void *C, const int ldc);
+
+/* Replace cblas_ssyr2k / cblas_dsyr2k / cblas_zsyr2k (include/cblas.h:468;
+ * implementations blas/dsyr2k.c:16-86 and siblings, host BLAS only):
+ * C = alpha op(A) op(B)^T + alpha op(B) op(A)^T + beta C on the uplo triangle. */
+void cblas_ssyr2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                  const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const float alpha,
+                  const float *A, const int lda, const float *B, const int ldb, const float beta,
+                  float *C, const int ldc);
+void cblas_dsyr2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                  const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const double alpha,
+                  const double *A, const int lda, const double *B, const int ldb, const double beta,
+                  double *C, const int ldc);
+void cblas_zsyr2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                  const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const void *alpha,
+                  const void *A, const int lda, const void *B, const int ldb, const void *beta,
+                  void *C, const int ldc);
+
+/* Replace the F77 wrappers ssyrk_ / dsyrk_ (blas/dsyrk.c:80-101) / zsyrk_ and
+ * ssyr2k_ / dsyr2k_ (blas/dsyr2k.c:88-) / zsyr2k_: uplo 'U'/'L', trans
+ * 'N'/'T'/'C', column-major, every argument by pointer. */
+void ssyrk_(char *uplo, char *trans, int *n, int *k, float *alpha, float *A, int *lda,
+            float *beta, float *C, int *ldc);
+void dsyrk_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda,
+            double *beta, double *C, int *ldc);
+void zsyrk_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda,
+            double *beta, double *C, int *ldc);
+void ssyr2k_(char *uplo, char *trans, int *n, int *k, float *alpha, float *A, int *lda, float *B,
+             int *ldb, float *beta, float *C, int *ldc);
+void dsyr2k_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda,
+             double *B, int *ldb, double *beta, double *C, int *ldc);
+void zsyr2k_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda,
+             double *B, int *ldb, double *beta, double *C, int *ldc);
 
 /* Replaces xerbla_, blas/error.c:5: prints
  * " ** On entry to <NAME> parameter number <info> had an illegal value".
@@ -153,6 +201,13 @@ int blasx_tile_plan(long long M, long long N, long long K, long long tile,
 int blasx_dgemm_device(int transa, int transb, int M, int N, int K, double alpha,
                        const double *A, int lda, const double *B, int ldb, double beta,
                        double *C, int ldc, void *stream);
+
+/* Device-resident DSYRK (column-major, uplo CblasUpper/CblasLower, trans
+ * CblasNoTrans/CblasTrans): C = alpha op(A) op(A)^T + beta C on the uplo
+ * triangle of the device matrix C, enqueued on `stream`; returns a status.
+ * No counterpart in the reference. */
+int blasx_dsyrk_device(int uplo, int trans, int N, int K, double alpha, const double *A, int lda,
+                       double beta, double *C, int ldc, void *stream);
 int blasx_sgemm_device(int transa, int transb, int M, int N, int K, float alpha,
                        const float *A, int lda, const float *B, int ldb, float beta, float *C,
                        int ldc, void *stream);

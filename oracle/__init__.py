@@ -140,6 +140,31 @@ def gemm_tiled(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, blo
     return C
 
 
+def tri_mask(uplo: str, N: int) -> np.ndarray:
+    """Boolean N x N mask of the entries ?SYRK / ?SYR2K update ('U': i <= j)."""
+    i, j = np.indices((N, N))
+    return i <= j if uplo == "U" else i >= j
+
+
+def syrk(uplo, trans, N, K, alpha, A, lda, beta, C, ldc, B=None, ldb=None):
+    """Restatement of BLAS ?SYRK (B None) and ?SYR2K, the operations the
+    reference hands to its CPU BLAS (blas/dsyrk.c:60-66, blas/dsyr2k.c:61-70):
+    C <- alpha op(A) op(A)^T + beta C, or alpha op(A) op(B)^T + alpha op(B)
+    op(A)^T + beta C, on the uplo triangle only; op(X) = X (trans 'N') or X^T.
+    Computed as tiled GEMMs on a copy of C whose triangle is copied back."""
+    ta, tb = ("N", "T") if trans == "N" else ("T", "N")
+    full = C.copy(order="F")
+    if B is None:
+        gemm_tiled(ta, tb, N, N, K, alpha, A, lda, A, lda, beta, full, ldc)
+    else:
+        gemm_tiled(ta, tb, N, N, K, alpha, A, lda, B, ldb, beta, full, ldc)
+        gemm_tiled(ta, tb, N, N, K, alpha, B, ldb, A, lda, 1.0, full, ldc)
+    m = tri_mask(uplo, N)
+    view, fv = C[:N, :N], full[:N, :N]
+    view[m] = fv[m]
+    return C
+
+
 def dd_entries(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, ii, jj):
     """Double-double values of sampled entries of alpha*op(A)op(B)+beta*C0.
 

@@ -7,6 +7,7 @@
 #define CBLAS_H
 enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
 enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 };
+enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 };
 #endif
 #include "blasx_b200.h"
 
@@ -22,6 +23,9 @@ int main(void) {
     int m = 4, n = 4, k = 4, ld = 4;
     double al = 1.0, be = 0.0;
     dgemm_(&ta, &tb, &m, &n, &k, &al, A, &ld, B, &ld, &be, C, &ld);
+    fflush(stdout);
+    /* DSYRK: ldc = 2 < N = 4: parameter 10 */
+    cblas_dsyrk(CblasColMajor, CblasUpper, CblasNoTrans, 4, 4, 1.0, A, 4, 0.0, C, 2);
     fflush(stdout);
     /* M = 0: quick return, no device needed */
     cblas_dgemm(CblasColMajor, CblasNoTrans, CblasNoTrans, 0, 4, 4, 1.0, A, 4, B, 4, 0.0, C, 4);

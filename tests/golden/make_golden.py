@@ -10,6 +10,11 @@ Also recorded: the exact xerbla_ lines the reference prints for each illegal
 argument (blas/dgemm.c:46-57, blas/error.c:5-8) and for the F77 wrappers
 (blas/dgemm.c:131-154).
 
+SYRK and SYR2K: the reference runs cblas_?syrk / cblas_?syr2k on its CPU BLAS
+for every size (blas/dsyrk.c:36-39, blas/dsyr2k.c); their outputs and the
+reference's xerbla_ lines for each illegal argument (blas/dsyrk.c:27-37,
+blas/dsyr2k.c:43-52, the F77 wrappers blas/dsyrk.c:80-101) are recorded too.
+
 Run in a container that has the reference tree:  python tests/golden/make_golden.py
 """
 import ctypes
@@ -99,6 +104,55 @@ def main():
         rec[key + "_meta"] = np.array([M, N, K, M, max(K, 1), M, ord("N"), ord("N")], dtype=np.int64)
         rec[key + "_scal"] = np.array([al, be], dtype=np.complex128)
         rec[key + "_A"] = A; rec[key + "_B"] = B; rec[key + "_C0"] = C0; rec[key + "_C"] = C
+    # SYRK / SYR2K outputs of the reference (its CPU BLAS path)
+    I, D, P = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    L = ref.L
+    L.cblas_dsyrk.argtypes = [I] * 5 + [D, P, I, D, P, I]
+    L.cblas_ssyrk.argtypes = [I] * 5 + [ctypes.c_float, P, I, ctypes.c_float, P, I]
+    L.cblas_zsyrk.argtypes = [I] * 5 + [P, P, I, P, P, I]
+    L.cblas_dsyr2k.argtypes = [I] * 5 + [D, P, I, P, I, D, P, I]
+    ns = 0
+    for tag, dt in (("d", np.float64), ("s", np.float32), ("z", np.complex128)):
+        for (N, K) in [(1, 1), (7, 3), (33, 65), (64, 17)]:
+            for uplo in (121, 122):
+                for trans in (111, 112):
+                    seed = 5000 + ns
+                    ra, ca = (N, K) if trans == 111 else (K, N)
+                    lda, ldc = ra + (ns % 2), N + (ns % 3)
+                    A = oracle.uniform((lda, ca), dt, seed)
+                    C = oracle.uniform((ldc, N), dt, seed + 1)
+                    C0 = C.copy(order="F")
+                    al, be = (1.5, -0.25) if tag != "z" else (complex(1.5, -0.5), complex(-0.25, 0.75))
+                    if tag == "d":
+                        L.cblas_dsyrk(102, uplo, trans, N, K, al, A.ctypes.data, lda, be, C.ctypes.data, ldc)
+                    elif tag == "s":
+                        L.cblas_ssyrk(102, uplo, trans, N, K, al, A.ctypes.data, lda, be, C.ctypes.data, ldc)
+                    else:
+                        pa = np.array([al.real, al.imag]); pb = np.array([be.real, be.imag])
+                        L.cblas_zsyrk(102, uplo, trans, N, K, pa.ctypes.data, A.ctypes.data, lda, pb.ctypes.data,
+                                      C.ctypes.data, ldc)
+                    key = f"syrk_{tag}_{ns}"
+                    rec[key + "_meta"] = np.array([N, K, uplo, trans, lda, ldc, seed], dtype=np.int64)
+                    rec[key + "_scal"] = np.array([al, be], dtype=np.complex128)
+                    rec[key + "_sum"] = np.array([np.sum(A), np.sum(C0)], dtype=np.complex128)
+                    rec[key + "_C"] = C
+                    ns += 1
+    for (N, K) in [(7, 3), (33, 65)]:
+        for uplo in (121, 122):
+            for trans in (111, 112):
+                seed = 6000 + ns
+                ra, ca = (N, K) if trans == 111 else (K, N)
+                A = oracle.uniform((ra, ca), np.float64, seed)
+                B = oracle.uniform((ra, ca), np.float64, seed + 1)
+                C = oracle.uniform((N, N), np.float64, seed + 2)
+                C0 = C.copy(order="F")
+                L.cblas_dsyr2k(102, uplo, trans, N, K, 1.5, A.ctypes.data, ra, B.ctypes.data, ra, -0.25,
+                               C.ctypes.data, N)
+                key = f"syr2k_d_{ns}"
+                rec[key + "_meta"] = np.array([N, K, uplo, trans, ra, N, seed], dtype=np.int64)
+                rec[key + "_sum"] = np.array([np.sum(A), np.sum(B), np.sum(C0)], dtype=np.complex128)
+                rec[key + "_C"] = C
+                ns += 1
     # xerbla lines for every info code of cblas_dgemm and the F77 wrapper
     A = np.zeros((4, 4)); B = np.zeros((4, 4)); C = np.ones((4, 4), order="F")
     bad = {
@@ -130,9 +184,34 @@ def main():
                                                   ctypes.byref(ld), ctypes.byref(be), Cz.ctypes.data,
                                                   ctypes.byref(ld)))
         lines.append(f"dgemm_{ta.decode()}{tb.decode()}|-|{out}")
+    # SYRK / SYR2K argument errors
+    Cs = np.ones((4, 4), order="F")
+    for info, kw in {1: dict(uplo=999), 2: dict(trans=999), 3: dict(N=-1), 4: dict(K=-1), 7: dict(lda=2),
+                     10: dict(ldc=2)}.items():
+        a = dict(uplo=121, trans=111, N=4, K=4, lda=4, ldc=4)
+        a.update(kw)
+        out = capture_stdout(lambda: L.cblas_dsyrk(102, a["uplo"], a["trans"], a["N"], a["K"], 1.0, A.ctypes.data,
+                                                   a["lda"], 0.0, Cs.ctypes.data, a["ldc"]))
+        lines.append(f"cblas_dsyrk|{info}|{out}")
+    for info, kw in {7: dict(lda=2), 9: dict(ldb=2), 12: dict(ldc=2)}.items():
+        a = dict(lda=4, ldb=4, ldc=4)
+        a.update(kw)
+        out = capture_stdout(lambda: L.cblas_dsyr2k(102, 121, 111, 4, 4, 1.0, A.ctypes.data, a["lda"], B.ctypes.data,
+                                                    a["ldb"], 0.0, Cs.ctypes.data, a["ldc"]))
+        lines.append(f"cblas_dsyr2k|{info}|{out}")
+    L.dsyrk_.argtypes = [P] * 10
+    for up, tr in [(b"X", b"N"), (b"U", b"Q"), (b"X", b"Q")]:
+        nn = ctypes.c_int(4); ld = ctypes.c_int(4)
+        al = ctypes.c_double(1.0); be = ctypes.c_double(0.0)
+        cu = ctypes.c_char(up); ct = ctypes.c_char(tr)
+        out = capture_stdout(lambda: L.dsyrk_(ctypes.byref(cu), ctypes.byref(ct), ctypes.byref(nn), ctypes.byref(nn),
+                                              ctypes.byref(al), A.ctypes.data, ctypes.byref(ld), ctypes.byref(be),
+                                              Cs.ctypes.data, ctypes.byref(ld)))
+        lines.append(f"dsyrk_{up.decode()}{tr.decode()}|-|{out}")
+    assert np.all(Cs == 1.0), "C must be untouched on argument errors"
     rec["xerbla"] = np.array(lines)
     np.savez_compressed(OUT, **rec)
-    print(f"wrote {OUT}: {n} cases + 3 edge cases + {len(lines)} xerbla lines")
+    print(f"wrote {OUT}: {n} GEMM cases + 3 edge cases + {ns} SYRK/SYR2K cases + {len(lines)} xerbla lines")
 
 
 if __name__ == "__main__":

@@ -1,4 +1,6 @@
 """Helpers that rebuild the golden cases (inputs from their seeds)."""
+import re
+
 import numpy as np
 
 import oracle
@@ -6,8 +8,12 @@ import oracle
 DT = {"d": np.float64, "s": np.float32, "z": np.complex128}
 
 
+GEMM_KEY = re.compile(r"^([dsz])_(\d+)_meta$")  # "<tag>_<n>_meta"; SYRK cases use their own prefixes
+
+
 def cases(golden, tags=("d", "s", "z")):
-    keys = sorted({k.rsplit("_", 1)[0] for k in golden.files if k.endswith("_meta") and k[0] in tags},
+    keys = sorted({k.rsplit("_", 1)[0] for k in golden.files
+                   if GEMM_KEY.match(k) and GEMM_KEY.match(k).group(1) in tags},
                   key=lambda s: (s[0], int(s.split("_")[1])))
     for key in keys:
         if key.startswith("edge"):

@@ -20,5 +20,6 @@ def test_c_program_links_and_reports(blx, tmp_path):
                          env=dict(os.environ, CUDA_VISIBLE_DEVICES="")).stdout
     assert " ** On entry to DGEMM  parameter number  8 had an illegal value\n" in out
     assert " ** On entry to DGEMM  parameter number  1 had an illegal value\n" in out
+    assert " ** On entry to DSYRK  parameter number 10 had an illegal value\n" in out
     assert "status=1" in out and "status=0 C0=1" in out
     assert "plan rc=0 loads=200 min_ratio=1.000" in out
