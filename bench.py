@@ -62,7 +62,7 @@ def parse():
                    help="--workload device: FP64, FP32 or complex128")
     p.add_argument("--rates", default="100,200,400",
                    help="--workload serving: offered Poisson rates (requests/s) to sweep")
-    p.add_argument("--workload", default="", choices=["", "c0", "ragged", "ooc", "c3", "serving", "device"],
+    p.add_argument("--workload", default="", choices=["", "c0", "ragged", "ooc", "c3", "serving", "device", "syrk"],
                    help="secondary measurements (one JSON line each) instead of the headline: ragged "
                         "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep, "
                         "the full serving stream (10,000 calls, dims to 16384), or a device-resident "
@@ -480,6 +480,58 @@ def run_workloads(args):
                       "h2d_bytes": st["h2d_bytes"], "d2h_bytes": st["d2h_bytes"],
                       "vs_openblas_max_ratio_to_2x_bound": ratio_ob, "openblas": ob.name,
                       "oracle_samples": args.samples, "bound_ratio": ratio, "max_normalised_error": err})
+    elif args.workload == "syrk":
+        # DSYRK C = A A^T + beta C (lower), N = K in {8192, 16384}: device-resident through
+        # blasx_dsyrk_device (emulated and native) and e2e through cblas_dsyrk on pinned host arrays;
+        # credited N^2 K flops (the triangle of the GEMM); accuracy on sampled lower-triangle entries
+        import oracle
+        for n in (8192, 16384):
+            tA, A = _host(torch, (n, n), "f64", 1)
+            tC, C0 = _host(torch, (n, n), "f64", 2)
+            dA = tA.cuda()
+            res = {}
+            for mode_name, mode in (("emulated", bx.MODE_OZAKI), ("native", bx.MODE_NATIVE)):
+                bx.set_dgemm_mode(mode)
+                dC = tC.cuda()
+                s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
+                call = lambda: bx.dsyrk_device("L", "N", n, n, 1.0, dA, n, 0.5, dC, n, stream=s)
+                assert call() == 0, bx.last_error()  # warm-up (C changes; only timing and path matter)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                for _ in range(2):
+                    assert call() == 0, bx.last_error()
+                e1.record(s); torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / 2
+                st = bx.call_stats()
+                # e2e on the host arrays, copies included; checked against the oracle
+                Ch = torch.empty_like(tC, pin_memory=True)
+                times = []
+                for _ in range(2):  # the first call also grows the device memory pool
+                    Ch.copy_(tC)
+                    t0 = time.perf_counter()
+                    bx.cblas_dsyrk(bx.CblasColMajor, bx.CblasLower, bx.CblasNoTrans, n, n, 1.0, tA.data_ptr(), n,
+                                   0.5, Ch.data_ptr(), n)
+                    times.append(time.perf_counter() - t0)
+                dt = times[-1]
+                assert bx.last_status() == 0, bx.last_error()
+                Cn = Ch.numpy().reshape(n, n).T  # column-major view
+                rng = np.random.default_rng(3)
+                ii = rng.integers(0, n, args.samples); jj = rng.integers(0, n, args.samples)
+                lo = ii >= jj
+                ii, jj = ii[lo], jj[lo]
+                val, bound = oracle.dd_entries("N", "T", n, n, n, 1.0, A, n, A, n, 0.5, C0, n, ii, jj)
+                ratio, err = oracle.componentwise_ratio(Cn, ii, jj, val, bound, n, np.float64)
+                res[mode_name] = {"tflops": float(n) ** 3 / (ms * 1e-3) / 1e12, "ms": ms, "path": st["path"],
+                                  "tflops_e2e": float(n) ** 3 / dt / 1e12, "seconds_e2e": dt,
+                                  "bound_ratio": ratio, "max_normalised_error": err}
+                del dC
+            bx.set_dgemm_mode(bx.MODE_AUTO)
+            lines.append({"workload": f"dsyrk lower NoTrans N=K={n}, beta 0.5, U[-1,1]", "flops_credited": "N^2 K",
+                          "samples_in_triangle": int(lo.sum()), **res,
+                          "speedup": res["emulated"]["tflops"] / res["native"]["tflops"]})
+            print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
+            del dA, tA, tC
     elif args.workload == "device":
         # device-resident n^3 NN calls through blasx_?gemm_device (for ncu captures of one kernel)
         n = args.size
