@@ -87,6 +87,7 @@ def lib() -> ctypes.CDLL:
         L.cblas_sgemm.argtypes = [_I] * 6 + [_F, _P, _I, _P, _I, _F, _P, _I]
         L.cblas_dgemm.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _D, _P, _I]
         L.cblas_zgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
+        L.cblas_cgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
         L.cblas_ssyrk.argtypes = [_I] * 5 + [_F, _P, _I, _F, _P, _I]
         L.cblas_dsyrk.argtypes = [_I] * 5 + [_D, _P, _I, _D, _P, _I]
         L.cblas_zsyrk.argtypes = [_I] * 5 + [_P, _P, _I, _P, _P, _I]
@@ -98,7 +99,7 @@ def lib() -> ctypes.CDLL:
         for f in ("ssyr2k_", "dsyr2k_", "zsyr2k_"):
             getattr(L, f).argtypes = [_P] * 12
         L.blasx_dsyrk_device.argtypes = [_I] * 4 + [_D, _P, _I, _D, _P, _I, _P]
-        for f in ("sgemm_", "dgemm_", "zgemm_"):
+        for f in ("sgemm_", "dgemm_", "cgemm_", "zgemm_"):
             getattr(L, f).argtypes = [_P] * 13
         L.xerbla_.argtypes = [ctypes.c_char_p, _P]
         L.blasx_last_status.restype = _I
@@ -110,6 +111,7 @@ def lib() -> ctypes.CDLL:
         L.blasx_dgemm_device.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_sgemm_device.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I, _P]
         L.blasx_zgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
+        L.blasx_cgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
         L.blasx_dgemm_device_noalloc.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_kernel_launch_count.restype = ctypes.c_uint64
         L.blasx_tile_plan.argtypes = [ctypes.c_longlong] * 5 + [_I, _I, ctypes.POINTER(TilePlanStats)]
@@ -245,6 +247,27 @@ def dsyrk_device(uplo, trans, N, K, alpha, A, lda, beta, C, ldc, stream=None):
     return lib().blasx_dsyrk_device(u, t, N, K, alpha, _addr(A), lda, beta, _addr(C), ldc, s)
 
 
+def _cpair32(v) -> np.ndarray:
+    v = complex(v)
+    return np.array([v.real, v.imag], dtype=np.float32)
+
+
+def cblas_cgemm(Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    al, be = _cpair32(alpha), _cpair32(beta)
+    lib().cblas_cgemm(Order, TransA, TransB, M, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb,
+                      be.ctypes.data, _addr(C), ldc)
+
+
+def cgemm_(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    ta = ctypes.c_char(transa.encode() if isinstance(transa, str) else transa)
+    tb = ctypes.c_char(transb.encode() if isinstance(transb, str) else transb)
+    ints = [ctypes.c_int(v) for v in (m, n, k, lda, ldb, ldc)]
+    al, be = _cpair32(alpha), _cpair32(beta)
+    r = ctypes.byref
+    lib().cgemm_(r(ta), r(tb), r(ints[0]), r(ints[1]), r(ints[2]), al.ctypes.data, _addr(A), r(ints[3]),
+                 _addr(B), r(ints[4]), be.ctypes.data, _addr(C), r(ints[5]))
+
+
 def _f77(fn, ctype, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cplx=False):
     ta = ctypes.c_char(transa.encode() if isinstance(transa, str) else transa)
     tb = ctypes.c_char(transb.encode() if isinstance(transb, str) else transb)
@@ -278,7 +301,8 @@ def gemm(transa, transb, alpha, A, B, beta, C):
     K = A.shape[1] if transa == "N" else A.shape[0]
     args = (CblasColMajor, TRANS[transa], TRANS[transb], M, N, K, alpha, A, max(1, A.shape[0]),
             B, max(1, B.shape[0]), beta, C, max(1, M))
-    {np.float32: cblas_sgemm, np.float64: cblas_dgemm, np.complex128: cblas_zgemm}[C.dtype.type](*args)
+    {np.float32: cblas_sgemm, np.float64: cblas_dgemm, np.complex64: cblas_cgemm,
+     np.complex128: cblas_zgemm}[C.dtype.type](*args)
     return C
 
 
@@ -298,6 +322,10 @@ def gemm_device(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, st
         return L.blasx_dgemm_device(ta, tb, M, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta, _addr(C), ldc, s)
     if dtype == "s":
         return L.blasx_sgemm_device(ta, tb, M, N, K, alpha, _addr(A), lda, _addr(B), ldb, beta, _addr(C), ldc, s)
+    if dtype == "c":
+        al, be = _cpair32(alpha), _cpair32(beta)
+        return L.blasx_cgemm_device(ta, tb, M, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb,
+                                    be.ctypes.data, _addr(C), ldc, s)
     al, be = _cpair(alpha), _cpair(beta)
     return L.blasx_zgemm_device(ta, tb, M, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb,
                                 be.ctypes.data, _addr(C), ldc, s)

@@ -16,7 +16,7 @@
 namespace bx {
 
 bool ozaki_selected(const Gemm &g, int mode) {
-    const int64_t kmax = g.dt == DType::C128 ? oz::kMaxK / 2 : oz::kMaxK;
+    const int64_t kmax = is_complex(g.dt) ? oz::kMaxK / 2 : oz::kMaxK;
     if (g.K > kmax || mode == 1) return false;
     if (mode == 2) return true;
     if (std::min(g.M, g.N) < 256) return false;
@@ -24,6 +24,7 @@ bool ozaki_selected(const Gemm &g, int mode) {
     switch (g.dt) {
         case DType::F64: return g.K >= 512 && work >= 6e9;
         case DType::F32: return g.K >= 256 && work >= 3e8;
+        case DType::C64: return g.K >= 256 && work >= 1.5e8;
         default: return g.K >= 256 && work >= 2e9;
     }
 }

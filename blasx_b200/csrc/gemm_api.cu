@@ -54,7 +54,7 @@ Gemm make_gemm(DType dt, int order, int ta, int tb, int M, int N, int K, cplx al
                const void *A, int lda, const void *B, int ldb, cplx beta, void *C, int ldc) {
     Gemm g;
     g.dt = dt;
-    if (dt != DType::C128) {  // ConjTrans on real data is Trans
+    if (!is_complex(dt)) {  // ConjTrans on real data is Trans
         if (ta == ConjT) ta = TransT;
         if (tb == ConjT) tb = TransT;
     }
@@ -151,6 +151,19 @@ void cblas_zgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA
                    lda, B, ldb, cplx{be[0], be[1]}, C, ldc);
 }
 
+// Replaces the reference's cblas_cgemm (blas/cgemm.c:14-106), whose GPU path
+// is commented out so that every call runs on its CPU BLAS. alpha, beta, A, B
+// and C point to interleaved (re, im) float pairs.
+void cblas_cgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K,
+                 const void *alpha, const void *A, const int lda, const void *B,
+                 const int ldb, const void *beta, void *C, const int ldc) {
+    const float *al = static_cast<const float *>(alpha);
+    const float *be = static_cast<const float *>(beta);
+    bx::host_entry("CGEMM ", DType::C64, Order, TransA, TransB, M, N, K, cplx{al[0], al[1]}, A,
+                   lda, B, ldb, cplx{be[0], be[1]}, C, ldc);
+}
+
 #define BX_F77_PROLOGUE(NAME)                                   \
     int ta = 0, tb = 0, info = -1;                              \
     if (!bx::f77_trans(transa, &ta)) info = 1;                  \
@@ -173,6 +186,13 @@ void dgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, d
     BX_F77_PROLOGUE("DGEMM ")
     cblas_dgemm(CblasColMajor, CBLAS_TRANSPOSE(ta), CBLAS_TRANSPOSE(tb), *m, *n, *k, *alpha, A,
                 *lda, B, *ldb, *beta, C, *ldc);
+}
+
+void cgemm_(char *transa, char *transb, int *m, int *n, int *k, float *alpha, float *A,
+            int *lda, float *B, int *ldb, float *beta, float *C, int *ldc) {
+    BX_F77_PROLOGUE("CGEMM ")
+    cblas_cgemm(CblasColMajor, CBLAS_TRANSPOSE(ta), CBLAS_TRANSPOSE(tb), *m, *n, *k, alpha, A,
+                *lda, B, *ldb, beta, C, *ldc);
 }
 
 void zgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, double *A,
@@ -202,6 +222,15 @@ int blasx_zgemm_device(int transa, int transb, int M, int N, int K, const void *
     const double *al = static_cast<const double *>(alpha);
     const double *be = static_cast<const double *>(beta);
     return bx::device_entry(DType::C128, transa, transb, M, N, K, cplx{al[0], al[1]}, A, lda, B,
+                            ldb, cplx{be[0], be[1]}, C, ldc, stream);
+}
+
+int blasx_cgemm_device(int transa, int transb, int M, int N, int K, const void *alpha,
+                       const void *A, int lda, const void *B, int ldb, const void *beta,
+                       void *C, int ldc, void *stream) {
+    const float *al = static_cast<const float *>(alpha);
+    const float *be = static_cast<const float *>(beta);
+    return bx::device_entry(DType::C64, transa, transb, M, N, K, cplx{al[0], al[1]}, A, lda, B,
                             ldb, cplx{be[0], be[1]}, C, ldc, stream);
 }
 

@@ -76,7 +76,7 @@ size_t default_budget(const Context *c) {
 int pick_tile(const Gemm &g) {
     const int t = config().tile.load();
     if (t) return t;
-    return g.dt == DType::F32 ? 4096 : (g.dt == DType::F64 ? 4096 : 2048);
+    return g.dt == DType::C128 ? 2048 : 4096;
 }
 
 // Copies the column panel [j0, j1) of op(B) (and of C) host -> device.

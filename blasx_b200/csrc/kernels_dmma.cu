@@ -509,7 +509,8 @@ template <bool CPLX, int KI> int launch_grouped_t(const GroupTable &tab, int til
 }  // namespace
 
 bool dmma_supported(const Gemm &g) {
-    return g.dt != DType::F32 && g.M <= INT32_MAX && g.N <= INT32_MAX && g.K <= INT32_MAX;
+    return (g.dt == DType::F64 || g.dt == DType::C128) && g.M <= INT32_MAX && g.N <= INT32_MAX &&
+           g.K <= INT32_MAX;
 }
 
 int launch_gemm_dmma_grouped(const Gemm *gs, int n, cudaStream_t s) {
@@ -520,7 +521,7 @@ int launch_gemm_dmma_grouped(const Gemm *gs, int n, cudaStream_t s) {
     tab.n = n;
     int64_t tiles = 0;
     for (int i = 0; i < n; ++i) {
-        if (gs[i].dt != gs[0].dt || gs[i].dt == DType::F32)
+        if (gs[i].dt != gs[0].dt || (gs[i].dt != DType::F64 && gs[i].dt != DType::C128))
             return set_error(BLASX_ERR_ARG, "grouped launch needs one FP64 or complex128 dtype");
         tab.p[i] = cplx ? make_params<true>(gs[i]) : make_params<false>(gs[i]);
         tab.p[i].guard = nullptr;

@@ -16,6 +16,9 @@ namespace {
 struct z2 {
     double re, im;
 };
+struct c2 {  // complex64: interleaved (re, im) floats
+    float re, im;
+};
 
 template <typename T> struct Arith;
 
@@ -52,10 +55,28 @@ template <> struct Arith<z2> {
     __device__ static V add(V a, V b) { return {a.re + b.re, a.im + b.im}; }
 };
 
+template <> struct Arith<c2> {
+    using V = c2;
+    __device__ static V zero() { return {0.f, 0.f}; }
+    __device__ static V fma(V a, V b, V c) {
+        c.re = fmaf(a.re, b.re, c.re);
+        c.re = fmaf(-a.im, b.im, c.re);
+        c.im = fmaf(a.re, b.im, c.im);
+        c.im = fmaf(a.im, b.re, c.im);
+        return c;
+    }
+    __device__ static V conj(V a) { return {a.re, -a.im}; }
+    __device__ static V mul(V a, V b) {
+        return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+    }
+    __device__ static V add(V a, V b) { return {a.re + b.re, a.im + b.im}; }
+};
+
 template <typename T> __host__ T from_cplx(cplx c);
 template <> __host__ float from_cplx<float>(cplx c) { return float(c.re); }
 template <> __host__ double from_cplx<double>(cplx c) { return c.re; }
 template <> __host__ z2 from_cplx<z2>(cplx c) { return {c.re, c.im}; }
+template <> __host__ c2 from_cplx<c2>(cplx c) { return {float(c.re), float(c.im)}; }
 
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
@@ -206,6 +227,7 @@ int launch_gemm_simt(const Gemm &g, cudaStream_t s) {
     switch (g.dt) {
         case DType::F32: return launch_simt_t<float>(g, s);
         case DType::F64: return launch_simt_t<double>(g, s);
+        case DType::C64: return launch_simt_t<c2>(g, s);
         default: return launch_simt_t<z2>(g, s);
     }
 }
@@ -215,6 +237,7 @@ int launch_add_scaled(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s)
     switch (g.dt) {
         case DType::F32: return launch_add_scaled_t<float>(g, X, ldx, s);
         case DType::F64: return launch_add_scaled_t<double>(g, X, ldx, s);
+        case DType::C64: return launch_add_scaled_t<c2>(g, X, ldx, s);
         default: return launch_add_scaled_t<z2>(g, X, ldx, s);
     }
 }
@@ -224,6 +247,7 @@ int launch_scale(const Gemm &g, cudaStream_t s) {
     switch (g.dt) {
         case DType::F32: return launch_scale_t<float>(g, s);
         case DType::F64: return launch_scale_t<double>(g, s);
+        case DType::C64: return launch_scale_t<c2>(g, s);
         default: return launch_scale_t<z2>(g, s);
     }
 }

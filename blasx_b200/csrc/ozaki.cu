@@ -96,10 +96,14 @@ CrtTables build_tables() {
 // ---- device helpers ---------------------------------------------------------
 
 template <typename T> struct Elem;
-template <> struct Elem<double> { static constexpr bool cplx = false; };
-template <> struct Elem<float> { static constexpr bool cplx = false; };
+// cplx: interleaved (re, im) pairs of R; single: the result is rounded to
+// FP32 accuracy (u = 2^-24), which sets the modulus count.
+template <> struct Elem<double> { static constexpr bool cplx = false, single = false; using R = double; };
+template <> struct Elem<float> { static constexpr bool cplx = false, single = true; using R = float; };
 struct zpair { double re, im; };
-template <> struct Elem<zpair> { static constexpr bool cplx = true; };
+template <> struct Elem<zpair> { static constexpr bool cplx = true, single = false; using R = double; };
+struct cpair { float re, im; };
+template <> struct Elem<cpair> { static constexpr bool cplx = true, single = true; using R = float; };
 
 // op(X) viewed as R rows x K: element (r, k) at p[k + r*ld] (kc) or p[r + k*ld].
 struct View {
@@ -114,9 +118,10 @@ __device__ __forceinline__ void load_elem(const View &v, int64_t r, int64_t k, b
                                           double &re, double &im) {
     const int64_t off = kc ? k + r * v.ld : r + k * v.ld;
     if constexpr (Elem<T>::cplx) {
-        const double *q = static_cast<const double *>(v.p) + 2 * off;
-        re = q[0];
-        im = v.conj ? -q[1] : q[1];
+        using R = typename Elem<T>::R;
+        const R *q = static_cast<const R *>(v.p) + 2 * off;
+        re = double(q[0]);
+        im = v.conj ? -double(q[1]) : double(q[1]);
     } else {
         re = double(static_cast<const T *>(v.p)[off]);
         im = 0.0;
@@ -620,14 +625,15 @@ __device__ __forceinline__ void recon_real(const ReconArgs &a, int64_t i0, int64
 
 // Complex outputs: residues of Re(C) are rows [0, Jp) of U, Im(C) rows
 // [Jp, 2 Jp); U planes are 2 Jp x Ip.
-template <int N>
+template <typename T, int N>
 __device__ __forceinline__ void recon_cplx(const ReconArgs &a, int64_t i0, int64_t j) {
+    using R = typename Elem<T>::R;
     const int64_t plane = 2 * a.Jp * a.Ip;
     uint32_t wr[N], wi[N];
     gather4<N>(a.U, plane, j * a.Ip + i0, wr);
     gather4<N>(a.U, plane, (a.Jp + j) * a.Ip + i0, wi);
     const int fj = a.fb[j];
-    double *C = static_cast<double *>(a.C);
+    R *C = static_cast<R *>(a.C);
 #pragma unroll 1
     for (int q = 0; q < 4; ++q) {
         const int64_t i = i0 + q;
@@ -639,15 +645,15 @@ __device__ __forceinline__ void recon_cplx(const ReconArgs &a, int64_t i0, int64
         const double xr = crt_to_double<N>(u, sc);
         unpack<N>(wi, q, u);
         const double xi = crt_to_double<N>(u, sc);
-        double *cp = C + 2 * (i + j * a.ldc);
+        R *cp = C + 2 * (i + j * a.ldc);
         double vr = a.ar * xr - a.ai * xi, vi = a.ar * xi + a.ai * xr;
         if (!a.beta_zero) {
-            const double cr = cp[0], ci = cp[1];
+            const double cr = double(cp[0]), ci = double(cp[1]);
             vr += a.br * cr - a.bi * ci;
             vi += a.br * ci + a.bi * cr;
         }
-        cp[0] = vr;
-        cp[1] = vi;
+        cp[0] = R(vr);
+        cp[1] = R(vi);
     }
 }
 
@@ -662,7 +668,7 @@ __global__ void __launch_bounds__(128) reconstruct_kernel(const ReconArgs a, con
     if (i0 >= a.M || j >= a.N) return;
 #define BX_RECON_CASE(NN)                                     \
     case NN:                                                  \
-        if constexpr (CPLX) recon_cplx<NN>(a, i0, j);         \
+        if constexpr (CPLX) recon_cplx<T, NN>(a, i0, j);      \
         else recon_real<T, NN>(a, i0, j);                     \
         break;
     switch (n) {
@@ -764,12 +770,12 @@ struct Plan {
 // op(B) = op(A)^T read from the same buffer (real types): the rows of op(A)
 // are the columns of op(B), so their statistics, exponents and slices agree.
 bool aliased(const Gemm &g) {
-    return g.dt != DType::C128 && g.A == g.B && g.lda == g.ldb && g.M == g.N &&
+    return !is_complex(g.dt) && g.A == g.B && g.lda == g.ldb && g.M == g.N &&
            (g.ta == NoTrans) != (g.tb == NoTrans);
 }
 
 Plan make_plan(const Gemm &g) {
-    const bool cplx = g.dt == DType::C128;
+    const bool cplx = is_complex(g.dt);
     const int64_t L = oz::kMaxModuli;
     Plan p;
     p.M = g.M; p.N = g.N; p.K = g.K;
@@ -821,7 +827,7 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
     if (!pl.alias) BX_TRY(launch_stats<T>(vb, bkc, sb, s));
     const oz::RowStats sbd = pl.alias ? sa : sb;  // aliased: the columns of op(B) are the rows of op(A)
     int *fbd = pl.alias ? ea : fb;
-    const double unit = std::is_same<T, float>::value ? std::ldexp(1.0, -24) : std::ldexp(1.0, -53);
+    const double unit = oz::Elem<T>::single ? std::ldexp(1.0, -24) : std::ldexp(1.0, -53);
     oz::decide_kernel<<<1, 1024, 0, s>>>(sa, M, sbd, N, K, unit, mode, forced_moduli(), dec);
     BX_CUDA(cudaGetLastError());
     count_launch();
@@ -875,8 +881,8 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
             gp.C = static_cast<char *>(g.C) + j0 * g.ldc * int64_t(elem_size(g.dt));
             gp.diag = g.diag + j0;
             gp.guard = &dec->nmod;
-            if (g.dt == DType::F32) BX_TRY(launch_gemm_simt(gp, s));
-            else BX_TRY(launch_gemm_dmma(gp, s));
+            if (dmma_supported(gp)) BX_TRY(launch_gemm_dmma(gp, s));
+            else BX_TRY(launch_gemm_simt(gp, s));
         }
         if (hooks && hooks->after_panel) BX_TRY(hooks->after_panel(hooks->ctx, j0, j1));
     }
@@ -887,8 +893,8 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
     if (!hooks) {
         Gemm gn = g;
         gn.guard = &dec->nmod;
-        if (g.dt == DType::F32) BX_TRY(launch_gemm_simt(gn, s));
-        else BX_TRY(launch_gemm_dmma(gn, s));
+        if (dmma_supported(gn)) BX_TRY(launch_gemm_dmma(gn, s));
+        else BX_TRY(launch_gemm_simt(gn, s));
     }
     cudaEvent_t ev4 = prof::mark(s);
     prof::span(prof::kSlice, ev0, ev1);
@@ -925,6 +931,7 @@ int ozaki_gemm(const Gemm &g, cudaStream_t s, int mode) {
     switch (g.dt) {
         case DType::F64: return ozaki_t<double>(g, s, mode);
         case DType::F32: return ozaki_t<float>(g, s, mode);
+        case DType::C64: return ozaki_t<oz::cpair>(g, s, mode);
         default: return ozaki_t<oz::zpair>(g, s, mode);
     }
 }
@@ -940,6 +947,9 @@ int ozaki_gemm_panels(const Gemm &g, cudaStream_t s, int mode, void *ws, int num
         case DType::F64:
             return ozaki_run<double>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks,
                                      clear_err);
+        case DType::C64:
+            return ozaki_run<oz::cpair>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks,
+                                        clear_err);
         case DType::F32:
             return ozaki_run<float>(g, s, mode, ws, num_sms, ctx->last_decision, ctx->last_error_flag, &hooks,
                                     clear_err);
@@ -959,6 +969,7 @@ int ozaki_gemm_step(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_s
     switch (g.dt) {
         case DType::F64: return ozaki_run<double>(g, s, mode, ws, num_sms, dec_host, err_host, nullptr, first);
         case DType::F32: return ozaki_run<float>(g, s, mode, ws, num_sms, dec_host, err_host, nullptr, first);
+        case DType::C64: return ozaki_run<oz::cpair>(g, s, mode, ws, num_sms, dec_host, err_host, nullptr, first);
         default: return ozaki_run<oz::zpair>(g, s, mode, ws, num_sms, dec_host, err_host, nullptr, first);
     }
 }
@@ -967,6 +978,7 @@ int ozaki_gemm_in(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms
     switch (g.dt) {
         case DType::F64: return ozaki_run<double>(g, s, mode, ws, num_sms, nullptr, nullptr);
         case DType::F32: return ozaki_run<float>(g, s, mode, ws, num_sms, nullptr, nullptr);
+        case DType::C64: return ozaki_run<oz::cpair>(g, s, mode, ws, num_sms, nullptr, nullptr);
         default: return ozaki_run<oz::zpair>(g, s, mode, ws, num_sms, nullptr, nullptr);
     }
 }

@@ -14,11 +14,12 @@
 
 namespace bx {
 
-enum class DType : int { F32 = 0, F64 = 1, C128 = 2 };
+enum class DType : int { F32 = 0, F64 = 1, C128 = 2, C64 = 3 };
 
 inline size_t elem_size(DType t) {
-    return t == DType::F32 ? 4 : (t == DType::F64 ? 8 : 16);
+    return t == DType::F32 ? 4 : (t == DType::C128 ? 16 : 8);
 }
+inline bool is_complex(DType t) { return t == DType::C128 || t == DType::C64; }
 
 struct cplx {
     double re, im;
@@ -66,7 +67,7 @@ struct Gemm {
         return uplo == 0 || (uplo == 1 ? r - c <= diag : r - c >= diag);
     }
     double flops() const {
-        return (dt == DType::C128 ? 8.0 : 2.0) * double(M) * double(N) * double(K);
+        return (is_complex(dt) ? 8.0 : 2.0) * double(M) * double(N) * double(K);
     }
 };
 

@@ -699,7 +699,7 @@ int submit(const Gemm &g) {
     // small native requests are mixed into grouped launches
     r->flops = 0;
     r->emulated = need_ab && ozaki_selected(g, config().dgemm_mode.load());
-    r->grouped = need_ab && !r->emulated && g.dt != DType::F32 && g.uplo == 0 &&
+    r->grouped = need_ab && !r->emulated && (g.dt == DType::F64 || g.dt == DType::C128) && g.uplo == 0 &&
                  g.flops() <= s->group_flops;
     if (need_ab) {
         r->bkey = Key{g.B, g.ldb, g.rows_b(), g.cols_b(), int(g.dt),

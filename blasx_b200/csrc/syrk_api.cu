@@ -31,7 +31,7 @@ namespace {
 int to_uplo(int u) { return u == CblasUpper ? 1 : (u == CblasLower ? 2 : 0); }
 
 int check_syr(DType dt, int order, int uplo, int trans, int N, int K, int lda, int ldb, int ldc, bool two) {
-    const bool trans_ok = trans == NoTrans || trans == TransT || (trans == ConjT && dt != DType::C128);
+    const bool trans_ok = trans == NoTrans || trans == TransT || (trans == ConjT && !is_complex(dt));
     // stored rows of A (and B): op(A) is N x K; row-major storage is the transpose
     const bool rows_n = (trans == NoTrans) != (order == CblasRowMajor);
     const int nrowa = rows_n ? N : K;

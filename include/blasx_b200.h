@@ -59,13 +59,23 @@ void cblas_zgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA
                  const void *alpha, const void *A, const int lda, const void *B,
                  const int ldb, const void *beta, void *C, const int ldc);
 
-/* Replace the F77 wrappers sgemm_ (blas/sgemm.c), dgemm_ (blas/dgemm.c:131-154)
- * and zgemm_ (blas/zgemm.c:133-156): every argument by pointer, trans chars
- * 'N'/'T'/'C' in either case, column-major. */
+/* Replaces cblas_cgemm, include/cblas.h:484 (implementation blas/cgemm.c:14-106,
+ * whose GPU path is commented out: the reference runs every CGEMM on its CPU
+ * BLAS). alpha, beta, A, B, C point to interleaved (re, im) float pairs. */
+void cblas_cgemm(const enum CBLAS_ORDER Order, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_TRANSPOSE TransB, const int M, const int N, const int K,
+                 const void *alpha, const void *A, const int lda, const void *B,
+                 const int ldb, const void *beta, void *C, const int ldc);
+
+/* Replace the F77 wrappers sgemm_ (blas/sgemm.c), dgemm_ (blas/dgemm.c:131-154),
+ * cgemm_ (blas/cgemm.c:109-) and zgemm_ (blas/zgemm.c:133-156): every argument
+ * by pointer, trans chars 'N'/'T'/'C' in either case, column-major. */
 void sgemm_(char *transa, char *transb, int *m, int *n, int *k, float *alpha, float *A,
             int *lda, float *B, int *ldb, float *beta, float *C, int *ldc);
 void dgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, double *A,
             int *lda, double *B, int *ldb, double *beta, double *C, int *ldc);
+void cgemm_(char *transa, char *transb, int *m, int *n, int *k, float *alpha, float *A,
+            int *lda, float *B, int *ldb, float *beta, float *C, int *ldc);
 void zgemm_(char *transa, char *transb, int *m, int *n, int *k, double *alpha, double *A,
             int *lda, double *B, int *ldb, double *beta, double *C, int *ldc);
 
@@ -202,18 +212,23 @@ int blasx_dgemm_device(int transa, int transb, int M, int N, int K, double alpha
                        const double *A, int lda, const double *B, int ldb, double beta,
                        double *C, int ldc, void *stream);
 
-/* Device-resident DSYRK (column-major, uplo CblasUpper/CblasLower, trans
- * CblasNoTrans/CblasTrans): C = alpha op(A) op(A)^T + beta C on the uplo
- * triangle of the device matrix C, enqueued on `stream`; returns a status.
- * No counterpart in the reference. */
-int blasx_dsyrk_device(int uplo, int trans, int N, int K, double alpha, const double *A, int lda,
-                       double beta, double *C, int ldc, void *stream);
 int blasx_sgemm_device(int transa, int transb, int M, int N, int K, float alpha,
                        const float *A, int lda, const float *B, int ldb, float beta, float *C,
                        int ldc, void *stream);
 int blasx_zgemm_device(int transa, int transb, int M, int N, int K, const void *alpha,
                        const void *A, int lda, const void *B, int ldb, const void *beta,
                        void *C, int ldc, void *stream);
+/* complex64: alpha, beta, A, B, C are interleaved (re, im) float pairs. */
+int blasx_cgemm_device(int transa, int transb, int M, int N, int K, const void *alpha,
+                       const void *A, int lda, const void *B, int ldb, const void *beta,
+                       void *C, int ldc, void *stream);
+
+/* Device-resident DSYRK (column-major, uplo CblasUpper/CblasLower, trans
+ * CblasNoTrans/CblasTrans): C = alpha op(A) op(A)^T + beta C on the uplo
+ * triangle of the device matrix C, enqueued on `stream`; returns a status.
+ * No counterpart in the reference. */
+int blasx_dsyrk_device(int uplo, int trans, int N, int K, double alpha, const double *A, int lda,
+                       double beta, double *C, int ldc, void *stream);
 
 /* Device-resident DGEMM that allocates no memory. No counterpart in the
  * reference. It is meant for callers that cannot let a library call

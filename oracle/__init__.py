@@ -40,7 +40,8 @@ ROWMAJOR, COLMAJOR = 101, 102
 TRANS_OF = {"N": NOTRANS, "T": TRANS, "C": CONJTRANS}
 
 # machine epsilons (unit roundoff) per dtype
-UNIT_ROUNDOFF = {np.float64: 2.0 ** -53, np.float32: 2.0 ** -24, np.complex128: 2.0 ** -53}
+UNIT_ROUNDOFF = {np.float64: 2.0 ** -53, np.float32: 2.0 ** -24, np.complex128: 2.0 ** -53,
+                 np.complex64: 2.0 ** -24}
 
 _lib = None
 _P = ctypes.c_void_p
@@ -64,6 +65,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_dgemm_tiled.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _I]
         L.oracle_sgemm_tiled.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I, _I]
         L.oracle_zgemm_tiled.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _I]
+        L.oracle_cgemm_tiled.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _I]
         L.oracle_dgemm_dd_entries.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _I64, _P, _P, _P, _P, _P]
         L.oracle_sgemm_dd_entries.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I, _I64, _P, _P, _P, _P, _P]
         L.oracle_zgemm_dd_entries.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _I64, _P, _P, _P, _P, _P]
@@ -72,6 +74,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_openblas_dgemm.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _D, _P, _I]
         L.oracle_openblas_sgemm.argtypes = [_I] * 6 + [_F, _P, _I, _P, _I, _F, _P, _I]
         L.oracle_openblas_zgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
+        L.oracle_openblas_cgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
         L.oracle_fill_uniform_f64.argtypes = [_P, _I64, ctypes.c_uint64, _D, _D]
         L.oracle_fill_uniform_f32.argtypes = [_P, _I64, ctypes.c_uint64, _F, _F]
         L.oracle_fill_spread_f64.argtypes = [_P, _I64, ctypes.c_uint64, _D]
@@ -95,10 +98,11 @@ def shape_of_op(trans: str, rows: int, cols: int) -> tuple[int, int]:
 def uniform(shape, dtype, seed: int, lo=-1.0, hi=1.0) -> np.ndarray:
     """Seeded U[lo,hi] column-major matrix (SplitMix64 counter RNG)."""
     dtype = np.dtype(dtype)
-    if dtype == np.complex128:
-        re = uniform(shape, np.float64, seed, lo, hi)
-        im = uniform(shape, np.float64, seed ^ 0x9E3779B9, lo, hi)
-        out = np.empty(shape, dtype=np.complex128, order="F")
+    if dtype in (np.complex128, np.complex64):
+        part = np.float64 if dtype == np.complex128 else np.float32
+        re = uniform(shape, part, seed, lo, hi)
+        im = uniform(shape, part, seed ^ 0x9E3779B9, lo, hi)
+        out = np.empty(shape, dtype=dtype, order="F")
         out.real, out.imag = re, im
         return out
     out = np.empty(shape, dtype=dtype, order="F")
@@ -131,6 +135,11 @@ def gemm_tiled(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, blo
         L.oracle_dgemm_tiled(ta, tb, M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc, block_dim)
     elif C.dtype == np.float32:
         L.oracle_sgemm_tiled(ta, tb, M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc, block_dim)
+    elif C.dtype == np.complex64:
+        al = np.array([complex(alpha).real, complex(alpha).imag], dtype=np.float32)
+        be = np.array([complex(beta).real, complex(beta).imag], dtype=np.float32)
+        L.oracle_cgemm_tiled(ta, tb, M, N, K, _ptr(al), _ptr(A), lda, _ptr(B), ldb, _ptr(be), _ptr(C), ldc,
+                             block_dim)
     elif C.dtype == np.complex128:
         al = np.array([complex(alpha).real, complex(alpha).imag])
         be = np.array([complex(beta).real, complex(beta).imag])
@@ -176,6 +185,10 @@ def dd_entries(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, ii
     jj = np.ascontiguousarray(jj, dtype=np.int64)
     n = ii.size
     L = lib()
+    if A.dtype == np.complex64:  # products of floats are exact in double: widen and use the complex128 sums
+        A = np.asfortranarray(A, dtype=np.complex128)
+        B = np.asfortranarray(B, dtype=np.complex128)
+        C0 = None if C0 is None else np.asfortranarray(C0, dtype=np.complex128)
     c0p = _ptr(C0) if (C0 is not None and beta != 0) else None
     if A.dtype == np.complex128:
         hi = np.empty(2 * n); lo = np.empty(2 * n); bd = np.empty(2 * n)
@@ -262,6 +275,12 @@ class OpenBLAS:
 
     def gemm(self, transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, order=COLMAJOR):
         ta, tb = TRANS_OF[transa], TRANS_OF[transb]
+        if C.dtype == np.complex64:
+            al = np.array([complex(alpha).real, complex(alpha).imag], dtype=np.float32)
+            be = np.array([complex(beta).real, complex(beta).imag], dtype=np.float32)
+            self.L.oracle_openblas_cgemm(order, ta, tb, M, N, K, _ptr(al), _ptr(A), lda, _ptr(B), ldb, _ptr(be),
+                                         _ptr(C), ldc)
+            return C
         if C.dtype == np.float64:
             self.L.oracle_openblas_dgemm(order, ta, tb, M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc)
         elif C.dtype == np.float32:
@@ -289,6 +308,7 @@ class Reference:
         L.cblas_dgemm.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _D, _P, _I]
         L.cblas_sgemm.argtypes = [_I] * 6 + [_F, _P, _I, _P, _I, _F, _P, _I]
         L.cblas_zgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
+        L.cblas_cgemm.argtypes = [_I] * 6 + [_P, _P, _I, _P, _I, _P, _P, _I]
         L.dgemm_.argtypes = [_P] * 13
         self.L = L
 
@@ -302,6 +322,10 @@ class Reference:
             self.L.cblas_dgemm(order, ta, tb, M, N, K, alpha, Ap, lda, Bp, ldb, beta, _ptr(C), ldc)
         elif C.dtype == np.float32:
             self.L.cblas_sgemm(order, ta, tb, M, N, K, alpha, Ap, lda, Bp, ldb, beta, _ptr(C), ldc)
+        elif C.dtype == np.complex64:
+            al = np.array([complex(alpha).real, complex(alpha).imag], dtype=np.float32)
+            be = np.array([complex(beta).real, complex(beta).imag], dtype=np.float32)
+            self.L.cblas_cgemm(order, ta, tb, M, N, K, _ptr(al), Ap, lda, Bp, ldb, _ptr(be), _ptr(C), ldc)
         else:
             al = np.array([complex(alpha).real, complex(alpha).imag])
             be = np.array([complex(beta).real, complex(beta).imag])

@@ -177,6 +177,74 @@ void oracle_zgemm_tiled(int transa, int transb, int M, int N, int K, const doubl
     }
 }
 
+/* complex64: the same tiled algorithm in float arithmetic (the precision of
+ * the reference's CPU cblas_cgemm, blas/cgemm.c:60-68) */
+static inline void getA_c(const float *A, int lda, int tr, long i, long k, float *re, float *im) {
+    const float *p = tr == NOTRANS ? &A[2 * (i + k * (long)lda)] : &A[2 * (k + i * (long)lda)];
+    *re = p[0];
+    *im = tr == CONJTRANS ? -p[1] : p[1];
+}
+static inline void getB_c(const float *B, int ldb, int tr, long k, long j, float *re, float *im) {
+    const float *p = tr == NOTRANS ? &B[2 * (k + j * (long)ldb)] : &B[2 * (j + k * (long)ldb)];
+    *re = p[0];
+    *im = tr == CONJTRANS ? -p[1] : p[1];
+}
+
+void oracle_cgemm_tiled(int transa, int transb, int M, int N, int K, const float *alpha,
+                        const float *A, int lda, const float *B, int ldb, const float *beta,
+                        float *C, int ldc, int bd) {
+    if (M <= 0 || N <= 0) return;
+    float ar = alpha[0], ai = alpha[1], br_ = beta[0], bi_ = beta[1];
+    int beta_zero = (br_ == 0 && bi_ == 0);
+    if (K <= 0 || (ar == 0 && ai == 0)) {
+        for (int c = 0; c < N; ++c)
+            for (int r = 0; r < M; ++r) {
+                float *p = &C[2 * (r + (long)c * ldc)];
+                if (beta_zero) { p[0] = 0; p[1] = 0; continue; }
+                float re = br_ * p[0] - bi_ * p[1], im = br_ * p[1] + bi_ * p[0];
+                p[0] = re; p[1] = im;
+            }
+        return;
+    }
+    int x = last_block(M, bd), y = last_block(N, bd), z = last_block(K, bd);
+    for (int t = 0; t <= (x + 1) * (y + 1) - 1; ++t) {
+        int i = t / (y + 1), k = t % (y + 1);
+        int mr, nc;
+        margin(M, N, bd, i, k, &mr, &nc);
+        for (int j = 0; j <= z; ++j) {
+            int kr, kc;
+            margin(K, K, bd, j, j, &kr, &kc);
+            (void)kc;
+            int first = (j == 0);
+            for (int c = 0; c < nc; ++c)
+                for (int r = 0; r < mr; ++r) {
+                    long gi = (long)i * bd + r, gj = (long)k * bd + c;
+                    float sr = 0, si = 0;
+                    for (int q = 0; q < kr; ++q) {
+                        long gk = (long)j * bd + q;
+                        float xr, xi, yr, yi;
+                        getA_c(A, lda, transa, gi, gk, &xr, &xi);
+                        getB_c(B, ldb, transb, gk, gj, &yr, &yi);
+                        sr = fmaf(xr, yr, sr); sr = fmaf(-xi, yi, sr);
+                        si = fmaf(xr, yi, si); si = fmaf(xi, yr, si);
+                    }
+                    float *p = &C[2 * (gi + gj * (long)ldc)];
+                    float tr = ar * sr - ai * si, ti = ar * si + ai * sr;
+                    if (first) {
+                        if (!beta_zero) {
+                            tr += br_ * p[0] - bi_ * p[1];
+                            ti += br_ * p[1] + bi_ * p[0];
+                        }
+                    } else {
+                        tr += p[0];
+                        ti += p[1];
+                    }
+                    p[0] = tr; p[1] = ti;
+                }
+        }
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Double-double sampled-entry oracle (Ogita-Rump-Oishi Dot2)                */
 /* ------------------------------------------------------------------------ */
@@ -338,7 +406,7 @@ typedef void (*zgemm64_t)(int, int, int, int64_t, int64_t, int64_t, const void *
 
 static void *g_blas;
 static int g_ilp64;
-static void *g_d, *g_s, *g_z;
+static void *g_d, *g_s, *g_z, *g_c;
 static char g_name[1024];
 
 int oracle_openblas_open(const char *paths) {
@@ -362,8 +430,10 @@ int oracle_openblas_open(const char *paths) {
         void *s = dlsym(h, sym);
         snprintf(sym, sizeof sym, "%scblas_zgemm%s", prefix, suffix);
         void *z = dlsym(h, sym);
+        snprintf(sym, sizeof sym, "%scblas_cgemm%s", prefix, suffix);
+        void *cg = dlsym(h, sym);
         if (!d || !s || !z) { dlclose(h); continue; }
-        g_blas = h; g_d = d; g_s = s; g_z = z; g_ilp64 = ilp;
+        g_blas = h; g_d = d; g_s = s; g_z = z; g_c = cg; g_ilp64 = ilp;
         char ver[128] = "";
         char vsym[256];
         snprintf(vsym, sizeof vsym, "%sopenblas_get_config%s", prefix, ilp ? "64_" : "");
@@ -398,6 +468,17 @@ int oracle_openblas_sgemm(int order, int transa, int transb, int M, int N, int K
         ((sgemm64_t)g_s)(order, transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     else
         ((sgemm32_t)g_s)(order, transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    return 0;
+}
+
+int oracle_openblas_cgemm(int order, int transa, int transb, int M, int N, int K,
+                          const float *alpha, const float *A, int lda, const float *B,
+                          int ldb, const float *beta, float *C, int ldc) {
+    if (!g_blas || !g_c) return -1;
+    if (g_ilp64)
+        ((zgemm64_t)g_c)(order, transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+        ((zgemm32_t)g_c)(order, transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     return 0;
 }
 

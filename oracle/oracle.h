@@ -41,6 +41,11 @@ void oracle_zgemm_tiled(int transa, int transb, int M, int N, int K, const doubl
                         const double *A, int lda, const double *B, int ldb, const double *beta,
                         double *C, int ldc, int block_dim);
 
+/* complex64 interleaved (re, im) floats; alpha/beta point to 2 floats */
+void oracle_cgemm_tiled(int transa, int transb, int M, int N, int K, const float *alpha,
+                        const float *A, int lda, const float *B, int ldb, const float *beta,
+                        float *C, int ldc, int block_dim);
+
 /* Sampled entries (ii[t], jj[t]) of alpha*op(A)*op(B) + beta*C0 in double-double.
  * hi/lo: the value as an unevaluated sum; bound: |alpha| sum|a||b| + |beta||c0|.
  * For zgemm hi/lo/bound hold 2 doubles (re, im) per entry; the bound is the
@@ -69,6 +74,9 @@ int oracle_openblas_dgemm(int order, int transa, int transb, int M, int N, int K
 int oracle_openblas_sgemm(int order, int transa, int transb, int M, int N, int K, float alpha,
                           const float *A, int lda, const float *B, int ldb, float beta,
                           float *C, int ldc);
+int oracle_openblas_cgemm(int order, int transa, int transb, int M, int N, int K,
+                          const float *alpha, const float *A, int lda, const float *B,
+                          int ldb, const float *beta, float *C, int ldc);
 int oracle_openblas_zgemm(int order, int transa, int transb, int M, int N, int K,
                           const double *alpha, const double *A, int lda, const double *B,
                           int ldb, const double *beta, double *C, int ldc);

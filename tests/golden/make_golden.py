@@ -15,6 +15,11 @@ for every size (blas/dsyrk.c:36-39, blas/dsyr2k.c); their outputs and the
 reference's xerbla_ lines for each illegal argument (blas/dsyrk.c:27-37,
 blas/dsyr2k.c:43-52, the F77 wrappers blas/dsyrk.c:80-101) are recorded too.
 
+The reference's CPU BLAS is multithreaded, so a run on another machine may
+differ from the recorded outputs in the last bits; the tests compare within
+the componentwise bound, and a regeneration should keep the recorded entries
+and add only new ones.
+
 Run in a container that has the reference tree:  python tests/golden/make_golden.py
 """
 import ctypes
@@ -56,10 +61,12 @@ def main():
     ref = oracle.Reference()
     rec = {}
     n = 0
-    dtypes = [("d", np.float64, "NT"), ("s", np.float32, "NT"), ("z", np.complex128, "NTC")]
+    # complex64 last, so that the earlier cases keep their numbering (and seeds)
+    dtypes = [("d", np.float64, "NT"), ("s", np.float32, "NT"), ("z", np.complex128, "NTC"),
+              ("c", np.complex64, "NTC")]
     for tag, dt, transes in dtypes:
         for (M, N, K) in SHAPES:
-            scal = ZSCALARS if tag == "z" else SCALARS
+            scal = ZSCALARS if tag in "zc" else SCALARS
             for ta in transes:
                 for tb in transes:
                     for si, (al, be) in enumerate(scal):
@@ -68,7 +75,7 @@ def main():
                             continue
                         if (M, N, K) in BIG and not (ta == "N" and tb == "N" and si <= 1):
                             continue
-                        if tag == "z":
+                        if tag in "zc":
                             al = complex(*al); be = complex(*be)
                         seed = 1000 + n
                         ra, ca = oracle.shape_of_op(ta, M, K)

@@ -5,10 +5,10 @@ import numpy as np
 
 import oracle
 
-DT = {"d": np.float64, "s": np.float32, "z": np.complex128}
+DT = {"d": np.float64, "s": np.float32, "z": np.complex128, "c": np.complex64}
 
 
-GEMM_KEY = re.compile(r"^([dsz])_(\d+)_meta$")  # "<tag>_<n>_meta"; SYRK cases use their own prefixes
+GEMM_KEY = re.compile(r"^([dszc])_(\d+)_meta$")  # "<tag>_<n>_meta"; SYRK cases use their own prefixes
 
 
 def cases(golden, tags=("d", "s", "z")):
@@ -23,7 +23,7 @@ def cases(golden, tags=("d", "s", "z")):
         M, N, K, lda, ldb, ldc, ta, tb = (int(v) for v in golden[key + "_meta"])
         ta, tb = chr(ta), chr(tb)
         al, be = golden[key + "_scal"]
-        if dt != np.complex128:
+        if dt not in (np.complex128, np.complex64):
             al, be = float(al.real), float(be.real)
         else:
             al, be = complex(al), complex(be)
@@ -64,7 +64,7 @@ def tol_ratio(case, got):
     if case["beta"] != 0:
         bound = bound + abs(case["beta"]) * np.abs(case["C0"][:M, :N]).astype(np.float64)
     u = oracle.UNIT_ROUNDOFF[np.dtype(dt).type]
-    gamma = (K + 2) * u * (2.0 if dt == np.complex128 else 1.0)
+    gamma = (K + 2) * u * (2.0 if dt in (np.complex128, np.complex64) else 1.0)
     err = np.abs(got[:M, :N].astype(np.complex128) - case["C"][:M, :N].astype(np.complex128))
     scale = np.maximum(bound, np.finfo(np.float64).tiny)
     return float(np.max(err / (gamma * scale))) if err.size else 0.0

@@ -104,3 +104,13 @@ def test_no_gpu_fails_loudly():
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=120)
     assert "STATUS 4 0.0" in r.stdout, (r.stdout, r.stderr)
     assert "no CUDA device" in r.stderr
+
+
+def test_cgemm_reports_like_the_other_gemms(blx):
+    # blas/cgemm.c:37-51 uses the same info numbering (first illegal argument wins)
+    A = np.zeros((4, 4), np.complex64); C = np.ones((4, 4), np.complex64, order="F")
+    out = _capture(lambda: blx.cblas_cgemm(102, 111, 111, 4, 4, 4, 1.0, A, 2, A, 4, 0.0, C, 4))
+    assert out == " ** On entry to CGEMM  parameter number  8 had an illegal value\n"
+    assert np.all(C == 1.0) and blx.last_status() == blx.BLASX_ERR_ARG
+    out = _capture(lambda: blx.cgemm_("X", "N", 4, 4, 4, 1.0, A, 4, A, 4, 0.0, C, 4))
+    assert "CGEMM  parameter number  1" in out

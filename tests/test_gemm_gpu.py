@@ -15,14 +15,15 @@ ORDER_COL = 102
 
 def run_case(blx, c, C=None, mode=None):
     C = c["C0"].copy(order="F") if C is None else C
-    fn = {np.float64: blx.cblas_dgemm, np.float32: blx.cblas_sgemm, np.complex128: blx.cblas_zgemm}[c["dt"]]
+    fn = {np.float64: blx.cblas_dgemm, np.float32: blx.cblas_sgemm, np.complex128: blx.cblas_zgemm,
+          np.complex64: blx.cblas_cgemm}[c["dt"]]
     fn(ORDER_COL, oracle.TRANS_OF[c["ta"]], oracle.TRANS_OF[c["tb"]], c["M"], c["N"], c["K"], c["alpha"],
        c["A"], c["lda"], c["B"], c["ldb"], c["beta"], C, c["ldc"])
     assert blx.last_status() == blx.BLASX_OK, blx.last_error()
     return C
 
 
-@pytest.mark.parametrize("tag", ["d", "s", "z"])
+@pytest.mark.parametrize("tag", ["d", "s", "z", "c"])
 def test_golden_cases(blx, golden, tag):
     for c in cases(golden, tags=(tag,)):
         C = run_case(blx, c)
@@ -42,18 +43,20 @@ def test_golden_edge_cases(blx, golden):
 
 
 def test_f77_wrappers(blx, golden):
-    for c in list(cases(golden))[::7]:
+    for c in list(cases(golden, tags=("d", "s", "z", "c")))[::7]:
         C = c["C0"].copy(order="F")
-        fn = {np.float64: blx.dgemm_, np.float32: blx.sgemm_, np.complex128: blx.zgemm_}[c["dt"]]
+        fn = {np.float64: blx.dgemm_, np.float32: blx.sgemm_, np.complex128: blx.zgemm_,
+              np.complex64: blx.cgemm_}[c["dt"]]
         fn(c["ta"].lower(), c["tb"], c["M"], c["N"], c["K"], c["alpha"], c["A"], c["lda"], c["B"], c["ldb"],
            c["beta"], C, c["ldc"])
         assert tol_ratio(c, C) <= 1.0, c["key"]
 
 
-@pytest.mark.parametrize("dt", [np.float64, np.float32, np.complex128])
+@pytest.mark.parametrize("dt", [np.float64, np.float32, np.complex128, np.complex64])
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T"), ("C", "N"), ("N", "C"), ("C", "C")])
 def test_random_vs_dd_oracle(blx, dt, ta, tb):
-    if dt != np.complex128 and "C" in (ta, tb):
+    cplx = dt in (np.complex128, np.complex64)
+    if not cplx and "C" in (ta, tb):
         pytest.skip("ConjTrans on real data is Trans (covered)")
     rng = np.random.default_rng(7)
     M, N, K = 517, 263, 1031
@@ -62,10 +65,10 @@ def test_random_vs_dd_oracle(blx, dt, ta, tb):
     A = oracle.uniform((ra + 3, ca), dt, 11)
     B = oracle.uniform((rb + 1, cb), dt, 12)
     C0 = oracle.uniform((M + 2, N), dt, 13)
-    alpha, beta = (1.5, -0.25) if dt != np.complex128 else (1.5 - 0.5j, -0.25 + 0.75j)
+    alpha, beta = (1.5, -0.25) if not cplx else (1.5 - 0.5j, -0.25 + 0.75j)
     C = C0.copy(order="F")
-    blx.gemm  # noqa
-    fn = {np.float64: blx.cblas_dgemm, np.float32: blx.cblas_sgemm, np.complex128: blx.cblas_zgemm}[dt]
+    fn = {np.float64: blx.cblas_dgemm, np.float32: blx.cblas_sgemm, np.complex128: blx.cblas_zgemm,
+          np.complex64: blx.cblas_cgemm}[dt]
     fn(ORDER_COL, oracle.TRANS_OF[ta], oracle.TRANS_OF[tb], M, N, K, alpha, A, ra + 3, B, rb + 1, beta, C, M + 2)
     assert blx.last_status() == blx.BLASX_OK, blx.last_error()
     ii = rng.integers(0, M, 2000); jj = rng.integers(0, N, 2000)

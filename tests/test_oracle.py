@@ -8,13 +8,13 @@ from golden_cases import cases, edge_cases, tol_ratio
 
 def test_generator_is_stable(golden):
     # the golden inputs are regenerated from seeds; their checksums must match
-    for c in cases(golden):
+    for c in cases(golden, tags=("d", "s", "z", "c")):
         np.testing.assert_allclose([np.sum(c["A"]), np.sum(c["B"]), np.sum(c["C0"])], c["sums"], rtol=1e-12, atol=1e-12)
 
 
 def test_tiled_restatement_matches_reference(golden):
     worst = 0.0
-    for c in cases(golden):
+    for c in cases(golden, tags=("d", "s", "z", "c")):
         C = c["C0"].copy(order="F")
         # small block size so the restatement exercises several tiles and ragged edges
         oracle.gemm_tiled(c["ta"], c["tb"], c["M"], c["N"], c["K"], c["alpha"], c["A"], c["lda"],
@@ -27,7 +27,7 @@ def test_tiled_restatement_matches_reference(golden):
 
 
 def test_dd_entries_match_reference(golden):
-    for c in cases(golden):
+    for c in cases(golden, tags=("d", "s", "z", "c")):
         M, N = c["M"], c["N"]
         ii, jj = np.meshgrid(np.arange(M), np.arange(N), indexing="ij")
         ii, jj = ii.ravel(), jj.ravel()
@@ -61,7 +61,7 @@ def test_openblas_matches_reference(golden):
         ob = oracle.OpenBLAS()
     except RuntimeError as e:
         pytest.skip(str(e))
-    for c in cases(golden, tags=("d", "z")):
+    for c in cases(golden, tags=("d", "z", "c")):
         C = c["C0"].copy(order="F")
         ob.gemm(c["ta"], c["tb"], c["M"], c["N"], c["K"], c["alpha"], c["A"], c["lda"], c["B"], c["ldb"],
                 c["beta"], C, c["ldc"])

@@ -22,7 +22,8 @@ def ozaki(blx):
 
 
 def run(blx, dt, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
-    fn = {np.float64: blx.cblas_dgemm, np.float32: blx.cblas_sgemm, np.complex128: blx.cblas_zgemm}[dt]
+    fn = {np.float64: blx.cblas_dgemm, np.float32: blx.cblas_sgemm, np.complex128: blx.cblas_zgemm,
+          np.complex64: blx.cblas_cgemm}[dt]
     fn(102, oracle.TRANS_OF[ta], oracle.TRANS_OF[tb], M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
     assert blx.last_status() == blx.BLASX_OK, blx.last_error()
     return blx.call_stats()
@@ -138,6 +139,26 @@ def test_sgemm_emulated_vs_oracle(ozaki, blx, ta, tb):
     assert st["path"] == 2 and 6 <= st["moduli"] <= 12, st
     ratio, _ = sampled_error(C, ta, tb, M, N, K, 1.5, A, lda, B, ldb, -0.25, C0, M, np.float32)
     assert ratio <= 1.0
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("C", "C"), ("T", "C"), ("C", "N")])
+def test_cgemm_emulated_vs_oracle(ozaki, blx, ta, tb):
+    """complex64 on the INT8 path: FP32 accuracy target (u = 2^-24), results
+    at least as accurate as the native complex64 kernel."""
+    M, N, K = 400, 300, 350
+    A, lda, B, ldb, C0 = make(np.complex64, ta, tb, M, N, K, 85)
+    C = C0.copy(order="F")
+    alpha, beta = 1.5 - 0.5j, -0.25 + 0.75j
+    st = run(blx, np.complex64, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, M)
+    assert st["path"] == 2 and 6 <= st["moduli"] <= 12, st
+    ratio, err = sampled_error(C, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, M, np.complex64)
+    assert ratio <= 1.0
+    blx.set_dgemm_mode(blx.MODE_NATIVE)
+    Cn = C0.copy(order="F")
+    run(blx, np.complex64, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, Cn, M)
+    blx.set_dgemm_mode(blx.MODE_OZAKI)
+    _, err_n = sampled_error(Cn, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, M, np.complex64)
+    assert err <= max(err_n, 2.0 ** -24), (err, err_n)
 
 
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("C", "C"), ("T", "C"), ("C", "N")])
