@@ -58,8 +58,8 @@ def parse():
     p.add_argument("--serving-threads", type=int, default=16)
     p.add_argument("--serving-rate", type=float, default=0.0,
                    help="offered requests/s over all threads (Poisson); 0 = back to back")
-    p.add_argument("--dtype", default="d", choices=["d", "s", "z"],
-                   help="--workload device: FP64, FP32 or complex128")
+    p.add_argument("--dtype", default="d", choices=["d", "s", "z", "c"],
+                   help="--workload device: FP64, FP32, complex128 or complex64")
     p.add_argument("--rates", default="100,200,400",
                    help="--workload serving: offered Poisson rates (requests/s) to sweep")
     p.add_argument("--workload", default="", choices=["", "c0", "ragged", "ooc", "c3", "serving", "device", "syrk"],
@@ -535,7 +535,7 @@ def run_workloads(args):
     elif args.workload == "device":
         # device-resident n^3 NN calls through blasx_?gemm_device (for ncu captures of one kernel)
         n = args.size
-        dt = {"d": torch.float64, "s": torch.float32, "z": torch.complex128}[args.dtype]
+        dt = {"d": torch.float64, "s": torch.float32, "z": torch.complex128, "c": torch.complex64}[args.dtype]
         g = torch.Generator(device="cuda").manual_seed(5)
         A = (torch.rand(n, n, dtype=dt, device="cuda", generator=g) - 0.5)
         B = (torch.rand(n, n, dtype=dt, device="cuda", generator=g) - 0.5)
@@ -559,7 +559,7 @@ def run_workloads(args):
         torch.cuda.synchronize()
         phases = {k: v["ms"] for k, v in bx.profile_read().items() if v["count"]}
         bx.profile_enable(False)
-        fl = (8.0 if args.dtype == "z" else 2.0) * n ** 3
+        fl = (8.0 if args.dtype in "zc" else 2.0) * n ** 3
         lines.append({"workload": f"device-resident {args.dtype}gemm NN {n}^3, mode {args.mode}",
                       "tflops": fl / (ms * 1e-3) / 1e12, "ms": ms, "path": st["path"], "moduli": st["moduli"],
                       "phases_ms": phases})
