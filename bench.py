@@ -62,7 +62,8 @@ def parse():
                    help="--workload device: FP64, FP32, complex128 or complex64")
     p.add_argument("--rates", default="100,200,400",
                    help="--workload serving: offered Poisson rates (requests/s) to sweep")
-    p.add_argument("--workload", default="", choices=["", "c0", "ragged", "ooc", "c3", "serving", "device", "syrk"],
+    p.add_argument("--workload", default="", choices=["", "c0", "ragged", "ooc", "c3", "serving", "device", "syrk",
+                                                    "symm"],
                    help="secondary measurements (one JSON line each) instead of the headline: ragged "
                         "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep, "
                         "the full serving stream (10,000 calls, dims to 16384), or a device-resident "
@@ -532,6 +533,54 @@ def run_workloads(args):
                           "speedup": res["emulated"]["tflops"] / res["native"]["tflops"]})
             print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
             del dA, tA, tC
+    elif args.workload == "symm":
+        # DSYMM C = A B + 0.5 C (Left, Lower) and DTRMM B = A B (Left, Upper, NoTrans, NonUnit),
+        # M = N in {8192, 16384}, through the drop-in calls on pinned host arrays (copies in the timed
+        # call), emulated and native; credited 2 M^2 N (SYMM) and M^2 N (TRMM) flops; accuracy on
+        # sampled entries against the double-double oracle on the completed A
+        import oracle
+        for n in (8192, 16384):
+            tA, A = _host(torch, (n, n), "f64", 11)
+            tB, B = _host(torch, (n, n), "f64", 12)
+            tC, C0 = _host(torch, (n, n), "f64", 13)
+            Hs = torch.empty_like(tC, pin_memory=True)
+            rng = np.random.default_rng(5)
+            ii = rng.integers(0, n, args.samples); jj = rng.integers(0, n, args.samples)
+            for op in ("dsymm", "dtrmm"):
+                res = {}
+                Af = oracle.complete("S" if op == "dsymm" else "T", "L" if op == "dsymm" else "U", A, n)
+                for mode_name, mode in (("emulated", bx.MODE_OZAKI), ("native", bx.MODE_NATIVE)):
+                    bx.set_dgemm_mode(mode)
+                    times = []
+                    for _ in range(2):  # the first call also grows the device memory pool
+                        Hs.copy_(tC if op == "dsymm" else tB)
+                        t0 = time.perf_counter()
+                        if op == "dsymm":
+                            bx.cblas_dsymm(bx.CblasColMajor, bx.CblasLeft, bx.CblasLower, n, n, 1.0, tA.data_ptr(),
+                                           n, tB.data_ptr(), n, 0.5, Hs.data_ptr(), n)
+                        else:
+                            bx.cblas_dtrmm(bx.CblasColMajor, bx.CblasLeft, bx.CblasUpper, bx.CblasNoTrans,
+                                           bx.CblasNonUnit, n, n, 1.0, tA.data_ptr(), n, Hs.data_ptr(), n)
+                        times.append(time.perf_counter() - t0)
+                    assert bx.last_status() == 0, bx.last_error()
+                    st = bx.call_stats()
+                    dt = times[-1]
+                    Cn = Hs.numpy().reshape(n, n).T  # column-major view
+                    if op == "dsymm":
+                        val, bound = oracle.dd_entries("N", "N", n, n, n, 1.0, Af, n, B, n, 0.5, C0, n, ii, jj)
+                    else:
+                        val, bound = oracle.dd_entries("N", "N", n, n, n, 1.0, Af, n, B, n, 0.0, C0, n, ii, jj)
+                    ratio, err = oracle.componentwise_ratio(Cn, ii, jj, val, bound, n, np.float64)
+                    flops = (2.0 if op == "dsymm" else 1.0) * float(n) ** 3
+                    res[mode_name] = {"tflops_e2e": flops / dt / 1e12, "seconds_e2e": dt, "path": st["path"],
+                                      "moduli": st["moduli"], "bound_ratio": ratio, "max_normalised_error": err}
+                bx.set_dgemm_mode(bx.MODE_AUTO)
+                lines.append({"workload": f"{op} M=N={n}, U[-1,1], host arrays (copies included)",
+                              "flops_credited": "2 M^2 N" if op == "dsymm" else "M^2 N", **res,
+                              "speedup_e2e": res["emulated"]["tflops_e2e"] / res["native"]["tflops_e2e"]})
+                print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
+                del Af
+            del tA, tB, tC, Hs
     elif args.workload == "device":
         # device-resident n^3 NN calls through blasx_?gemm_device (for ncu captures of one kernel)
         n = args.size

@@ -99,6 +99,12 @@ def lib() -> ctypes.CDLL:
         for f in ("ssyr2k_", "dsyr2k_", "zsyr2k_"):
             getattr(L, f).argtypes = [_P] * 12
         L.blasx_dsyrk_device.argtypes = [_I] * 4 + [_D, _P, _I, _D, _P, _I, _P]
+        for t, sc in (("s", _F), ("d", _D), ("c", _P), ("z", _P)):
+            for kind in ("symm", "hemm") if t in "cz" else ("symm",):
+                getattr(L, f"cblas_{t}{kind}").argtypes = [_I] * 5 + [sc, _P, _I, _P, _I, sc, _P, _I]
+                getattr(L, f"{t}{kind}_").argtypes = [_P] * 12
+            getattr(L, f"cblas_{t}trmm").argtypes = [_I] * 7 + [sc, _P, _I, _P, _I]
+            getattr(L, f"{t}trmm_").argtypes = [_P] * 11
         for f in ("sgemm_", "dgemm_", "cgemm_", "zgemm_"):
             getattr(L, f).argtypes = [_P] * 13
         L.xerbla_.argtypes = [ctypes.c_char_p, _P]
@@ -266,6 +272,99 @@ def cgemm_(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
     r = ctypes.byref
     lib().cgemm_(r(ta), r(tb), r(ints[0]), r(ints[1]), r(ints[2]), al.ctypes.data, _addr(A), r(ints[3]),
                  _addr(B), r(ints[4]), be.ctypes.data, _addr(C), r(ints[5]))
+
+
+SIDE = {"L": 141, "R": 142}
+DIAG = {"N": 131, "U": 132}
+CblasLeft, CblasRight = 141, 142
+CblasNonUnit, CblasUnit = 131, 132
+
+
+def _scalar_value(tag, v):
+    """A cblas_ scalar: by value for s / d, the address of an (re, im) pair
+    for c / z. The second item keeps the pair alive for the call."""
+    if tag in "sd":
+        return v, None
+    pair = _cpair32(v) if tag == "c" else _cpair(v)
+    return pair.ctypes.data, pair
+
+
+def _scalar_ref(tag, v):
+    """An F77 scalar: always by address."""
+    if tag in "sd":
+        box = (ctypes.c_float if tag == "s" else ctypes.c_double)(v)
+        return ctypes.addressof(box), box
+    pair = _cpair32(v) if tag == "c" else _cpair(v)
+    return pair.ctypes.data, pair
+
+
+def _char(c):
+    return ctypes.c_char(c.encode() if isinstance(c, str) else c)
+
+
+def _symm_fn(tag, kind):
+    name = f"cblas_{tag}{kind}"
+
+    def call(Order, Side, Uplo, M, N, alpha, A, lda, B, ldb, beta, C, ldc):
+        al, keep_a = _scalar_value(tag, alpha)
+        be, keep_b = _scalar_value(tag, beta)
+        getattr(lib(), name)(Order, Side, Uplo, M, N, al, _addr(A), lda, _addr(B), ldb, be, _addr(C), ldc)
+
+    call.__name__ = call.__qualname__ = name
+    return call
+
+
+def _trmm_fn(tag):
+    name = f"cblas_{tag}trmm"
+
+    def call(Order, Side, Uplo, TransA, Diag, M, N, alpha, A, lda, B, ldb):
+        al, keep = _scalar_value(tag, alpha)
+        getattr(lib(), name)(Order, Side, Uplo, TransA, Diag, M, N, al, _addr(A), lda, _addr(B), ldb)
+
+    call.__name__ = call.__qualname__ = name
+    return call
+
+
+def _symm_f77(tag, kind):
+    name = f"{tag}{kind}_"
+
+    def call(side, uplo, m, n, alpha, A, lda, B, ldb, beta, C, ldc):
+        sd, up = _char(side), _char(uplo)
+        ints = [ctypes.c_int(v) for v in (m, n, lda, ldb, ldc)]
+        pa, keep_a = _scalar_ref(tag, alpha)
+        pb, keep_b = _scalar_ref(tag, beta)
+        r = ctypes.byref
+        getattr(lib(), name)(r(sd), r(up), r(ints[0]), r(ints[1]), pa, _addr(A), r(ints[2]), _addr(B),
+                             r(ints[3]), pb, _addr(C), r(ints[4]))
+
+    call.__name__ = call.__qualname__ = name
+    return call
+
+
+def _trmm_f77(tag):
+    name = f"{tag}trmm_"
+
+    def call(side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb):
+        chars = [_char(c) for c in (side, uplo, transa, diag)]
+        ints = [ctypes.c_int(v) for v in (m, n, lda, ldb)]
+        pa, keep = _scalar_ref(tag, alpha)
+        r = ctypes.byref
+        getattr(lib(), name)(*(r(c) for c in chars), r(ints[0]), r(ints[1]), pa, _addr(A), r(ints[2]),
+                             _addr(B), r(ints[3]))
+
+    call.__name__ = call.__qualname__ = name
+    return call
+
+
+# cblas_?symm / ?hemm / ?trmm and their F77 forms (blas/dsymm.c, blas/zhemm.c,
+# blas/dtrmm.c in the reference): same argument order and meaning.
+cblas_ssymm, cblas_dsymm = _symm_fn("s", "symm"), _symm_fn("d", "symm")
+cblas_csymm, cblas_zsymm = _symm_fn("c", "symm"), _symm_fn("z", "symm")
+cblas_chemm, cblas_zhemm = _symm_fn("c", "hemm"), _symm_fn("z", "hemm")
+cblas_strmm, cblas_dtrmm, cblas_ctrmm, cblas_ztrmm = (_trmm_fn(t) for t in "sdcz")
+ssymm_, dsymm_, csymm_, zsymm_ = (_symm_f77(t, "symm") for t in "sdcz")
+chemm_, zhemm_ = _symm_f77("c", "hemm"), _symm_f77("z", "hemm")
+strmm_, dtrmm_, ctrmm_, ztrmm_ = (_trmm_f77(t) for t in "sdcz")
 
 
 def _f77(fn, ctype, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cplx=False):

@@ -346,6 +346,126 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
 
 bool want_ozaki(const Gemm &g, int mode) { return ozaki_selected(g, mode); }
 
+// Width of the diagonal blocks a triangular operand keeps on the native path
+// when the rest of the product is emulated.
+constexpr int kTriDiagBlock = 256;
+
+// Triangular operand on the emulated path: the diagonal blocks of the
+// (completed) triangle are moved to dg_diag and zeroed in place, the
+// emulated GEMM runs on the block-off-diagonal part, and the diagonal blocks
+// are added with the native kernel (beta 1). Every emulated sum then spans
+// at least kTriDiagBlock dense terms or none: the tip of the triangle (a
+// single nonzero per row or column, where a per-row scaled emulation loses
+// relative accuracy) is computed natively. The native share of the work is
+// about kTriDiagBlock / K; a triangle within one block runs natively whole.
+int tri_split_gemm(const Gemm &dg, bool tri_is_a, void *diag, cudaStream_t s) {
+    const size_t es = elem_size(dg.dt);
+    const int64_t n = dg.K, nb = kTriDiagBlock;
+    if (n <= nb) {
+        call_stats().path = 1;
+        return dmma_supported(dg) ? launch_gemm_dmma(dg, s) : launch_gemm_simt(dg, s);
+    }
+    void *T = tri_is_a ? const_cast<void *>(dg.A) : const_cast<void *>(dg.B);
+    const int64_t ldt = tri_is_a ? dg.lda : dg.ldb;
+    BX_TRY(launch_split_diag_blocks(dg.dt, T, ldt, n, int(nb), diag, s));
+    BX_TRY(device_gemm(dg, s));
+    for (int64_t j0 = 0; j0 < n; j0 += nb) {
+        const int64_t bs = std::min(nb, n - j0);
+        Gemm b = dg;
+        b.beta = cplx{1.0, 0.0};
+        b.K = bs;
+        const char *blk = static_cast<const char *>(diag) + size_t(j0) * nb * es;
+        if (tri_is_a) {  // C(J, :) += alpha op(A)(J, J) B(J, :)
+            b.M = bs;
+            b.A = blk; b.lda = nb;
+            b.B = static_cast<const char *>(dg.B) + size_t(j0) * es;  // tb is NoTrans
+            b.C = static_cast<char *>(dg.C) + size_t(j0) * es;
+        } else {  // C(:, J) += alpha A(:, J) op(B)(J, J)
+            b.N = bs;
+            b.A = static_cast<const char *>(dg.A) + size_t(j0) * dg.lda * es;  // ta is NoTrans
+            b.B = blk; b.ldb = nb;
+            b.C = static_cast<char *>(dg.C) + size_t(j0) * dg.ldc * es;
+        }
+        BX_TRY(dmma_supported(b) ? launch_gemm_dmma(b, s) : launch_gemm_simt(b, s));
+    }
+    return BLASX_OK;
+}
+
+// SYMM / HEMM / TRMM: an operand stored as one triangle (a_form / b_form) is
+// completed on its device copy before one device GEMM (native or emulated
+// by the precision mode; see tri_split_gemm for a triangular operand on the
+// emulated path). In core only: A, B and C (when read) are copied whole, the
+// product runs, and C is copied back. C may be the same host buffer as B
+// (TRMM): B is on the device before anything is written back.
+int host_formed(const Gemm &g, Context *c, blasx_call_stats &st, int mode) {
+    const size_t es = elem_size(g.dt);
+    const bool need_ab = !(g.alpha_zero() || g.K == 0);
+    const bool read_c = !g.beta_zero();
+    DeviceOps d;
+    d.s = c->compute;
+    d.lda = round_up(g.rows_a(), 32);
+    d.ldb = round_up(g.rows_b(), 32);
+    d.ldc = round_up(g.M, 32);
+    const size_t bytes_a = need_ab ? size_t(d.lda) * g.cols_a() * es : 0;
+    const size_t bytes_b = need_ab ? size_t(d.ldb) * g.cols_b() * es : 0;
+    const size_t bytes_c = size_t(d.ldc) * g.N * es;
+    Gemm dg = g;
+    dg.A = nullptr; dg.lda = d.lda;
+    dg.B = nullptr; dg.ldb = d.ldb;
+    dg.ldc = d.ldc;
+    dg.a_form = dg.b_form = 0;
+    const bool oz = need_ab && ozaki_selected(dg, mode);
+    const bool tri_a = g.a_form >= kTriUpper, tri_b = g.b_form >= kTriUpper;
+    const bool split = oz && (tri_a || tri_b);
+    const size_t bytes_diag = split && g.K > kTriDiagBlock ? size_t(kTriDiagBlock) * g.K * es : 0;
+    const size_t bytes_ws = oz ? ozaki_scratch_bytes(dg) : 0;
+    if (bytes_a + bytes_b + bytes_c + bytes_ws + bytes_diag > default_budget(c))
+        return set_error(BLASX_ERR_UNSUPPORTED,
+                         "symmetric / Hermitian / triangular operand: %zu bytes exceed the HBM budget",
+                         bytes_a + bytes_b + bytes_c + bytes_ws);
+    HostPin pins;
+    BX_TRY(pins.pin(g.A, need_ab ? host_extent(g.lda, g.rows_a(), g.cols_a(), es) : 0));
+    BX_TRY(pins.pin(g.B, need_ab ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
+    BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
+    cudaStream_t s = c->compute;
+    if (need_ab) {
+        BX_CUDA(cudaMallocAsync(&d.A, bytes_a ? bytes_a : 256, s));
+        BX_CUDA(cudaMallocAsync(&d.B, bytes_b ? bytes_b : 256, s));
+        BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
+                                  cudaMemcpyHostToDevice, s));
+        BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
+                                  cudaMemcpyHostToDevice, s));
+        st.h2d_bytes += double(es) * (g.rows_a() * g.cols_a() + g.rows_b() * g.cols_b());
+        BX_TRY(launch_complete_operand(g.dt, g.a_form, d.A, d.lda, g.rows_a(), s));
+        BX_TRY(launch_complete_operand(g.dt, g.b_form, d.B, d.ldb, g.rows_b(), s));
+    }
+    BX_CUDA(cudaMallocAsync(&d.C, bytes_c, s));
+    if (read_c) {
+        BX_CUDA(cudaMemcpy2DAsync(d.C, d.ldc * es, g.C, g.ldc * es, g.M * es, g.N, cudaMemcpyHostToDevice, s));
+        st.h2d_bytes += double(es) * g.M * g.N;
+    }
+    dg.A = d.A; dg.B = d.B; dg.C = d.C;
+    if (split) {
+        if (bytes_diag) BX_CUDA(cudaMallocAsync(&d.ws, bytes_diag, s));
+        BX_TRY(tri_split_gemm(dg, tri_a, d.ws, s));
+    } else if (need_ab) {
+        BX_TRY(device_gemm(dg, s));
+    } else {
+        BX_TRY(launch_scale(dg, s));
+        st.path = 3;
+    }
+    BX_CUDA(cudaMemcpy2DAsync(g.C, g.ldc * es, d.C, d.ldc * es, g.M * es, g.N, cudaMemcpyDeviceToHost, s));
+    st.d2h_bytes += double(es) * g.M * g.N;
+    BX_CUDA(cudaStreamSynchronize(s));
+    if (st.path == 2) {
+        resolve_decision(st);
+        if (*c->last_error_flag)
+            return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
+                             *c->last_error_flag);
+    }
+    return BLASX_OK;
+}
+
 }  // namespace
 
 int host_gemm(const Gemm &g) {
@@ -361,6 +481,11 @@ int host_gemm(const Gemm &g) {
     // a triangular output keeps the other triangle: C always makes the round trip
     const bool read_c = !g.beta_zero() || g.uplo != 0;
     const int mode = config().dgemm_mode.load();
+    if (g.a_form || g.b_form) {
+        const int rc = host_formed(g, c, st, mode);
+        st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
+    }
     const bool oz = need_ab && want_ozaki(g, mode);
 
     DeviceOps d;

@@ -8,6 +8,15 @@ namespace bx {
 
 // C = beta * C (alpha == 0 or K == 0); C is not read when beta == 0.
 int launch_scale(const Gemm &g, cudaStream_t s);
+// Completes the n x n operand X (ld ldx, device, in place) from its stored
+// triangle according to `form` (an OperandForm): mirror, conjugate-mirror, or
+// zero the other triangle (and set a unit diagonal). Entries of the stored
+// triangle are only read, except Hermitian diagonals (imaginary part set to
+// zero) and unit diagonals (set to one).
+int launch_complete_operand(DType dt, int form, void *X, int64_t ldx, int64_t n, cudaStream_t s);
+// Moves the nb x nb diagonal blocks of the n x n device matrix X into D
+// (ld nb, n columns: block J in columns J nb ..) and zeroes them in X.
+int launch_split_diag_blocks(DType dt, void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s);
 // g.C (g.M x g.N, ld g.ldc) += g.beta * X (ld ldx); nothing when beta == 0.
 int launch_add_scaled(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s);
 

@@ -25,6 +25,8 @@ template <typename T> struct Arith;
 template <> struct Arith<float> {
     using V = float;
     __device__ static V zero() { return 0.f; }
+    __device__ static V one() { return 1.f; }
+    __device__ static V real_part(V a) { return a; }
     __device__ static V fma(V a, V b, V c) { return fmaf(a, b, c); }
     __device__ static V conj(V a) { return a; }
     __device__ static V mul(V a, V b) { return a * b; }
@@ -33,6 +35,8 @@ template <> struct Arith<float> {
 template <> struct Arith<double> {
     using V = double;
     __device__ static V zero() { return 0.0; }
+    __device__ static V one() { return 1.0; }
+    __device__ static V real_part(V a) { return a; }
     __device__ static V fma(V a, V b, V c) { return ::fma(a, b, c); }
     __device__ static V conj(V a) { return a; }
     __device__ static V mul(V a, V b) { return a * b; }
@@ -41,6 +45,8 @@ template <> struct Arith<double> {
 template <> struct Arith<z2> {
     using V = z2;
     __device__ static V zero() { return {0.0, 0.0}; }
+    __device__ static V one() { return {1.0, 0.0}; }
+    __device__ static V real_part(V a) { return {a.re, 0.0}; }
     __device__ static V fma(V a, V b, V c) {
         c.re = ::fma(a.re, b.re, c.re);
         c.re = ::fma(-a.im, b.im, c.re);
@@ -58,6 +64,8 @@ template <> struct Arith<z2> {
 template <> struct Arith<c2> {
     using V = c2;
     __device__ static V zero() { return {0.f, 0.f}; }
+    __device__ static V one() { return {1.f, 0.f}; }
+    __device__ static V real_part(V a) { return {a.re, 0.f}; }
     __device__ static V fma(V a, V b, V c) {
         c.re = fmaf(a.re, b.re, c.re);
         c.re = fmaf(-a.im, b.im, c.re);
@@ -196,6 +204,63 @@ template <typename T> int launch_add_scaled_t(const Gemm &g, const void *X, int6
     return BLASX_OK;
 }
 
+// One thread per entry of column j = blockIdx.y (grid-strided over j).
+template <typename T>
+__global__ void complete_operand_kernel(int form, T *__restrict__ X, int64_t ldx, int n) {
+    using Ar = Arith<T>;
+    const bool upper = form == kSymUpper || form == kHermUpper || form == kTriUpper || form == kTriUpperUnit;
+    const bool herm = form == kHermUpper || form == kHermLower;
+    const bool tri = form >= kTriUpper;
+    const bool unit = form == kTriUpperUnit || form == kTriLowerUnit;
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y)
+        for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+             i += int64_t(gridDim.x) * blockDim.x) {
+            T *xp = &X[i + j * ldx];
+            if (i == j) {
+                if (unit) *xp = Ar::one();
+                else if (herm) *xp = Ar::real_part(*xp);
+                continue;
+            }
+            const bool stored = upper ? i < j : i > j;
+            if (stored) continue;
+            if (tri) *xp = Ar::zero();
+            else *xp = herm ? Ar::conj(X[j + i * ldx]) : X[j + i * ldx];
+        }
+}
+
+template <typename T> int launch_complete_t(int form, void *X, int64_t ldx, int64_t n, cudaStream_t s) {
+    dim3 grid(unsigned(std::min<int64_t>(8, (n + 255) / 256)), unsigned(std::min<int64_t>(n, 65535)));
+    complete_operand_kernel<T><<<grid, 256, 0, s>>>(form, static_cast<T *>(X), ldx, int(n));
+    BX_CUDA(cudaGetLastError());
+    count_launch();
+    return BLASX_OK;
+}
+
+// Moves the nb x nb diagonal blocks of the n x n matrix X (the last one
+// ragged) into D (column-major, ld nb: block J in columns J nb .. J nb + bs)
+// and zeroes them in X. One thread per entry of column j = blockIdx.y (grid-
+// strided); each entry is read and written by that thread only. T is an
+// opaque element of the right size.
+template <typename T>
+__global__ void split_diag_blocks_kernel(T *__restrict__ X, int64_t ldx, int n, int nb, T *__restrict__ D) {
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
+        const int64_t r0 = (j / nb) * nb;
+        const int64_t r1 = r0 + nb < n ? r0 + nb : n;
+        for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+            D[(i - r0) + j * nb] = X[i + j * ldx];
+            X[i + j * ldx] = T{};
+        }
+    }
+}
+
+template <typename T> int launch_split_t(void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s) {
+    dim3 grid(1, unsigned(std::min<int64_t>(n, 65535)));
+    split_diag_blocks_kernel<T><<<grid, 256, 0, s>>>(static_cast<T *>(X), ldx, int(n), nb, static_cast<T *>(D));
+    BX_CUDA(cudaGetLastError());
+    count_launch();
+    return BLASX_OK;
+}
+
 template <typename T> int launch_simt_t(const Gemm &g, cudaStream_t s) {
     dim3 grid(unsigned((g.M + BM - 1) / BM), unsigned((g.N + BN - 1) / BN));
     if (grid.y > 65535) return set_error(BLASX_ERR_UNSUPPORTED, "N too large for SIMT grid");
@@ -229,6 +294,25 @@ int launch_gemm_simt(const Gemm &g, cudaStream_t s) {
         case DType::F64: return launch_simt_t<double>(g, s);
         case DType::C64: return launch_simt_t<c2>(g, s);
         default: return launch_simt_t<z2>(g, s);
+    }
+}
+
+int launch_complete_operand(DType dt, int form, void *X, int64_t ldx, int64_t n, cudaStream_t s) {
+    if (form == kGeneral || n <= 0) return BLASX_OK;
+    switch (dt) {
+        case DType::F32: return launch_complete_t<float>(form, X, ldx, n, s);
+        case DType::F64: return launch_complete_t<double>(form, X, ldx, n, s);
+        case DType::C64: return launch_complete_t<c2>(form, X, ldx, n, s);
+        default: return launch_complete_t<z2>(form, X, ldx, n, s);
+    }
+}
+
+int launch_split_diag_blocks(DType dt, void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s) {
+    if (n <= 0) return BLASX_OK;
+    switch (elem_size(dt)) {
+        case 4: return launch_split_t<uint32_t>(X, ldx, n, nb, D, s);
+        case 8: return launch_split_t<uint64_t>(X, ldx, n, nb, D, s);
+        default: return launch_split_t<uint4>(X, ldx, n, nb, D, s);
     }
 }
 

@@ -27,6 +27,17 @@ struct cplx {
 
 enum Trans : int { NoTrans = 111, TransT = 112, ConjT = 113 };
 
+// How a square operand is stored (SYMM / HEMM / TRMM): the named triangle
+// holds the data; the rest is implied (mirrored, conjugate-mirrored, or zero
+// with a stored or unit diagonal).
+enum OperandForm : int {
+    kGeneral = 0,
+    kSymUpper, kSymLower,          // X = X^T
+    kHermUpper, kHermLower,        // X = X^H (diagonal imaginary parts are taken as zero)
+    kTriUpper, kTriLower,          // zero outside the triangle
+    kTriUpperUnit, kTriLowerUnit,  // zero outside, ones on the diagonal
+};
+
 // One column-major GEMM C = alpha op(A) op(B) + beta C. Pointers are host or
 // device addresses depending on the caller; leading dimensions in elements.
 struct Gemm {
@@ -53,6 +64,9 @@ struct Gemm {
     // diagonal for a block of a larger C. Entries outside are not touched.
     int uplo = 0;
     int64_t diag = 0;
+    // Stored form of a square A (or B): only one triangle holds data, and the
+    // operand is completed on the device before the product (SYMM, HEMM, TRMM).
+    int a_form = 0, b_form = 0;  // an OperandForm
 
     bool alpha_zero() const { return alpha.re == 0 && alpha.im == 0; }
     bool beta_zero() const { return beta.re == 0 && beta.im == 0; }

@@ -27,13 +27,15 @@
 extern "C" {
 #endif
 
-/* Enum values of the reference's include/cblas.h:11-12 (skipped when a
+/* Enum values of the reference's include/cblas.h:11-15 (skipped when a
  * cblas.h guarded by CBLAS_H was included first). */
 #if !defined(CBLAS_H) && !defined(CBLAS_ENUM_DEFINED_H)
 #define CBLAS_ENUM_DEFINED_H
 enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
 enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 };
 enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 };
+enum CBLAS_DIAG { CblasNonUnit = 131, CblasUnit = 132 };
+enum CBLAS_SIDE { CblasLeft = 141, CblasRight = 142 };
 #endif
 
 /* ------------------------------------------------------------------------ */
@@ -125,6 +127,85 @@ void dsyr2k_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, 
              double *B, int *ldb, double *beta, double *C, int *ldc);
 void zsyr2k_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda,
              double *B, int *ldb, double *beta, double *C, int *ldc);
+
+/* Replace cblas_ssymm / cblas_dsymm / cblas_csymm / cblas_zsymm
+ * (include/cblas.h:429,459,489,519; implementations blas/dsymm.c:16-72 and
+ * siblings, which always run on the host BLAS) and cblas_chemm / cblas_zhemm
+ * (include/cblas.h:548,563; blas/zhemm.c:16-77): C = alpha A B + beta C (Side
+ * Left, A M x M) or alpha B A + beta C (Right, A N x N), A symmetric
+ * (Hermitian for ?hemm) and read from its Uplo triangle only. On the GPU:
+ * the stored triangle is completed on the device, then the GEMM runs. */
+void cblas_ssymm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const int M, const int N, const float alpha,
+                 const float *A, const int lda, const float *B, const int ldb, const float beta,
+                 float *C, const int ldc);
+void cblas_dsymm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const int M, const int N, const double alpha,
+                 const double *A, const int lda, const double *B, const int ldb, const double beta,
+                 double *C, const int ldc);
+void cblas_csymm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, const void *B, const int ldb, const void *beta,
+                 void *C, const int ldc);
+void cblas_zsymm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, const void *B, const int ldb, const void *beta,
+                 void *C, const int ldc);
+void cblas_chemm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, const void *B, const int ldb, const void *beta,
+                 void *C, const int ldc);
+void cblas_zhemm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, const void *B, const int ldb, const void *beta,
+                 void *C, const int ldc);
+
+/* Replace cblas_strmm / cblas_dtrmm / cblas_ctrmm / cblas_ztrmm
+ * (include/cblas.h:443,473,503,533; implementations blas/dtrmm.c:17-64 and
+ * siblings, host BLAS only): B = alpha op(A) B (Side Left) or alpha B op(A)
+ * (Right), A triangular (Uplo, Diag), op(A) = A, A^T or A^H. B is read whole
+ * before the product overwrites it. */
+void cblas_strmm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const float alpha,
+                 const float *A, const int lda, float *B, const int ldb);
+void cblas_dtrmm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const double alpha,
+                 const double *A, const int lda, double *B, const int ldb);
+void cblas_ctrmm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, void *B, const int ldb);
+void cblas_ztrmm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, void *B, const int ldb);
+
+/* Replace the F77 wrappers ?symm_ (blas/dsymm.c:74-95), ?hemm_ (blas/zhemm.c:
+ * 80-99) and ?trmm_ (blas/dtrmm.c:67-91): side 'L'/'R', uplo 'U'/'L', transa
+ * 'N'/'T'/'C', diag 'N'/'U', column-major, every argument by pointer; complex
+ * scalars are (re, im) pairs. */
+void ssymm_(char *side, char *uplo, int *m, int *n, float *alpha, float *A, int *lda, float *B,
+            int *ldb, float *beta, float *C, int *ldc);
+void dsymm_(char *side, char *uplo, int *m, int *n, double *alpha, double *A, int *lda, double *B,
+            int *ldb, double *beta, double *C, int *ldc);
+void csymm_(char *side, char *uplo, int *m, int *n, float *alpha, float *A, int *lda, float *B,
+            int *ldb, float *beta, float *C, int *ldc);
+void zsymm_(char *side, char *uplo, int *m, int *n, double *alpha, double *A, int *lda, double *B,
+            int *ldb, double *beta, double *C, int *ldc);
+void chemm_(char *side, char *uplo, int *m, int *n, float *alpha, float *A, int *lda, float *B,
+            int *ldb, float *beta, float *C, int *ldc);
+void zhemm_(char *side, char *uplo, int *m, int *n, double *alpha, double *A, int *lda, double *B,
+            int *ldb, double *beta, double *C, int *ldc);
+void strmm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, float *alpha,
+            float *A, int *lda, float *B, int *ldb);
+void dtrmm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, double *alpha,
+            double *A, int *lda, double *B, int *ldb);
+void ctrmm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, float *alpha,
+            float *A, int *lda, float *B, int *ldb);
+void ztrmm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, double *alpha,
+            double *A, int *lda, double *B, int *ldb);
 
 /* Replaces xerbla_, blas/error.c:5: prints
  * " ** On entry to <NAME> parameter number <info> had an illegal value".

@@ -174,6 +174,58 @@ def syrk(uplo, trans, N, K, alpha, A, lda, beta, C, ldc, B=None, ldb=None):
     return C
 
 
+def complete(kind, uplo, X, n, diag="N"):
+    """The full n x n matrix that BLAS reads from the uplo triangle of X:
+    kind 'S' symmetric (mirror), 'H' Hermitian (conjugate mirror, the
+    imaginary parts of the diagonal taken as zero), 'T' triangular (zero
+    outside, ones on the diagonal when diag is 'U'). Entries outside the
+    triangle of X are never read. Returns a new Fortran-ordered array."""
+    S = np.array(X[:n, :n], order="F")
+    keep = tri_mask(uplo, n)
+    strict = keep & ~np.eye(n, dtype=bool)
+    if kind == "T":
+        S[~keep] = 0
+        if diag == "U":
+            np.fill_diagonal(S, 1)
+        return S
+    other = S.T.conj() if kind == "H" else S.T
+    S = np.where(strict, S, np.where(strict.T, other, S))
+    if kind == "H":
+        np.fill_diagonal(S, np.diag(S).real)
+    return np.asfortranarray(S)
+
+
+def symm(side, uplo, M, N, alpha, A, lda, B, ldb, beta, C, ldc, herm=False):
+    """Restatement of BLAS ?SYMM / ?HEMM, which the reference hands to its CPU
+    BLAS for every size (blas/dsymm.c:44-57, blas/zhemm.c): C <- alpha A B +
+    beta C (side 'L', A M x M) or alpha B A + beta C (side 'R', A N x N), A
+    read from its uplo triangle only. A tiled GEMM on the completed A."""
+    na = M if side == "L" else N
+    Af = complete("H" if herm else "S", uplo, A, na)
+    if side == "L":
+        gemm_tiled("N", "N", M, N, M, alpha, Af, na, B, ldb, beta, C, ldc)
+    else:
+        gemm_tiled("N", "N", M, N, N, alpha, B, ldb, Af, na, beta, C, ldc)
+    return C
+
+
+def trmm(side, uplo, transa, diag, M, N, alpha, A, lda, B, ldb):
+    """Restatement of BLAS ?TRMM, which the reference hands to its CPU BLAS
+    (blas/dtrmm.c:43-60): B <- alpha op(A) B (side 'L', A M x M) or alpha B
+    op(A) ('R', A N x N), A triangular (uplo, diag), op(A) = A, A^T or A^H.
+    A tiled GEMM on the completed A into a fresh buffer, copied into B."""
+    na = M if side == "L" else N
+    Af = complete("T", uplo, A, na, diag)
+    Bin = np.array(B[:M, :N], order="F")
+    out = np.zeros((M, N), dtype=B.dtype, order="F")
+    if side == "L":
+        gemm_tiled(transa, "N", M, N, M, alpha, Af, na, Bin, M, 0.0, out, M)
+    else:
+        gemm_tiled("N", transa, M, N, N, alpha, Bin, M, Af, na, 0.0, out, M)
+    B[:M, :N] = out
+    return B
+
+
 def dd_entries(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, ii, jj):
     """Double-double values of sampled entries of alpha*op(A)op(B)+beta*C0.
 

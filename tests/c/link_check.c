@@ -8,6 +8,8 @@
 enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
 enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 };
 enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 };
+enum CBLAS_DIAG { CblasNonUnit = 131, CblasUnit = 132 };
+enum CBLAS_SIDE { CblasLeft = 141, CblasRight = 142 };
 #endif
 #include "blasx_b200.h"
 
@@ -26,6 +28,14 @@ int main(void) {
     fflush(stdout);
     /* DSYRK: ldc = 2 < N = 4: parameter 10 */
     cblas_dsyrk(CblasColMajor, CblasUpper, CblasNoTrans, 4, 4, 1.0, A, 4, 0.0, C, 2);
+    fflush(stdout);
+    /* DSYMM: ldb = 2 < M = 4: parameter 9; ZHEMM: bad side; DTRMM: bad diag */
+    cblas_dsymm(CblasColMajor, CblasLeft, CblasUpper, 4, 4, 1.0, A, 4, B, 2, 0.0, C, 4);
+    fflush(stdout);
+    double one[2] = {1.0, 0.0};
+    cblas_zhemm(CblasColMajor, (enum CBLAS_SIDE)0, CblasUpper, 2, 2, one, A, 2, B, 2, one, C, 2);
+    fflush(stdout);
+    cblas_dtrmm(CblasColMajor, CblasRight, CblasLower, CblasTrans, (enum CBLAS_DIAG)7, 4, 4, 1.0, A, 4, C, 4);
     fflush(stdout);
     /* M = 0: quick return, no device needed */
     cblas_dgemm(CblasColMajor, CblasNoTrans, CblasNoTrans, 0, 4, 4, 1.0, A, 4, B, 4, 0.0, C, 4);

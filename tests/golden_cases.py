@@ -68,3 +68,130 @@ def tol_ratio(case, got):
     err = np.abs(got[:M, :N].astype(np.complex128) - case["C"][:M, :N].astype(np.complex128))
     scale = np.maximum(bound, np.finfo(np.float64).tiny)
     return float(np.max(err / (gamma * scale))) if err.size else 0.0
+
+
+# ---- SYMM / HEMM / TRMM fixtures (tests/golden/symm_trmm_golden.npz) --------
+
+SYMM_GOLDEN_DT = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}
+SIDE_OF = {141: "L", 142: "R"}
+UPLO_OF = {121: "U", 122: "L"}
+TRANS_OF = {111: "N", 112: "T", 113: "C"}
+DIAG_OF = {131: "N", 132: "U"}
+
+
+def poison(kind, uplo, A, na, diag="N"):
+    """NaN in the entries of A that BLAS does not reference: the triangle
+    opposite uplo, the diagonal for Diag = Unit; the imaginary parts of a
+    Hermitian diagonal get a nonzero value that BLAS must ignore."""
+    i, j = np.indices((na, na))
+    hidden = (i > j) if uplo == "U" else (i < j)
+    V = A[:na, :na]
+    V[hidden] = np.nan
+    if kind == "T" and diag == "U":
+        np.fill_diagonal(V, np.nan)
+    if kind == "H":
+        d = np.diag(V).copy()
+        np.fill_diagonal(V, d.real + 1j * 0.375)
+
+
+def symm_fill(kind, tag, meta):
+    """Inputs of one SYMM / HEMM (kind 'S' / 'H') or TRMM ('T') case from its
+    meta row, and the column-major form of the problem.
+      'S' / 'H': meta = order, side, uplo, M, N, lda, ldb, ldc, seed
+      'T'      : meta = order, side, uplo, trans, diag, M, N, lda, ldb, seed
+    Arrays are Fortran-ordered with the leading dimension first: a row-major
+    (101) matrix with r rows and leading dimension ld is the array of shape
+    (ld, r), whose columns are the matrix's rows. The column-major problem of
+    a row-major call has side and uplo flipped and M, N swapped."""
+    dt = SYMM_GOLDEN_DT[tag]
+    meta = [int(v) for v in meta]
+    if kind in "SH":
+        order, side, uplo, M, N, lda, ldb, ldc, seed = meta
+        trans, diag = 111, 131
+    else:
+        order, side, uplo, trans, diag, M, N, lda, ldb, seed = meta
+        ldc = ldb
+    rm = order == 101
+    side_s, uplo_s = SIDE_OF[side], UPLO_OF[uplo]
+    cm = dict(side=side_s, uplo=uplo_s, M=M, N=N, trans=TRANS_OF[trans], diag=DIAG_OF[diag])
+    if rm:
+        cm.update(side="R" if side_s == "L" else "L", uplo="L" if uplo_s == "U" else "U", M=N, N=M)
+    na = cm["M"] if cm["side"] == "L" else cm["N"]
+    A = oracle.uniform((lda, na), dt, seed)
+    poison(kind, cm["uplo"], A, na, cm["diag"])
+    B = oracle.uniform((ldb, cm["N"]), dt, seed + 1)
+    out = dict(order=order, side=side, uplo=uplo, trans=trans, diag=diag, M=M, N=N, lda=lda, ldb=ldb,
+               ldc=ldc, A=A, B=B, na=na, cm=cm, dt=dt)
+    if kind in "SH":
+        out["C"] = oracle.uniform((ldc, cm["N"]), dt, seed + 2)
+    return out
+
+
+def symm_checksum(x):
+    parts = [np.nansum(x["A"]), np.nansum(x["B"])] + ([np.nansum(x["C"])] if "C" in x else [])
+    return np.array(parts, dtype=np.complex128)
+
+
+def symm_keys(golden, prefix):
+    return sorted({k.rsplit("_", 1)[0] for k in golden.files if k.startswith(prefix)},
+                  key=lambda k: int(k.split("_")[-1]))
+
+
+def symm_case(golden, key):
+    """(kind, tag, inputs, alpha, beta, reference output) of one fixture key."""
+    kind = {"symm": "S", "hemm": "H", "trmm": "T"}[key.split("_")[0]]
+    tag = key.split("_")[1]
+    x = symm_fill(kind, tag, golden[key + "_meta"])
+    assert np.allclose(symm_checksum(x), golden[key + "_sum"]), "fixture generator changed"
+    sc = golden[key + "_scal"]
+    real = tag in "sd"
+    al = float(sc[0].real) if real else complex(sc[0])
+    be = (float(sc[1].real) if real else complex(sc[1])) if kind in "SH" else None
+    return kind, tag, x, al, be, golden[key + "_C"]
+
+
+def symm_bound(kind, x, al, be):
+    """Componentwise bound on |computed - reference| over the column-major
+    output block: both results carry at most (K + 2) u (|alpha| |op(A)| |B| +
+    |beta| |C0|) each (twice that for complex), K the order of A."""
+    cm, na = x["cm"], x["na"]
+    M, N = cm["M"], cm["N"]
+    Af = oracle.complete({"S": "S", "H": "H", "T": "T"}[kind], cm["uplo"], x["A"], na, cm["diag"])
+    aA = np.abs(Af).astype(np.float64)
+    if cm["trans"] != "N":
+        aA = aA.T
+    aB = np.abs(x["B"][:M, :N]).astype(np.float64)
+    prod = aA @ aB if cm["side"] == "L" else aB @ aA
+    bound = abs(al) * prod
+    if kind in "SH" and be != 0:
+        bound = bound + abs(be) * np.abs(x["C"][:M, :N]).astype(np.float64)
+    dt = x["dt"]
+    u = oracle.UNIT_ROUNDOFF[np.dtype(dt).type]
+    cplx = np.issubdtype(dt, np.complexfloating)
+    return 2 * (na + 2) * u * (2.0 if cplx else 1.0) * bound
+
+
+def symm_oracle(kind, x, al, be):
+    """The oracle's result for one case, on copies (column-major problem)."""
+    cm = x["cm"]
+    if kind in "SH":
+        C = x["C"].copy(order="F")
+        return oracle.symm(cm["side"], cm["uplo"], cm["M"], cm["N"], al, x["A"], x["lda"], x["B"], x["ldb"], be,
+                           C, x["ldc"], herm=kind == "H")
+    B = x["B"].copy(order="F")
+    return oracle.trmm(cm["side"], cm["uplo"], cm["trans"], cm["diag"], cm["M"], cm["N"], al, x["A"], x["lda"], B,
+                       x["ldb"])
+
+
+def symm_check(kind, x, got, want, al, be):
+    """got against the reference output: the M x N block (column-major view)
+    within the bound, finite, and every padding row exactly the input."""
+    cm = x["cm"]
+    M, N = cm["M"], cm["N"]
+    before = x["C"] if kind in "SH" else x["B"]
+    assert np.array_equal(got[M:], before[M:], equal_nan=True)
+    blk = got[:M, :N]
+    assert np.all(np.isfinite(blk)), "a non-referenced entry of A was read"
+    err = np.abs(blk.astype(np.complex128) - want[:M, :N].astype(np.complex128))
+    bound = symm_bound(kind, x, al, be)
+    assert np.all(err <= bound), float(np.max(err / np.maximum(bound, 1e-300)))

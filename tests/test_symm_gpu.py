@@ -1,0 +1,230 @@
+"""GPU tests of cblas_?symm / ?hemm / ?trmm: the reference's own outputs
+(golden fixtures, its CPU BLAS path; the entries BLAS must not read hold NaN)
+on the native and the emulated paths, larger cases against the double-double
+oracle, and the F77 wrappers."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from golden_cases import symm_case, symm_check, symm_keys
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_SYMM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "symm_trmm_golden.npz")
+
+
+@pytest.fixture(scope="module")
+def sgolden():
+    return np.load(GOLDEN_SYMM)
+
+
+@pytest.fixture(params=["native", "ozaki"])
+def mode(blx, request):
+    prev = blx.set_dgemm_mode(blx.MODE_NATIVE if request.param == "native" else blx.MODE_OZAKI)
+    yield request.param
+    blx.set_dgemm_mode(prev)
+
+
+def run_case(blx, kind, tag, x, al, be):
+    """The library call the reference made for this case; returns the output array."""
+    if kind in "SH":
+        C = x["C"].copy(order="F")
+        fn = getattr(blx, f"cblas_{tag}{'symm' if kind == 'S' else 'hemm'}")
+        fn(x["order"], x["side"], x["uplo"], x["M"], x["N"], al, x["A"], x["lda"], x["B"], x["ldb"], be, C,
+           x["ldc"])
+        out = C
+    else:
+        out = x["B"].copy(order="F")
+        getattr(blx, f"cblas_{tag}trmm")(x["order"], x["side"], x["uplo"], x["trans"], x["diag"], x["M"], x["N"],
+                                         al, x["A"], x["lda"], out, x["ldb"])
+    assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+    return out
+
+
+@pytest.mark.parametrize("prefix", ["symm_", "hemm_", "trmm_"])
+def test_matches_reference_outputs(blx, sgolden, mode, prefix):
+    for key in symm_keys(sgolden, prefix):
+        kind, tag, x, al, be, want = symm_case(sgolden, key)
+        got = run_case(blx, kind, tag, x, al, be)
+        symm_check(kind, x, got, want, al, be)
+
+
+def sample(M, N, seed, n=5000):
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, M, n), rng.integers(0, N, n)
+
+
+def check_dd(C, ta, tb, M, N, K, al, X, ldx, Y, ldy, be, C0, ldc, seed):
+    ii, jj = sample(M, N, seed)
+    val, bound = oracle.dd_entries(ta, tb, M, N, K, al, X, ldx, Y, ldy, be, C0, ldc, ii, jj)
+    ratio, err = oracle.componentwise_ratio(C, ii, jj, val, bound, K, C.dtype.type)
+    assert ratio <= 1.0, ratio
+    return err
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("dt,herm", [(np.float64, False), (np.complex128, False), (np.complex128, True)])
+def test_symm_large_vs_oracle(blx, mode, side, uplo, dt, herm):
+    """Larger than one tile, ragged; A's other triangle is NaN. The emulated
+    path is at least as accurate as the native kernel on the same inputs."""
+    M, N = 1100, 900
+    na = M if side == "L" else N
+    A = oracle.uniform((na + 3, na), dt, 11)
+    i, j = np.indices((na, na))
+    A[:na, :na][(i > j) if uplo == "U" else (i < j)] = np.nan
+    B = oracle.uniform((M + 1, N), dt, 12)
+    C0 = oracle.uniform((M + 2, N), dt, 13)
+    al, be = (1.25, -0.5) if dt == np.float64 else (complex(1.25, 0.5), complex(-0.5, 0.25))
+    tag = "d" if dt == np.float64 else "z"
+    fn = getattr(blx, f"cblas_{tag}{'hemm' if herm else 'symm'}")
+
+    def call():
+        C = C0.copy(order="F")
+        fn(102, blx.SIDE[side], blx.UPLO[uplo], M, N, al, A, na + 3, B, M + 1, be, C, M + 2)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        return C
+
+    C = call()
+    assert blx.call_stats()["path"] == (2 if mode == "ozaki" else 1), blx.call_stats()
+    assert np.array_equal(C[M:], C0[M:])
+    Af = oracle.complete("H" if herm else "S", uplo, A, na)
+    args = (Af, na, B, M + 1) if side == "L" else (B, M + 1, Af, na)
+    err = check_dd(C, "N", "N", M, N, na, al, *args, be, C0, M + 2, 21)
+    if mode == "ozaki":
+        blx.set_dgemm_mode(blx.MODE_NATIVE)
+        Cn = call()
+        blx.set_dgemm_mode(blx.MODE_OZAKI)
+        err_n = check_dd(Cn, "N", "N", M, N, na, al, *args, be, C0, M + 2, 21)
+        assert err <= max(err_n, 2.0 ** -53), (err, err_n)
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo,trans,diag", [("U", "N", "N"), ("L", "T", "U"), ("U", "C", "U"), ("L", "N", "N")])
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
+def test_trmm_large_vs_oracle(blx, mode, side, uplo, trans, diag, dt):
+    """B = alpha op(A) B in place, A's other triangle (and a unit diagonal) NaN."""
+    if trans == "C" and dt == np.float64:
+        trans = "T"
+    M, N = 1000, 1300
+    na = M if side == "L" else N
+    A = oracle.uniform((na, na), dt, 31)
+    i, j = np.indices((na, na))
+    A[(i > j) if uplo == "U" else (i < j)] = np.nan
+    if diag == "U":
+        np.fill_diagonal(A, np.nan)
+    B0 = oracle.uniform((M + 1, N), dt, 32)
+    B = B0.copy(order="F")
+    al = 0.75 if dt == np.float64 else complex(0.75, -0.5)
+    tag = "d" if dt == np.float64 else "z"
+    getattr(blx, f"cblas_{tag}trmm")(102, blx.SIDE[side], blx.UPLO[uplo], blx.TRANS[trans], blx.DIAG[diag], M, N,
+                                     al, A, na, B, M + 1)
+    assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+    assert blx.call_stats()["path"] == (2 if mode == "ozaki" else 1), blx.call_stats()
+    assert np.array_equal(B[M:], B0[M:])
+    Af = oracle.complete("T", uplo, A, na, diag)
+    Z = np.zeros_like(B0)
+    if side == "L":
+        check_dd(B, trans, "N", M, N, M, al, Af, na, B0, M + 1, 0.0, Z, M + 1, 41)
+    else:
+        check_dd(B, "N", trans, M, N, N, al, B0, M + 1, Af, na, 0.0, Z, M + 1, 41)
+
+
+def test_f77_wrappers_match_cblas(blx):
+    M, N = 300, 200
+    A = oracle.uniform((M, M), np.float64, 51)
+    B = oracle.uniform((M, N), np.float64, 52)
+    C0 = oracle.uniform((M, N), np.float64, 53)
+    C1, C2 = C0.copy(order="F"), C0.copy(order="F")
+    blx.cblas_dsymm(102, 141, 122, M, N, 0.5, A, M, B, M, 2.0, C1, M)
+    blx.dsymm_("l", "L", M, N, 0.5, A, M, B, M, 2.0, C2, M)
+    assert np.array_equal(C1, C2)
+    Az = oracle.uniform((N, N), np.complex128, 54)
+    Bz = oracle.uniform((M, N), np.complex128, 55)
+    B1, B2 = Bz.copy(order="F"), Bz.copy(order="F")
+    blx.cblas_ztrmm(102, 142, 121, 113, 132, M, N, complex(1, 2), Az, N, B1, M)
+    blx.ztrmm_("R", "u", "c", "U", M, N, complex(1, 2), Az, N, B2, M)
+    assert np.array_equal(B1, B2)
+    Ac = oracle.uniform((M, M), np.complex64, 56)
+    Bc = oracle.uniform((M, N), np.complex64, 57)
+    Cc0 = oracle.uniform((M, N), np.complex64, 58)
+    D1, D2 = Cc0.copy(order="F"), Cc0.copy(order="F")
+    blx.cblas_chemm(102, 141, 121, M, N, complex(0.5, 0.5), Ac, M, Bc, M, complex(1, 0), D1, M)
+    blx.chemm_("L", "U", M, N, complex(0.5, 0.5), Ac, M, Bc, M, complex(1, 0), D2, M)
+    assert np.array_equal(D1, D2)
+
+
+def test_over_the_budget_fails_loudly(blx):
+    """Operands that do not fit the HBM budget are reported, not computed
+    elsewhere: the output is left unchanged."""
+    blx.set_hbm_budget(8 << 20)
+    try:
+        M, N = 1024, 1024
+        A = oracle.uniform((M, M), np.float64, 61)
+        B = oracle.uniform((M, N), np.float64, 62)
+        C0 = oracle.uniform((M, N), np.float64, 63)
+        C = C0.copy(order="F")
+        blx.cblas_dsymm(102, 141, 121, M, N, 1.0, A, M, B, M, 1.0, C, M)
+        assert blx.last_status() == blx.BLASX_ERR_UNSUPPORTED
+        assert np.array_equal(C, C0)
+    finally:
+        blx.set_hbm_budget(0)
+
+
+def test_symm_while_serving(blx):
+    blx.serve_start(0, 0, 4)
+    try:
+        M, N = 700, 500
+        A = oracle.uniform((M, M), np.float64, 71)
+        B = oracle.uniform((M, N), np.float64, 72)
+        C0 = oracle.uniform((M, N), np.float64, 73)
+        C = C0.copy(order="F")
+        blx.cblas_dsymm(102, 141, 121, M, N, 1.0, A, M, B, M, 1.0, C, M)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+    finally:
+        blx.serve_stop()
+    want = oracle.symm("L", "U", M, N, 1.0, A, M, B, M, 1.0, C0.copy(order="F"), M)
+    np.testing.assert_allclose(C, want, rtol=1e-11, atol=1e-11)
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.complex64, np.float64])
+@pytest.mark.parametrize("side,uplo", [("R", "L"), ("L", "U")])
+def test_trmm_emulated_is_componentwise_accurate_at_the_tip(blx, dt, side, uplo):
+    """Emulated path with the triangle wider than one diagonal block: the
+    diagonal blocks run natively, so the tip of a unit triangle (one nonzero,
+    the 1) reproduces alpha B exactly, and for the single-precision types every
+    entry is within the componentwise bound of the exact product."""
+    prev = blx.set_dgemm_mode(blx.MODE_OZAKI)
+    try:
+        M, N = 600, 700
+        na = M if side == "L" else N
+        A = oracle.uniform((na, na), dt, 91)
+        B0 = oracle.uniform((M, N), dt, 92)
+        B = B0.copy(order="F")
+        tag = {np.float32: "s", np.complex64: "c", np.float64: "d"}[dt]
+        getattr(blx, f"cblas_{tag}trmm")(102, blx.SIDE[side], blx.UPLO[uplo], 111, 132, M, N, 0.5, A, na, B, M)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        assert blx.call_stats()["path"] == 2, blx.call_stats()
+        if side == "R":  # lower, unit: the last column of A is e_N
+            assert np.array_equal(B[:, -1], (0.5 * B0[:, -1]).astype(dt))
+        else:  # upper, unit: the last row of A is e_M^T
+            assert np.array_equal(B[-1, :], (0.5 * B0[-1, :]).astype(dt))
+        Af = oracle.complete("T", uplo, A, na, "U")
+        if dt == np.float64:
+            Z = np.zeros_like(B0)
+            if side == "L":
+                check_dd(B, "N", "N", M, N, M, 0.5, Af, na, B0, M, 0.0, Z, M, 93)
+            else:
+                check_dd(B, "N", "N", M, N, N, 0.5, B0, M, Af, na, 0.0, Z, M, 93)
+            return
+        wide = np.complex128 if dt == np.complex64 else np.float64
+        exact = 0.5 * (Af.astype(wide) @ B0.astype(wide) if side == "L" else B0.astype(wide) @ Af.astype(wide))
+        aA, aB = np.abs(Af).astype(np.float64), np.abs(B0).astype(np.float64)
+        scale = 0.5 * (aA @ aB if side == "L" else aB @ aA)
+        bound = (na + 2) * 2.0 ** -24 * (2.0 if dt == np.complex64 else 1.0) * scale
+        err = np.abs(B.astype(wide) - exact)
+        assert np.all(err <= bound), float(np.max(err / np.maximum(bound, 1e-300)))
+    finally:
+        blx.set_dgemm_mode(prev)
