@@ -534,10 +534,11 @@ def run_workloads(args):
             print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
             del dA, tA, tC
     elif args.workload == "symm":
-        # DSYMM C = A B + 0.5 C (Left, Lower) and DTRMM B = A B (Left, Upper, NoTrans, NonUnit),
-        # M = N in {8192, 16384}, through the drop-in calls on pinned host arrays (copies in the timed
-        # call), emulated and native; credited 2 M^2 N (SYMM) and M^2 N (TRMM) flops; accuracy on
-        # sampled entries against the double-double oracle on the completed A
+        # DSYMM C = A B + 0.5 C (Left, Lower), DTRMM B = A B and DTRSM B = A^-1 B (Left, Upper,
+        # NoTrans, NonUnit), M = N in {8192, 16384}, through the drop-in calls on pinned host arrays
+        # (copies in the timed call), emulated and native; credited 2 M^2 N (SYMM) and M^2 N (TRMM,
+        # TRSM) flops; accuracy on sampled entries against the double-double oracle on the completed
+        # A (for TRSM the backward error: the residual A X - B in units of (n + 2) u (|A||X| + |B|))
         import oracle
         for n in (8192, 16384):
             tA, A = _host(torch, (n, n), "f64", 11)
@@ -546,9 +547,17 @@ def run_workloads(args):
             Hs = torch.empty_like(tC, pin_memory=True)
             rng = np.random.default_rng(5)
             ii = rng.integers(0, n, args.samples); jj = rng.integers(0, n, args.samples)
-            for op in ("dsymm", "dtrmm"):
+            # DTRSM's triangle made well conditioned: A / n + 2 I
+            tT = torch.empty_like(tA, pin_memory=True)
+            tT.copy_(tA / n)
+            tT.diagonal().add_(2.0)
+            T = np.asarray(tT.numpy()).T
+            for op in ("dsymm", "dtrmm", "dtrsm"):
                 res = {}
-                Af = oracle.complete("S" if op == "dsymm" else "T", "L" if op == "dsymm" else "U", A, n)
+                if op == "dsymm":
+                    Af = oracle.complete("S", "L", A, n)
+                else:
+                    Af = oracle.complete("T", "U", T if op == "dtrsm" else A, n)
                 for mode_name, mode in (("emulated", bx.MODE_OZAKI), ("native", bx.MODE_NATIVE)):
                     bx.set_dgemm_mode(mode)
                     times = []
@@ -559,28 +568,33 @@ def run_workloads(args):
                             bx.cblas_dsymm(bx.CblasColMajor, bx.CblasLeft, bx.CblasLower, n, n, 1.0, tA.data_ptr(),
                                            n, tB.data_ptr(), n, 0.5, Hs.data_ptr(), n)
                         else:
-                            bx.cblas_dtrmm(bx.CblasColMajor, bx.CblasLeft, bx.CblasUpper, bx.CblasNoTrans,
-                                           bx.CblasNonUnit, n, n, 1.0, tA.data_ptr(), n, Hs.data_ptr(), n)
+                            fn = bx.cblas_dtrmm if op == "dtrmm" else bx.cblas_dtrsm
+                            fn(bx.CblasColMajor, bx.CblasLeft, bx.CblasUpper, bx.CblasNoTrans, bx.CblasNonUnit, n, n,
+                               1.0, (tA if op == "dtrmm" else tT).data_ptr(), n, Hs.data_ptr(), n)
                         times.append(time.perf_counter() - t0)
                     assert bx.last_status() == 0, bx.last_error()
                     st = bx.call_stats()
                     dt = times[-1]
                     Cn = Hs.numpy().reshape(n, n).T  # column-major view
-                    if op == "dsymm":
-                        val, bound = oracle.dd_entries("N", "N", n, n, n, 1.0, Af, n, B, n, 0.5, C0, n, ii, jj)
+                    if op == "dtrsm":  # backward error: residual A X - B of sampled entries, double-double
+                        val, bound = oracle.dd_entries("N", "N", n, n, n, 1.0, Af, n, Cn, n, -1.0, B, n, ii, jj)
+                        ratio = float(np.max(np.abs(val) / ((n + 2) * 2.0 ** -53 * bound)))
+                        err = float(np.max(np.abs(val) / bound))
                     else:
-                        val, bound = oracle.dd_entries("N", "N", n, n, n, 1.0, Af, n, B, n, 0.0, C0, n, ii, jj)
-                    ratio, err = oracle.componentwise_ratio(Cn, ii, jj, val, bound, n, np.float64)
+                        val, bound = oracle.dd_entries("N", "N", n, n, n, 1.0, Af, n, B, n,
+                                                       0.5 if op == "dsymm" else 0.0, C0, n, ii, jj)
+                        ratio, err = oracle.componentwise_ratio(Cn, ii, jj, val, bound, n, np.float64)
                     flops = (2.0 if op == "dsymm" else 1.0) * float(n) ** 3
                     res[mode_name] = {"tflops_e2e": flops / dt / 1e12, "seconds_e2e": dt, "path": st["path"],
                                       "moduli": st["moduli"], "bound_ratio": ratio, "max_normalised_error": err}
                 bx.set_dgemm_mode(bx.MODE_AUTO)
-                lines.append({"workload": f"{op} M=N={n}, U[-1,1], host arrays (copies included)",
+                lines.append({"workload": f"{op} M=N={n}, U[-1,1]{' (A / n + 2 I)' if op == 'dtrsm' else ''}, "
+                                          "host arrays (copies included)",
                               "flops_credited": "2 M^2 N" if op == "dsymm" else "M^2 N", **res,
                               "speedup_e2e": res["emulated"]["tflops_e2e"] / res["native"]["tflops_e2e"]})
                 print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
                 del Af
-            del tA, tB, tC, Hs
+            del tA, tB, tC, Hs, tT
     elif args.workload == "device":
         # device-resident n^3 NN calls through blasx_?gemm_device (for ncu captures of one kernel)
         n = args.size

@@ -103,8 +103,9 @@ def lib() -> ctypes.CDLL:
             for kind in ("symm", "hemm") if t in "cz" else ("symm",):
                 getattr(L, f"cblas_{t}{kind}").argtypes = [_I] * 5 + [sc, _P, _I, _P, _I, sc, _P, _I]
                 getattr(L, f"{t}{kind}_").argtypes = [_P] * 12
-            getattr(L, f"cblas_{t}trmm").argtypes = [_I] * 7 + [sc, _P, _I, _P, _I]
-            getattr(L, f"{t}trmm_").argtypes = [_P] * 11
+            for kind in ("trmm", "trsm"):
+                getattr(L, f"cblas_{t}{kind}").argtypes = [_I] * 7 + [sc, _P, _I, _P, _I]
+                getattr(L, f"{t}{kind}_").argtypes = [_P] * 11
         for f in ("sgemm_", "dgemm_", "cgemm_", "zgemm_"):
             getattr(L, f).argtypes = [_P] * 13
         L.xerbla_.argtypes = [ctypes.c_char_p, _P]
@@ -314,8 +315,8 @@ def _symm_fn(tag, kind):
     return call
 
 
-def _trmm_fn(tag):
-    name = f"cblas_{tag}trmm"
+def _trmm_fn(tag, kind="trmm"):
+    name = f"cblas_{tag}{kind}"
 
     def call(Order, Side, Uplo, TransA, Diag, M, N, alpha, A, lda, B, ldb):
         al, keep = _scalar_value(tag, alpha)
@@ -341,8 +342,8 @@ def _symm_f77(tag, kind):
     return call
 
 
-def _trmm_f77(tag):
-    name = f"{tag}trmm_"
+def _trmm_f77(tag, kind="trmm"):
+    name = f"{tag}{kind}_"
 
     def call(side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb):
         chars = [_char(c) for c in (side, uplo, transa, diag)]
@@ -356,8 +357,9 @@ def _trmm_f77(tag):
     return call
 
 
-# cblas_?symm / ?hemm / ?trmm and their F77 forms (blas/dsymm.c, blas/zhemm.c,
-# blas/dtrmm.c in the reference): same argument order and meaning.
+# cblas_?symm / ?hemm / ?trmm / ?trsm and their F77 forms (blas/dsymm.c,
+# blas/zhemm.c, blas/dtrmm.c, blas/dtrsm.c in the reference): same argument
+# order and meaning.
 cblas_ssymm, cblas_dsymm = _symm_fn("s", "symm"), _symm_fn("d", "symm")
 cblas_csymm, cblas_zsymm = _symm_fn("c", "symm"), _symm_fn("z", "symm")
 cblas_chemm, cblas_zhemm = _symm_fn("c", "hemm"), _symm_fn("z", "hemm")
@@ -365,6 +367,8 @@ cblas_strmm, cblas_dtrmm, cblas_ctrmm, cblas_ztrmm = (_trmm_fn(t) for t in "sdcz
 ssymm_, dsymm_, csymm_, zsymm_ = (_symm_f77(t, "symm") for t in "sdcz")
 chemm_, zhemm_ = _symm_f77("c", "hemm"), _symm_f77("z", "hemm")
 strmm_, dtrmm_, ctrmm_, ztrmm_ = (_trmm_f77(t) for t in "sdcz")
+cblas_strsm, cblas_dtrsm, cblas_ctrsm, cblas_ztrsm = (_trmm_fn(t, "trsm") for t in "sdcz")
+strsm_, dtrsm_, ctrsm_, ztrsm_ = (_trmm_f77(t, "trsm") for t in "sdcz")
 
 
 def _f77(fn, ctype, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cplx=False):

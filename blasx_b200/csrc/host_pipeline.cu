@@ -468,6 +468,67 @@ int host_formed(const Gemm &g, Context *c, blasx_call_stats &st, int mode) {
 
 }  // namespace
 
+// TRSM on host operands: A (the order-K triangle, copied whole) and B to the
+// device, the recursive solve (trsm_device), B back. In core only, like
+// host_formed; the scratch of the largest update GEMM is part of the budget.
+int host_trsm(const Trsm &t) {
+    auto t0 = std::chrono::steady_clock::now();
+    blasx_call_stats &st = call_stats();
+    st = blasx_call_stats{};
+    if (t.M == 0 || t.N == 0) return BLASX_OK;
+    Context *c = context();
+    if (!c) return last_status();
+    std::lock_guard<std::mutex> lk(c->host_mu);
+    const int mode = config().dgemm_mode.load();
+    const size_t es = elem_size(t.dt);
+    const int64_t K = t.order();
+    const bool need_a = !(t.alpha.re == 0 && t.alpha.im == 0);
+    DeviceOps d;
+    d.s = c->compute;
+    d.lda = round_up(K, 32);
+    d.ldb = round_up(t.M, 32);
+    Trsm dt = t;
+    dt.lda = d.lda;
+    dt.ldb = d.ldb;
+    const size_t bytes_a = need_a ? size_t(d.lda) * K * es : 0;
+    const size_t bytes_b = size_t(d.ldb) * t.N * es;
+    const Gemm top = trsm_top_update(dt);
+    const size_t bytes_ws = need_a && top.K > 0 && ozaki_selected(top, mode) ? ozaki_scratch_bytes(top) : 0;
+    if (bytes_a + bytes_b + bytes_ws > default_budget(c))
+        return set_error(BLASX_ERR_UNSUPPORTED, "triangular solve: %zu bytes exceed the HBM budget",
+                         bytes_a + bytes_b + bytes_ws);
+    HostPin pins;
+    BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
+    BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
+    cudaStream_t s = c->compute;
+    if (need_a) {
+        BX_CUDA(cudaMallocAsync(&d.A, bytes_a, s));
+        BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, s));
+        st.h2d_bytes += double(es) * K * K;
+    }
+    BX_CUDA(cudaMallocAsync(&d.B, bytes_b, s));
+    if (need_a) {  // alpha == 0 writes zeros without reading B
+        BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, t.B, t.ldb * es, t.M * es, t.N, cudaMemcpyHostToDevice, s));
+        st.h2d_bytes += double(es) * t.M * t.N;
+    }
+    dt.A = d.A;
+    dt.B = d.B;
+    bool emulated = false;
+    BX_TRY(trsm_device(dt, s, &emulated));
+    BX_CUDA(cudaMemcpy2DAsync(t.B, t.ldb * es, d.B, d.ldb * es, t.M * es, t.N, cudaMemcpyDeviceToHost, s));
+    st.d2h_bytes += double(es) * t.M * t.N;
+    BX_CUDA(cudaStreamSynchronize(s));
+    st.path = !need_a ? 3 : (emulated ? 2 : 1);
+    if (emulated) {
+        resolve_decision(st);
+        if (*c->last_error_flag)
+            return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
+                             *c->last_error_flag);
+    }
+    st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return BLASX_OK;
+}
+
 int host_gemm(const Gemm &g) {
     auto t0 = std::chrono::steady_clock::now();
     blasx_call_stats &st = call_stats();

@@ -10,4 +10,9 @@ namespace bx {
 // complete on return. Records status and call statistics for the thread.
 int host_gemm(const Gemm &g);
 
+// Triangular solve (TRSM) whose A and B are host pointers; synchronous, B
+// holds the solution on return. In core only (BLASX_ERR_UNSUPPORTED beyond
+// the HBM budget, B unchanged).
+int host_trsm(const Trsm &t);
+
 }  // namespace bx

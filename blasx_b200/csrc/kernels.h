@@ -37,5 +37,13 @@ int launch_gemm_dmma_grouped(const Gemm *gs, int n, cudaStream_t s);
 // Device-resident GEMM of any dtype through the best available path.
 // Uses library-owned scratch memory for the Ozaki path.
 int device_gemm(const Gemm &g, cudaStream_t s);
+// Triangular solve on device operands (t.A, t.B device pointers): recursive
+// halving into device_gemm updates (native or emulated by the precision
+// mode) and a substitution kernel for blocks of <= 64 rows. Sets *emulated
+// when any update took the emulated path.
+int trsm_device(const Trsm &t, cudaStream_t s, bool *emulated);
+// The largest update GEMM trsm_device issues for t (its scratch bounds the
+// solve's), or a Gemm with K == 0 when the triangle is a single leaf.
+Gemm trsm_top_update(const Trsm &t);
 
 }  // namespace bx

@@ -7,84 +7,12 @@
 // INT8 tensor-core path.
 #include <algorithm>
 
+#include "arith.cuh"
 #include "kernels.h"
 
 namespace bx {
 
 namespace {
-
-struct z2 {
-    double re, im;
-};
-struct c2 {  // complex64: interleaved (re, im) floats
-    float re, im;
-};
-
-template <typename T> struct Arith;
-
-template <> struct Arith<float> {
-    using V = float;
-    __device__ static V zero() { return 0.f; }
-    __device__ static V one() { return 1.f; }
-    __device__ static V real_part(V a) { return a; }
-    __device__ static V fma(V a, V b, V c) { return fmaf(a, b, c); }
-    __device__ static V conj(V a) { return a; }
-    __device__ static V mul(V a, V b) { return a * b; }
-    __device__ static V add(V a, V b) { return a + b; }
-};
-template <> struct Arith<double> {
-    using V = double;
-    __device__ static V zero() { return 0.0; }
-    __device__ static V one() { return 1.0; }
-    __device__ static V real_part(V a) { return a; }
-    __device__ static V fma(V a, V b, V c) { return ::fma(a, b, c); }
-    __device__ static V conj(V a) { return a; }
-    __device__ static V mul(V a, V b) { return a * b; }
-    __device__ static V add(V a, V b) { return a + b; }
-};
-template <> struct Arith<z2> {
-    using V = z2;
-    __device__ static V zero() { return {0.0, 0.0}; }
-    __device__ static V one() { return {1.0, 0.0}; }
-    __device__ static V real_part(V a) { return {a.re, 0.0}; }
-    __device__ static V fma(V a, V b, V c) {
-        c.re = ::fma(a.re, b.re, c.re);
-        c.re = ::fma(-a.im, b.im, c.re);
-        c.im = ::fma(a.re, b.im, c.im);
-        c.im = ::fma(a.im, b.re, c.im);
-        return c;
-    }
-    __device__ static V conj(V a) { return {a.re, -a.im}; }
-    __device__ static V mul(V a, V b) {
-        return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
-    }
-    __device__ static V add(V a, V b) { return {a.re + b.re, a.im + b.im}; }
-};
-
-template <> struct Arith<c2> {
-    using V = c2;
-    __device__ static V zero() { return {0.f, 0.f}; }
-    __device__ static V one() { return {1.f, 0.f}; }
-    __device__ static V real_part(V a) { return {a.re, 0.f}; }
-    __device__ static V fma(V a, V b, V c) {
-        c.re = fmaf(a.re, b.re, c.re);
-        c.re = fmaf(-a.im, b.im, c.re);
-        c.im = fmaf(a.re, b.im, c.im);
-        c.im = fmaf(a.im, b.re, c.im);
-        return c;
-    }
-    __device__ static V conj(V a) { return {a.re, -a.im}; }
-    __device__ static V mul(V a, V b) {
-        return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
-    }
-    __device__ static V add(V a, V b) { return {a.re + b.re, a.im + b.im}; }
-};
-
-template <typename T> __host__ T from_cplx(cplx c);
-template <> __host__ float from_cplx<float>(cplx c) { return float(c.re); }
-template <> __host__ double from_cplx<double>(cplx c) { return c.re; }
-template <> __host__ z2 from_cplx<z2>(cplx c) { return {c.re, c.im}; }
-template <> __host__ c2 from_cplx<c2>(cplx c) { return {float(c.re), float(c.im)}; }
 
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 

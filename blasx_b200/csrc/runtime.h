@@ -85,6 +85,23 @@ struct Gemm {
     }
 };
 
+// One triangular solve with many right-hand sides, column-major: op(A) X =
+// alpha B (left) or X op(A) = alpha B (right), X overwriting B (M x N). A is
+// the order-K triangle (K = M left, N right); only its `lower` (or upper)
+// triangle is read, and not its diagonal when `unit`.
+struct Trsm {
+    DType dt;
+    bool left, lower, unit;
+    int trans;  // NoTrans, TransT, ConjT (ConjT is TransT for real types)
+    int64_t M, N;
+    cplx alpha;
+    const void *A;
+    int64_t lda;
+    void *B;
+    int64_t ldb;
+    int64_t order() const { return left ? M : N; }
+};
+
 // Records `status` and a formatted message for the calling thread, prints it
 // to stderr and returns `status`.
 int set_error(int status, const char *fmt, ...) __attribute__((format(printf, 2, 3)));

@@ -1,5 +1,5 @@
-// symm_trmm_api.cu -- cblas_?symm, cblas_?hemm, cblas_?trmm and their F77
-// wrappers on the GPU.
+// symm_trmm_api.cu -- cblas_?symm, cblas_?hemm, cblas_?trmm, cblas_?trsm and
+// their F77 wrappers on the GPU.
 //
 // The reference declares these but always runs them on its host BLAS (for
 // instance blas/dsymm.c:44-57 and blas/dtrmm.c:49-60 select the CPU in every
@@ -12,13 +12,17 @@
 //                C = alpha B A + beta C (side Right, A is N x N)
 //   TRMM         B = alpha op(A) B (Left) or alpha B op(A) (Right); B is read
 //                whole before the result is written back into it.
+//   TRSM         solves op(A) X = alpha B (Left) or X op(A) = alpha B (Right)
+//                for X, which overwrites B (trsm.cu: recursive halving into
+//                GEMM updates and a substitution kernel).
 // Row-major calls are the column-major problem with side and uplo flipped and
 // M, N swapped (the reference ignores Order).
 //
 // Argument checks follow the reference's order (blas/dsymm.c:29-36,
 // blas/dtrmm.c:32-40): the first illegal argument is reported through xerbla_
 // -- SYMM / HEMM: 1 Side, 2 Uplo, 3 M, 4 N, 7 lda, 9 ldb, 12 ldc; TRMM: 1 Side,
-// 2 Uplo, 3 TransA, 4 Diag, 5 M, 6 N, 9 lda, 11 ldb. The F77 wrappers report
+// 2 Uplo, 3 TransA, 4 Diag, 5 M, 6 N, 9 lda, 11 ldb; TRSM the same codes
+// (blas/dtrsm.c:31-38). The F77 wrappers report
 // the first bad character argument likewise (blas/dsymm.c:83-84,
 // blas/dtrmm.c:76-80). CHEMM / ZHEMM report under the reference's names
 // "CHEMM" / "ZHEMM", without the trailing blank (blas/zhemm.c:14).
@@ -132,6 +136,42 @@ void trmm_entry(const char *name, DType dt, int order, int side, int uplo, int t
     trmm_col(name, dt, side, uplo, trans, diag, M, N, alpha, A, lda, B, ldb);
 }
 
+void trsm_col(const char *name, DType dt, int side, int uplo, int trans, int diag, int M, int N,
+              cplx alpha, const void *A, int lda, void *B, int ldb) {
+    int info = 0;
+    const int nrowa = side == CblasLeft ? M : N;
+    auto mx1 = [](int v) { return v > 1 ? v : 1; };
+    if (lda < mx1(nrowa)) info = 9;
+    else if (ldb < mx1(M)) info = 11;
+    if (info) return report(name, info);
+    if (M == 0 || N == 0) return;
+    Trsm t;
+    t.dt = dt;
+    t.left = side == CblasLeft;
+    t.lower = uplo == CblasLower;
+    t.unit = diag == CblasUnit;
+    t.trans = (!is_complex(dt) && trans == ConjT) ? TransT : trans;
+    t.M = M; t.N = N;
+    t.alpha = alpha;
+    t.A = A; t.lda = lda;
+    t.B = B; t.ldb = ldb;
+    host_trsm(t);
+}
+
+void trsm_entry(const char *name, DType dt, int order, int side, int uplo, int trans, int diag, int M,
+                int N, cplx alpha, const void *A, int lda, void *B, int ldb) {
+    clear_error();
+    if (!side_ok(side)) return report(name, 1);
+    if (!uplo_ok(uplo)) return report(name, 2);
+    if (!trans_ok(trans)) return report(name, 3);
+    if (!diag_ok(diag)) return report(name, 4);
+    if (M < 0) return report(name, 5);
+    if (N < 0) return report(name, 6);
+    if (order == CblasRowMajor)
+        return trsm_col(name, dt, flip_side(side), flip_uplo(uplo), trans, diag, N, M, alpha, A, lda, B, ldb);
+    trsm_col(name, dt, side, uplo, trans, diag, M, N, alpha, A, lda, B, ldb);
+}
+
 bool f77_side(const char *c, int *s) {
     switch (*c) {
         case 'L': case 'l': *s = CblasLeft; return true;
@@ -209,6 +249,19 @@ BX_TRMM("CTRMM ", cblas_ctrmm, DType::C64, const void *, void, bx::c_scalar)
 BX_TRMM("ZTRMM ", cblas_ztrmm, DType::C128, const void *, void, bx::z_scalar)
 #undef BX_TRMM
 
+#define BX_TRSM(NAME, CNAME, DT, STYPE, ET, TOSC)                                                       \
+    void CNAME(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side, const enum CBLAS_UPLO Uplo,     \
+               const enum CBLAS_TRANSPOSE TransA, const enum CBLAS_DIAG Diag, const int M, const int N,  \
+               STYPE alpha, const ET *A, const int lda, ET *B, const int ldb) {                         \
+        bx::trsm_entry(NAME, DT, Order, Side, Uplo, TransA, Diag, M, N, TOSC(alpha), A, lda, B, ldb);   \
+    }
+
+BX_TRSM("STRSM ", cblas_strsm, DType::F32, const float, float, bx::real_scalar)
+BX_TRSM("DTRSM ", cblas_dtrsm, DType::F64, const double, double, bx::real_scalar)
+BX_TRSM("CTRSM ", cblas_ctrsm, DType::C64, const void *, void, bx::c_scalar)
+BX_TRSM("ZTRSM ", cblas_ztrsm, DType::C128, const void *, void, bx::z_scalar)
+#undef BX_TRSM
+
 // F77 wrappers. Scalars by pointer: one real for S/D, an (re, im) pair for C/Z.
 #define BX_F77_SYMM(NAME, FNAME, CNAME, RT, SCAL)                                                      \
     void FNAME(char *side, char *uplo, int *m, int *n, RT *alpha, RT *A, int *lda, RT *B, int *ldb,     \
@@ -230,7 +283,7 @@ BX_F77_SYMM("CHEMM", chemm_, cblas_chemm, float, BX_PTR)
 BX_F77_SYMM("ZHEMM", zhemm_, cblas_zhemm, double, BX_PTR)
 #undef BX_F77_SYMM
 
-#define BX_F77_TRMM(NAME, FNAME, CNAME, RT, SCAL)                                                      \
+#define BX_F77_TRI(NAME, FNAME, CNAME, RT, SCAL)                                                      \
     void FNAME(char *side, char *uplo, char *transa, char *diag, int *m, int *n, RT *alpha, RT *A,      \
                int *lda, RT *B, int *ldb) {                                                             \
         int sd = 0, up = 0, tr = 0, dg = 0, info = 0;                                                  \
@@ -242,11 +295,15 @@ BX_F77_SYMM("ZHEMM", zhemm_, cblas_zhemm, double, BX_PTR)
         CNAME(CblasColMajor, CBLAS_SIDE(sd), CBLAS_UPLO(up), CBLAS_TRANSPOSE(tr), CBLAS_DIAG(dg), *m, *n, \
               SCAL(alpha), A, *lda, B, *ldb);                                                           \
     }
-BX_F77_TRMM("STRMM ", strmm_, cblas_strmm, float, BX_REAL)
-BX_F77_TRMM("DTRMM ", dtrmm_, cblas_dtrmm, double, BX_REAL)
-BX_F77_TRMM("CTRMM ", ctrmm_, cblas_ctrmm, float, BX_PTR)
-BX_F77_TRMM("ZTRMM ", ztrmm_, cblas_ztrmm, double, BX_PTR)
-#undef BX_F77_TRMM
+BX_F77_TRI("STRMM ", strmm_, cblas_strmm, float, BX_REAL)
+BX_F77_TRI("DTRMM ", dtrmm_, cblas_dtrmm, double, BX_REAL)
+BX_F77_TRI("CTRMM ", ctrmm_, cblas_ctrmm, float, BX_PTR)
+BX_F77_TRI("ZTRMM ", ztrmm_, cblas_ztrmm, double, BX_PTR)
+BX_F77_TRI("STRSM ", strsm_, cblas_strsm, float, BX_REAL)
+BX_F77_TRI("DTRSM ", dtrsm_, cblas_dtrsm, double, BX_REAL)
+BX_F77_TRI("CTRSM ", ctrsm_, cblas_ctrsm, float, BX_PTR)
+BX_F77_TRI("ZTRSM ", ztrsm_, cblas_ztrsm, double, BX_PTR)
+#undef BX_F77_TRI
 #undef BX_REAL
 #undef BX_PTR
 

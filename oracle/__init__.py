@@ -226,6 +226,39 @@ def trmm(side, uplo, transa, diag, M, N, alpha, A, lda, B, ldb):
     return B
 
 
+def trsm(side, uplo, transa, diag, M, N, alpha, A, lda, B, ldb):
+    """Restatement of BLAS ?TRSM, which the reference hands to its CPU BLAS
+    (blas/dtrsm.c:44-61): solves op(A) X = alpha B (side 'L', A M x M) or
+    X op(A) = alpha B ('R', A N x N) for X, which overwrites B; A triangular
+    (uplo, diag), only its uplo triangle read. Column-oriented substitution
+    as in reference BLAS, vectorised over the right-hand sides; in float64 /
+    complex128 whatever the input type, rounded to B's type at the end."""
+    na = M if side == "L" else N
+    wide = np.complex128 if np.iscomplexobj(B) else np.float64
+    T = complete("T", uplo, A, na, diag).astype(wide)
+    if transa == "T":
+        T = T.T
+    elif transa == "C":
+        T = T.conj().T
+    X = alpha * np.array(B[:M, :N], dtype=wide)
+    if side == "R":  # X op(A) = alpha B  <=>  op(A)^T X^T = alpha B^T
+        T, X = T.T, X.T
+    n = T.shape[0]
+    # the system matrix is op(A) (left) or op(A)^T (right): lower when the
+    # stored triangle, transposed or not, ends up below the diagonal
+    lower = (uplo == "L") == ((transa == "N") == (side == "L"))
+    order = range(n) if lower else range(n - 1, -1, -1)
+    for k in order:
+        if diag != "U":
+            X[k, :] /= T[k, k]
+        rest = slice(k + 1, n) if lower else slice(0, k)
+        X[rest, :] -= np.outer(T[rest, k], X[k, :])
+    if side == "R":
+        X = X.T
+    B[:M, :N] = X.astype(B.dtype)
+    return B
+
+
 def dd_entries(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, ii, jj):
     """Double-double values of sampled entries of alpha*op(A)op(B)+beta*C0.
 

@@ -1,10 +1,11 @@
-"""Generate the SYMM / HEMM / TRMM golden fixtures from the reference library.
+"""Generate the SYMM / HEMM / TRMM / TRSM golden fixtures from the reference library.
 
 The reference (linnanwang/BLASX) is compiled from its own, unmodified sources
 into ``oracle/_ref/libblasx_ref.so`` by ``oracle/Makefile``. Its cblas_?symm,
-cblas_?hemm and cblas_?trmm send every call to its CPU BLAS (blas/dsymm.c:
-44-57, blas/zhemm.c, blas/dtrmm.c:43-60), passing Order through, so the
-outputs recorded here -- column-major and row-major -- are the reference's own.
+cblas_?hemm, cblas_?trmm and cblas_?trsm send every call to its CPU BLAS
+(blas/dsymm.c:44-57, blas/zhemm.c, blas/dtrmm.c:43-60, blas/dtrsm.c:44-61),
+passing Order through, so the outputs recorded here -- column-major and
+row-major -- are the reference's own.
 
 The triangle of A that BLAS does not reference is filled with NaN (and so is
 the diagonal for Diag = Unit, and the imaginary parts of a Hermitian diagonal
@@ -14,9 +15,10 @@ value. Inputs are regenerated from their seeds by
 the generator.
 
 Also recorded: the reference's xerbla_ lines for each illegal argument of
-cblas_dsymm, cblas_zhemm, cblas_dtrmm (blas/dsymm.c:29-36, blas/zhemm.c:30-41,
-blas/dtrmm.c:32-40) and of their F77 wrappers (blas/dsymm.c:82-88,
-blas/zhemm.c:88-94, blas/dtrmm.c:76-84).
+cblas_dsymm, cblas_zhemm, cblas_dtrmm, cblas_dtrsm (blas/dsymm.c:29-36,
+blas/zhemm.c:30-41, blas/dtrmm.c:32-40, blas/dtrsm.c:31-38) and of their F77
+wrappers (blas/dsymm.c:82-88, blas/zhemm.c:88-94, blas/dtrmm.c:76-84,
+blas/dtrsm.c:86-94).
 
 Run in a container that has the reference tree:  python tests/golden/make_golden_symm.py
 """
@@ -142,6 +144,39 @@ def main():
                                 rec[key + "_sum"] = checksum(x["A"], B0)
                                 rec[key + "_C"] = x["B"]
                                 n += 1
+    # TRSM (well-conditioned triangles, see golden_cases.symm_fill)
+    for tag in "sdcz":
+        getattr(L, f"cblas_{tag}trsm").argtypes = [I] * 7 + [{"s": ctypes.c_float, "d": ctypes.c_double}.get(tag, P),
+                                                            P, I, P, I]
+        for (M, N) in SHAPES[:3]:
+            for side in "LR":
+                for uplo in "UL":
+                    for trans in ("NTC" if tag in "cz" else "NT"):
+                        for diag in "NU":
+                            for order in (102, 101):
+                                if order == 101 and (M, N) != (7, 5):
+                                    continue
+                                seed = 20000 + 10 * n
+                                na = M if side == "L" else N
+                                rows_b = M if order == 102 else max(M, N)
+                                lda, ldb = na + n % 3, rows_b + n % 2
+                                meta = [order, SIDE[side], UPLO[uplo], TRANS[trans], DIAG[diag], M, N, lda, ldb,
+                                        seed]
+                                x = symm_fill("X", tag, meta)
+                                B0 = x["B"].copy(order="F")
+                                al = scalars(tag, n)[0] if n % 5 else (0.0 if tag in "sd" else 0j)
+                                pa, ka = scalar_arg(tag, al)
+                                out = capture_stdout(lambda: getattr(L, f"cblas_{tag}trsm")(
+                                    order, SIDE[side], UPLO[uplo], TRANS[trans], DIAG[diag], M, N, pa,
+                                    x["A"].ctypes.data, lda, x["B"].ctypes.data, ldb))
+                                assert out == "", out
+                                assert np.all(np.isfinite(x["B"])), (tag, M, N, side, uplo, trans, diag, order)
+                                key = f"trsm_{tag}_{n}"
+                                rec[key + "_meta"] = np.array(meta, dtype=np.int64)
+                                rec[key + "_scal"] = np.array([al], dtype=np.complex128)
+                                rec[key + "_sum"] = checksum(x["A"], B0)
+                                rec[key + "_C"] = x["B"]
+                                n += 1
     # xerbla lines
     A = np.zeros((4, 4)); B = np.zeros((4, 4)); C = np.ones((4, 4), order="F")
     Az = np.zeros((4, 4), dtype=np.complex128); Bz = Az.copy(); Cz = np.ones((4, 4), dtype=np.complex128, order="F")
@@ -165,6 +200,9 @@ def main():
         out = capture_stdout(lambda: L.cblas_dtrmm(102, a["side"], a["uplo"], a["trans"], a["diag"], a["M"], a["N"],
                                                    1.0, A.ctypes.data, a["lda"], C.ctypes.data, a["ldb"]))
         lines.append(f"cblas_dtrmm|{info}|{out}")
+        out = capture_stdout(lambda: L.cblas_dtrsm(102, a["side"], a["uplo"], a["trans"], a["diag"], a["M"], a["N"],
+                                                   1.0, A.ctypes.data, a["lda"], C.ctypes.data, a["ldb"]))
+        lines.append(f"cblas_dtrsm|{info}|{out}")
     r = ctypes.byref
     four = ctypes.c_int(4)
     al = ctypes.c_double(1.0); be = ctypes.c_double(0.0)
@@ -183,10 +221,13 @@ def main():
         out = capture_stdout(lambda: L.dtrmm_(*(r(c) for c in cc), r(four), r(four), r(al), A.ctypes.data, r(four),
                                               C.ctypes.data, r(four)))
         lines.append(f"dtrmm_{b''.join(chars).decode()}|-|{out}")
+        out = capture_stdout(lambda: L.dtrsm_(*(r(c) for c in cc), r(four), r(four), r(al), A.ctypes.data, r(four),
+                                              C.ctypes.data, r(four)))
+        lines.append(f"dtrsm_{b''.join(chars).decode()}|-|{out}")
     assert np.all(C == 1.0) and np.all(Cz == 1.0), "outputs must be untouched on argument errors"
     rec["xerbla"] = np.array(lines)
     np.savez_compressed(OUT, **rec)
-    print(f"wrote {OUT}: {n} SYMM/HEMM/TRMM cases + {len(lines)} xerbla lines")
+    print(f"wrote {OUT}: {n} SYMM/HEMM/TRMM/TRSM cases + {len(lines)} xerbla lines")
 
 
 if __name__ == "__main__":

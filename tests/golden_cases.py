@@ -95,10 +95,12 @@ def poison(kind, uplo, A, na, diag="N"):
 
 
 def symm_fill(kind, tag, meta):
-    """Inputs of one SYMM / HEMM (kind 'S' / 'H') or TRMM ('T') case from its
-    meta row, and the column-major form of the problem.
+    """Inputs of one SYMM / HEMM (kind 'S' / 'H'), TRMM ('T') or TRSM ('X')
+    case from its meta row, and the column-major form of the problem.
       'S' / 'H': meta = order, side, uplo, M, N, lda, ldb, ldc, seed
-      'T'      : meta = order, side, uplo, trans, diag, M, N, lda, ldb, seed
+      'T' / 'X': meta = order, side, uplo, trans, diag, M, N, lda, ldb, seed
+    TRSM's triangle is made well conditioned: off-diagonal entries
+    U[-1, 1] / order, diagonal 2 + U[-1, 1] / order.
     Arrays are Fortran-ordered with the leading dimension first: a row-major
     (101) matrix with r rows and leading dimension ld is the array of shape
     (ld, r), whose columns are the matrix's rows. The column-major problem of
@@ -118,7 +120,10 @@ def symm_fill(kind, tag, meta):
         cm.update(side="R" if side_s == "L" else "L", uplo="L" if uplo_s == "U" else "U", M=N, N=M)
     na = cm["M"] if cm["side"] == "L" else cm["N"]
     A = oracle.uniform((lda, na), dt, seed)
-    poison(kind, cm["uplo"], A, na, cm["diag"])
+    if kind == "X":
+        A /= na
+        A[np.arange(na), np.arange(na)] += 2
+    poison("T" if kind == "X" else kind, cm["uplo"], A, na, cm["diag"])
     B = oracle.uniform((ldb, cm["N"]), dt, seed + 1)
     out = dict(order=order, side=side, uplo=uplo, trans=trans, diag=diag, M=M, N=N, lda=lda, ldb=ldb,
                ldc=ldc, A=A, B=B, na=na, cm=cm, dt=dt)
@@ -139,7 +144,7 @@ def symm_keys(golden, prefix):
 
 def symm_case(golden, key):
     """(kind, tag, inputs, alpha, beta, reference output) of one fixture key."""
-    kind = {"symm": "S", "hemm": "H", "trmm": "T"}[key.split("_")[0]]
+    kind = {"symm": "S", "hemm": "H", "trmm": "T", "trsm": "X"}[key.split("_")[0]]
     tag = key.split("_")[1]
     x = symm_fill(kind, tag, golden[key + "_meta"])
     assert np.allclose(symm_checksum(x), golden[key + "_sum"]), "fixture generator changed"
@@ -148,6 +153,25 @@ def symm_case(golden, key):
     al = float(sc[0].real) if real else complex(sc[0])
     be = (float(sc[1].real) if real else complex(sc[1])) if kind in "SH" else None
     return kind, tag, x, al, be, golden[key + "_C"]
+
+
+def trsm_bound(x, al, X):
+    """Componentwise forward-error bound of a triangular solve against the
+    solution X (both sides' roundings): 2 (K + 2) u |T^-1| (|T| |X| + |alpha B|)
+    (left, T = op(A)), mirrored for the right side; twice that for complex."""
+    cm, na = x["cm"], x["na"]
+    M, N = cm["M"], cm["N"]
+    dt = x["dt"]
+    cplx = np.issubdtype(dt, np.complexfloating)
+    wide = np.complex128 if cplx else np.float64
+    T = oracle.complete("T", cm["uplo"], x["A"], na, cm["diag"]).astype(wide)
+    T = {"N": T, "T": T.T, "C": T.conj().T}[cm["trans"]]
+    aTi = np.abs(np.linalg.inv(T))
+    aT, aX = np.abs(T), np.abs(X[:M, :N].astype(wide))
+    aB = abs(al) * np.abs(x["B"][:M, :N].astype(wide))
+    scale = aTi @ (aT @ aX + aB) if cm["side"] == "L" else (aX @ aT + aB) @ aTi
+    u = oracle.UNIT_ROUNDOFF[np.dtype(dt).type]
+    return 2 * (na + 2) * u * (2.0 if cplx else 1.0) * scale
 
 
 def symm_bound(kind, x, al, be):
@@ -179,6 +203,9 @@ def symm_oracle(kind, x, al, be):
         return oracle.symm(cm["side"], cm["uplo"], cm["M"], cm["N"], al, x["A"], x["lda"], x["B"], x["ldb"], be,
                            C, x["ldc"], herm=kind == "H")
     B = x["B"].copy(order="F")
+    if kind == "X":
+        return oracle.trsm(cm["side"], cm["uplo"], cm["trans"], cm["diag"], cm["M"], cm["N"], al, x["A"], x["lda"],
+                           B, x["ldb"])
     return oracle.trmm(cm["side"], cm["uplo"], cm["trans"], cm["diag"], cm["M"], cm["N"], al, x["A"], x["lda"], B,
                        x["ldb"])
 
@@ -193,5 +220,5 @@ def symm_check(kind, x, got, want, al, be):
     blk = got[:M, :N]
     assert np.all(np.isfinite(blk)), "a non-referenced entry of A was read"
     err = np.abs(blk.astype(np.complex128) - want[:M, :N].astype(np.complex128))
-    bound = symm_bound(kind, x, al, be)
+    bound = trsm_bound(x, al, want) if kind == "X" else symm_bound(kind, x, al, be)
     assert np.all(err <= bound), float(np.max(err / np.maximum(bound, 1e-300)))

@@ -1,4 +1,4 @@
-"""GPU tests of cblas_?symm / ?hemm / ?trmm: the reference's own outputs
+"""GPU tests of cblas_?symm / ?hemm / ?trmm / ?trsm: the reference's own outputs
 (golden fixtures, its CPU BLAS path; the entries BLAS must not read hold NaN)
 on the native and the emulated paths, larger cases against the double-double
 oracle, and the F77 wrappers."""
@@ -37,13 +37,14 @@ def run_case(blx, kind, tag, x, al, be):
         out = C
     else:
         out = x["B"].copy(order="F")
-        getattr(blx, f"cblas_{tag}trmm")(x["order"], x["side"], x["uplo"], x["trans"], x["diag"], x["M"], x["N"],
-                                         al, x["A"], x["lda"], out, x["ldb"])
+        getattr(blx, f"cblas_{tag}{'trmm' if kind == 'T' else 'trsm'}")(
+            x["order"], x["side"], x["uplo"], x["trans"], x["diag"], x["M"], x["N"], al, x["A"], x["lda"], out,
+            x["ldb"])
     assert blx.last_status() == blx.BLASX_OK, blx.last_error()
     return out
 
 
-@pytest.mark.parametrize("prefix", ["symm_", "hemm_", "trmm_"])
+@pytest.mark.parametrize("prefix", ["symm_", "hemm_", "trmm_", "trsm_"])
 def test_matches_reference_outputs(blx, sgolden, mode, prefix):
     for key in symm_keys(sgolden, prefix):
         kind, tag, x, al, be, want = symm_case(sgolden, key)
@@ -228,3 +229,80 @@ def test_trmm_emulated_is_componentwise_accurate_at_the_tip(blx, dt, side, uplo)
         assert np.all(err <= bound), float(np.max(err / np.maximum(bound, 1e-300)))
     finally:
         blx.set_dgemm_mode(prev)
+
+
+def dominant_triangle(dt, na, uplo, diag, seed):
+    """A well-conditioned triangle (off-diagonal U[-1, 1] / na, diagonal 2 +
+    U[-1, 1] / na) with NaN in every entry BLAS must not read."""
+    A = oracle.uniform((na, na), dt, seed) / na
+    A[np.arange(na), np.arange(na)] += 2
+    i, j = np.indices((na, na))
+    A[(i > j) if uplo == "U" else (i < j)] = np.nan
+    if diag == "U":
+        np.fill_diagonal(A, np.nan)
+    return A
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo,trans,diag", [("U", "N", "N"), ("L", "T", "U"), ("U", "C", "N"), ("L", "N", "U")])
+@pytest.mark.parametrize("dt", [np.float64, np.complex128, np.float32, np.complex64])
+def test_trsm_large_backward_error(blx, mode, side, uplo, trans, diag, dt):
+    """B := alpha op(A)^-1 B (or B op(A)^-1), 1000 x 1300 with ragged leading
+    dimensions (recursion down to ragged 64-row leaves): the residual
+    op(A) X - alpha B of sampled entries, in double-double, is within
+    2 (K + 2) u (|op(A)| |X| + |alpha| |B|)."""
+    if trans == "C" and dt in (np.float64, np.float32):
+        trans = "T"
+    M, N = 1000, 1300
+    na = M if side == "L" else N
+    A = dominant_triangle(dt, na, uplo, diag, 31)
+    B0 = oracle.uniform((M + 1, N), dt, 32)
+    B = B0.copy(order="F")
+    al = 0.75 if dt in (np.float64, np.float32) else complex(0.75, -0.5)
+    tag = {np.float64: "d", np.complex128: "z", np.float32: "s", np.complex64: "c"}[dt]
+    getattr(blx, f"cblas_{tag}trsm")(102, blx.SIDE[side], blx.UPLO[uplo], blx.TRANS[trans], blx.DIAG[diag], M, N,
+                                     al, A, na, B, M + 1)
+    assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+    st = blx.call_stats()
+    if mode == "ozaki":
+        assert st["path"] == 2, st
+    assert np.array_equal(B[M:], B0[M:]) and np.all(np.isfinite(B))
+    Af = oracle.complete("T", uplo, A, na, diag)
+    ii, jj = sample(M, N, 43)
+    if side == "L":
+        val, bound = oracle.dd_entries(trans, "N", M, N, M, 1.0, Af, na, B, M + 1, -al, B0, M + 1, ii, jj)
+    else:
+        val, bound = oracle.dd_entries("N", trans, M, N, N, 1.0, B, M + 1, Af, na, -al, B0, M + 1, ii, jj)
+    u = oracle.UNIT_ROUNDOFF[np.dtype(dt).type] * (2.0 if np.issubdtype(dt, np.complexfloating) else 1.0)
+    ratio = np.max(np.abs(val) / (2 * (na + 2) * u * bound))
+    assert ratio <= 1.0, ratio
+
+
+def test_trsm_row_major_is_the_transposed_problem(blx):
+    M, N = 300, 200
+    A = dominant_triangle(np.float64, M, "U", "N", 61)
+    B = oracle.uniform((N, M), np.float64, 62)  # row-major M x N = column-major N x M
+    Brm, Bcm = B.copy(order="F"), B.copy(order="F")
+    blx.cblas_dtrsm(101, 141, 121, 111, 131, M, N, 1.5, A.T.copy(order="F"), M, Brm, N)
+    assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+    blx.cblas_dtrsm(102, 142, 122, 111, 131, N, M, 1.5, A.T.copy(order="F"), M, Bcm, N)
+    np.testing.assert_array_equal(Brm, Bcm)
+
+
+def test_trsm_alpha_zero_sets_b_to_zero_without_reading_a(blx):
+    M, N = 100, 70
+    A = np.full((M, M), np.nan, order="F")
+    B = oracle.uniform((M, N), np.float64, 63)
+    blx.cblas_dtrsm(102, 141, 121, 111, 131, M, N, 0.0, A, M, B, M)
+    assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+    assert np.all(B == 0.0) and blx.call_stats()["path"] == 3
+
+
+def test_trsm_f77_matches_cblas(blx):
+    M, N = 500, 300
+    A = dominant_triangle(np.complex128, N, "L", "N", 64)
+    B0 = oracle.uniform((M, N), np.complex128, 65)
+    B1, B2 = B0.copy(order="F"), B0.copy(order="F")
+    blx.cblas_ztrsm(102, 142, 122, 113, 131, M, N, complex(1, -1), A, N, B1, M)
+    blx.ztrsm_("r", "L", "C", "n", M, N, complex(1, -1), A, N, B2, M)
+    assert np.array_equal(B1, B2)

@@ -1,8 +1,8 @@
-"""CPU tests of the SYMM / HEMM / TRMM restatement in the oracle and of the
-library's argument checking for them, both pinned to the reference: the
+"""CPU tests of the SYMM / HEMM / TRMM / TRSM restatement in the oracle and of
+the library's argument checking for them, both pinned to the reference: the
 fixtures hold the reference's own outputs (its CPU BLAS path, which it uses
-for every SYMM / HEMM / TRMM call, column-major and row-major) and its xerbla_
-lines (tests/golden/make_golden_symm.py)."""
+for every SYMM / HEMM / TRMM / TRSM call, column-major and row-major) and its
+xerbla_ lines (tests/golden/make_golden_symm.py)."""
 import os
 
 import numpy as np
@@ -26,9 +26,10 @@ def test_fixture_counts(sgolden):
     assert len(symm_keys(sgolden, "hemm_")) == 2 * 20
     # 3 shapes x 2 x 2 x trans (2 real, 3 complex) x 2 diags, + one row-major shape
     assert len(symm_keys(sgolden, "trmm_")) == 2 * (48 + 16) + 2 * (72 + 24)
+    assert len(symm_keys(sgolden, "trsm_")) == 2 * (48 + 16) + 2 * (72 + 24)
 
 
-@pytest.mark.parametrize("prefix", ["symm_", "hemm_", "trmm_"])
+@pytest.mark.parametrize("prefix", ["symm_", "hemm_", "trmm_", "trsm_"])
 def test_oracle_matches_reference(sgolden, prefix):
     for key in symm_keys(sgolden, prefix):
         kind, tag, x, al, be, want = symm_case(sgolden, key)
@@ -70,13 +71,14 @@ TRMM_BAD = {1: dict(side=999), 2: dict(uplo=999), 3: dict(trans=999), 4: dict(di
 
 
 @pytest.mark.parametrize("info", sorted(TRMM_BAD))
-def test_trmm_xerbla_matches_reference(blx, sgolden, info):
-    want = [str(l) for l in sgolden["xerbla"] if str(l).startswith(f"cblas_dtrmm|{info}|")][0].split("|", 2)[2]
+@pytest.mark.parametrize("fn", ["cblas_dtrmm", "cblas_dtrsm"])
+def test_trmm_xerbla_matches_reference(blx, sgolden, fn, info):
+    want = [str(l) for l in sgolden["xerbla"] if str(l).startswith(f"{fn}|{info}|")][0].split("|", 2)[2]
     a = dict(side=141, uplo=121, trans=111, diag=131, M=4, N=4, lda=4, ldb=4)
     a.update(TRMM_BAD[info])
     A = np.zeros((4, 4)); B = np.ones((4, 4), order="F")
-    got = _capture(lambda: blx.cblas_dtrmm(102, a["side"], a["uplo"], a["trans"], a["diag"], a["M"], a["N"], 1.0,
-                                           A, a["lda"], B, a["ldb"]))
+    got = _capture(lambda: getattr(blx, fn)(102, a["side"], a["uplo"], a["trans"], a["diag"], a["M"], a["N"], 1.0,
+                                            A, a["lda"], B, a["ldb"]))
     assert got == want
     assert np.all(B == 1.0) and blx.last_status() == blx.BLASX_ERR_ARG
 
@@ -93,10 +95,11 @@ def test_f77_symm_errors_match_reference(blx, sgolden, fn, sd, up):
 
 
 @pytest.mark.parametrize("chars", ["XUNN", "LQNN", "LUQN", "LUNQ", "XQQQ", "LUQQ"])
-def test_f77_trmm_errors_match_reference(blx, sgolden, chars):
-    want = [str(l) for l in sgolden["xerbla"] if str(l).startswith(f"dtrmm_{chars}|")][0].split("|", 2)[2]
+@pytest.mark.parametrize("fn", ["dtrmm_", "dtrsm_"])
+def test_f77_trmm_errors_match_reference(blx, sgolden, fn, chars):
+    want = [str(l) for l in sgolden["xerbla"] if str(l).startswith(f"{fn}{chars}|")][0].split("|", 2)[2]
     A = np.zeros((4, 4)); B = np.ones((4, 4), order="F")
-    got = _capture(lambda: blx.dtrmm_(*chars, 4, 4, 1.0, A, 4, B, 4))
+    got = _capture(lambda: getattr(blx, fn)(*chars, 4, 4, 1.0, A, 4, B, 4))
     assert got == want
     assert np.all(B == 1.0)
 
@@ -117,3 +120,5 @@ def test_row_major_uses_the_row_major_leading_dimension(blx):
     assert "DSYMM  parameter number  9" in out
     out = _capture(lambda: blx.cblas_dtrmm(101, 141, 121, 111, 131, 8, 4, 1.0, A, 8, C, 3))
     assert "DTRMM  parameter number 11" in out and np.all(C == 1.0)
+    out = _capture(lambda: blx.cblas_dtrsm(101, 141, 121, 111, 131, 8, 4, 1.0, A, 8, C, 3))
+    assert "DTRSM  parameter number 11" in out and np.all(C == 1.0)
