@@ -99,6 +99,7 @@ def lib() -> ctypes.CDLL:
         for f in ("ssyr2k_", "dsyr2k_", "zsyr2k_"):
             getattr(L, f).argtypes = [_P] * 12
         L.blasx_dsyrk_device.argtypes = [_I] * 4 + [_D, _P, _I, _D, _P, _I, _P]
+        L.blasx_dtrsm_device.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _P]
         for t, sc in (("s", _F), ("d", _D), ("c", _P), ("z", _P)):
             for kind in ("symm", "hemm") if t in "cz" else ("symm",):
                 getattr(L, f"cblas_{t}{kind}").argtypes = [_I] * 5 + [sc, _P, _I, _P, _I, sc, _P, _I]
@@ -252,6 +253,13 @@ def dsyrk_device(uplo, trans, N, K, alpha, A, lda, beta, C, ldc, stream=None):
     u = UPLO[uplo] if isinstance(uplo, str) else uplo
     t = TRANS[trans] if isinstance(trans, str) else trans
     return lib().blasx_dsyrk_device(u, t, N, K, alpha, _addr(A), lda, beta, _addr(C), ldc, s)
+
+
+def dtrsm_device(side, uplo, trans, diag, M, N, alpha, A, lda, B, ldb, stream=None):
+    """Device-resident DTRSM on device pointers (ints or tensors with data_ptr)."""
+    s = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else _addr(stream))
+    args = [SIDE.get(side, side), UPLO.get(uplo, uplo), TRANS.get(trans, trans), DIAG.get(diag, diag)]
+    return lib().blasx_dtrsm_device(*args, M, N, alpha, _addr(A), lda, _addr(B), ldb, s)
 
 
 def _cpair32(v) -> np.ndarray:

@@ -300,10 +300,25 @@ __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, d
     }
     cp_async_wait<0>();
 
-    // epilogue: C = alpha acc + beta C (C unread when beta == 0)
+    // epilogue: C = alpha acc + beta C (C unread when beta == 0). The C values
+    // of one row block (NT x 4 per thread) are all loaded before any store of
+    // that block, so their DRAM round trips overlap instead of alternating
+    // with the stores.
     const int64_t es = CPLX ? 2 : 1;
 #pragma unroll
     for (int i = 0; i < MT; ++i) {
+        double cin[NT][4][PLANES];
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int row = m0 + wm * (MT * 16) + i * 16 + g + (r >= 2 ? 8 : 0);
+                const int col = n0 + wn * (NT * 8) + j * 8 + 2 * t + (r & 1);
+                const bool in = !p.beta_zero && row < p.M && col < p.N && tri_keep(p.uplo, p.diag, row, col);
+                const double *cp = p.C + (row + int64_t(col) * p.ldc) * es;
+#pragma unroll
+                for (int pl = 0; pl < PLANES; ++pl) cin[j][r][pl] = in ? cp[pl] : 0.0;
+            }
 #pragma unroll
         for (int j = 0; j < NT; ++j) {
 #pragma unroll
@@ -314,14 +329,14 @@ __device__ __forceinline__ void dmma_tile(const DmmaParams &p, const int tile, d
                 double *cp = p.C + (row + int64_t(col) * p.ldc) * es;
                 if (!CPLX) {
                     double v = p.alpha_re * acc[0][i][j][r];
-                    if (!p.beta_zero) v = fma(p.beta_re, *cp, v);
+                    if (!p.beta_zero) v = fma(p.beta_re, cin[j][r][0], v);
                     *cp = v;
                 } else {
                     const double xr = acc[0][i][j][r], xi = acc[IM][i][j][r];
                     double vr = p.alpha_re * xr - p.alpha_im * xi;
                     double vi = p.alpha_re * xi + p.alpha_im * xr;
                     if (!p.beta_zero) {
-                        const double cr = cp[0], ci = cp[1];
+                        const double cr = cin[j][r][0], ci = cin[j][r][PLANES - 1];
                         vr += p.beta_re * cr - p.beta_im * ci;
                         vi += p.beta_re * ci + p.beta_im * cr;
                     }

@@ -26,6 +26,8 @@
 // the first bad character argument likewise (blas/dsymm.c:83-84,
 // blas/dtrmm.c:76-80). CHEMM / ZHEMM report under the reference's names
 // "CHEMM" / "ZHEMM", without the trailing blank (blas/zhemm.c:14).
+#include <algorithm>
+
 #include "host_pipeline.h"
 #include "kernels.h"
 #include "runtime.h"
@@ -213,6 +215,37 @@ cplx c_scalar(const void *p) {
 }
 
 }  // namespace
+
+int trsm_device_entry(DType dt, int side, int uplo, int trans, int diag, int M, int N, cplx alpha,
+                      const void *A, int lda, void *B, int ldb, cudaStream_t s) {
+    clear_error();
+    int info = 0;
+    const int nrowa = side == CblasLeft ? M : N;
+    if (!side_ok(side)) info = 1;
+    else if (!uplo_ok(uplo)) info = 2;
+    else if (!trans_ok(trans)) info = 3;
+    else if (!diag_ok(diag)) info = 4;
+    else if (M < 0) info = 5;
+    else if (N < 0) info = 6;
+    else if (lda < std::max(1, nrowa)) info = 9;
+    else if (ldb < std::max(1, M)) info = 11;
+    if (info) return set_error(BLASX_ERR_ARG, "device trsm parameter %d illegal", info);
+    if (M == 0 || N == 0) return BLASX_OK;
+    if (!context()) return last_status();
+    Trsm t;
+    t.dt = dt;
+    t.left = side == CblasLeft;
+    t.lower = uplo == CblasLower;
+    t.unit = diag == CblasUnit;
+    t.trans = (!is_complex(dt) && trans == ConjT) ? TransT : trans;
+    t.M = M; t.N = N;
+    t.alpha = alpha;
+    t.A = A; t.lda = lda;
+    t.B = B; t.ldb = ldb;
+    bool emulated = false;
+    return trsm_device(t, s, &emulated);
+}
+
 }  // namespace bx
 
 using bx::cplx;
@@ -304,6 +337,12 @@ BX_F77_TRI("DTRSM ", dtrsm_, cblas_dtrsm, double, BX_REAL)
 BX_F77_TRI("CTRSM ", ctrsm_, cblas_ctrsm, float, BX_PTR)
 BX_F77_TRI("ZTRSM ", ztrsm_, cblas_ztrsm, double, BX_PTR)
 #undef BX_F77_TRI
+
+int blasx_dtrsm_device(int side, int uplo, int trans, int diag, int M, int N, double alpha, const double *A,
+                       int lda, double *B, int ldb, void *stream) {
+    return bx::trsm_device_entry(DType::F64, side, uplo, trans, diag, M, N, cplx{alpha, 0.0}, A, lda, B, ldb,
+                                 static_cast<cudaStream_t>(stream));
+}
 #undef BX_REAL
 #undef BX_PTR
 

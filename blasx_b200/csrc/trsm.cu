@@ -7,7 +7,7 @@
 // emulated on the INT8 tensor cores where the precision mode selects it),
 // solve the second half. The top-level updates carry most of the K^2 * (M or
 // N) work with K up to K/2, the shape the emulated GEMM needs; blocks of at
-// most kLeaf rows are solved by substitution in one kernel.
+// most 64 rows (32 complex) are solved by substitution in one kernel.
 //
 // Every GEMM reads op(A) only in an off-diagonal rectangle inside the stored
 // triangle, and the substitution kernel reads only the stored triangle of its
@@ -21,114 +21,115 @@
 namespace bx {
 namespace {
 
-constexpr int kLeaf = 64;                      // order of a substitution block
-constexpr int kVecs = 64;                      // right-hand-side vectors per CTA
-constexpr int kGroups = 4;                     // thread (v, g) owns rows g, g + 4, ...
-constexpr int kRows = kLeaf / kGroups;         // rows per thread
-constexpr int kThreads = kVecs * kGroups;
+// Order of a substitution block: one right-hand-side vector of it lives in
+// one thread's registers (64 doubles, or 32 complex doubles).
+template <typename T> struct LeafDim {
+    static constexpr int n = 64;
+};
+template <> struct LeafDim<z2> {
+    static constexpr int n = 32;
+};
+template <> struct LeafDim<c2> {
+    static constexpr int n = 32;
+};
+constexpr int kLeafThreads = 64;  // right-hand-side vectors per CTA
+
+int leaf_order(DType dt) { return is_complex(dt) ? 32 : 64; }
 
 template <typename T> __device__ inline T negate(T a) { return -a; }
 template <> __device__ inline z2 negate<z2>(z2 a) { return {-a.re, -a.im}; }
 template <> __device__ inline c2 negate<c2>(c2 a) { return {-a.re, -a.im}; }
 
-// Solves S x = c for nvec vectors at once, S the bs x bs (bs <= kLeaf)
-// system matrix of one diagonal block: S = op(A_block) for a left solve, the
+// Solves S x = c for nvec vectors at once, S the bs x bs (bs <= L) system
+// matrix of one diagonal block: S = op(A_block) for a left solve, the
 // transpose of op(A_block) for a right solve (x op(A) = c is op(A)^T x^T =
 // c^T). S[i][k] is A[i + k lda] (s_trans = 0) or A[k + i lda] (s_trans = 1),
-// conjugated when s_conj. S is lower (forward substitution) or upper
-// (backward); only that triangle of S, and its diagonal unless unit, is read.
-// Vector v, element i: left: C[i + v ldc] (columns of B); right: C[v + i ldc]
-// (rows of B). Each vector is scaled by `scale` (alpha) on load.
+// conjugated when s_conj. S is lower (FORWARD substitution) or upper; only
+// that triangle of S, and its diagonal unless UNIT, is read. Vector v,
+// element i: left: C[i + v ldc] (columns of B); right: C[v + i ldc] (rows of
+// B). Each vector is scaled by `scale` (alpha) on load.
 //
-// Thread (v, g) keeps elements g, g + 4, ... of vector v in registers. Step k
-// (in substitution order): the owner of element k divides by the diagonal
-// and publishes x_k in xs[k & 1][v]; after one barrier every thread applies
-// c_i -= S[i][k] x_k to its later elements. The two xs rows alternate, so the
-// write of step k + 1 never meets a read of step k (those finished before
-// the barrier of step k + 1).
-template <typename T>
-__global__ void __launch_bounds__(kThreads)
+// Shared memory holds S by columns (St[k * L + i] = S[i][k]), zero outside
+// the triangle, and the reciprocals of its diagonal. Each thread solves one
+// vector held in registers: the substitution is unrolled over the L x L
+// block, so every register index and loop bound is a compile-time constant,
+// and all threads read the same St entry at a time (a broadcast). A block
+// smaller than L is padded with zero right-hand sides and unit diagonal,
+// which leave the real rows unchanged.
+template <typename T, bool FORWARD, bool UNIT>
+__global__ void __launch_bounds__(kLeafThreads)
     trsm_leaf_kernel(const T *__restrict__ A, int64_t lda, T *__restrict__ C, int64_t ldc, int bs,
-                     int64_t nvec, int left, int s_trans, int s_conj, int unit, int forward, T scale) {
+                     int64_t nvec, int left, int s_trans, int s_conj, T scale) {
     using Ar = Arith<T>;
+    constexpr int L = LeafDim<T>::n;
     extern __shared__ __align__(16) unsigned char smem[];
-    T *S = reinterpret_cast<T *>(smem);  // S[i * kLeaf + k]
-    T *xs = S + kLeaf * kLeaf;           // xs[buf * kVecs + v]
-    const int tid = threadIdx.x;
-    const int v = tid % kVecs, g = tid / kVecs;
-    const int64_t vg = int64_t(blockIdx.x) * kVecs + v;
-    const bool live = vg < nvec;
-
-    for (int e = tid; e < bs * bs; e += kThreads) {
-        const int i = e % bs, k = e / bs;
-        const bool used = forward ? i > k : i < k;
+    T *St = reinterpret_cast<T *>(smem);  // St[k * L + i] = S[i][k]
+    T *rdiag = St + L * L;                // 1 / S[k][k]
+    for (int e = threadIdx.x; e < L * L; e += blockDim.x) {
+        const int i = e % L, k = e / L;
         T val = Ar::zero();
-        if (used || (i == k && !unit)) {
+        if (i < bs && k < bs && (FORWARD ? i > k : i < k)) {
             val = s_trans ? A[k + int64_t(i) * lda] : A[i + int64_t(k) * lda];
             if (s_conj) val = Ar::conj(val);
         }
-        S[i * kLeaf + k] = val;
+        St[e] = val;
     }
-    T c[kRows];
-#pragma unroll
-    for (int m = 0; m < kRows; ++m) {
-        const int i = g + kGroups * m;
-        c[m] = Ar::zero();
-        if (live && i < bs) c[m] = Ar::mul(scale, left ? C[i + vg * ldc] : C[vg + int64_t(i) * ldc]);
+    for (int k = threadIdx.x; k < L; k += blockDim.x) {
+        T r = Ar::one();
+        if (!UNIT && k < bs) {
+            T d = A[k + int64_t(k) * lda];
+            if (s_conj) d = Ar::conj(d);
+            r = quot(Ar::one(), d);
+        }
+        rdiag[k] = r;
     }
     __syncthreads();
-
-    for (int step = 0; step < bs; ++step) {
-        const int k = forward ? step : bs - 1 - step;
-        T *xb = xs + (step & 1) * kVecs;
-        if (g == k % kGroups) {
-            const int mk = k / kGroups;
+    const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= nvec) return;
+    T c[L];
 #pragma unroll
-            for (int m = 0; m < kRows; ++m)
-                if (m == mk) {
-                    T x = c[m];
-                    if (!unit) x = quot(x, S[k * kLeaf + k]);
-                    c[m] = x;
-                    xb[v] = x;
-                }
-        }
-        __syncthreads();
-        const T xk = xb[v];
-#pragma unroll
-        for (int m = 0; m < kRows; ++m) {
-            const int i = g + kGroups * m;
-            if (i < bs && (forward ? i > k : i < k)) c[m] = Ar::fma(negate(S[i * kLeaf + k]), xk, c[m]);
-        }
+    for (int i = 0; i < L; ++i) {
+        c[i] = Ar::zero();
+        if (i < bs) c[i] = Ar::mul(scale, left ? C[i + v * ldc] : C[v + int64_t(i) * ldc]);
     }
-    if (!live) return;
 #pragma unroll
-    for (int m = 0; m < kRows; ++m) {
-        const int i = g + kGroups * m;
-        if (i < bs) (left ? C[i + vg * ldc] : C[vg + int64_t(i) * ldc]) = c[m];
+    for (int s = 0; s < L; ++s) {
+        const int k = FORWARD ? s : L - 1 - s;
+        if (!UNIT) c[k] = Ar::mul(c[k], rdiag[k]);
+        const T xk = c[k];
+        const T *col = St + k * L;
+#pragma unroll
+        for (int i = FORWARD ? k + 1 : 0; i < (FORWARD ? L : k); ++i) c[i] = Ar::fma(negate(col[i]), xk, c[i]);
     }
+#pragma unroll
+    for (int i = 0; i < L; ++i)
+        if (i < bs) (left ? C[i + v * ldc] : C[v + int64_t(i) * ldc]) = c[i];
 }
 
-template <typename T> size_t leaf_smem() { return sizeof(T) * (kLeaf * kLeaf + 2 * kVecs); }
+template <typename T> size_t leaf_smem() { return sizeof(T) * (LeafDim<T>::n * (LeafDim<T>::n + 1)); }
 
-template <typename T>
-int launch_leaf_t(const Trsm &t, int64_t lo, int64_t hi, cplx scale, int s_trans, int forward, cudaStream_t s) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        BX_CUDA(cudaFuncSetAttribute(trsm_leaf_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(leaf_smem<T>())));
-        attr_set = true;
-    }
+template <typename T, bool FORWARD, bool UNIT>
+int launch_leaf_k(const Trsm &t, int64_t lo, int64_t hi, cplx scale, int s_trans, cudaStream_t s) {
     const int64_t nvec = t.left ? t.N : t.M;
     const T *A = static_cast<const T *>(t.A) + lo + lo * t.lda;
     T *C = static_cast<T *>(t.B) + (t.left ? lo : lo * t.ldb);
-    const int64_t blocks = (nvec + kVecs - 1) / kVecs;
+    const int64_t blocks = (nvec + kLeafThreads - 1) / kLeafThreads;
     if (blocks > 0x7fffffff) return set_error(BLASX_ERR_UNSUPPORTED, "trsm: too many right-hand sides");
     const bool conj = is_complex(t.dt) && t.trans == ConjT;
-    trsm_leaf_kernel<T><<<unsigned(blocks), kThreads, leaf_smem<T>(), s>>>(
-        A, t.lda, C, t.ldb, int(hi - lo), nvec, t.left, s_trans, conj, t.unit, forward, from_cplx<T>(scale));
+    trsm_leaf_kernel<T, FORWARD, UNIT><<<unsigned(blocks), kLeafThreads, leaf_smem<T>(), s>>>(
+        A, t.lda, C, t.ldb, int(hi - lo), nvec, t.left, s_trans, conj, from_cplx<T>(scale));
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;
+}
+
+template <typename T>
+int launch_leaf_t(const Trsm &t, int64_t lo, int64_t hi, cplx scale, int s_trans, int forward, cudaStream_t s) {
+    if (forward)
+        return t.unit ? launch_leaf_k<T, true, true>(t, lo, hi, scale, s_trans, s)
+                      : launch_leaf_k<T, true, false>(t, lo, hi, scale, s_trans, s);
+    return t.unit ? launch_leaf_k<T, false, true>(t, lo, hi, scale, s_trans, s)
+                  : launch_leaf_k<T, false, false>(t, lo, hi, scale, s_trans, s);
 }
 
 int launch_leaf(const Trsm &t, int64_t lo, int64_t hi, cplx scale, int s_trans, int forward, cudaStream_t s) {
@@ -151,10 +152,10 @@ int s_trans_of(const Trsm &t) { return t.left ? t.trans != NoTrans : t.trans == 
 bool forward_of(const Trsm &t) { return t.lower != bool(s_trans_of(t)); }
 
 // The two halves of [lo, hi) in solve order: the first has a multiple of
-// kLeaf rows.
+// the leaf order rows.
 void split(const Trsm &t, Range r, Range *first, Range *second) {
-    const int64_t n = r.size();
-    const int64_t half = std::min(n - 1, (n / 2 + kLeaf - 1) / kLeaf * kLeaf);
+    const int64_t n = r.size(), lf = leaf_order(t.dt);
+    const int64_t half = std::min(n - 1, (n / 2 + lf - 1) / lf * lf);
     if (forward_of(t)) {
         *first = {r.lo, r.lo + half};
         *second = {r.lo + half, r.hi};
@@ -202,7 +203,7 @@ Gemm update_gemm(const Trsm &t, Range tgt, Range src, cplx scale) {
 }
 
 int solve(const Trsm &t, Range r, cplx scale, cudaStream_t s, bool *emulated) {
-    if (r.size() <= kLeaf) return launch_leaf(t, r.lo, r.hi, scale, s_trans_of(t), forward_of(t), s);
+    if (r.size() <= leaf_order(t.dt)) return launch_leaf(t, r.lo, r.hi, scale, s_trans_of(t), forward_of(t), s);
     Range first, second;
     split(t, r, &first, &second);
     BX_TRY(solve(t, first, scale, s, emulated));
@@ -215,7 +216,7 @@ int solve(const Trsm &t, Range r, cplx scale, cudaStream_t s, bool *emulated) {
 
 Gemm trsm_top_update(const Trsm &t) {
     const Range all{0, t.order()};
-    if (all.size() <= kLeaf) {
+    if (all.size() <= leaf_order(t.dt)) {
         Gemm g = update_gemm(t, all, all, t.alpha);
         g.K = 0;
         return g;

@@ -311,6 +311,14 @@ int blasx_cgemm_device(int transa, int transb, int M, int N, int K, const void *
 int blasx_dsyrk_device(int uplo, int trans, int N, int K, double alpha, const double *A, int lda,
                        double beta, double *C, int ldc, void *stream);
 
+/* Device-resident DTRSM (column-major; side CblasLeft/CblasRight, uplo, trans,
+ * diag as for cblas_dtrsm): solves op(A) X = alpha B or X op(A) = alpha B for
+ * the device matrix B (overwritten by X), enqueued on `stream`; returns a
+ * status. Update GEMMs follow the precision mode. No counterpart in the
+ * reference. */
+int blasx_dtrsm_device(int side, int uplo, int trans, int diag, int M, int N, double alpha,
+                       const double *A, int lda, double *B, int ldb, void *stream);
+
 /* Device-resident DGEMM that allocates no memory. No counterpart in the
  * reference. It is meant for callers that cannot let a library call
  * cudaMalloc: a framework whose own allocator has already reserved the
