@@ -50,11 +50,12 @@ struct Events {
 struct DeviceOps {
     void *A = nullptr, *B = nullptr, *C = nullptr, *ws = nullptr;
     void *C0 = nullptr;  // input C, when the emulated path accumulates K-blocks into C
+    void *diag = nullptr;  // diagonal blocks of a triangular operand (tri_split)
     bool b_is_a = false;  // B is the same host buffer as A (SYRK): one device copy
     int64_t lda = 0, ldb = 0, ldc = 0;
     cudaStream_t s = nullptr;
     ~DeviceOps() {
-        for (void *p : {A, b_is_a ? nullptr : B, C, ws, C0})
+        for (void *p : {A, b_is_a ? nullptr : B, C, ws, C0, diag})
             if (p) cudaFreeAsync(p, s);
     }
 };
@@ -121,6 +122,81 @@ int panel_count(const Gemm &g) {
     return int(std::max<int64_t>(1, std::min<int64_t>(16, g.N / 1024)));
 }
 
+// ---- operands stored as one triangle (SYMM, HEMM, TRMM) ---------------------
+// Gemm::a_form / b_form name the stored triangle of a square operand. Its
+// device copy lands whole; complete_forms then fills in the rest in place
+// (mirror, conjugate mirror, or zeros and a unit diagonal) before any GEMM
+// reads it.
+
+// Width of the diagonal blocks a triangular operand keeps on the native path
+// when the rest of the product is emulated.
+constexpr int kTriDiagBlock = 256;
+
+bool tri_form(int f) { return f >= kTriUpper; }
+
+// Triangular operand on the emulated path (tri_split): the diagonal blocks of
+// the completed triangle move to d.diag and are zeroed in place, the emulated
+// GEMM runs on the block-off-diagonal part, and tri_diag_panel adds the
+// diagonal blocks with the native kernel (beta 1), panel by panel. Every
+// emulated sum then spans at least kTriDiagBlock dense terms or none: the tip
+// of the triangle (a single nonzero per row or column, where a per-row scaled
+// emulation loses relative accuracy) is computed natively. The native share
+// of the work is about kTriDiagBlock / K. A triangle within one block runs on
+// the native path whole.
+int complete_forms(const Gemm &g, const DeviceOps &d, cudaStream_t s) {
+    BX_TRY(launch_complete_operand(g.dt, g.a_form, d.A, d.lda, g.rows_a(), s));
+    BX_TRY(launch_complete_operand(g.dt, g.b_form, d.B, d.ldb, g.rows_b(), s));
+    if (d.diag) {
+        const bool on_a = tri_form(g.a_form);
+        BX_TRY(launch_split_diag_blocks(g.dt, on_a ? d.A : d.B, on_a ? d.lda : d.ldb, g.K, kTriDiagBlock, d.diag,
+                                        s));
+    }
+    return BLASX_OK;
+}
+
+// C(:, j0:j1) += alpha x (the diagonal-block part of the product) for a
+// tri_split GEMM dg on device operands (its triangle's blocks in diag).
+int tri_diag_panel(const Gemm &dg, bool tri_is_a, const void *diag, int64_t j0, int64_t j1, cudaStream_t s) {
+    const size_t es = elem_size(dg.dt);
+    const int64_t n = dg.K, nb = kTriDiagBlock;
+    const char *D = static_cast<const char *>(diag);
+    std::vector<Gemm> blocks;
+    for (int64_t b0 = 0; b0 < n; b0 += nb) {
+        const int64_t bs = std::min(nb, n - b0);
+        Gemm b = dg;
+        b.beta = cplx{1.0, 0.0};
+        b.K = bs;
+        b.uplo = 0;
+        if (tri_is_a) {  // C(J, j0:j1) += alpha op(A)(J, J) B(J, j0:j1); tb is NoTrans
+            b.M = bs;
+            b.N = j1 - j0;
+            b.A = D + size_t(b0) * nb * es;
+            b.lda = nb;
+            b.B = static_cast<const char *>(dg.B) + size_t(b0 + j0 * dg.ldb) * es;
+            b.C = static_cast<char *>(dg.C) + size_t(b0 + j0 * dg.ldc) * es;
+        } else {  // C(:, c0:c1) += alpha A(:, J) op(B)(J, c0:c1), [c0, c1) = J and [j0, j1); ta is NoTrans
+            const int64_t c0 = std::max(b0, j0), c1 = std::min(b0 + bs, j1);
+            if (c0 >= c1) continue;
+            b.N = c1 - c0;
+            b.A = static_cast<const char *>(dg.A) + size_t(b0) * dg.lda * es;
+            // the block is stored at D columns b0 .. b0 + bs (ld nb); op(B)(J, c0:c1) is its columns
+            // c0 .. c1 (NoTrans) or its rows c0 - b0 .. c1 - b0 (Trans / ConjTrans)
+            b.B = dg.tb == NoTrans ? D + size_t(c0) * nb * es : D + size_t((c0 - b0) + b0 * nb) * es;
+            b.ldb = nb;
+            b.C = static_cast<char *>(dg.C) + size_t(c0) * dg.ldc * es;
+        }
+        blocks.push_back(b);
+    }
+    // FP64 / complex128: the blocks go out in grouped launches of the DMMA kernel
+    if (!blocks.empty() && dmma_supported(blocks[0])) {
+        for (size_t i = 0; i < blocks.size(); i += kMaxGroup)
+            BX_TRY(launch_gemm_dmma_grouped(blocks.data() + i, int(std::min<size_t>(kMaxGroup, blocks.size() - i)), s));
+        return BLASX_OK;
+    }
+    for (const Gemm &b : blocks) BX_TRY(launch_gemm_simt(b, s));
+    return BLASX_OK;
+}
+
 // ---- in-core, native kernels ----------------------------------------------
 int incore_native(const Gemm &g, Context *c, DeviceOps &d, bool need_ab, bool read_c,
                   blasx_call_stats &st) {
@@ -134,14 +210,20 @@ int incore_native(const Gemm &g, Context *c, DeviceOps &d, bool need_ab, bool re
         BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
                                   cudaMemcpyHostToDevice, c->h2d));
         st.h2d_bytes += double(es) * g.rows_a() * g.cols_a();
+        if (g.b_form) {  // a stored triangle is completed whole: B lands before the panels
+            BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
+                                      cudaMemcpyHostToDevice, c->h2d));
+            st.h2d_bytes += double(es) * g.rows_b() * g.cols_b();
+        }
     }
     const int panels = panel_count(g);
     for (int p = 0; p < panels; ++p) {
         const int64_t j0 = g.N * p / panels, j1 = g.N * (p + 1) / panels;
-        BX_TRY(copy_panel_in(g, d, j0, j1, need_ab, read_c, c->h2d, st));
+        BX_TRY(copy_panel_in(g, d, j0, j1, need_ab && !g.b_form, read_c, c->h2d, st));
         cudaEvent_t in = ev.make();
         BX_CUDA(cudaEventRecord(in, c->h2d));
         BX_CUDA(cudaStreamWaitEvent(c->compute, in, 0));
+        if (p == 0 && need_ab) BX_TRY(complete_forms(g, d, c->compute));
         Gemm p_g = g;
         p_g.N = j1 - j0;
         p_g.A = d.A; p_g.lda = d.lda;
@@ -175,10 +257,12 @@ struct OzPanelCtx {
     Context *c;
     Events *ev;
     blasx_call_stats *st;
+    const Gemm *dg = nullptr;  // device operands; set with d->diag (tri_split)
 };
 
 int oz_after_panel(void *vctx, int64_t j0, int64_t j1) {
     auto *x = static_cast<OzPanelCtx *>(vctx);
+    if (x->d->diag) BX_TRY(tri_diag_panel(*x->dg, tri_form(x->g->a_form), x->d->diag, j0, j1, x->c->compute));
     cudaEvent_t done = x->ev->make();
     BX_CUDA(cudaEventRecord(done, x->c->compute));
     BX_CUDA(cudaStreamWaitEvent(x->c->d2h, done, 0));
@@ -315,7 +399,8 @@ int incore_ozaki_kblocks(const Gemm &g, Context *c, DeviceOps &d, int mode, blas
 
 int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
                  blasx_call_stats &st) {
-    if (kblock_count(g) > 1) return incore_ozaki_kblocks(g, c, d, mode, st);
+    // K-blocks copy A and B in pieces; a stored triangle is completed whole
+    if (kblock_count(g) > 1 && !g.a_form && !g.b_form) return incore_ozaki_kblocks(g, c, d, mode, st);
     Events ev;
     const size_t es = elem_size(g.dt);
     cudaEvent_t start = ev.make();
@@ -337,7 +422,9 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
     dg.A = d.A; dg.lda = d.lda;
     dg.B = d.B; dg.ldb = d.ldb;
     dg.C = d.C; dg.ldc = d.ldc;
-    OzPanelCtx pctx{&g, &d, c, &ev, &st};
+    dg.a_form = dg.b_form = 0;
+    BX_TRY(complete_forms(g, d, c->compute));
+    OzPanelCtx pctx{&g, &d, c, &ev, &st, &dg};
     PanelHooks hooks{panel_count(g), read_c ? &oz_before_reconstruct : nullptr, &oz_after_panel,
                      &pctx};
     BX_TRY(ozaki_gemm_panels(dg, c->compute, mode, d.ws, c->num_sms, hooks));
@@ -346,131 +433,79 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
 
 bool want_ozaki(const Gemm &g, int mode) { return ozaki_selected(g, mode); }
 
-// Width of the diagonal blocks a triangular operand keeps on the native path
-// when the rest of the product is emulated.
-constexpr int kTriDiagBlock = 256;
-
-// Triangular operand on the emulated path: the diagonal blocks of the
-// (completed) triangle are moved to dg_diag and zeroed in place, the
-// emulated GEMM runs on the block-off-diagonal part, and the diagonal blocks
-// are added with the native kernel (beta 1). Every emulated sum then spans
-// at least kTriDiagBlock dense terms or none: the tip of the triangle (a
-// single nonzero per row or column, where a per-row scaled emulation loses
-// relative accuracy) is computed natively. The native share of the work is
-// about kTriDiagBlock / K; a triangle within one block runs natively whole.
-int tri_split_gemm(const Gemm &dg, bool tri_is_a, void *diag, cudaStream_t s) {
-    const size_t es = elem_size(dg.dt);
-    const int64_t n = dg.K, nb = kTriDiagBlock;
-    if (n <= nb) {
-        call_stats().path = 1;
-        return dmma_supported(dg) ? launch_gemm_dmma(dg, s) : launch_gemm_simt(dg, s);
-    }
-    void *T = tri_is_a ? const_cast<void *>(dg.A) : const_cast<void *>(dg.B);
-    const int64_t ldt = tri_is_a ? dg.lda : dg.ldb;
-    BX_TRY(launch_split_diag_blocks(dg.dt, T, ldt, n, int(nb), diag, s));
-    BX_TRY(device_gemm(dg, s));
-    for (int64_t j0 = 0; j0 < n; j0 += nb) {
-        const int64_t bs = std::min(nb, n - j0);
-        Gemm b = dg;
-        b.beta = cplx{1.0, 0.0};
-        b.K = bs;
-        const char *blk = static_cast<const char *>(diag) + size_t(j0) * nb * es;
-        if (tri_is_a) {  // C(J, :) += alpha op(A)(J, J) B(J, :)
-            b.M = bs;
-            b.A = blk; b.lda = nb;
-            b.B = static_cast<const char *>(dg.B) + size_t(j0) * es;  // tb is NoTrans
-            b.C = static_cast<char *>(dg.C) + size_t(j0) * es;
-        } else {  // C(:, J) += alpha A(:, J) op(B)(J, J)
-            b.N = bs;
-            b.A = static_cast<const char *>(dg.A) + size_t(j0) * dg.lda * es;  // ta is NoTrans
-            b.B = blk; b.ldb = nb;
-            b.C = static_cast<char *>(dg.C) + size_t(j0) * dg.ldc * es;
-        }
-        BX_TRY(dmma_supported(b) ? launch_gemm_dmma(b, s) : launch_gemm_simt(b, s));
-    }
-    return BLASX_OK;
-}
-
-// SYMM / HEMM / TRMM: an operand stored as one triangle (a_form / b_form) is
-// completed on its device copy before one device GEMM (native or emulated
-// by the precision mode; see tri_split_gemm for a triangular operand on the
-// emulated path). In core only: A, B and C (when read) are copied whole, the
-// product runs, and C is copied back. C may be the same host buffer as B
-// (TRMM): B is on the device before anything is written back.
-int host_formed(const Gemm &g, Context *c, blasx_call_stats &st, int mode) {
-    const size_t es = elem_size(g.dt);
-    const bool need_ab = !(g.alpha_zero() || g.K == 0);
-    const bool read_c = !g.beta_zero();
-    DeviceOps d;
-    d.s = c->compute;
-    d.lda = round_up(g.rows_a(), 32);
-    d.ldb = round_up(g.rows_b(), 32);
-    d.ldc = round_up(g.M, 32);
-    const size_t bytes_a = need_ab ? size_t(d.lda) * g.cols_a() * es : 0;
-    const size_t bytes_b = need_ab ? size_t(d.ldb) * g.cols_b() * es : 0;
-    const size_t bytes_c = size_t(d.ldc) * g.N * es;
-    Gemm dg = g;
-    dg.A = nullptr; dg.lda = d.lda;
-    dg.B = nullptr; dg.ldb = d.ldb;
-    dg.ldc = d.ldc;
-    dg.a_form = dg.b_form = 0;
-    const bool oz = need_ab && ozaki_selected(dg, mode);
-    const bool tri_a = g.a_form >= kTriUpper, tri_b = g.b_form >= kTriUpper;
-    const bool split = oz && (tri_a || tri_b);
-    const size_t bytes_diag = split && g.K > kTriDiagBlock ? size_t(kTriDiagBlock) * g.K * es : 0;
-    const size_t bytes_ws = oz ? ozaki_scratch_bytes(dg) : 0;
-    if (bytes_a + bytes_b + bytes_c + bytes_ws + bytes_diag > default_budget(c))
-        return set_error(BLASX_ERR_UNSUPPORTED,
-                         "symmetric / Hermitian / triangular operand: %zu bytes exceed the HBM budget",
-                         bytes_a + bytes_b + bytes_c + bytes_ws);
-    HostPin pins;
-    BX_TRY(pins.pin(g.A, need_ab ? host_extent(g.lda, g.rows_a(), g.cols_a(), es) : 0));
-    BX_TRY(pins.pin(g.B, need_ab ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
-    BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
-    cudaStream_t s = c->compute;
-    if (need_ab) {
-        BX_CUDA(cudaMallocAsync(&d.A, bytes_a ? bytes_a : 256, s));
-        BX_CUDA(cudaMallocAsync(&d.B, bytes_b ? bytes_b : 256, s));
-        BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
-                                  cudaMemcpyHostToDevice, s));
-        BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
-                                  cudaMemcpyHostToDevice, s));
-        st.h2d_bytes += double(es) * (g.rows_a() * g.cols_a() + g.rows_b() * g.cols_b());
-        BX_TRY(launch_complete_operand(g.dt, g.a_form, d.A, d.lda, g.rows_a(), s));
-        BX_TRY(launch_complete_operand(g.dt, g.b_form, d.B, d.ldb, g.rows_b(), s));
-    }
-    BX_CUDA(cudaMallocAsync(&d.C, bytes_c, s));
-    if (read_c) {
-        BX_CUDA(cudaMemcpy2DAsync(d.C, d.ldc * es, g.C, g.ldc * es, g.M * es, g.N, cudaMemcpyHostToDevice, s));
-        st.h2d_bytes += double(es) * g.M * g.N;
-    }
-    dg.A = d.A; dg.B = d.B; dg.C = d.C;
-    if (split) {
-        if (bytes_diag) BX_CUDA(cudaMallocAsync(&d.ws, bytes_diag, s));
-        BX_TRY(tri_split_gemm(dg, tri_a, d.ws, s));
-    } else if (need_ab) {
-        BX_TRY(device_gemm(dg, s));
-    } else {
-        BX_TRY(launch_scale(dg, s));
-        st.path = 3;
-    }
-    BX_CUDA(cudaMemcpy2DAsync(g.C, g.ldc * es, d.C, d.ldc * es, g.M * es, g.N, cudaMemcpyDeviceToHost, s));
-    st.d2h_bytes += double(es) * g.M * g.N;
-    BX_CUDA(cudaStreamSynchronize(s));
-    if (st.path == 2) {
-        resolve_decision(st);
-        if (*c->last_error_flag)
-            return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
-                             *c->last_error_flag);
-    }
-    return BLASX_OK;
-}
-
 }  // namespace
 
-// TRSM on host operands: A (the order-K triangle, copied whole) and B to the
-// device, the recursive solve (trsm_device), B back. In core only, like
-// host_formed; the scratch of the largest update GEMM is part of the budget.
+// TRSM with its copies overlapped: along the top-level split of the
+// triangle, the H2D stream copies the first diagonal block of A and the
+// first part of B, then the off-diagonal block and the rest of B, then the
+// second diagonal block; the compute stream solves the first part as soon
+// as its inputs landed, applies the update, and solves the second part; the
+// D2H stream returns each part of X as soon as it is final. The parts of B
+// are rows (left) or columns (right); A's off-diagonal block is op(A)[second,
+// first] (left) or op(A)[first, second] (right) as stored.
+static int trsm_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Context *c, int64_t f0, int64_t f1,
+                          int64_t s0, int64_t s1, bool *emulated, blasx_call_stats &st) {
+    const size_t es = elem_size(t.dt);
+    Events ev;
+    cudaEvent_t start = ev.make();
+    BX_CUDA(cudaEventRecord(start, c->compute));  // the device buffers are allocated on compute
+    BX_CUDA(cudaStreamWaitEvent(c->h2d, start, 0));
+    BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
+    auto copy_a = [&](int64_t r0, int64_t r1, int64_t c0, int64_t c1) -> int {
+        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.A) + (r0 + c0 * d.lda) * es, d.lda * es,
+                                  static_cast<const char *>(t.A) + (r0 + c0 * t.lda) * es, t.lda * es,
+                                  (r1 - r0) * es, c1 - c0, cudaMemcpyHostToDevice, c->h2d));
+        st.h2d_bytes += double(es) * (r1 - r0) * (c1 - c0);
+        return BLASX_OK;
+    };
+    // part [p0, p1) of B: rows (left) or columns (right)
+    auto copy_b = [&](int64_t p0, int64_t p1, bool in) -> int {
+        const int64_t off = t.left ? p0 : p0 * t.ldb, doff = t.left ? p0 : p0 * d.ldb;
+        const int64_t rows = t.left ? p1 - p0 : t.M, cols = t.left ? t.N : p1 - p0;
+        char *dev = static_cast<char *>(d.B) + doff * es;
+        char *host = static_cast<char *>(t.B) + off * es;
+        if (in)
+            BX_CUDA(cudaMemcpy2DAsync(dev, d.ldb * es, host, t.ldb * es, rows * es, cols, cudaMemcpyHostToDevice,
+                                      c->h2d));
+        else
+            BX_CUDA(cudaMemcpy2DAsync(host, t.ldb * es, dev, d.ldb * es, rows * es, cols, cudaMemcpyDeviceToHost,
+                                      c->d2h));
+        (in ? st.h2d_bytes : st.d2h_bytes) += double(es) * rows * cols;
+        return BLASX_OK;
+    };
+    auto handoff = [&](cudaStream_t from, cudaStream_t to) -> int {
+        cudaEvent_t e = ev.make();
+        BX_CUDA(cudaEventRecord(e, from));
+        BX_CUDA(cudaStreamWaitEvent(to, e, 0));
+        return BLASX_OK;
+    };
+    const bool off_tgt_first = t.left == (t.trans == NoTrans);  // stored rows of the off-diagonal block
+    BX_TRY(copy_a(f0, f1, f0, f1));
+    BX_TRY(copy_b(f0, f1, true));
+    BX_TRY(handoff(c->h2d, c->compute));
+    BX_TRY(trsm_solve_part(dt, f0, f1, t.alpha, c->compute, emulated));
+    BX_TRY(handoff(c->compute, c->d2h));
+    BX_TRY(copy_b(f0, f1, false));
+    if (off_tgt_first) BX_TRY(copy_a(s0, s1, f0, f1));
+    else BX_TRY(copy_a(f0, f1, s0, s1));
+    BX_TRY(copy_b(s0, s1, true));
+    BX_TRY(handoff(c->h2d, c->compute));
+    BX_TRY(trsm_update_part(dt, s0, s1, f0, f1, t.alpha, c->compute, emulated));
+    BX_TRY(copy_a(s0, s1, s0, s1));
+    BX_TRY(handoff(c->h2d, c->compute));
+    BX_TRY(trsm_solve_part(dt, s0, s1, cplx{1.0, 0.0}, c->compute, emulated));
+    BX_TRY(handoff(c->compute, c->d2h));
+    BX_TRY(copy_b(s0, s1, false));
+    BX_CUDA(cudaStreamSynchronize(c->h2d));
+    BX_CUDA(cudaStreamSynchronize(c->compute));
+    BX_CUDA(cudaStreamSynchronize(c->d2h));
+    return BLASX_OK;
+}
+
+// TRSM on host operands: A (the order-K triangle) and B to the device, the
+// recursive solve, B back; copies overlap the solve along its top-level split
+// (trsm_pipelined). In core only, like the stored-triangle operands of
+// host_gemm; the scratch of the largest update GEMM is part of the budget.
 int host_trsm(const Trsm &t) {
     auto t0 = std::chrono::steady_clock::now();
     blasx_call_stats &st = call_stats();
@@ -501,23 +536,25 @@ int host_trsm(const Trsm &t) {
     BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
     cudaStream_t s = c->compute;
-    if (need_a) {
-        BX_CUDA(cudaMallocAsync(&d.A, bytes_a, s));
-        BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, s));
-        st.h2d_bytes += double(es) * K * K;
-    }
-    BX_CUDA(cudaMallocAsync(&d.B, bytes_b, s));
-    if (need_a) {  // alpha == 0 writes zeros without reading B
-        BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, t.B, t.ldb * es, t.M * es, t.N, cudaMemcpyHostToDevice, s));
-        st.h2d_bytes += double(es) * t.M * t.N;
-    }
+    if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, s));
+    BX_CUDA(cudaMallocAsync(&d.B, bytes_b, s));  // alpha == 0 writes zeros without reading B
     dt.A = d.A;
     dt.B = d.B;
     bool emulated = false;
-    BX_TRY(trsm_device(dt, s, &emulated));
-    BX_CUDA(cudaMemcpy2DAsync(t.B, t.ldb * es, d.B, d.ldb * es, t.M * es, t.N, cudaMemcpyDeviceToHost, s));
-    st.d2h_bytes += double(es) * t.M * t.N;
-    BX_CUDA(cudaStreamSynchronize(s));
+    int64_t f0, f1, s0, s1;
+    if (!need_a || !trsm_halves(dt, &f0, &f1, &s0, &s1)) {
+        if (need_a) {
+            BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, s));
+            BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, t.B, t.ldb * es, t.M * es, t.N, cudaMemcpyHostToDevice, s));
+            st.h2d_bytes += double(es) * (double(K) * K + double(t.M) * t.N);
+        }
+        BX_TRY(trsm_device(dt, s, &emulated));
+        BX_CUDA(cudaMemcpy2DAsync(t.B, t.ldb * es, d.B, d.ldb * es, t.M * es, t.N, cudaMemcpyDeviceToHost, s));
+        st.d2h_bytes += double(es) * t.M * t.N;
+        BX_CUDA(cudaStreamSynchronize(s));
+    } else {
+        BX_TRY(trsm_pipelined(t, dt, d, c, f0, f1, s0, s1, &emulated, st));
+    }
     st.path = !need_a ? 3 : (emulated ? 2 : 1);
     if (emulated) {
         resolve_decision(st);
@@ -542,12 +579,11 @@ int host_gemm(const Gemm &g) {
     // a triangular output keeps the other triangle: C always makes the round trip
     const bool read_c = !g.beta_zero() || g.uplo != 0;
     const int mode = config().dgemm_mode.load();
-    if (g.a_form || g.b_form) {
-        const int rc = host_formed(g, c, st, mode);
-        st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        return rc;
-    }
-    const bool oz = need_ab && want_ozaki(g, mode);
+    const bool formed = g.a_form || g.b_form;
+    bool oz = need_ab && want_ozaki(g, mode);
+    // a triangle within one diagonal block runs natively whole (see tri_split)
+    if (oz && (tri_form(g.a_form) || tri_form(g.b_form)) && g.K <= kTriDiagBlock) oz = false;
+    const bool tri_split = oz && (tri_form(g.a_form) || tri_form(g.b_form));
 
     DeviceOps d;
     d.s = c->compute;
@@ -561,12 +597,18 @@ int host_gemm(const Gemm &g) {
     Gemm probe = g;
     probe.lda = d.lda; probe.ldb = d.ldb; probe.ldc = d.ldc;
     if (!d.b_is_a) probe.B = nullptr;  // the scratch shares slices only when the device copy is shared
+    probe.a_form = probe.b_form = 0;
     const size_t bytes_ws = oz ? ozaki_scratch_bytes(probe) : 0;
-    const size_t bytes_c0 = (oz && read_c && kblock_count(g) > 1) ? bytes_c : 0;
+    const size_t bytes_c0 = (oz && read_c && kblock_count(g) > 1 && !formed) ? bytes_c : 0;
+    const size_t bytes_diag = tri_split ? size_t(kTriDiagBlock) * g.K * es : 0;
     const size_t budget = default_budget(c);
 
     HostPin pins;
-    if (bytes_a + bytes_b + bytes_c + bytes_c0 + bytes_ws > budget && need_ab) {
+    const size_t total = bytes_a + bytes_b + bytes_c + bytes_c0 + bytes_ws + bytes_diag;
+    if (total > budget && need_ab && formed)  // a stored triangle is completed whole, in core
+        return set_error(BLASX_ERR_UNSUPPORTED,
+                         "symmetric / Hermitian / triangular operand: %zu bytes exceed the HBM budget", total);
+    if (total > budget && need_ab) {
         // out-of-core: HBM tile cache under the byte budget; each K-step on
         // the emulated path when the precision mode picks it for a step's shape
         const int T = pick_tile(g);
@@ -592,6 +634,7 @@ int host_gemm(const Gemm &g) {
     BX_CUDA(cudaMallocAsync(&d.C, bytes_c, c->compute));
     if (oz) BX_CUDA(cudaMallocAsync(&d.ws, bytes_ws, c->compute));
     if (bytes_c0) BX_CUDA(cudaMallocAsync(&d.C0, bytes_c0, c->compute));
+    if (bytes_diag) BX_CUDA(cudaMallocAsync(&d.diag, bytes_diag, c->compute));
     const int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
                       : incore_native(g, c, d, need_ab, read_c, st);
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -45,5 +45,15 @@ int trsm_device(const Trsm &t, cudaStream_t s, bool *emulated);
 // The largest update GEMM trsm_device issues for t (its scratch bounds the
 // solve's), or a Gemm with K == 0 when the triangle is a single leaf.
 Gemm trsm_top_update(const Trsm &t);
+// The top-level split of trsm_device: solve order first, then second (false
+// when the triangle is a single leaf). trsm_solve_part solves rows (left) or
+// columns (right) [lo, hi) whose right-hand sides are scale * B;
+// trsm_update_part applies B[tgt] = scale B[tgt] - op(A)[tgt, src] X[src] (or
+// the right-side mirror). Together: solve(first, alpha), update(second, first,
+// alpha), solve(second, 1) is trsm_device.
+bool trsm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi);
+int trsm_solve_part(const Trsm &t, int64_t lo, int64_t hi, cplx scale, cudaStream_t s, bool *emulated);
+int trsm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cplx scale,
+                     cudaStream_t s, bool *emulated);
 
 }  // namespace bx

@@ -439,13 +439,16 @@ int dmma_geometry(int64_t M, int64_t N) {
             n = 148;
         return n;
     }();
-    auto busy = [&](int64_t tiles, int per_sm) {
+    // share of the SM slots of all waves that hold useful output: occupancy
+    // of the last wave times the part of each tile inside M x N
+    auto useful = [&](int64_t edge, int per_sm) {
+        const int64_t tiles = ((M + edge - 1) / edge) * ((N + edge - 1) / edge);
         const int64_t slots = int64_t(sms) * per_sm;
         const int64_t waves = (tiles + slots - 1) / slots;
-        return double(tiles) / double(waves * slots);
+        return double(M) * double(N) / (double(waves * slots) * double(edge * edge));
     };
-    const double big = busy(((M + 127) / 128) * ((N + 127) / 128), 1);
-    const double small = 0.85 * busy(((M + 63) / 64) * ((N + 63) / 64), 2);
+    const double big = useful(128, 1);
+    const double small = 0.85 * useful(64, 2);
     return small > big ? 1 : 0;
 }
 

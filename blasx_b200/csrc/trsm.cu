@@ -32,13 +32,23 @@ template <> struct LeafDim<z2> {
 template <> struct LeafDim<c2> {
     static constexpr int n = 32;
 };
-constexpr int kLeafThreads = 64;  // right-hand-side vectors per CTA
+constexpr int kLeafVecs = 64;     // right-hand-side vectors per CTA
+constexpr int kLanes = 4;         // lanes per vector: lane j owns rows j, j + 4, ...
+constexpr int kLeafThreads = kLeafVecs * kLanes;
 
 int leaf_order(DType dt) { return is_complex(dt) ? 32 : 64; }
 
 template <typename T> __device__ inline T negate(T a) { return -a; }
 template <> __device__ inline z2 negate<z2>(z2 a) { return {-a.re, -a.im}; }
 template <> __device__ inline c2 negate<c2>(c2 a) { return {-a.re, -a.im}; }
+
+template <typename T> __device__ inline T shfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <> __device__ inline z2 shfl<z2>(z2 v, int src) {
+    return {__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
+}
+template <> __device__ inline c2 shfl<c2>(c2 v, int src) {
+    return {__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
+}
 
 // Solves S x = c for nvec vectors at once, S the bs x bs (bs <= L) system
 // matrix of one diagonal block: S = op(A_block) for a left solve, the
@@ -50,70 +60,123 @@ template <> __device__ inline c2 negate<c2>(c2 a) { return {-a.re, -a.im}; }
 // B). Each vector is scaled by `scale` (alpha) on load.
 //
 // Shared memory holds S by columns (St[k * L + i] = S[i][k]), zero outside
-// the triangle, and the reciprocals of its diagonal. Each thread solves one
-// vector held in registers: the substitution is unrolled over the L x L
-// block, so every register index and loop bound is a compile-time constant,
-// and all threads read the same St entry at a time (a broadcast). A block
-// smaller than L is padded with zero right-hand sides and unit diagonal,
-// which leave the real rows unchanged.
+// the triangle, the reciprocals of its diagonal and, for a left solve, the
+// CTA's vectors: they are columns of B, which consecutive threads load and
+// store row by row (coalesced) through shared memory. Four adjacent lanes
+// solve one vector held in their registers, lane j owning rows j, j + 4, ...
+// The substitution is unrolled over the L x L block, so every register index
+// is a compile-time constant; at step k the lane owning row k scales it by
+// 1 / S[k][k], a shuffle hands x_k to the other three, and each lane updates
+// its later rows (no barrier). A block smaller than L is padded with zero
+// right-hand sides and unit diagonal, which leave the real rows unchanged.
 template <typename T, bool FORWARD, bool UNIT>
 __global__ void __launch_bounds__(kLeafThreads)
     trsm_leaf_kernel(const T *__restrict__ A, int64_t lda, T *__restrict__ C, int64_t ldc, int bs,
                      int64_t nvec, int left, int s_trans, int s_conj, T scale) {
     using Ar = Arith<T>;
     constexpr int L = LeafDim<T>::n;
+    constexpr int R = L / kLanes;  // rows per lane
     extern __shared__ __align__(16) unsigned char smem[];
     T *St = reinterpret_cast<T *>(smem);  // St[k * L + i] = S[i][k]
     T *rdiag = St + L * L;                // 1 / S[k][k]
-    for (int e = threadIdx.x; e < L * L; e += blockDim.x) {
-        const int i = e % L, k = e / L;
-        T val = Ar::zero();
-        if (i < bs && k < bs && (FORWARD ? i > k : i < k)) {
-            val = s_trans ? A[k + int64_t(i) * lda] : A[i + int64_t(k) * lda];
-            if (s_conj) val = Ar::conj(val);
+    T *Cs = rdiag + L;                    // left: Cs[v * (L + 1) + i], this CTA's vectors
+    const int64_t v0 = int64_t(blockIdx.x) * kLeafVecs;
+    const int tid = threadIdx.x;
+    // global -> shared: every load of a thread is issued before its stores
+    constexpr int kStPer = L * L / kLeafThreads, kCsPer = L * kLeafVecs / kLeafThreads;
+    static_assert(kStPer * kLeafThreads == L * L && kCsPer * kLeafThreads == L * kLeafVecs, "whole batches");
+    if (left) {  // a left vector is a column of B: consecutive threads take consecutive rows
+        T tmp[kCsPer];
+#pragma unroll
+        for (int q = 0; q < kCsPer; ++q) {
+            const int e = tid + q * kLeafThreads, i = e % L, vv = e / L;
+            tmp[q] = (i < bs && v0 + vv < nvec) ? C[i + (v0 + vv) * ldc] : Ar::zero();
         }
-        St[e] = val;
+#pragma unroll
+        for (int q = 0; q < kCsPer; ++q) {
+            const int e = tid + q * kLeafThreads;
+            Cs[(e / L) * (L + 1) + e % L] = tmp[q];
+        }
     }
-    for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    {
+        T tmp[kStPer];
+#pragma unroll
+        for (int q = 0; q < kStPer; ++q) {
+            const int e = tid + q * kLeafThreads, i = e % L, k = e / L;
+            tmp[q] = Ar::zero();
+            if (i < bs && k < bs && (FORWARD ? i > k : i < k))
+                tmp[q] = s_trans ? A[k + int64_t(i) * lda] : A[i + int64_t(k) * lda];
+        }
+#pragma unroll
+        for (int q = 0; q < kStPer; ++q) St[tid + q * kLeafThreads] = s_conj ? Ar::conj(tmp[q]) : tmp[q];
+    }
+    if (tid < L) {
         T r = Ar::one();
-        if (!UNIT && k < bs) {
-            T d = A[k + int64_t(k) * lda];
+        if (!UNIT && tid < bs) {
+            T d = A[tid + int64_t(tid) * lda];
             if (s_conj) d = Ar::conj(d);
             r = quot(Ar::one(), d);
         }
-        rdiag[k] = r;
+        rdiag[tid] = r;
     }
     __syncthreads();
-    const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (v >= nvec) return;
-    T c[L];
+    const int j = tid % kLanes, vl = tid / kLanes;
+    const int64_t v = v0 + vl;
+    const bool live = v < nvec;
+    const int base = tid & ~(kLanes - 1);  // lane 0 of this vector's group
+    T c[R];
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-        c[i] = Ar::zero();
-        if (i < bs) c[i] = Ar::mul(scale, left ? C[i + v * ldc] : C[v + int64_t(i) * ldc]);
+    for (int m = 0; m < R; ++m) {
+        const int i = j + kLanes * m;
+        c[m] = Ar::zero();
+        if (i < bs && live) c[m] = Ar::mul(scale, left ? Cs[vl * (L + 1) + i] : C[v + int64_t(i) * ldc]);
     }
 #pragma unroll
     for (int s = 0; s < L; ++s) {
         const int k = FORWARD ? s : L - 1 - s;
-        if (!UNIT) c[k] = Ar::mul(c[k], rdiag[k]);
-        const T xk = c[k];
+        const int mk = k / kLanes, jk = k % kLanes;
+        if (!UNIT && j == jk) c[mk] = Ar::mul(c[mk], rdiag[k]);
+        const T xk = shfl(c[mk], base + jk);
         const T *col = St + k * L;
 #pragma unroll
-        for (int i = FORWARD ? k + 1 : 0; i < (FORWARD ? L : k); ++i) c[i] = Ar::fma(negate(col[i]), xk, c[i]);
+        for (int m = 0; m < R; ++m) {
+            const int i = j + kLanes * m;
+            if (FORWARD ? (kLanes * m + kLanes - 1 > k && i > k) : (kLanes * m < k && i < k))
+                c[m] = Ar::fma(negate(col[i]), xk, c[m]);
+        }
+    }
+    if (!left) {
+        if (live)
+#pragma unroll
+            for (int m = 0; m < R; ++m) {
+                const int i = j + kLanes * m;
+                if (i < bs) C[v + int64_t(i) * ldc] = c[m];
+            }
+        return;
     }
 #pragma unroll
-    for (int i = 0; i < L; ++i)
-        if (i < bs) (left ? C[i + v * ldc] : C[v + int64_t(i) * ldc]) = c[i];
+    for (int m = 0; m < R; ++m) Cs[vl * (L + 1) + j + kLanes * m] = c[m];
+    __syncthreads();
+    for (int e = tid; e < L * kLeafVecs; e += kLeafThreads) {
+        const int i = e % L, vv = e / L;
+        if (i < bs && v0 + vv < nvec) C[i + (v0 + vv) * ldc] = Cs[vv * (L + 1) + i];
+    }
 }
 
-template <typename T> size_t leaf_smem() { return sizeof(T) * (LeafDim<T>::n * (LeafDim<T>::n + 1)); }
+template <typename T> size_t leaf_smem() {
+    constexpr int L = LeafDim<T>::n;
+    return sizeof(T) * (L * (L + 1) + kLeafVecs * (L + 1));
+}
 
 template <typename T, bool FORWARD, bool UNIT>
 int launch_leaf_k(const Trsm &t, int64_t lo, int64_t hi, cplx scale, int s_trans, cudaStream_t s) {
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        trsm_leaf_kernel<T, FORWARD, UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(leaf_smem<T>()));
+    BX_CUDA(attr);
     const int64_t nvec = t.left ? t.N : t.M;
     const T *A = static_cast<const T *>(t.A) + lo + lo * t.lda;
     T *C = static_cast<T *>(t.B) + (t.left ? lo : lo * t.ldb);
-    const int64_t blocks = (nvec + kLeafThreads - 1) / kLeafThreads;
+    const int64_t blocks = (nvec + kLeafVecs - 1) / kLeafVecs;
     if (blocks > 0x7fffffff) return set_error(BLASX_ERR_UNSUPPORTED, "trsm: too many right-hand sides");
     const bool conj = is_complex(t.dt) && t.trans == ConjT;
     trsm_leaf_kernel<T, FORWARD, UNIT><<<unsigned(blocks), kLeafThreads, leaf_smem<T>(), s>>>(
@@ -213,6 +276,27 @@ int solve(const Trsm &t, Range r, cplx scale, cudaStream_t s, bool *emulated) {
 }
 
 }  // namespace
+
+bool trsm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi) {
+    const Range all{0, t.order()};
+    if (all.size() <= leaf_order(t.dt)) return false;
+    Range first, second;
+    split(t, all, &first, &second);
+    *first_lo = first.lo; *first_hi = first.hi;
+    *second_lo = second.lo; *second_hi = second.hi;
+    return true;
+}
+
+int trsm_solve_part(const Trsm &t, int64_t lo, int64_t hi, cplx scale, cudaStream_t s, bool *emulated) {
+    return solve(t, Range{lo, hi}, scale, s, emulated);
+}
+
+int trsm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cplx scale,
+                     cudaStream_t s, bool *emulated) {
+    BX_TRY(device_gemm(update_gemm(t, Range{tgt_lo, tgt_hi}, Range{src_lo, src_hi}, scale), s));
+    if (call_stats().path == 2) *emulated = true;
+    return BLASX_OK;
+}
 
 Gemm trsm_top_update(const Trsm &t) {
     const Range all{0, t.order()};
