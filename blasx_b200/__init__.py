@@ -94,9 +94,15 @@ def lib() -> ctypes.CDLL:
         L.cblas_ssyr2k.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I]
         L.cblas_dsyr2k.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I]
         L.cblas_zsyr2k.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I]
-        for f in ("ssyrk_", "dsyrk_", "zsyrk_"):
+        L.cblas_csyrk.argtypes = [_I] * 5 + [_P, _P, _I, _P, _P, _I]
+        L.cblas_csyr2k.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I]
+        L.cblas_cherk.argtypes = [_I] * 5 + [_F, _P, _I, _F, _P, _I]
+        L.cblas_zherk.argtypes = [_I] * 5 + [_D, _P, _I, _D, _P, _I]
+        L.cblas_cher2k.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _F, _P, _I]
+        L.cblas_zher2k.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _D, _P, _I]
+        for f in ("ssyrk_", "dsyrk_", "zsyrk_", "csyrk_", "cherk_", "zherk_"):
             getattr(L, f).argtypes = [_P] * 10
-        for f in ("ssyr2k_", "dsyr2k_", "zsyr2k_"):
+        for f in ("ssyr2k_", "dsyr2k_", "zsyr2k_", "csyr2k_", "cher2k_", "zher2k_"):
             getattr(L, f).argtypes = [_P] * 12
         L.blasx_dsyrk_device.argtypes = [_I] * 4 + [_D, _P, _I, _D, _P, _I, _P]
         L.blasx_dtrsm_device.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _P]
@@ -213,12 +219,13 @@ def cblas_zsyr2k(Order, Uplo, Trans, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
                        be.ctypes.data, _addr(C), ldc)
 
 
-def _f77_syr(fn, ctype, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, B=None, ldb=None, cplx=False):
+def _f77_syr(fn, ctype, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, B=None, ldb=None, cplx=False,
+             pair=None):
     u = ctypes.c_char(uplo.encode() if isinstance(uplo, str) else uplo)
     t = ctypes.c_char(trans.encode() if isinstance(trans, str) else trans)
     ints = [ctypes.c_int(v) for v in (n, k, lda, ldc, ldb or 1)]
     if cplx:
-        al, be = _cpair(alpha), _cpair(beta)
+        al, be = (pair or _cpair)(alpha), (pair or _cpair)(beta)
         pa, pb = al.ctypes.data, be.ctypes.data
     else:
         al, be = ctype(alpha), ctype(beta)
@@ -241,6 +248,79 @@ def dsyrk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
 
 def zsyrk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
     _f77_syr(lib().zsyrk_, None, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, cplx=True)
+
+
+def cblas_csyrk(Order, Uplo, Trans, N, K, alpha, A, lda, beta, C, ldc):
+    al, be = _cpair32(alpha), _cpair32(beta)
+    lib().cblas_csyrk(Order, Uplo, Trans, N, K, al.ctypes.data, _addr(A), lda, be.ctypes.data, _addr(C), ldc)
+
+
+def cblas_csyr2k(Order, Uplo, Trans, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    al, be = _cpair32(alpha), _cpair32(beta)
+    lib().cblas_csyr2k(Order, Uplo, Trans, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb, be.ctypes.data,
+                       _addr(C), ldc)
+
+
+def cblas_cherk(Order, Uplo, Trans, N, K, alpha, A, lda, beta, C, ldc):
+    lib().cblas_cherk(Order, Uplo, Trans, N, K, float(alpha), _addr(A), lda, float(beta), _addr(C), ldc)
+
+
+def cblas_zherk(Order, Uplo, Trans, N, K, alpha, A, lda, beta, C, ldc):
+    lib().cblas_zherk(Order, Uplo, Trans, N, K, float(alpha), _addr(A), lda, float(beta), _addr(C), ldc)
+
+
+def cblas_cher2k(Order, Uplo, Trans, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    al = _cpair32(alpha)
+    lib().cblas_cher2k(Order, Uplo, Trans, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb, float(beta),
+                       _addr(C), ldc)
+
+
+def cblas_zher2k(Order, Uplo, Trans, N, K, alpha, A, lda, B, ldb, beta, C, ldc):
+    al = _cpair(alpha)
+    lib().cblas_zher2k(Order, Uplo, Trans, N, K, al.ctypes.data, _addr(A), lda, _addr(B), ldb, float(beta),
+                       _addr(C), ldc)
+
+
+def _f77_her(fn, ctype, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, B=None, ldb=None, pair=None):
+    """F77 HERK / HER2K: real beta (and real HERK alpha) by pointer; HER2K's
+    complex alpha as an (re, im) pair of `pair` (_cpair32 or _cpair)."""
+    u, t = _char(uplo), _char(trans)
+    ints = [ctypes.c_int(v) for v in (n, k, lda, ldc, ldb or 1)]
+    be = ctype(beta)
+    if pair is None:
+        al = ctype(alpha)
+        pa = ctypes.addressof(al)
+    else:
+        al = pair(alpha)
+        pa = al.ctypes.data
+    r = ctypes.byref
+    if B is None:
+        fn(r(u), r(t), r(ints[0]), r(ints[1]), pa, _addr(A), r(ints[2]), r(be), _addr(C), r(ints[3]))
+    else:
+        fn(r(u), r(t), r(ints[0]), r(ints[1]), pa, _addr(A), r(ints[2]), _addr(B), r(ints[4]), r(be), _addr(C),
+           r(ints[3]))
+
+
+def cherk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
+    _f77_her(lib().cherk_, ctypes.c_float, uplo, trans, n, k, alpha, A, lda, beta, C, ldc)
+
+
+def zherk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
+    _f77_her(lib().zherk_, ctypes.c_double, uplo, trans, n, k, alpha, A, lda, beta, C, ldc)
+
+
+def cher2k_(uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    _f77_her(lib().cher2k_, ctypes.c_float, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, B=B, ldb=ldb,
+             pair=_cpair32)
+
+
+def zher2k_(uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    _f77_her(lib().zher2k_, ctypes.c_double, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, B=B, ldb=ldb,
+             pair=_cpair)
+
+
+def csyrk_(uplo, trans, n, k, alpha, A, lda, beta, C, ldc):
+    _f77_syr(lib().csyrk_, None, uplo, trans, n, k, alpha, A, lda, beta, C, ldc, cplx=True, pair=_cpair32)
 
 
 def dsyr2k_(uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C, ldc):

@@ -238,6 +238,7 @@ int incore_native(const Gemm &g, Context *c, DeviceOps &d, bool need_ab, bool re
         } else {
             BX_TRY(launch_scale(p_g, c->compute));
         }
+        if (g.herm_out) BX_TRY(launch_real_diagonal(g.dt, p_g.C, d.ldc, g.M, j1 - j0, j0 + g.diag, c->compute));
         cudaEvent_t done = ev.make();
         BX_CUDA(cudaEventRecord(done, c->compute));
         BX_CUDA(cudaStreamWaitEvent(c->d2h, done, 0));
@@ -263,6 +264,9 @@ struct OzPanelCtx {
 int oz_after_panel(void *vctx, int64_t j0, int64_t j1) {
     auto *x = static_cast<OzPanelCtx *>(vctx);
     if (x->d->diag) BX_TRY(tri_diag_panel(*x->dg, tri_form(x->g->a_form), x->d->diag, j0, j1, x->c->compute));
+    if (x->g->herm_out)
+        BX_TRY(launch_real_diagonal(x->g->dt, static_cast<char *>(x->d->C) + j0 * x->d->ldc * elem_size(x->g->dt),
+                                    x->d->ldc, x->g->M, j1 - j0, j0 + x->g->diag, x->c->compute));
     cudaEvent_t done = x->ev->make();
     BX_CUDA(cudaEventRecord(done, x->c->compute));
     BX_CUDA(cudaStreamWaitEvent(x->c->d2h, done, 0));

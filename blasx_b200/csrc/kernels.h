@@ -14,6 +14,9 @@ int launch_scale(const Gemm &g, cudaStream_t s);
 // triangle are only read, except Hermitian diagonals (imaginary part set to
 // zero) and unit diagonals (set to one).
 int launch_complete_operand(DType dt, int form, void *X, int64_t ldx, int64_t n, cudaStream_t s);
+// Zeroes the imaginary parts of the entries (r, c) of the m x n device block
+// C (ld ldc) with r - c == off; nothing for real types.
+int launch_real_diagonal(DType dt, void *C, int64_t ldc, int64_t m, int64_t n, int64_t off, cudaStream_t s);
 // Moves the nb x nb diagonal blocks of the n x n device matrix X into D
 // (ld nb, n columns: block J in columns J nb ..) and zeroes them in X.
 int launch_split_diag_blocks(DType dt, void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s);

@@ -235,6 +235,28 @@ int launch_complete_operand(DType dt, int form, void *X, int64_t ldx, int64_t n,
     }
 }
 
+// One thread per diagonal entry: (r, r - off) for r in the block.
+template <typename R>
+__global__ void real_diagonal_kernel(R *C, int64_t ldc, int64_t m, int64_t n, int64_t off) {
+    const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    const int64_t r = (off > 0 ? off : 0) + t, c = r - off;
+    if (r < m && c >= 0 && c < n) C[2 * (r + c * ldc) + 1] = R(0);
+}
+
+int launch_real_diagonal(DType dt, void *C, int64_t ldc, int64_t m, int64_t n, int64_t off, cudaStream_t s) {
+    if (!is_complex(dt) || m <= 0 || n <= 0) return BLASX_OK;
+    const int64_t len = std::min(m - std::max<int64_t>(off, 0), n + std::min<int64_t>(off, 0));
+    if (len <= 0) return BLASX_OK;
+    const unsigned blocks = unsigned((len + 255) / 256);
+    if (dt == DType::C128)
+        real_diagonal_kernel<double><<<blocks, 256, 0, s>>>(static_cast<double *>(C), ldc, m, n, off);
+    else
+        real_diagonal_kernel<float><<<blocks, 256, 0, s>>>(static_cast<float *>(C), ldc, m, n, off);
+    BX_CUDA(cudaGetLastError());
+    count_launch();
+    return BLASX_OK;
+}
+
 int launch_split_diag_blocks(DType dt, void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s) {
     if (n <= 0) return BLASX_OK;
     switch (elem_size(dt)) {

@@ -67,6 +67,10 @@ struct Gemm {
     // Stored form of a square A (or B): only one triangle holds data, and the
     // operand is completed on the device before the product (SYMM, HEMM, TRMM).
     int a_form = 0, b_form = 0;  // an OperandForm
+    // Hermitian output (HERK, HER2K): the imaginary parts of C's diagonal
+    // entries (row == col, shifted by diag like uplo) are set to zero once
+    // the product is complete.
+    bool herm_out = false;
 
     bool alpha_zero() const { return alpha.re == 0 && alpha.im == 0; }
     bool beta_zero() const { return beta.re == 0 && beta.im == 0; }

@@ -225,6 +225,8 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
         BX_CUDA(cudaEventRecord(lastuse[size_t(s.b.slot)], c->compute));
         used[size_t(s.a.slot)] = used[size_t(s.b.slot)] = true;
         if (s.last_k) {
+            if (g.herm_out)  // the global diagonal (row - col == diag) in this tile's coordinates
+                BX_TRY(launch_real_diagonal(g.dt, c_ptr(cs), T, m, n, d.diag, c->compute));
             BX_CUDA(cudaEventRecord(c_done[cs], c->compute));
             BX_CUDA(cudaStreamWaitEvent(c->d2h, c_done[cs], 0));
             char *dst = hC + (int64_t(s.i) * T + int64_t(s.j) * T * g.ldc) * int64_t(es);

@@ -112,6 +112,40 @@ void cblas_zsyr2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
                   const void *A, const int lda, const void *B, const int ldb, const void *beta,
                   void *C, const int ldc);
 
+/* Replace cblas_csyrk / cblas_csyr2k (include/cblas.h:494,498; blas/csyrk.c,
+ * blas/csyr2k.c, host BLAS only): the complex64 forms of the above (alpha,
+ * beta, A, B, C interleaved (re, im) float pairs; ConjTrans illegal). */
+void cblas_csyrk(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                 const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const void *alpha,
+                 const void *A, const int lda, const void *beta, void *C, const int ldc);
+void cblas_csyr2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                  const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const void *alpha,
+                  const void *A, const int lda, const void *B, const int ldb, const void *beta,
+                  void *C, const int ldc);
+
+/* Replace cblas_cherk / cblas_zherk (include/cblas.h:553,568; blas/zherk.c:
+ * 14-78, host BLAS only): C = alpha op(A) op(A)^H + beta C on the uplo
+ * triangle, alpha and beta real, Trans CblasNoTrans or CblasConjTrans
+ * (CblasTrans is illegal, info 2); the imaginary parts of C's diagonal are
+ * set to zero. cblas_cher2k / cblas_zher2k (include/cblas.h:557,572;
+ * blas/zher2k.c:15-86): C = alpha op(A) op(B)^H + conj(alpha) op(B) op(A)^H
+ * + beta C, beta real. ZHER2K reports argument errors under the name
+ * "ZHERK", as the reference does (blas/zher2k.c:13). */
+void cblas_cherk(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                 const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const float alpha,
+                 const void *A, const int lda, const float beta, void *C, const int ldc);
+void cblas_zherk(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                 const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const double alpha,
+                 const void *A, const int lda, const double beta, void *C, const int ldc);
+void cblas_cher2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                  const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const void *alpha,
+                  const void *A, const int lda, const void *B, const int ldb, const float beta,
+                  void *C, const int ldc);
+void cblas_zher2k(const enum CBLAS_ORDER Order, const enum CBLAS_UPLO Uplo,
+                  const enum CBLAS_TRANSPOSE Trans, const int N, const int K, const void *alpha,
+                  const void *A, const int lda, const void *B, const int ldb, const double beta,
+                  void *C, const int ldc);
+
 /* Replace the F77 wrappers ssyrk_ / dsyrk_ (blas/dsyrk.c:80-101) / zsyrk_ and
  * ssyr2k_ / dsyr2k_ (blas/dsyr2k.c:88-) / zsyr2k_: uplo 'U'/'L', trans
  * 'N'/'T'/'C', column-major, every argument by pointer. */
@@ -127,6 +161,21 @@ void dsyr2k_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, 
              double *B, int *ldb, double *beta, double *C, int *ldc);
 void zsyr2k_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda,
              double *B, int *ldb, double *beta, double *C, int *ldc);
+/* csyrk_ / csyr2k_ (complex64 scalars as (re, im) float pairs), cherk_ /
+ * zherk_ (real alpha, beta) and cher2k_ / zher2k_ (complex alpha, real beta):
+ * blas/csyrk.c:76-, blas/zherk.c:81-104, blas/zher2k.c:89-118. */
+void csyrk_(char *uplo, char *trans, int *n, int *k, float *alpha, float *A, int *lda, float *beta,
+            float *C, int *ldc);
+void csyr2k_(char *uplo, char *trans, int *n, int *k, float *alpha, float *A, int *lda, float *B,
+             int *ldb, float *beta, float *C, int *ldc);
+void cherk_(char *uplo, char *trans, int *n, int *k, float *alpha, float *A, int *lda, float *beta,
+            float *C, int *ldc);
+void zherk_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda, double *beta,
+            double *C, int *ldc);
+void cher2k_(char *uplo, char *trans, int *n, int *k, float *alpha, float *A, int *lda, float *B, int *ldb,
+             float *beta, float *C, int *ldc);
+void zher2k_(char *uplo, char *trans, int *n, int *k, double *alpha, double *A, int *lda, double *B,
+             int *ldb, double *beta, double *C, int *ldc);
 
 /* Replace cblas_ssymm / cblas_dsymm / cblas_csymm / cblas_zsymm
  * (include/cblas.h:429,459,489,519; implementations blas/dsymm.c:16-72 and

@@ -174,6 +174,29 @@ def syrk(uplo, trans, N, K, alpha, A, lda, beta, C, ldc, B=None, ldb=None):
     return C
 
 
+def herk(uplo, trans, N, K, alpha, A, lda, beta, C, ldc, B=None, ldb=None):
+    """Restatement of BLAS ?HERK (B None) and ?HER2K, which the reference
+    hands to its CPU BLAS (blas/zherk.c:44-77, blas/zher2k.c:50-86): C <-
+    alpha op(A) op(A)^H + beta C, or alpha op(A) op(B)^H + conj(alpha) op(B)
+    op(A)^H + beta C, on the uplo triangle only, op(X) = X (trans 'N') or
+    X^H ('C'); the imaginary parts of C's diagonal are taken as zero on input
+    and set to zero on output. Tiled GEMMs on a copy of C whose triangle is
+    copied back."""
+    ta, tb = ("N", "C") if trans == "N" else ("C", "N")
+    full = C.copy(order="F")
+    if B is None:
+        gemm_tiled(ta, tb, N, N, K, alpha, A, lda, A, lda, beta, full, ldc)
+    else:
+        gemm_tiled(ta, tb, N, N, K, alpha, A, lda, B, ldb, beta, full, ldc)
+        gemm_tiled(ta, tb, N, N, K, np.conj(alpha), B, ldb, A, lda, 1.0, full, ldc)
+    m = tri_mask(uplo, N)
+    view, fv = C[:N, :N], full[:N, :N]
+    view[m] = fv[m]
+    d = np.arange(N)
+    view[d, d] = view[d, d].real
+    return C
+
+
 def complete(kind, uplo, X, n, diag="N"):
     """The full n x n matrix that BLAS reads from the uplo triangle of X:
     kind 'S' symmetric (mirror), 'H' Hermitian (conjugate mirror, the

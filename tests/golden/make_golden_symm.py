@@ -1,4 +1,5 @@
-"""Generate the SYMM / HEMM / TRMM / TRSM golden fixtures from the reference library.
+"""Generate the SYMM / HEMM / TRMM / TRSM and HERK / HER2K / CSYRK / CSYR2K
+golden fixtures from the reference library.
 
 The reference (linnanwang/BLASX) is compiled from its own, unmodified sources
 into ``oracle/_ref/libblasx_ref.so`` by ``oracle/Makefile``. Its cblas_?symm,
@@ -34,7 +35,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 import oracle  # noqa: E402
-from golden_cases import symm_fill  # noqa: E402
+from golden_cases import rank_k_fill, symm_fill  # noqa: E402
 from make_golden import capture_stdout  # noqa: E402
 
 OUT = os.path.join(HERE, "symm_trmm_golden.npz")
@@ -177,6 +178,55 @@ def main():
                                 rec[key + "_sum"] = checksum(x["A"], B0)
                                 rec[key + "_C"] = x["B"]
                                 n += 1
+    # HERK / HER2K (C/Z) and CSYRK / CSYR2K: C with NaN outside its triangle
+    # and, for HERK, garbage imaginary parts on its diagonal (golden_cases.rank_k_fill)
+    D_, F_ = ctypes.c_double, ctypes.c_float
+    L.cblas_cherk.argtypes = [I] * 5 + [F_, P, I, F_, P, I]
+    L.cblas_zherk.argtypes = [I] * 5 + [D_, P, I, D_, P, I]
+    L.cblas_cher2k.argtypes = [I] * 5 + [P, P, I, P, I, F_, P, I]
+    L.cblas_zher2k.argtypes = [I] * 5 + [P, P, I, P, I, D_, P, I]
+    L.cblas_csyrk.argtypes = [I] * 5 + [P, P, I, P, P, I]
+    L.cblas_csyr2k.argtypes = [I] * 5 + [P, P, I, P, I, P, P, I]
+    for tag in "cz":
+        for kind in ("herk", "her2k") + (("syrk", "syr2k") if tag == "c" else ()):
+            herm = kind.startswith("her")
+            for (N, K) in [(1, 1), (7, 3), (33, 65), (64, 17)]:
+                for uplo in (121, 122):
+                    for trans in (111, 113 if herm else 112):
+                        for order in (102, 101):
+                            if order == 101 and (N, K) != (7, 3):
+                                continue
+                            seed = 20000 + 10 * n
+                            # the reference checks lda against the column-major rule whatever the Order
+                            rows = N if trans == 111 else K
+                            lda = (rows if order == 102 else max(N, K)) + n % 2
+                            ldc = N + n % 3
+                            meta = [order, uplo, trans, N, K, lda, lda + 1, ldc, seed]
+                            x = rank_k_fill(kind, tag, meta)
+                            C0 = x["C"].copy(order="F")
+                            if kind == "herk":
+                                al, be = [(1.5, -0.25), (0.0, 2.0), (-0.5, 0.0)][n % 3]
+                                pa, pb = al, be
+                            else:
+                                al = [complex(1.5, -0.5), 0j, complex(0.5, 1.0)][n % 3]
+                                be = -0.25 if herm else complex(-0.25, 0.75)
+                                pa, ka = scalar_arg(tag, al)
+                                pb, kb = (be, None) if herm else scalar_arg(tag, be)
+                            fn = getattr(L, f"cblas_{tag}{kind}")
+                            args = [order, uplo, trans, N, K, pa, x["A"].ctypes.data, lda]
+                            if x["B"] is not None:
+                                args += [x["B"].ctypes.data, lda + 1]
+                            args += [pb, x["C"].ctypes.data, ldc]
+                            out = capture_stdout(lambda: fn(*args))
+                            assert out == "", out
+                            key = f"{kind}_{tag}_{n}"
+                            rec[key + "_meta"] = np.array(meta, dtype=np.int64)
+                            rec[key + "_scal"] = np.array([al, be], dtype=np.complex128)
+                            parts = [np.nansum(x["A"]), np.nansum(C0)] + (
+                                [np.nansum(x["B"])] if x["B"] is not None else [])
+                            rec[key + "_sum"] = np.array(parts, dtype=np.complex128)
+                            rec[key + "_C"] = x["C"]
+                            n += 1
     # xerbla lines
     A = np.zeros((4, 4)); B = np.zeros((4, 4)); C = np.ones((4, 4), order="F")
     Az = np.zeros((4, 4), dtype=np.complex128); Bz = Az.copy(); Cz = np.ones((4, 4), dtype=np.complex128, order="F")
@@ -224,10 +274,30 @@ def main():
         out = capture_stdout(lambda: L.dtrsm_(*(r(c) for c in cc), r(four), r(four), r(al), A.ctypes.data, r(four),
                                               C.ctypes.data, r(four)))
         lines.append(f"dtrsm_{b''.join(chars).decode()}|-|{out}")
+    for info, kw in {1: dict(uplo=999), 2: dict(trans=112), 3: dict(N=-1), 4: dict(K=-1), 7: dict(lda=2),
+                     10: dict(ldc=2)}.items():
+        a = dict(uplo=121, trans=111, N=4, K=4, lda=4, ldc=4)
+        a.update(kw)
+        out = capture_stdout(lambda: L.cblas_zherk(102, a["uplo"], a["trans"], a["N"], a["K"], 1.0, Az.ctypes.data,
+                                                   a["lda"], 0.0, Cz.ctypes.data, a["ldc"]))
+        lines.append(f"cblas_zherk|{info}|{out}")
+    for info, kw in {2: dict(trans=112), 9: dict(ldb=2), 12: dict(ldc=2)}.items():
+        a = dict(trans=111, ldb=4, ldc=4)
+        a.update(kw)
+        out = capture_stdout(lambda: L.cblas_zher2k(102, 121, a["trans"], 4, 4, one.ctypes.data, Az.ctypes.data, 4,
+                                                    Bz.ctypes.data, a["ldb"], 0.0, Cz.ctypes.data, a["ldc"]))
+        lines.append(f"cblas_zher2k|{info}|{out}")
+    L.zherk_.argtypes = [P] * 10
+    for up, tr in [(b"X", b"N"), (b"U", b"Q"), (b"U", b"T")]:
+        cu, ct = ctypes.c_char(up), ctypes.c_char(tr)
+        alz, bez = ctypes.c_double(1.0), ctypes.c_double(0.0)
+        out = capture_stdout(lambda: L.zherk_(r(cu), r(ct), r(four), r(four), r(alz), Az.ctypes.data, r(four),
+                                              r(bez), Cz.ctypes.data, r(four)))
+        lines.append(f"zherk_{up.decode()}{tr.decode()}|-|{out}")
     assert np.all(C == 1.0) and np.all(Cz == 1.0), "outputs must be untouched on argument errors"
     rec["xerbla"] = np.array(lines)
     np.savez_compressed(OUT, **rec)
-    print(f"wrote {OUT}: {n} SYMM/HEMM/TRMM/TRSM cases + {len(lines)} xerbla lines")
+    print(f"wrote {OUT}: {n} SYMM/HEMM/TRMM/TRSM/HERK/HER2K/CSYRK/CSYR2K cases + {len(lines)} xerbla lines")
 
 
 if __name__ == "__main__":

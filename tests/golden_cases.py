@@ -222,3 +222,81 @@ def symm_check(kind, x, got, want, al, be):
     err = np.abs(blk.astype(np.complex128) - want[:M, :N].astype(np.complex128))
     bound = trsm_bound(x, al, want) if kind == "X" else symm_bound(kind, x, al, be)
     assert np.all(err <= bound), float(np.max(err / np.maximum(bound, 1e-300)))
+
+
+# ---- HERK / HER2K (C/Z) and CSYRK / CSYR2K fixtures ---------------------------
+# meta = order, uplo, trans, N, K, lda, ldb, ldc, seed. The column-major problem
+# of a row-major call has uplo flipped and NoTrans / (Conj)Trans swapped.
+
+def rank_k_fill(kind, tag, meta):
+    """Inputs of one 'herk', 'her2k', 'syrk' or 'syr2k' case: A (and B), C
+    with NaN in the triangle BLAS does not reference and, for the Hermitian
+    kinds, a nonzero imaginary part on C's diagonal (which BLAS takes as
+    zero)."""
+    dt = SYMM_GOLDEN_DT[tag]
+    order, uplo, trans, N, K, lda, ldb, ldc, seed = (int(v) for v in meta)
+    herm = kind.startswith("her")
+    rm = order == 101
+    cm_uplo = UPLO_OF[uplo] if not rm else ("L" if uplo == 121 else "U")
+    ctr = "C" if herm else "T"
+    cm_trans = ("N" if trans == 111 else ctr) if not rm else (ctr if trans == 111 else "N")
+    cols = K if cm_trans == "N" else N
+    A = oracle.uniform((lda, cols), dt, seed)
+    B = oracle.uniform((ldb, cols), dt, seed + 1) if kind.endswith("2k") else None
+    C = oracle.uniform((ldc, N), dt, seed + 2)
+    i, j = np.indices((N, N))
+    C[:N, :N][(i > j) if cm_uplo == "U" else (i < j)] = np.nan
+    if herm:
+        d = np.arange(N)
+        C[d, d] = C[d, d].real + 0.375j
+    return dict(A=A, B=B, C=C, N=N, K=K, lda=lda, ldb=ldb, ldc=ldc, uplo=uplo, trans=trans, order=order,
+                cm_uplo=cm_uplo, cm_trans=cm_trans, dt=dt, kind=kind)
+
+
+def rank_k_case(golden, key):
+    kind, tag = key.split("_")[0], key.split("_")[1]
+    x = rank_k_fill(kind, tag, golden[key + "_meta"])
+    parts = [np.nansum(x["A"]), np.nansum(x["C"])] + ([np.nansum(x["B"])] if x["B"] is not None else [])
+    assert np.allclose(np.array(parts, dtype=np.complex128), golden[key + "_sum"]), "fixture generator changed"
+    al, be = (complex(v) for v in golden[key + "_scal"])
+    if kind == "herk":
+        al, be = al.real, be.real
+    elif kind == "her2k":
+        be = be.real
+    return kind, tag, x, al, be, golden[key + "_C"]
+
+
+def rank_k_oracle(x, al, be):
+    C = x["C"].copy(order="F")
+    B, ldb = (x["B"], x["ldb"]) if x["B"] is not None else (None, None)
+    if x["kind"].startswith("her"):
+        if x["kind"] == "her2k" and x["order"] == 101:  # the transposed problem's alpha is conj(alpha)
+            al = np.conj(al)
+        return oracle.herk(x["cm_uplo"], x["cm_trans"], x["N"], x["K"], al, x["A"], x["lda"], be, C, x["ldc"], B, ldb)
+    return oracle.syrk(x["cm_uplo"], x["cm_trans"], x["N"], x["K"], al, x["A"], x["lda"], be, C, x["ldc"], B, ldb)
+
+
+def rank_k_check(x, got, want, al, be):
+    """The uplo triangle within the componentwise bound, the other triangle and
+    the rows beyond N unchanged (NaN included), a real diagonal for HERK."""
+    N, K = x["N"], x["K"]
+    C0 = x["C"]
+    m = oracle.tri_mask(x["cm_uplo"], N)
+    assert np.array_equal(got[N:], C0[N:], equal_nan=True)
+    assert np.array_equal(got[:N, :N][~m], C0[:N, :N][~m], equal_nan=True)
+    if x["kind"].startswith("her"):
+        assert np.all(np.diag(got[:N, :N]).imag == 0)
+    wide = np.complex128
+    A = x["A"].astype(wide)
+    opA = A[:N, :K] if x["cm_trans"] == "N" else (A[:K, :N].conj().T if x["cm_trans"] == "C" else A[:K, :N].T)
+    if x["B"] is not None:
+        Bw = x["B"].astype(wide)
+        opB = Bw[:N, :K] if x["cm_trans"] == "N" else Bw[:K, :N].T
+        prod = np.abs(opA) @ np.abs(opB).T + np.abs(opB) @ np.abs(opA).T
+    else:
+        prod = np.abs(opA) @ np.abs(opA).T
+    c0 = np.nan_to_num(np.abs(C0[:N, :N].astype(wide)))
+    u = oracle.UNIT_ROUNDOFF[np.dtype(x["dt"]).type]
+    bound = 2 * 2 * (K + 2) * u * (abs(al) * prod + abs(be) * c0)
+    err = np.abs(got[:N, :N].astype(wide) - want[:N, :N].astype(wide))[m]
+    assert np.all(err <= bound[m]), float(np.max(err / np.maximum(bound[m], 1e-300)))

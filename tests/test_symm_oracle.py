@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 import oracle
-from golden_cases import symm_case, symm_check, symm_keys, symm_oracle
+from golden_cases import (rank_k_case, rank_k_check, rank_k_oracle, symm_case, symm_check, symm_keys,
+                          symm_oracle)
 from test_abi import _capture
 
 GOLDEN_SYMM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "symm_trmm_golden.npz")
@@ -122,3 +123,60 @@ def test_row_major_uses_the_row_major_leading_dimension(blx):
     assert "DTRMM  parameter number 11" in out and np.all(C == 1.0)
     out = _capture(lambda: blx.cblas_dtrsm(101, 141, 121, 111, 131, 8, 4, 1.0, A, 8, C, 3))
     assert "DTRSM  parameter number 11" in out and np.all(C == 1.0)
+
+
+RANK_K = ["herk_", "her2k_", "syrk_c", "syr2k_c"]
+
+
+def rank_k_keys(golden, prefix):
+    return [k for k in symm_keys(golden, prefix.split("_")[0] + "_") if k.startswith(prefix)]
+
+
+def test_rank_k_fixture_counts(sgolden):
+    # 4 shapes x 2 triangles x 2 transposes column-major, + 4 row-major; per type
+    assert len(rank_k_keys(sgolden, "herk_")) == 2 * 20
+    assert len(rank_k_keys(sgolden, "her2k_")) == 2 * 20
+    assert len(rank_k_keys(sgolden, "syrk_c")) == 20 and len(rank_k_keys(sgolden, "syr2k_c")) == 20
+
+
+@pytest.mark.parametrize("prefix", RANK_K)
+def test_rank_k_oracle_matches_reference(sgolden, prefix):
+    for key in rank_k_keys(sgolden, prefix):
+        kind, tag, x, al, be, want = rank_k_case(sgolden, key)
+        rank_k_check(x, rank_k_oracle(x, al, be), want, al, be)
+
+
+HERK_BAD = {1: dict(uplo=999), 2: dict(trans=112), 3: dict(N=-1), 4: dict(K=-1), 7: dict(lda=2), 10: dict(ldc=2)}
+
+
+@pytest.mark.parametrize("info", sorted(HERK_BAD))
+def test_herk_xerbla_matches_reference(blx, sgolden, info):
+    want = [str(l) for l in sgolden["xerbla"] if str(l).startswith(f"cblas_zherk|{info}|")][0].split("|", 2)[2]
+    a = dict(uplo=121, trans=111, N=4, K=4, lda=4, ldc=4)
+    a.update(HERK_BAD[info])
+    A = np.zeros((4, 4), np.complex128); C = np.ones((4, 4), np.complex128, order="F")
+    got = _capture(lambda: blx.cblas_zherk(102, a["uplo"], a["trans"], a["N"], a["K"], 1.0, A, a["lda"], 0.0, C,
+                                           a["ldc"]))
+    assert got == want
+    assert np.all(C == 1.0) and blx.last_status() == blx.BLASX_ERR_ARG
+
+
+@pytest.mark.parametrize("info,kw", [(2, dict(trans=112)), (9, dict(ldb=2)), (12, dict(ldc=2))])
+def test_her2k_xerbla_matches_reference(blx, sgolden, info, kw):
+    """ZHER2K reports under the reference's name for it, "ZHERK"."""
+    want = [str(l) for l in sgolden["xerbla"] if str(l).startswith(f"cblas_zher2k|{info}|")][0].split("|", 2)[2]
+    a = dict(trans=111, ldb=4, ldc=4)
+    a.update(kw)
+    A = np.zeros((4, 4), np.complex128); C = np.ones((4, 4), np.complex128, order="F")
+    got = _capture(lambda: blx.cblas_zher2k(102, 121, a["trans"], 4, 4, 1.0, A, 4, A, a["ldb"], 0.0, C, a["ldc"]))
+    assert got == want
+    assert np.all(C == 1.0)
+
+
+@pytest.mark.parametrize("up,tr", [("X", "N"), ("U", "Q"), ("U", "T")])
+def test_f77_herk_errors_match_reference(blx, sgolden, up, tr):
+    want = [str(l) for l in sgolden["xerbla"] if str(l).startswith(f"zherk_{up}{tr}|")][0].split("|", 2)[2]
+    A = np.zeros((4, 4), np.complex128); C = np.ones((4, 4), np.complex128, order="F")
+    got = _capture(lambda: blx.zherk_(up, tr, 4, 4, 1.0, A, 4, 0.0, C, 4))
+    assert got == want
+    assert np.all(C == 1.0)
