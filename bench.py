@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--rates", default="100,200,400",
                    help="--workload serving: offered Poisson rates (requests/s) to sweep")
     p.add_argument("--workload", default="", choices=["", "c0", "ragged", "ooc", "c3", "serving", "device", "syrk",
-                                                    "symm"],
+                                                    "symm", "trsm"],
                    help="secondary measurements (one JSON line each) instead of the headline: ragged "
                         "mixed-dtype calls, out-of-core 40960^3 with a 24 GB cache, emulated vs native sweep, "
                         "the full serving stream (10,000 calls, dims to 16384), or a device-resident "
@@ -650,6 +650,29 @@ def run_workloads(args):
         lines.append({"workload": f"device-resident {args.dtype}gemm NN {n}^3, mode {args.mode}",
                       "tflops": fl / (ms * 1e-3) / 1e12, "ms": ms, "path": st["path"], "moduli": st["moduli"],
                       "phases_ms": phases})
+        bx.set_dgemm_mode(bx.MODE_AUTO)
+    elif args.workload == "trsm":
+        # device-resident DTRSM Left Upper NoTrans NonUnit, M = N = --size, A / n + 2 I (well
+        # conditioned), through blasx_dtrsm_device (for ncu captures of the solve's kernels)
+        n = args.size
+        g = torch.Generator(device="cuda").manual_seed(5)
+        T = (torch.rand(n, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1) / n
+        T.diagonal().add_(2.0)
+        B = torch.rand(n, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        bx.set_dgemm_mode({"auto": bx.MODE_AUTO, "native": bx.MODE_NATIVE, "ozaki": bx.MODE_OZAKI}[args.mode])
+        s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
+        call = lambda: bx.dtrsm_device("L", "U", "N", "N", n, n, 1.0, T, n, B, n, stream=s)
+        for _ in range(args.warmup):
+            assert call() == 0, bx.last_error()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            assert call() == 0, bx.last_error()
+        e1.record(s); torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(1, args.steps)
+        lines.append({"workload": f"device-resident dtrsm Left Upper NoTrans NonUnit {n}, mode {args.mode}",
+                      "flops_credited": "M^2 N", "tflops": float(n) ** 3 / (ms * 1e-3) / 1e12, "ms": ms})
         bx.set_dgemm_mode(bx.MODE_AUTO)
     elif args.workload == "serving":
         # the serving stream at full size: 10,000 calls from 16 threads, Poisson
