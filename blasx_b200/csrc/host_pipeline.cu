@@ -609,9 +609,11 @@ int host_gemm(const Gemm &g) {
 
     HostPin pins;
     const size_t total = bytes_a + bytes_b + bytes_c + bytes_c0 + bytes_ws + bytes_diag;
-    if (total > budget && need_ab && formed)  // a stored triangle is completed whole, in core
-        return set_error(BLASX_ERR_UNSUPPORTED,
-                         "symmetric / Hermitian / triangular operand: %zu bytes exceed the HBM budget", total);
+    // out of core, a symmetric / Hermitian operand is read tile by tile from its
+    // stored triangle; a triangular one (TRMM, whose result overwrites the B it
+    // reads) stays in core
+    if (total > budget && need_ab && (tri_form(g.a_form) || tri_form(g.b_form)))
+        return set_error(BLASX_ERR_UNSUPPORTED, "triangular operand: %zu bytes exceed the HBM budget", total);
     if (total > budget && need_ab) {
         // out-of-core: HBM tile cache under the byte budget; each K-step on
         // the emulated path when the precision mode picks it for a step's shape

@@ -146,13 +146,34 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
     const char *hB = static_cast<const char *>(g.B);
     char *hC = static_cast<char *>(g.C);
 
+    // A symmetric / Hermitian operand stored as one triangle (SYMM, HEMM; its
+    // op is NoTrans): a tile of its stored triangle loads as it is; a tile
+    // of the other triangle is the (conjugate) transpose of the stored tile
+    // across the diagonal, which loads in its place and multiplies with a
+    // transposed op; a diagonal tile is completed in place once it lands.
+    auto form_of = [&](int op) { return op == 0 ? g.a_form : g.b_form; };
+    enum { kStored = 0, kMirrored = 1, kDiagonal = 2 };
+    auto tile_kind = [&](int op, int r, int col) {
+        const int f = form_of(op);
+        if (!f) return int(kStored);
+        if (r == col) return int(kDiagonal);
+        const bool upper = f == kSymUpper || f == kHermUpper;
+        return (r < col) == upper ? int(kStored) : int(kMirrored);
+    };
+    auto mirrored_op = [&](int op) {
+        const int f = form_of(op);
+        return (f == kHermUpper || f == kHermLower) ? int(ConjT) : int(TransT);
+    };
+
     // host address and extent of an operand tile (stored layout)
     auto load_tile = [&](const TileUse &u, const TileStep &s) -> int {
         const bool isA = u.key.op == 0;
         const int64_t rows_op = isA ? ext(s.i, g.M) : ext(s.k, g.K);  // op() rows
         const int64_t cols_op = isA ? ext(s.k, g.K) : ext(s.j, g.N);
         const int64_t r0 = int64_t(isA ? s.i : s.k) * T, c0 = int64_t(isA ? s.k : s.j) * T;
-        const bool tr = isA ? g.ta != NoTrans : g.tb != NoTrans;
+        const int kind = tile_kind(u.key.op, isA ? s.i : s.k, isA ? s.k : s.j);
+        // a mirrored tile copies the stored block across the diagonal, as a transposed op would
+        const bool tr = kind == kMirrored || (isA ? g.ta != NoTrans : g.tb != NoTrans);
         const int64_t srow = tr ? c0 : r0, scol = tr ? r0 : c0;
         const int64_t nrow = tr ? cols_op : rows_op, ncol = tr ? rows_op : cols_op;
         const int64_t ld = isA ? g.lda : g.ldb;
@@ -160,6 +181,8 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
         if (used[size_t(u.slot)]) BX_CUDA(cudaStreamWaitEvent(c->h2d, lastuse[size_t(u.slot)], 0));
         BX_CUDA(cudaMemcpy2DAsync(op_ptr(u.slot), size_t(T) * es, src, size_t(ld) * es,
                                   size_t(nrow) * es, size_t(ncol), cudaMemcpyHostToDevice, c->h2d));
+        if (kind == kDiagonal)
+            BX_TRY(launch_complete_operand(g.dt, form_of(u.key.op), op_ptr(u.slot), T, rows_op, c->h2d));
         BX_CUDA(cudaEventRecord(ready[size_t(u.slot)], c->h2d));
         st.h2d_bytes += double(nrow) * ncol * es;
         return BLASX_OK;
@@ -211,6 +234,9 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
         d.M = m; d.N = n; d.K = k;
         d.A = op_ptr(s.a.slot); d.lda = T;
         d.B = op_ptr(s.b.slot); d.ldb = T;
+        if (tile_kind(0, s.i, s.k) == kMirrored) d.ta = mirrored_op(0);
+        if (tile_kind(1, s.k, s.j) == kMirrored) d.tb = mirrored_op(1);
+        d.a_form = d.b_form = 0;
         d.C = c_ptr(cs); d.ldc = T;
         if (!s.first_k) d.beta = cplx{1.0, 0.0};
         d.guard = nullptr;

@@ -23,7 +23,9 @@ size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es);
 // `budget` bytes (policy: 0 Belady, 1 LRU). Synchronous. With ws_bytes > 0
 // every K-step runs on the emulated (Ozaki) path in precision mode `mode`,
 // on a scratch of ws_bytes carved from the same budget; otherwise on the
-// native kernels.
+// native kernels. A symmetric or Hermitian operand stored as one triangle
+// (Gemm::a_form / b_form of SYMM, HEMM) is read from its stored triangle tile
+// by tile; triangular forms are not supported here.
 int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int tile, int policy,
                     size_t ws_bytes = 0, int mode = 0);
 

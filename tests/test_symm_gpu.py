@@ -157,23 +157,6 @@ def test_f77_wrappers_match_cblas(blx):
     assert np.array_equal(D1, D2)
 
 
-def test_over_the_budget_fails_loudly(blx):
-    """Operands that do not fit the HBM budget are reported, not computed
-    elsewhere: the output is left unchanged."""
-    blx.set_hbm_budget(8 << 20)
-    try:
-        M, N = 1024, 1024
-        A = oracle.uniform((M, M), np.float64, 61)
-        B = oracle.uniform((M, N), np.float64, 62)
-        C0 = oracle.uniform((M, N), np.float64, 63)
-        C = C0.copy(order="F")
-        blx.cblas_dsymm(102, 141, 121, M, N, 1.0, A, M, B, M, 1.0, C, M)
-        assert blx.last_status() == blx.BLASX_ERR_UNSUPPORTED
-        assert np.array_equal(C, C0)
-    finally:
-        blx.set_hbm_budget(0)
-
-
 def test_symm_while_serving(blx):
     blx.serve_start(0, 0, 4)
     try:
@@ -306,3 +289,56 @@ def test_trsm_f77_matches_cblas(blx):
     blx.cblas_ztrsm(102, 142, 122, 113, 131, M, N, complex(1, -1), A, N, B1, M)
     blx.ztrsm_("r", "L", "C", "n", M, N, complex(1, -1), A, N, B2, M)
     assert np.array_equal(B1, B2)
+
+
+@pytest.mark.parametrize("side,uplo,dt,herm", [("L", "U", np.float64, False), ("R", "L", np.float64, False),
+                                                ("L", "L", np.complex128, True), ("R", "U", np.complex128, True)])
+@pytest.mark.parametrize("emulated", [False, True])
+def test_symm_out_of_core(blx, side, uplo, dt, herm, emulated):
+    """A 64 MiB budget forces the tile cache: tiles of the unstored triangle
+    (NaN here) are read from the stored one across the diagonal, diagonal
+    tiles are completed on arrival."""
+    blx.set_hbm_budget(64 << 20)
+    blx.set_tile(512)
+    prev = blx.set_dgemm_mode(blx.MODE_OZAKI if emulated else blx.MODE_NATIVE)
+    try:
+        M, N = (2000, 1800) if dt == np.float64 else (1500, 1400)  # A, B, C exceed the budget together
+        na = M if side == "L" else N
+        A = oracle.uniform((na + 1, na), dt, 81)
+        i, j = np.indices((na, na))
+        A[:na, :na][(i > j) if uplo == "U" else (i < j)] = np.nan
+        if herm:
+            d = np.arange(na)
+            A[d, d] = A[d, d].real + 0.25j  # imaginary parts of a Hermitian diagonal are not read
+        B = oracle.uniform((M, N), dt, 82)
+        C0 = oracle.uniform((M, N), dt, 83)
+        C = C0.copy(order="F")
+        al, be = (0.75, 0.5) if dt == np.float64 else (complex(0.75, 0.25), complex(0.5, -0.5))
+        fn = getattr(blx, f"cblas_{'z' if herm else 'd'}{'hemm' if herm else 'symm'}")
+        fn(102, blx.SIDE[side], blx.UPLO[uplo], M, N, al, A, na + 1, B, M, be, C, M)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        st = blx.call_stats()
+        assert st["tile"] == 512 and st["path"] == (2 if emulated else 1), st
+        Af = oracle.complete("H" if herm else "S", uplo, A, na)
+        args = (Af, na, B, M) if side == "L" else (B, M, Af, na)
+        check_dd(C, "N", "N", M, N, na, al, *args, be, C0, M, 85)
+    finally:
+        blx.set_hbm_budget(0)
+        blx.set_tile(0)
+        blx.set_dgemm_mode(prev)
+
+
+def test_trmm_over_the_budget_fails_loudly(blx):
+    """TRMM writes its result into the B it reads, so it stays in core: a
+    problem beyond the budget is reported and B is left unchanged."""
+    blx.set_hbm_budget(8 << 20)
+    try:
+        M = N = 1024
+        A = oracle.uniform((M, M), np.float64, 91)
+        B0 = oracle.uniform((M, N), np.float64, 92)
+        B = B0.copy(order="F")
+        blx.cblas_dtrmm(102, 141, 121, 111, 131, M, N, 1.0, A, M, B, M)
+        assert blx.last_status() == blx.BLASX_ERR_UNSUPPORTED
+        assert np.array_equal(B, B0)
+    finally:
+        blx.set_hbm_budget(0)
