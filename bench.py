@@ -533,6 +533,40 @@ def run_workloads(args):
                           "speedup": res["emulated"]["tflops"] / res["native"]["tflops"]})
             print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
             del dA, tA, tC
+        # ZHERK C = A A^H + 0.5 C (lower), N = K = 8192, complex128, e2e through cblas_zherk on pinned host
+        # arrays (copies included), emulated and native; credited 4 N^2 K flops (the triangle of a complex GEMM)
+        n = 8192
+        tA, A = _host(torch, (n, n), "c128", 21)
+        tC, C0 = _host(torch, (n, n), "c128", 22)
+        Ch = torch.empty_like(tC, pin_memory=True)
+        rng = np.random.default_rng(4)
+        ii = rng.integers(0, n, args.samples); jj = rng.integers(0, n, args.samples)
+        lo = ii > jj
+        ii, jj = ii[lo], jj[lo]
+        res = {}
+        for mode_name, mode in (("emulated", bx.MODE_OZAKI), ("native", bx.MODE_NATIVE)):
+            bx.set_dgemm_mode(mode)
+            times = []
+            for _ in range(2):  # the first call also grows the device memory pool
+                Ch.copy_(tC)
+                t0 = time.perf_counter()
+                bx.cblas_zherk(bx.CblasColMajor, bx.CblasLower, bx.CblasNoTrans, n, n, 1.0, tA.data_ptr(), n, 0.5,
+                               Ch.data_ptr(), n)
+                times.append(time.perf_counter() - t0)
+            assert bx.last_status() == 0, bx.last_error()
+            st = bx.call_stats()
+            Cn = Ch.numpy().reshape(n, n).T
+            val, bound = oracle.dd_entries("N", "C", n, n, n, 1.0, A, n, A, n, 0.5, C0, n, ii, jj)
+            ratio, err = oracle.componentwise_ratio(Cn, ii, jj, val, bound, n, np.complex128)
+            res[mode_name] = {"tflops_e2e": 4.0 * float(n) ** 3 / times[-1] / 1e12, "seconds_e2e": times[-1],
+                              "path": st["path"], "bound_ratio": ratio, "max_normalised_error": err,
+                              "diag_imag_zero": bool(np.all(np.diag(Cn).imag == 0))}
+        bx.set_dgemm_mode(bx.MODE_AUTO)
+        lines.append({"workload": f"zherk lower NoTrans N=K={n}, beta 0.5, U[-1,1] complex, host arrays",
+                      "flops_credited": "4 N^2 K", **res,
+                      "speedup_e2e": res["emulated"]["tflops_e2e"] / res["native"]["tflops_e2e"]})
+        print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
+        del tA, tC, Ch
     elif args.workload == "symm":
         # DSYMM C = A B + 0.5 C (Left, Lower), DTRMM B = A B and DTRSM B = A^-1 B (Left, Upper,
         # NoTrans, NonUnit), M = N in {8192, 16384}, through the drop-in calls on pinned host arrays
