@@ -40,6 +40,10 @@ int launch_gemm_dmma_grouped(const Gemm *gs, int n, cudaStream_t s);
 // Device-resident GEMM of any dtype through the best available path.
 // Uses library-owned scratch memory for the Ozaki path.
 int device_gemm(const Gemm &g, cudaStream_t s);
+// FP32 on the CUDA cores with a 128 x 128 tile per CTA, for problems of at
+// least one wave of such tiles (launch_gemm_simt picks it by sgemm128_fits).
+bool sgemm128_fits(const Gemm &g);
+int launch_sgemm128(const Gemm &g, cudaStream_t s);
 // Triangular solve on device operands (t.A, t.B device pointers): recursive
 // halving into device_gemm updates (native or emulated by the precision
 // mode) and a substitution kernel for blocks of <= 64 rows. Sets *emulated

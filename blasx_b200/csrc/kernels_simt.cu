@@ -218,7 +218,7 @@ template <typename T> int launch_scale_t(const Gemm &g, cudaStream_t s) {
 
 int launch_gemm_simt(const Gemm &g, cudaStream_t s) {
     switch (g.dt) {
-        case DType::F32: return launch_simt_t<float>(g, s);
+        case DType::F32: return sgemm128_fits(g) ? launch_sgemm128(g, s) : launch_simt_t<float>(g, s);
         case DType::F64: return launch_simt_t<double>(g, s);
         case DType::C64: return launch_simt_t<c2>(g, s);
         default: return launch_simt_t<z2>(g, s);

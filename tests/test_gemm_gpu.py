@@ -128,3 +128,60 @@ def test_threads_concurrent_calls(blx):
     [x.join() for x in th]
     assert not errs
     assert max(results.values()) < 1e-12
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+@pytest.mark.parametrize("beta", [0.0, -0.75])
+def test_sgemm_native_wide_tile(blx, ta, tb, beta):
+    """FP32 on the native path with at least one wave of 128 x 128 tiles (the
+    8 x 8-per-thread kernel): ragged in M, N and K, padded leading dimensions;
+    with beta = 0, C holds NaN that must not be read."""
+    prev = blx.set_dgemm_mode(blx.MODE_NATIVE)
+    try:
+        M, N, K = 1701, 1509, 999
+        ra, ca = oracle.shape_of_op(ta, M, K)
+        rb, cb = oracle.shape_of_op(tb, K, N)
+        A = oracle.uniform((ra + 5, ca), np.float32, 21)
+        B = oracle.uniform((rb + 3, cb), np.float32, 22)
+        C0 = oracle.uniform((M + 2, N), np.float32, 23)
+        if beta == 0.0:
+            C0[:M] = np.nan
+        C = C0.copy(order="F")
+        blx.cblas_sgemm(ORDER_COL, oracle.TRANS_OF[ta], oracle.TRANS_OF[tb], M, N, K, 1.25, A, ra + 5, B, rb + 3,
+                        beta, C, M + 2)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        assert blx.call_stats()["path"] == 1
+        np.testing.assert_array_equal(C[M:, :], C0[M:, :])
+        rng = np.random.default_rng(9)
+        ii = rng.integers(0, M, 4000); jj = rng.integers(0, N, 4000)
+        ii[:4] = [0, M - 1, 127, 128]; jj[:4] = [0, N - 1, 128, 127]  # tile corners and the ragged edge
+        Cr = np.nan_to_num(C0)
+        val, bound = oracle.dd_entries(ta, tb, M, N, K, 1.25, A, ra + 5, B, rb + 3, beta, Cr, M + 2, ii, jj)
+        ratio, _ = oracle.componentwise_ratio(C, ii, jj, val, bound, K, np.float32)
+        assert ratio <= 1.0
+    finally:
+        blx.set_dgemm_mode(prev)
+
+
+def test_ssyrk_native_wide_tile(blx):
+    """The triangular mask of the 128 x 128 FP32 kernel: SSYRK upper on the
+    native path, the other triangle bit for bit unchanged."""
+    prev = blx.set_dgemm_mode(blx.MODE_NATIVE)
+    try:
+        N, K = 1900, 700
+        A = oracle.uniform((N, K), np.float32, 31)
+        C0 = oracle.uniform((N, N), np.float32, 32)
+        C = C0.copy(order="F")
+        blx.cblas_ssyrk(ORDER_COL, 121, 111, N, K, 0.5, A, N, 2.0, C, N)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        m = oracle.tri_mask("U", N)
+        np.testing.assert_array_equal(C[~m], C0[~m])
+        rng = np.random.default_rng(10)
+        ii = rng.integers(0, N, 4000); jj = rng.integers(0, N, 4000)
+        keep = ii <= jj
+        ii, jj = ii[keep], jj[keep]
+        val, bound = oracle.dd_entries("N", "T", N, N, K, 0.5, A, N, A, N, 2.0, C0, N, ii, jj)
+        ratio, _ = oracle.componentwise_ratio(C, ii, jj, val, bound, K, np.float32)
+        assert ratio <= 1.0
+    finally:
+        blx.set_dgemm_mode(prev)
