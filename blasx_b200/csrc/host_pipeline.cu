@@ -50,7 +50,7 @@ struct Events {
 struct DeviceOps {
     void *A = nullptr, *B = nullptr, *C = nullptr, *ws = nullptr;
     void *C0 = nullptr;  // input C, when the emulated path accumulates K-blocks into C
-    void *diag = nullptr;  // diagonal blocks of a triangular operand (tri_split)
+    void *diag = nullptr;  // TRMM: one completed diagonal block
     bool b_is_a = false;  // B is the same host buffer as A (SYRK): one device copy
     int64_t lda = 0, ldb = 0, ldc = 0;
     cudaStream_t s = nullptr;
@@ -122,79 +122,14 @@ int panel_count(const Gemm &g) {
     return int(std::max<int64_t>(1, std::min<int64_t>(16, g.N / 1024)));
 }
 
-// ---- operands stored as one triangle (SYMM, HEMM, TRMM) ---------------------
+// ---- operands stored as one triangle (SYMM, HEMM) ---------------------------
 // Gemm::a_form / b_form name the stored triangle of a square operand. Its
 // device copy lands whole; complete_forms then fills in the rest in place
-// (mirror, conjugate mirror, or zeros and a unit diagonal) before any GEMM
-// reads it.
+// (mirror or conjugate mirror) before any GEMM reads it.
 
-// Width of the diagonal blocks a triangular operand keeps on the native path
-// when the rest of the product is emulated.
-constexpr int kTriDiagBlock = 256;
-
-bool tri_form(int f) { return f >= kTriUpper; }
-
-// Triangular operand on the emulated path (tri_split): the diagonal blocks of
-// the completed triangle move to d.diag and are zeroed in place, the emulated
-// GEMM runs on the block-off-diagonal part, and tri_diag_panel adds the
-// diagonal blocks with the native kernel (beta 1), panel by panel. Every
-// emulated sum then spans at least kTriDiagBlock dense terms or none: the tip
-// of the triangle (a single nonzero per row or column, where a per-row scaled
-// emulation loses relative accuracy) is computed natively. The native share
-// of the work is about kTriDiagBlock / K. A triangle within one block runs on
-// the native path whole.
 int complete_forms(const Gemm &g, const DeviceOps &d, cudaStream_t s) {
     BX_TRY(launch_complete_operand(g.dt, g.a_form, d.A, d.lda, g.rows_a(), s));
-    BX_TRY(launch_complete_operand(g.dt, g.b_form, d.B, d.ldb, g.rows_b(), s));
-    if (d.diag) {
-        const bool on_a = tri_form(g.a_form);
-        BX_TRY(launch_split_diag_blocks(g.dt, on_a ? d.A : d.B, on_a ? d.lda : d.ldb, g.K, kTriDiagBlock, d.diag,
-                                        s));
-    }
-    return BLASX_OK;
-}
-
-// C(:, j0:j1) += alpha x (the diagonal-block part of the product) for a
-// tri_split GEMM dg on device operands (its triangle's blocks in diag).
-int tri_diag_panel(const Gemm &dg, bool tri_is_a, const void *diag, int64_t j0, int64_t j1, cudaStream_t s) {
-    const size_t es = elem_size(dg.dt);
-    const int64_t n = dg.K, nb = kTriDiagBlock;
-    const char *D = static_cast<const char *>(diag);
-    std::vector<Gemm> blocks;
-    for (int64_t b0 = 0; b0 < n; b0 += nb) {
-        const int64_t bs = std::min(nb, n - b0);
-        Gemm b = dg;
-        b.beta = cplx{1.0, 0.0};
-        b.K = bs;
-        b.uplo = 0;
-        if (tri_is_a) {  // C(J, j0:j1) += alpha op(A)(J, J) B(J, j0:j1); tb is NoTrans
-            b.M = bs;
-            b.N = j1 - j0;
-            b.A = D + size_t(b0) * nb * es;
-            b.lda = nb;
-            b.B = static_cast<const char *>(dg.B) + size_t(b0 + j0 * dg.ldb) * es;
-            b.C = static_cast<char *>(dg.C) + size_t(b0 + j0 * dg.ldc) * es;
-        } else {  // C(:, c0:c1) += alpha A(:, J) op(B)(J, c0:c1), [c0, c1) = J and [j0, j1); ta is NoTrans
-            const int64_t c0 = std::max(b0, j0), c1 = std::min(b0 + bs, j1);
-            if (c0 >= c1) continue;
-            b.N = c1 - c0;
-            b.A = static_cast<const char *>(dg.A) + size_t(b0) * dg.lda * es;
-            // the block is stored at D columns b0 .. b0 + bs (ld nb); op(B)(J, c0:c1) is its columns
-            // c0 .. c1 (NoTrans) or its rows c0 - b0 .. c1 - b0 (Trans / ConjTrans)
-            b.B = dg.tb == NoTrans ? D + size_t(c0) * nb * es : D + size_t((c0 - b0) + b0 * nb) * es;
-            b.ldb = nb;
-            b.C = static_cast<char *>(dg.C) + size_t(c0) * dg.ldc * es;
-        }
-        blocks.push_back(b);
-    }
-    // FP64 / complex128: the blocks go out in grouped launches of the DMMA kernel
-    if (!blocks.empty() && dmma_supported(blocks[0])) {
-        for (size_t i = 0; i < blocks.size(); i += kMaxGroup)
-            BX_TRY(launch_gemm_dmma_grouped(blocks.data() + i, int(std::min<size_t>(kMaxGroup, blocks.size() - i)), s));
-        return BLASX_OK;
-    }
-    for (const Gemm &b : blocks) BX_TRY(launch_gemm_simt(b, s));
-    return BLASX_OK;
+    return launch_complete_operand(g.dt, g.b_form, d.B, d.ldb, g.rows_b(), s);
 }
 
 // ---- in-core, native kernels ----------------------------------------------
@@ -258,12 +193,10 @@ struct OzPanelCtx {
     Context *c;
     Events *ev;
     blasx_call_stats *st;
-    const Gemm *dg = nullptr;  // device operands; set with d->diag (tri_split)
 };
 
 int oz_after_panel(void *vctx, int64_t j0, int64_t j1) {
     auto *x = static_cast<OzPanelCtx *>(vctx);
-    if (x->d->diag) BX_TRY(tri_diag_panel(*x->dg, tri_form(x->g->a_form), x->d->diag, j0, j1, x->c->compute));
     if (x->g->herm_out)
         BX_TRY(launch_real_diagonal(x->g->dt, static_cast<char *>(x->d->C) + j0 * x->d->ldc * elem_size(x->g->dt),
                                     x->d->ldc, x->g->M, j1 - j0, j0 + x->g->diag, x->c->compute));
@@ -428,7 +361,7 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
     dg.C = d.C; dg.ldc = d.ldc;
     dg.a_form = dg.b_form = 0;
     BX_TRY(complete_forms(g, d, c->compute));
-    OzPanelCtx pctx{&g, &d, c, &ev, &st, &dg};
+    OzPanelCtx pctx{&g, &d, c, &ev, &st};
     PanelHooks hooks{panel_count(g), read_c ? &oz_before_reconstruct : nullptr, &oz_after_panel,
                      &pctx};
     BX_TRY(ozaki_gemm_panels(dg, c->compute, mode, d.ws, c->num_sms, hooks));
@@ -439,16 +372,22 @@ bool want_ozaki(const Gemm &g, int mode) { return ozaki_selected(g, mode); }
 
 }  // namespace
 
-// TRSM with its copies overlapped: along the top-level split of the
-// triangle, the H2D stream copies the first diagonal block of A and the
+// TRSM and TRMM with their copies overlapped. Along the top-level split of
+// the triangle the H2D stream copies the first diagonal block of A and the
 // first part of B, then the off-diagonal block and the rest of B, then the
-// second diagonal block; the compute stream solves the first part as soon
-// as its inputs landed, applies the update, and solves the second part; the
-// D2H stream returns each part of X as soon as it is final. The parts of B
-// are rows (left) or columns (right); A's off-diagonal block is op(A)[second,
-// first] (left) or op(A)[first, second] (right) as stored.
-static int trsm_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Context *c, int64_t f0, int64_t f1,
-                          int64_t s0, int64_t s1, bool *emulated, blasx_call_stats &st) {
+// second diagonal block; the compute stream starts on the first part as
+// soon as its inputs landed; the D2H stream returns each part of B as soon
+// as it is final. The parts of B are rows (left) or columns (right).
+//   solve:    solve(first, alpha); second = alpha second - op(A)[second, first] X_first;
+//             solve(second); the first part is final after its solve.
+//   multiply: multiply(first); first += alpha op(A)[first, second] B_second (the
+//             second part's original values); multiply(second); the first
+//             part is final after the update.
+// The off-diagonal block is stored as op(A)[tgt, src] (left, NoTrans) or its
+// transpose.
+static int tri_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Context *c, bool mult,
+                         const TrmmScratch &w, int64_t f0, int64_t f1, int64_t s0, int64_t s1, bool *emulated,
+                         blasx_call_stats &st) {
     const size_t es = elem_size(t.dt);
     Events ev;
     cudaEvent_t start = ev.make();
@@ -483,21 +422,34 @@ static int trsm_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Con
         BX_CUDA(cudaStreamWaitEvent(to, e, 0));
         return BLASX_OK;
     };
+    // the update writes tgt from src: the second part from the first (solve), or the reverse (multiply)
+    const int64_t t0 = mult ? f0 : s0, t1 = mult ? f1 : s1, r0 = mult ? s0 : f0, r1 = mult ? s1 : f1;
     const bool off_tgt_first = t.left == (t.trans == NoTrans);  // stored rows of the off-diagonal block
     BX_TRY(copy_a(f0, f1, f0, f1));
     BX_TRY(copy_b(f0, f1, true));
     BX_TRY(handoff(c->h2d, c->compute));
-    BX_TRY(trsm_solve_part(dt, f0, f1, t.alpha, c->compute, emulated));
-    BX_TRY(handoff(c->compute, c->d2h));
-    BX_TRY(copy_b(f0, f1, false));
-    if (off_tgt_first) BX_TRY(copy_a(s0, s1, f0, f1));
-    else BX_TRY(copy_a(f0, f1, s0, s1));
+    if (mult) {
+        BX_TRY(trmm_part(dt, f0, f1, w, c->compute, emulated));
+    } else {
+        BX_TRY(trsm_solve_part(dt, f0, f1, t.alpha, c->compute, emulated));
+        BX_TRY(handoff(c->compute, c->d2h));
+        BX_TRY(copy_b(f0, f1, false));
+    }
+    if (off_tgt_first) BX_TRY(copy_a(t0, t1, r0, r1));
+    else BX_TRY(copy_a(r0, r1, t0, t1));
     BX_TRY(copy_b(s0, s1, true));
     BX_TRY(handoff(c->h2d, c->compute));
-    BX_TRY(trsm_update_part(dt, s0, s1, f0, f1, t.alpha, c->compute, emulated));
+    if (mult) {
+        BX_TRY(trmm_update_part(dt, f0, f1, s0, s1, c->compute, emulated));
+        BX_TRY(handoff(c->compute, c->d2h));
+        BX_TRY(copy_b(f0, f1, false));
+    } else {
+        BX_TRY(trsm_update_part(dt, s0, s1, f0, f1, t.alpha, c->compute, emulated));
+    }
     BX_TRY(copy_a(s0, s1, s0, s1));
     BX_TRY(handoff(c->h2d, c->compute));
-    BX_TRY(trsm_solve_part(dt, s0, s1, cplx{1.0, 0.0}, c->compute, emulated));
+    if (mult) BX_TRY(trmm_part(dt, s0, s1, w, c->compute, emulated));
+    else BX_TRY(trsm_solve_part(dt, s0, s1, cplx{1.0, 0.0}, c->compute, emulated));
     BX_TRY(handoff(c->compute, c->d2h));
     BX_TRY(copy_b(s0, s1, false));
     BX_CUDA(cudaStreamSynchronize(c->h2d));
@@ -506,11 +458,12 @@ static int trsm_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Con
     return BLASX_OK;
 }
 
-// TRSM on host operands: A (the order-K triangle) and B to the device, the
-// recursive solve, B back; copies overlap the solve along its top-level split
-// (trsm_pipelined). In core only, like the stored-triangle operands of
-// host_gemm; the scratch of the largest update GEMM is part of the budget.
-int host_trsm(const Trsm &t) {
+// TRSM (mult false) or TRMM (mult true) on host operands: A (the order-K
+// triangle) and B to the device, the recursive solve or multiply, B back;
+// copies overlap the compute along its top-level split (tri_pipelined). In
+// core only: B is both read and written, and the scratch of the largest
+// update GEMM (and TRMM's leaf scratch) is part of the budget.
+static int host_tri(const Trsm &t, bool mult) {
     auto t0 = std::chrono::steady_clock::now();
     blasx_call_stats &st = call_stats();
     st = blasx_call_stats{};
@@ -531,33 +484,42 @@ int host_trsm(const Trsm &t) {
     dt.ldb = d.ldb;
     const size_t bytes_a = need_a ? size_t(d.lda) * K * es : 0;
     const size_t bytes_b = size_t(d.ldb) * t.N * es;
-    const Gemm top = trsm_top_update(dt);
+    const Gemm top = mult ? trmm_top_update(dt) : trsm_top_update(dt);
     const size_t bytes_ws = need_a && top.K > 0 && ozaki_selected(top, mode) ? ozaki_scratch_bytes(top) : 0;
-    if (bytes_a + bytes_b + bytes_ws > default_budget(c))
-        return set_error(BLASX_ERR_UNSUPPORTED, "triangular solve: %zu bytes exceed the HBM budget",
-                         bytes_a + bytes_b + bytes_ws);
+    TrmmScratch w = mult ? trmm_scratch_sizes(dt) : TrmmScratch{};
+    const size_t bytes_w = need_a ? w.diag_bytes + w.temp_bytes : 0;
+    if (bytes_a + bytes_b + bytes_ws + bytes_w > default_budget(c))
+        return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: %zu bytes exceed the HBM budget",
+                         mult ? "multiply" : "solve", bytes_a + bytes_b + bytes_ws + bytes_w);
     HostPin pins;
     BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
     cudaStream_t s = c->compute;
     if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, s));
     BX_CUDA(cudaMallocAsync(&d.B, bytes_b, s));  // alpha == 0 writes zeros without reading B
+    if (bytes_w) {
+        BX_CUDA(cudaMallocAsync(&d.diag, w.diag_bytes, s));
+        BX_CUDA(cudaMallocAsync(&d.C0, w.temp_bytes, s));
+        w.diag = d.diag;
+        w.temp = d.C0;
+    }
     dt.A = d.A;
     dt.B = d.B;
     bool emulated = false;
     int64_t f0, f1, s0, s1;
-    if (!need_a || !trsm_halves(dt, &f0, &f1, &s0, &s1)) {
+    const bool split = need_a && (mult ? trmm_halves(dt, &f0, &f1, &s0, &s1) : trsm_halves(dt, &f0, &f1, &s0, &s1));
+    if (!split) {
         if (need_a) {
             BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, s));
             BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, t.B, t.ldb * es, t.M * es, t.N, cudaMemcpyHostToDevice, s));
             st.h2d_bytes += double(es) * (double(K) * K + double(t.M) * t.N);
         }
-        BX_TRY(trsm_device(dt, s, &emulated));
+        BX_TRY(mult ? trmm_device(dt, w, s, &emulated) : trsm_device(dt, s, &emulated));
         BX_CUDA(cudaMemcpy2DAsync(t.B, t.ldb * es, d.B, d.ldb * es, t.M * es, t.N, cudaMemcpyDeviceToHost, s));
         st.d2h_bytes += double(es) * t.M * t.N;
         BX_CUDA(cudaStreamSynchronize(s));
     } else {
-        BX_TRY(trsm_pipelined(t, dt, d, c, f0, f1, s0, s1, &emulated, st));
+        BX_TRY(tri_pipelined(t, dt, d, c, mult, w, f0, f1, s0, s1, &emulated, st));
     }
     st.path = !need_a ? 3 : (emulated ? 2 : 1);
     if (emulated) {
@@ -569,6 +531,9 @@ int host_trsm(const Trsm &t) {
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return BLASX_OK;
 }
+
+int host_trsm(const Trsm &t) { return host_tri(t, false); }
+int host_trmm(const Trsm &t) { return host_tri(t, true); }
 
 int host_gemm(const Gemm &g) {
     auto t0 = std::chrono::steady_clock::now();
@@ -584,10 +549,7 @@ int host_gemm(const Gemm &g) {
     const bool read_c = !g.beta_zero() || g.uplo != 0;
     const int mode = config().dgemm_mode.load();
     const bool formed = g.a_form || g.b_form;
-    bool oz = need_ab && want_ozaki(g, mode);
-    // a triangle within one diagonal block runs natively whole (see tri_split)
-    if (oz && (tri_form(g.a_form) || tri_form(g.b_form)) && g.K <= kTriDiagBlock) oz = false;
-    const bool tri_split = oz && (tri_form(g.a_form) || tri_form(g.b_form));
+    const bool oz = need_ab && want_ozaki(g, mode);
 
     DeviceOps d;
     d.s = c->compute;
@@ -604,16 +566,12 @@ int host_gemm(const Gemm &g) {
     probe.a_form = probe.b_form = 0;
     const size_t bytes_ws = oz ? ozaki_scratch_bytes(probe) : 0;
     const size_t bytes_c0 = (oz && read_c && kblock_count(g) > 1 && !formed) ? bytes_c : 0;
-    const size_t bytes_diag = tri_split ? size_t(kTriDiagBlock) * g.K * es : 0;
     const size_t budget = default_budget(c);
 
     HostPin pins;
-    const size_t total = bytes_a + bytes_b + bytes_c + bytes_c0 + bytes_ws + bytes_diag;
-    // out of core, a symmetric / Hermitian operand is read tile by tile from its
-    // stored triangle; a triangular one (TRMM, whose result overwrites the B it
-    // reads) stays in core
-    if (total > budget && need_ab && (tri_form(g.a_form) || tri_form(g.b_form)))
-        return set_error(BLASX_ERR_UNSUPPORTED, "triangular operand: %zu bytes exceed the HBM budget", total);
+    const size_t total = bytes_a + bytes_b + bytes_c + bytes_c0 + bytes_ws;
+    // out of core, a symmetric / Hermitian operand (SYMM, HEMM) is read tile by
+    // tile from its stored triangle (tiled_host_gemm)
     if (total > budget && need_ab) {
         // out-of-core: HBM tile cache under the byte budget; each K-step on
         // the emulated path when the precision mode picks it for a step's shape
@@ -640,7 +598,6 @@ int host_gemm(const Gemm &g) {
     BX_CUDA(cudaMallocAsync(&d.C, bytes_c, c->compute));
     if (oz) BX_CUDA(cudaMallocAsync(&d.ws, bytes_ws, c->compute));
     if (bytes_c0) BX_CUDA(cudaMallocAsync(&d.C0, bytes_c0, c->compute));
-    if (bytes_diag) BX_CUDA(cudaMallocAsync(&d.diag, bytes_diag, c->compute));
     const int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
                       : incore_native(g, c, d, need_ab, read_c, st);
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -14,5 +14,8 @@ int host_gemm(const Gemm &g);
 // holds the solution on return. In core only (BLASX_ERR_UNSUPPORTED beyond
 // the HBM budget, B unchanged).
 int host_trsm(const Trsm &t);
+// Triangular multiply (TRMM: B = alpha op(A) B or alpha B op(A), described by
+// a Trsm), host pointers, synchronous, in core only like host_trsm.
+int host_trmm(const Trsm &t);
 
 }  // namespace bx

@@ -17,9 +17,6 @@ int launch_complete_operand(DType dt, int form, void *X, int64_t ldx, int64_t n,
 // Zeroes the imaginary parts of the entries (r, c) of the m x n device block
 // C (ld ldc) with r - c == off; nothing for real types.
 int launch_real_diagonal(DType dt, void *C, int64_t ldc, int64_t m, int64_t n, int64_t off, cudaStream_t s);
-// Moves the nb x nb diagonal blocks of the n x n device matrix X into D
-// (ld nb, n columns: block J in columns J nb ..) and zeroes them in X.
-int launch_split_diag_blocks(DType dt, void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s);
 // g.C (g.M x g.N, ld g.ldc) += g.beta * X (ld ldx); nothing when beta == 0.
 int launch_add_scaled(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s);
 
@@ -59,6 +56,24 @@ Gemm trsm_top_update(const Trsm &t);
 // the right-side mirror). Together: solve(first, alpha), update(second, first,
 // alpha), solve(second, 1) is trsm_device.
 bool trsm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi);
+// TRMM (a Trsm describes it: B = alpha op(A) B or alpha B op(A), in place):
+// recursive halving into GEMM updates plus leaves of at most 256 rows that
+// multiply by their completed diagonal block on the native kernels. Its
+// scratch: one diagonal block and one leaf's vectors.
+struct TrmmScratch {
+    void *diag = nullptr, *temp = nullptr;
+    int64_t ldt = 0;
+    size_t diag_bytes = 0, temp_bytes = 0;
+};
+TrmmScratch trmm_scratch_sizes(const Trsm &t);
+int trmm_device(const Trsm &t, const TrmmScratch &w, cudaStream_t s, bool *emulated);
+// The top-level split of trmm_device: multiply first, update first from
+// second (with second's original values), multiply second.
+bool trmm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi);
+int trmm_part(const Trsm &t, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s, bool *emulated);
+int trmm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cudaStream_t s,
+                     bool *emulated);
+Gemm trmm_top_update(const Trsm &t);
 int trsm_solve_part(const Trsm &t, int64_t lo, int64_t hi, cplx scale, cudaStream_t s, bool *emulated);
 int trsm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cplx scale,
                      cudaStream_t s, bool *emulated);

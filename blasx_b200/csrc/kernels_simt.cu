@@ -164,31 +164,6 @@ template <typename T> int launch_complete_t(int form, void *X, int64_t ldx, int6
     return BLASX_OK;
 }
 
-// Moves the nb x nb diagonal blocks of the n x n matrix X (the last one
-// ragged) into D (column-major, ld nb: block J in columns J nb .. J nb + bs)
-// and zeroes them in X. One thread per entry of column j = blockIdx.y (grid-
-// strided); each entry is read and written by that thread only. T is an
-// opaque element of the right size.
-template <typename T>
-__global__ void split_diag_blocks_kernel(T *__restrict__ X, int64_t ldx, int n, int nb, T *__restrict__ D) {
-    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
-        const int64_t r0 = (j / nb) * nb;
-        const int64_t r1 = r0 + nb < n ? r0 + nb : n;
-        for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-            D[(i - r0) + j * nb] = X[i + j * ldx];
-            X[i + j * ldx] = T{};
-        }
-    }
-}
-
-template <typename T> int launch_split_t(void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s) {
-    dim3 grid(1, unsigned(std::min<int64_t>(n, 65535)));
-    split_diag_blocks_kernel<T><<<grid, 256, 0, s>>>(static_cast<T *>(X), ldx, int(n), nb, static_cast<T *>(D));
-    BX_CUDA(cudaGetLastError());
-    count_launch();
-    return BLASX_OK;
-}
-
 template <typename T> int launch_simt_t(const Gemm &g, cudaStream_t s) {
     dim3 grid(unsigned((g.M + BM - 1) / BM), unsigned((g.N + BN - 1) / BN));
     if (grid.y > 65535) return set_error(BLASX_ERR_UNSUPPORTED, "N too large for SIMT grid");
@@ -255,15 +230,6 @@ int launch_real_diagonal(DType dt, void *C, int64_t ldc, int64_t m, int64_t n, i
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;
-}
-
-int launch_split_diag_blocks(DType dt, void *X, int64_t ldx, int64_t n, int nb, void *D, cudaStream_t s) {
-    if (n <= 0) return BLASX_OK;
-    switch (elem_size(dt)) {
-        case 4: return launch_split_t<uint32_t>(X, ldx, n, nb, D, s);
-        case 8: return launch_split_t<uint64_t>(X, ldx, n, nb, D, s);
-        default: return launch_split_t<uint4>(X, ldx, n, nb, D, s);
-    }
 }
 
 int launch_add_scaled(const Gemm &g, const void *X, int64_t ldx, cudaStream_t s) {

@@ -27,9 +27,10 @@ struct cplx {
 
 enum Trans : int { NoTrans = 111, TransT = 112, ConjT = 113 };
 
-// How a square operand is stored (SYMM / HEMM / TRMM): the named triangle
-// holds the data; the rest is implied (mirrored, conjugate-mirrored, or zero
-// with a stored or unit diagonal).
+// How a square operand is stored: the named triangle holds the data, the rest
+// is implied (mirrored, conjugate-mirrored, or zero with a stored or unit
+// diagonal). SYMM / HEMM operands use the first four, TRMM's diagonal blocks
+// the triangular ones.
 enum OperandForm : int {
     kGeneral = 0,
     kSymUpper, kSymLower,          // X = X^T
@@ -65,7 +66,7 @@ struct Gemm {
     int uplo = 0;
     int64_t diag = 0;
     // Stored form of a square A (or B): only one triangle holds data, and the
-    // operand is completed on the device before the product (SYMM, HEMM, TRMM).
+    // operand is completed on the device before the product (SYMM, HEMM).
     int a_form = 0, b_form = 0;  // an OperandForm
     // Hermitian output (HERK, HER2K): the imaginary parts of C's diagonal
     // entries (row == col, shifted by diag like uplo) are set to zero once
@@ -90,9 +91,10 @@ struct Gemm {
 };
 
 // One triangular solve with many right-hand sides, column-major: op(A) X =
-// alpha B (left) or X op(A) = alpha B (right), X overwriting B (M x N). A is
-// the order-K triangle (K = M left, N right); only its `lower` (or upper)
-// triangle is read, and not its diagonal when `unit`.
+// alpha B (left) or X op(A) = alpha B (right), X overwriting B (M x N); the
+// same fields describe a triangular multiply (TRMM), B = alpha op(A) B or
+// alpha B op(A). A is the order-K triangle (K = M left, N right); only its
+// `lower` (or upper) triangle is read, and not its diagonal when `unit`.
 struct Trsm {
     DType dt;
     bool left, lower, unit;

@@ -3,15 +3,16 @@
 //
 // The reference declares these but always runs them on its host BLAS (for
 // instance blas/dsymm.c:44-57 and blas/dtrmm.c:49-60 select the CPU in every
-// branch of their dispatchers). Here each one is a GEMM whose square operand
-// is stored as one triangle: the host path copies it to the device, completes
-// it there from its stored triangle (mirror for SYMM, conjugate mirror for
-// HEMM, zeros and an optional unit diagonal for TRMM), and runs the product on
-// the native or emulated path like any GEMM.
+// branch of their dispatchers). Here:
 //   SYMM / HEMM  C = alpha A B + beta C (side Left, A is M x M) or
-//                C = alpha B A + beta C (side Right, A is N x N)
-//   TRMM         B = alpha op(A) B (Left) or alpha B op(A) (Right); B is read
-//                whole before the result is written back into it.
+//                C = alpha B A + beta C (side Right, A is N x N): a GEMM
+//                whose square operand is stored as one triangle; the host
+//                path completes it on the device (mirror, or conjugate
+//                mirror) and runs the product on the native or emulated path
+//                like any GEMM, in or out of core.
+//   TRMM         B = alpha op(A) B (Left) or alpha B op(A) (Right), in place
+//                (trsm.cu: recursive halving into GEMM updates and leaves
+//                that multiply by their completed diagonal block).
 //   TRSM         solves op(A) X = alpha B (Left) or X op(A) = alpha B (Right)
 //                for X, which overwrites B (trsm.cu: recursive halving into
 //                GEMM updates and a substitution kernel).
@@ -101,27 +102,17 @@ void trmm_col(const char *name, DType dt, int side, int uplo, int trans, int dia
     else if (ldb < mx1(M)) info = 11;
     if (info) return report(name, info);
     if (M == 0 || N == 0) return;
-    if (!is_complex(dt) && trans == ConjT) trans = TransT;
-    const bool unit = diag == CblasUnit;
-    const int form = uplo == CblasUpper ? (unit ? kTriUpperUnit : kTriUpper)
-                                        : (unit ? kTriLowerUnit : kTriLower);
-    Gemm g;
-    g.dt = dt;
-    g.M = M; g.N = N;
-    if (side == CblasLeft) {  // B = alpha op(A) B
-        g.K = M;
-        g.ta = trans; g.tb = NoTrans;
-        g.A = A; g.lda = lda; g.B = B; g.ldb = ldb;
-        g.a_form = form;
-    } else {  // B = alpha B op(A)
-        g.K = N;
-        g.ta = NoTrans; g.tb = trans;
-        g.A = B; g.lda = ldb; g.B = A; g.ldb = lda;
-        g.b_form = form;
-    }
-    g.alpha = alpha; g.beta = cplx{0.0, 0.0};
-    g.C = B; g.ldc = ldb;
-    host_gemm(g);
+    Trsm t;
+    t.dt = dt;
+    t.left = side == CblasLeft;
+    t.lower = uplo == CblasLower;
+    t.unit = diag == CblasUnit;
+    t.trans = (!is_complex(dt) && trans == ConjT) ? TransT : trans;
+    t.M = M; t.N = N;
+    t.alpha = alpha;
+    t.A = A; t.lda = lda;
+    t.B = B; t.ldb = ldb;
+    host_trmm(t);
 }
 
 void trmm_entry(const char *name, DType dt, int order, int side, int uplo, int trans, int diag, int M,

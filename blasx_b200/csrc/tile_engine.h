@@ -25,7 +25,7 @@ size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es);
 // on a scratch of ws_bytes carved from the same budget; otherwise on the
 // native kernels. A symmetric or Hermitian operand stored as one triangle
 // (Gemm::a_form / b_form of SYMM, HEMM) is read from its stored triangle tile
-// by tile; triangular forms are not supported here.
+// by tile.
 int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int tile, int policy,
                     size_t ws_bytes = 0, int mode = 0);
 

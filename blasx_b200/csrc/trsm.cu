@@ -1,5 +1,5 @@
-// trsm.cu -- triangular solve with many right-hand sides on device operands
-// (the compute of cblas_?trsm).
+// trsm.cu -- triangular solve (cblas_?trsm) and triangular multiply
+// (cblas_?trmm) with many right-hand sides on device operands.
 //
 // op(A) X = alpha B (left) or X op(A) = alpha B (right) is solved by
 // recursive halving of the order-K triangle: solve the first half, update
@@ -228,17 +228,17 @@ void split(const Trsm &t, Range r, Range *first, Range *second) {
     }
 }
 
-// B[tgt] = scale B[tgt] - op(A)[tgt, src] X[src] (left) or
-// B[:, tgt] = scale B[:, tgt] - X[:, src] op(A)[src, tgt] (right).
-Gemm update_gemm(const Trsm &t, Range tgt, Range src, cplx scale) {
+// B[tgt] = beta B[tgt] + alpha op(A)[tgt, src] B[src] (left) or
+// B[:, tgt] = beta B[:, tgt] + alpha B[:, src] op(A)[src, tgt] (right).
+Gemm update_gemm(const Trsm &t, Range tgt, Range src, cplx alpha, cplx beta) {
     const size_t es = elem_size(t.dt);
     const char *A = static_cast<const char *>(t.A);
     char *B = static_cast<char *>(t.B);
     const int tr = (t.trans == ConjT && !is_complex(t.dt)) ? TransT : t.trans;
     Gemm g;
     g.dt = t.dt;
-    g.alpha = cplx{-1.0, 0.0};
-    g.beta = scale;
+    g.alpha = alpha;
+    g.beta = beta;
     g.K = src.size();
     if (t.left) {
         g.M = tgt.size();
@@ -265,14 +265,81 @@ Gemm update_gemm(const Trsm &t, Range tgt, Range src, cplx scale) {
     return g;
 }
 
+constexpr cplx kMinusOne{-1.0, 0.0}, kOne{1.0, 0.0};
+
 int solve(const Trsm &t, Range r, cplx scale, cudaStream_t s, bool *emulated) {
     if (r.size() <= leaf_order(t.dt)) return launch_leaf(t, r.lo, r.hi, scale, s_trans_of(t), forward_of(t), s);
     Range first, second;
     split(t, r, &first, &second);
     BX_TRY(solve(t, first, scale, s, emulated));
-    BX_TRY(device_gemm(update_gemm(t, second, first, scale), s));
+    BX_TRY(device_gemm(update_gemm(t, second, first, kMinusOne, scale), s));
     if (call_stats().path == 2) *emulated = true;
     return solve(t, second, cplx{1.0, 0.0}, s, emulated);
+}
+
+// ---- TRMM: B = alpha op(A) B or alpha B op(A), in place -------------------
+// With the vectors of B (columns for a left multiply, rows for a right one)
+// the product is v <- alpha S v, S = op(A) or op(A)^T as for the solve. It
+// recurses over halves P (earlier rows of S) and Q: for S lower,
+// v_Q <- alpha S_QQ v_Q + alpha S_QP v_P needs the original v_P, so Q goes
+// first (its multiply, then one GEMM update from P), then P; for S upper,
+// P goes first. Every GEMM reads op(A) in an off-diagonal rectangle inside
+// the stored triangle. A leaf of at most kTrmmLeaf rows multiplies by its
+// diagonal block, completed (zeros, unit diagonal) in a scratch copy, on
+// the native kernels: the emulated path never sees a triangle's tip, whose
+// single nonzero per row would lose accuracy under per-row scaling.
+constexpr int kTrmmLeaf = 256;
+
+void trmm_split(const Trsm &t, Range r, Range *first, Range *second) {
+    const int64_t n = r.size();
+    const int64_t half = std::min(n - 1, (n / 2 + kTrmmLeaf - 1) / kTrmmLeaf * kTrmmLeaf);
+    const Range lo{r.lo, r.lo + half}, hi{r.lo + half, r.hi};
+    *first = forward_of(t) ? hi : lo;
+    *second = forward_of(t) ? lo : hi;
+}
+
+int trmm_leaf(const Trsm &t, Range r, const TrmmScratch &w, cudaStream_t s) {
+    const size_t es = elem_size(t.dt);
+    const int64_t bs = r.size();
+    const char *A = static_cast<const char *>(t.A);
+    char *B = static_cast<char *>(t.B);
+    BX_CUDA(cudaMemcpy2DAsync(w.diag, size_t(kTrmmLeaf) * es, A + (r.lo + r.lo * t.lda) * es, size_t(t.lda) * es,
+                              size_t(bs) * es, size_t(bs), cudaMemcpyDeviceToDevice, s));
+    const int form = t.lower ? (t.unit ? kTriLowerUnit : kTriLower) : (t.unit ? kTriUpperUnit : kTriUpper);
+    BX_TRY(launch_complete_operand(t.dt, form, w.diag, kTrmmLeaf, bs, s));
+    const int tr = (t.trans == ConjT && !is_complex(t.dt)) ? TransT : t.trans;
+    Gemm g;
+    g.dt = t.dt;
+    g.alpha = t.alpha;
+    g.beta = cplx{0.0, 0.0};
+    g.K = bs;
+    if (t.left) {  // rows r of B: B_r = alpha op(A_rr) B_r
+        BX_CUDA(cudaMemcpy2DAsync(w.temp, size_t(w.ldt) * es, B + r.lo * es, size_t(t.ldb) * es, size_t(bs) * es,
+                                  size_t(t.N), cudaMemcpyDeviceToDevice, s));
+        g.M = bs; g.N = t.N;
+        g.ta = tr; g.A = w.diag; g.lda = kTrmmLeaf;
+        g.tb = NoTrans; g.B = w.temp; g.ldb = w.ldt;
+        g.C = B + r.lo * es;
+    } else {  // columns r of B: B_r = alpha B_r op(A_rr)
+        BX_CUDA(cudaMemcpy2DAsync(w.temp, size_t(w.ldt) * es, B + r.lo * t.ldb * es, size_t(t.ldb) * es,
+                                  size_t(t.M) * es, size_t(bs), cudaMemcpyDeviceToDevice, s));
+        g.M = t.M; g.N = bs;
+        g.ta = NoTrans; g.A = w.temp; g.lda = w.ldt;
+        g.tb = tr; g.B = w.diag; g.ldb = kTrmmLeaf;
+        g.C = B + r.lo * t.ldb * es;
+    }
+    g.ldc = t.ldb;
+    return dmma_supported(g) ? launch_gemm_dmma(g, s) : launch_gemm_simt(g, s);
+}
+
+int multiply(const Trsm &t, Range r, const TrmmScratch &w, cudaStream_t s, bool *emulated) {
+    if (r.size() <= kTrmmLeaf) return trmm_leaf(t, r, w, s);
+    Range first, second;
+    trmm_split(t, r, &first, &second);
+    BX_TRY(multiply(t, first, w, s, emulated));
+    BX_TRY(device_gemm(update_gemm(t, first, second, t.alpha, kOne), s));
+    if (call_stats().path == 2) *emulated = true;
+    return multiply(t, second, w, s, emulated);
 }
 
 }  // namespace
@@ -293,7 +360,7 @@ int trsm_solve_part(const Trsm &t, int64_t lo, int64_t hi, cplx scale, cudaStrea
 
 int trsm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cplx scale,
                      cudaStream_t s, bool *emulated) {
-    BX_TRY(device_gemm(update_gemm(t, Range{tgt_lo, tgt_hi}, Range{src_lo, src_hi}, scale), s));
+    BX_TRY(device_gemm(update_gemm(t, Range{tgt_lo, tgt_hi}, Range{src_lo, src_hi}, kMinusOne, scale), s));
     if (call_stats().path == 2) *emulated = true;
     return BLASX_OK;
 }
@@ -301,13 +368,13 @@ int trsm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_
 Gemm trsm_top_update(const Trsm &t) {
     const Range all{0, t.order()};
     if (all.size() <= leaf_order(t.dt)) {
-        Gemm g = update_gemm(t, all, all, t.alpha);
+        Gemm g = update_gemm(t, all, all, kMinusOne, t.alpha);
         g.K = 0;
         return g;
     }
     Range first, second;
     split(t, all, &first, &second);
-    return update_gemm(t, second, first, t.alpha);
+    return update_gemm(t, second, first, kMinusOne, t.alpha);
 }
 
 int trsm_device(const Trsm &t, cudaStream_t s, bool *emulated) {
@@ -324,6 +391,68 @@ int trsm_device(const Trsm &t, cudaStream_t s, bool *emulated) {
         return launch_scale(z, s);
     }
     return solve(t, Range{0, t.order()}, t.alpha, s, emulated);
+}
+
+}  // namespace bx
+
+namespace bx {
+
+TrmmScratch trmm_scratch_sizes(const Trsm &t) {
+    TrmmScratch w;
+    const size_t es = elem_size(t.dt);
+    w.ldt = t.left ? kTrmmLeaf : (t.M + 31) / 32 * 32;
+    w.diag_bytes = size_t(kTrmmLeaf) * kTrmmLeaf * es;
+    w.temp_bytes = size_t(w.ldt) * size_t(t.left ? t.N : kTrmmLeaf) * es;
+    return w;
+}
+
+bool trmm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi) {
+    const Range all{0, t.order()};
+    if (all.size() <= kTrmmLeaf) return false;
+    Range first, second;
+    trmm_split(t, all, &first, &second);
+    *first_lo = first.lo; *first_hi = first.hi;
+    *second_lo = second.lo; *second_hi = second.hi;
+    return true;
+}
+
+int trmm_part(const Trsm &t, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s, bool *emulated) {
+    return multiply(t, Range{lo, hi}, w, s, emulated);
+}
+
+int trmm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cudaStream_t s,
+                     bool *emulated) {
+    BX_TRY(device_gemm(update_gemm(t, Range{tgt_lo, tgt_hi}, Range{src_lo, src_hi}, t.alpha, kOne), s));
+    if (call_stats().path == 2) *emulated = true;
+    return BLASX_OK;
+}
+
+Gemm trmm_top_update(const Trsm &t) {
+    const Range all{0, t.order()};
+    if (all.size() <= kTrmmLeaf) {
+        Gemm g = update_gemm(t, all, all, t.alpha, kOne);
+        g.K = 0;
+        return g;
+    }
+    Range first, second;
+    trmm_split(t, all, &first, &second);
+    return update_gemm(t, first, second, t.alpha, kOne);
+}
+
+int trmm_device(const Trsm &t, const TrmmScratch &w, cudaStream_t s, bool *emulated) {
+    *emulated = false;
+    if (t.M == 0 || t.N == 0) return BLASX_OK;
+    if (t.alpha.re == 0 && t.alpha.im == 0) {  // B = 0; A is not read
+        Gemm z;
+        z.dt = t.dt;
+        z.ta = z.tb = NoTrans;
+        z.M = t.M; z.N = t.N; z.K = 0;
+        z.alpha = cplx{0.0, 0.0}; z.beta = cplx{0.0, 0.0};
+        z.A = nullptr; z.lda = 1; z.B = nullptr; z.ldb = 1;
+        z.C = t.B; z.ldc = t.ldb;
+        return launch_scale(z, s);
+    }
+    return multiply(t, Range{0, t.order()}, w, s, emulated);
 }
 
 }  // namespace bx
