@@ -458,11 +458,115 @@ static int tri_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Cont
     return BLASX_OK;
 }
 
+// TRSM / TRMM whose B does not fit the HBM budget beside A: the vectors of B
+// (columns for a left solve or multiply, rows for a right one) are
+// independent, so B streams through two device panels while A stays
+// resident. Panel p + 1 is copied in while panel p computes, and each panel
+// goes back as soon as it is done; a panel buffer is refilled only after its
+// previous contents left. The panel width is the largest that fits (at least
+// 256 vectors); A itself must fit.
+static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t budget, blasx_call_stats &st) {
+    const size_t es = elem_size(t.dt);
+    const int64_t K = t.order(), nvec = t.left ? t.N : t.M;
+    const int64_t lda = round_up(K, 32);
+    const bool need_a = !(t.alpha.re == 0 && t.alpha.im == 0);  // alpha == 0: B = 0, A and B not read
+    const size_t bytes_a = need_a ? size_t(lda) * K * es : 0;
+    // device extent of a panel of w vectors: K x w (left, ld K) or w x K (right, ld w)
+    auto panel_desc = [&](int64_t wv) {
+        Trsm p = t;
+        p.lda = lda;
+        if (t.left) { p.N = wv; p.ldb = round_up(K, 32); }
+        else { p.M = wv; p.ldb = round_up(wv, 32); }
+        return p;
+    };
+    auto need = [&](int64_t wv) {
+        const Trsm p = panel_desc(wv);
+        const Gemm top = mult ? trmm_top_update(p) : trsm_top_update(p);
+        const size_t ws = top.K > 0 && ozaki_selected(top, mode) ? ozaki_scratch_bytes(top) : 0;
+        const TrmmScratch w = mult ? trmm_scratch_sizes(p) : TrmmScratch{};
+        const size_t panel = size_t(p.ldb) * size_t(t.left ? wv : K) * es;
+        return bytes_a + 2 * panel + ws + w.diag_bytes + w.temp_bytes;
+    };
+    int64_t wv = nvec;
+    while (wv > 256 && need(wv) > budget) wv = (wv / 2 + 31) / 32 * 32;
+    if (wv >= nvec || need(wv) > budget)
+        return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: A (%zu bytes) leaves no room for panels of B in "
+                         "the HBM budget", mult ? "multiply" : "solve", bytes_a);
+    const Trsm full = panel_desc(wv);
+    const size_t panel_bytes = size_t(full.ldb) * size_t(t.left ? wv : K) * es;
+    TrmmScratch w = mult ? trmm_scratch_sizes(full) : TrmmScratch{};
+    HostPin pins;
+    BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
+    BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
+    DeviceOps d;
+    d.s = c->compute;
+    if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, c->compute));
+    BX_CUDA(cudaMallocAsync(&d.B, 2 * panel_bytes, c->compute));
+    if (mult && need_a) {
+        BX_CUDA(cudaMallocAsync(&d.diag, w.diag_bytes, c->compute));
+        BX_CUDA(cudaMallocAsync(&d.C0, w.temp_bytes, c->compute));
+        w.diag = d.diag;
+        w.temp = d.C0;
+    }
+    Events ev;
+    auto handoff = [&](cudaStream_t from, cudaStream_t to) -> int {
+        cudaEvent_t e = ev.make();
+        BX_CUDA(cudaEventRecord(e, from));
+        BX_CUDA(cudaStreamWaitEvent(to, e, 0));
+        return BLASX_OK;
+    };
+    BX_TRY(handoff(c->compute, c->h2d));  // the buffers are allocated on compute
+    if (need_a) {
+        BX_CUDA(cudaMemcpy2DAsync(d.A, lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, c->h2d));
+        st.h2d_bytes += double(es) * K * K;
+    }
+    cudaEvent_t out_done[2] = {nullptr, nullptr};
+    bool emulated = false;
+    for (int64_t v0 = 0, p = 0; v0 < nvec; v0 += wv, ++p) {
+        const int64_t v1 = std::min(nvec, v0 + wv), n = v1 - v0;
+        const int buf = int(p & 1);
+        Trsm tp = panel_desc(n);
+        tp.A = d.A;
+        tp.B = static_cast<char *>(d.B) + buf * panel_bytes;
+        tp.ldb = full.ldb;
+        char *host = static_cast<char *>(t.B) + (t.left ? v0 * t.ldb : v0) * int64_t(es);
+        const int64_t rows = t.left ? t.M : n, cols = t.left ? n : t.N;
+        if (out_done[buf]) BX_CUDA(cudaStreamWaitEvent(c->h2d, out_done[buf], 0));
+        if (need_a) {
+            BX_CUDA(cudaMemcpy2DAsync(tp.B, tp.ldb * es, host, t.ldb * es, rows * es, cols, cudaMemcpyHostToDevice,
+                                      c->h2d));
+            st.h2d_bytes += double(es) * rows * cols;
+        }
+        BX_TRY(handoff(c->h2d, c->compute));
+        bool e = false;
+        BX_TRY(mult ? trmm_device(tp, w, c->compute, &e) : trsm_device(tp, c->compute, &e));
+        emulated |= e;
+        BX_TRY(handoff(c->compute, c->d2h));
+        BX_CUDA(cudaMemcpy2DAsync(host, t.ldb * es, tp.B, tp.ldb * es, rows * es, cols, cudaMemcpyDeviceToHost,
+                                  c->d2h));
+        st.d2h_bytes += double(es) * rows * cols;
+        if (!out_done[buf]) out_done[buf] = ev.make();
+        BX_CUDA(cudaEventRecord(out_done[buf], c->d2h));
+    }
+    BX_CUDA(cudaStreamSynchronize(c->h2d));
+    BX_CUDA(cudaStreamSynchronize(c->compute));
+    BX_CUDA(cudaStreamSynchronize(c->d2h));
+    st.path = !need_a ? 3 : (emulated ? 2 : 1);
+    st.tile = int(wv);  // the panel width, in vectors
+    if (emulated) {
+        resolve_decision(st);
+        if (*c->last_error_flag)
+            return set_error(BLASX_ERR_TIMEOUT, "emulated GEMM: bounded device wait expired (flag %d)",
+                             *c->last_error_flag);
+    }
+    return BLASX_OK;
+}
+
 // TRSM (mult false) or TRMM (mult true) on host operands: A (the order-K
 // triangle) and B to the device, the recursive solve or multiply, B back;
-// copies overlap the compute along its top-level split (tri_pipelined). In
-// core only: B is both read and written, and the scratch of the largest
-// update GEMM (and TRMM's leaf scratch) is part of the budget.
+// copies overlap the compute along its top-level split (tri_pipelined). The
+// scratch of the largest update GEMM (and TRMM's leaf scratch) is part of
+// the budget; a B beyond it streams in panels (tri_panels).
 static int host_tri(const Trsm &t, bool mult) {
     auto t0 = std::chrono::steady_clock::now();
     blasx_call_stats &st = call_stats();
@@ -488,9 +592,12 @@ static int host_tri(const Trsm &t, bool mult) {
     const size_t bytes_ws = need_a && top.K > 0 && ozaki_selected(top, mode) ? ozaki_scratch_bytes(top) : 0;
     TrmmScratch w = mult ? trmm_scratch_sizes(dt) : TrmmScratch{};
     const size_t bytes_w = need_a ? w.diag_bytes + w.temp_bytes : 0;
-    if (bytes_a + bytes_b + bytes_ws + bytes_w > default_budget(c))
-        return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: %zu bytes exceed the HBM budget",
-                         mult ? "multiply" : "solve", bytes_a + bytes_b + bytes_ws + bytes_w);
+    const size_t budget = default_budget(c);
+    if (bytes_a + bytes_b + bytes_ws + bytes_w > budget) {
+        const int rc = tri_panels(t, c, mult, mode, budget, st);
+        st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
+    }
     HostPin pins;
     BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));

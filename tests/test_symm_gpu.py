@@ -328,14 +328,65 @@ def test_symm_out_of_core(blx, side, uplo, dt, herm, emulated):
         blx.set_dgemm_mode(prev)
 
 
-def test_trmm_over_the_budget_fails_loudly(blx):
-    """TRMM writes its result into the B it reads, so it stays in core: a
-    problem beyond the budget is reported and B is left unchanged."""
-    blx.set_hbm_budget(8 << 20)
+@pytest.mark.parametrize("emulated", [False, True])
+def test_trsm_streams_b_beyond_the_budget(blx, emulated):
+    """B (74 MB) does not fit a 48 MiB budget beside A (8 MB): its columns
+    stream through two device panels while A stays resident; the residual
+    of every panel is within the backward-error bound."""
+    blx.set_hbm_budget(48 << 20)
+    prev = blx.set_dgemm_mode(blx.MODE_OZAKI if emulated else blx.MODE_NATIVE)
     try:
-        M = N = 1024
-        A = oracle.uniform((M, M), np.float64, 91)
-        B0 = oracle.uniform((M, N), np.float64, 92)
+        M, N = 1024, 9000
+        A = dominant_triangle(np.float64, M, "L", "N", 71)
+        B0 = oracle.uniform((M, N), np.float64, 72)
+        B = B0.copy(order="F")
+        blx.cblas_dtrsm(102, 141, 122, 111, 131, M, N, 0.5, A, M, B, M)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        st = blx.call_stats()
+        assert 0 < st["tile"] < N and st["path"] == (2 if emulated else 1), st
+        Af = oracle.complete("T", "L", A, M, "N")
+        ii, jj = sample(M, N, 73)
+        jj[:3] = [0, N - 1, st["tile"]]  # both ends and a panel boundary
+        val, bound = oracle.dd_entries("N", "N", M, N, M, 1.0, Af, M, B, M, -0.5, B0, M, ii, jj)
+        assert np.max(np.abs(val) / (2 * (M + 2) * 2.0 ** -53 * bound)) <= 1.0
+    finally:
+        blx.set_hbm_budget(0)
+        blx.set_dgemm_mode(prev)
+
+
+def test_trmm_streams_b_rows_beyond_the_budget(blx):
+    """A right multiply streams B by rows: ZTRMM with B 48 MB under a 32 MiB budget."""
+    blx.set_hbm_budget(32 << 20)
+    try:
+        M, N = 5000, 600
+        A = oracle.uniform((N, N), np.complex128, 81)
+        i, j = np.indices((N, N))
+        A[i < j] = np.nan  # lower: the upper triangle is not read
+        B0 = oracle.uniform((M, N), np.complex128, 82)
+        B = B0.copy(order="F")
+        al = complex(0.5, -0.25)
+        blx.cblas_ztrmm(102, 142, 122, 113, 131, M, N, al, A, N, B, M)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        assert 0 < blx.call_stats()["tile"] < M
+        Af = oracle.complete("T", "L", A, N, "N")
+        check_dd(B, "N", "C", M, N, N, al, B0, M, Af, N, 0.0, np.zeros_like(B0), M, 83)
+    finally:
+        blx.set_hbm_budget(0)
+
+
+def test_tri_beyond_the_budget(blx):
+    """alpha = 0 streams zeros into B without reading A; an A that does not fit
+    the budget is reported, and B is left unchanged."""
+    blx.set_hbm_budget(4 << 20)
+    try:
+        M, N = 1024, 1024  # A alone is 8 MB
+        A = np.full((M, M), np.nan, order="F")
+        B = oracle.uniform((M, N), np.float64, 91)
+        blx.cblas_dtrsm(102, 141, 121, 111, 131, M, N, 0.0, A, M, B, M)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        assert np.all(B == 0.0)
+        A = oracle.uniform((M, M), np.float64, 92)
+        B0 = oracle.uniform((M, N), np.float64, 93)
         B = B0.copy(order="F")
         blx.cblas_dtrmm(102, 141, 121, 111, 131, M, N, 1.0, A, M, B, M)
         assert blx.last_status() == blx.BLASX_ERR_UNSUPPORTED
