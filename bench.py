@@ -43,7 +43,7 @@ PUBLISHED_BLASX_1GPU_16384_GFLOPS = 1153.4  # performance_data/GEMM.xlsx row 17 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=16384)
@@ -78,6 +78,10 @@ def parse():
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
+    """nvidia-smi clock samples (every 50 ms) during a timed region. nvidia-smi
+    takes a while to start, so entering waits (up to 5 s) for its first sample
+    before the region begins; each line is stamped on arrival, and the summary
+    keeps the lines that arrived between entering and leaving."""
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
@@ -85,7 +89,8 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, line)
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -94,16 +99,25 @@ class ClockSampler:
                  "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.monotonic() + 5.0
+            while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except (OSError, FileNotFoundError):
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def __exit__(self, *exc):
+        self.t1 = time.monotonic()
         if self.proc:
+            n = len(self.lines)  # one more sample after the region, up to 0.5 s
+            deadline = time.monotonic() + 0.5
+            while len(self.lines) == n and time.monotonic() < deadline:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -113,7 +127,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        # the samples of the region, with the first one after it (its reading covers the region's end)
+        inside = [l for t, l in self.lines if self.t0 <= t <= self.t1]
+        after = [l for t, l in self.lines if t > self.t1][:1]
+        for l in inside + after:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
