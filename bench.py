@@ -603,28 +603,30 @@ def run_workloads(args):
             tT.copy_(tA / n)
             tT.diagonal().add_(2.0)
             T = np.asarray(tT.numpy()).T
-            # device-resident DTRSM (the solve alone), per precision mode
+            # device-resident DTRSM and DTRMM (the compute alone), per precision mode
             dT, dB0 = tT.cuda(), tB.cuda()
-            dev = {}
-            for mode_name, mode in (("auto", bx.MODE_AUTO), ("emulated", bx.MODE_OZAKI), ("native", bx.MODE_NATIVE)):
-                bx.set_dgemm_mode(mode)
-                dB = dB0.clone()
-                s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
-                call = lambda: bx.dtrsm_device("L", "U", "N", "N", n, n, 1.0, dT, n, dB, n, stream=s)
-                assert call() == 0, bx.last_error()
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(s)
-                for _ in range(2):
+            for op, fn in (("dtrsm", bx.dtrsm_device), ("dtrmm", bx.dtrmm_device)):
+                dev = {}
+                for mode_name, mode in (("auto", bx.MODE_AUTO), ("emulated", bx.MODE_OZAKI),
+                                        ("native", bx.MODE_NATIVE)):
+                    bx.set_dgemm_mode(mode)
+                    dB = dB0.clone()
+                    s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
+                    call = lambda: fn("L", "U", "N", "N", n, n, 1.0, dT, n, dB, n, stream=s)
                     assert call() == 0, bx.last_error()
-                e1.record(s); torch.cuda.synchronize()
-                ms = e0.elapsed_time(e1) / 2
-                dev[mode_name] = {"tflops": float(n) ** 3 / (ms * 1e-3) / 1e12, "ms": ms}
-                del dB
-            bx.set_dgemm_mode(bx.MODE_AUTO)
-            lines.append({"workload": f"dtrsm device-resident Left Upper NoTrans NonUnit M=N={n} (A / n + 2 I)",
-                          "flops_credited": "M^2 N", **dev})
-            print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(s)
+                    for _ in range(2):
+                        assert call() == 0, bx.last_error()
+                    e1.record(s); torch.cuda.synchronize()
+                    ms = e0.elapsed_time(e1) / 2
+                    dev[mode_name] = {"tflops": float(n) ** 3 / (ms * 1e-3) / 1e12, "ms": ms}
+                    del dB
+                bx.set_dgemm_mode(bx.MODE_AUTO)
+                lines.append({"workload": f"{op} device-resident Left Upper NoTrans NonUnit M=N={n} (A / n + 2 I)",
+                              "flops_credited": "M^2 N", **dev})
+                print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
             del dT, dB0
             for op in ("dsymm", "dtrmm", "dtrsm"):
                 res = {}

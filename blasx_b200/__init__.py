@@ -106,6 +106,7 @@ def lib() -> ctypes.CDLL:
             getattr(L, f).argtypes = [_P] * 12
         L.blasx_dsyrk_device.argtypes = [_I] * 4 + [_D, _P, _I, _D, _P, _I, _P]
         L.blasx_dtrsm_device.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _P]
+        L.blasx_dtrmm_device.argtypes = [_I] * 6 + [_D, _P, _I, _P, _I, _P]
         for t, sc in (("s", _F), ("d", _D), ("c", _P), ("z", _P)):
             for kind in ("symm", "hemm") if t in "cz" else ("symm",):
                 getattr(L, f"cblas_{t}{kind}").argtypes = [_I] * 5 + [sc, _P, _I, _P, _I, sc, _P, _I]
@@ -340,6 +341,13 @@ def dtrsm_device(side, uplo, trans, diag, M, N, alpha, A, lda, B, ldb, stream=No
     s = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else _addr(stream))
     args = [SIDE.get(side, side), UPLO.get(uplo, uplo), TRANS.get(trans, trans), DIAG.get(diag, diag)]
     return lib().blasx_dtrsm_device(*args, M, N, alpha, _addr(A), lda, _addr(B), ldb, s)
+
+
+def dtrmm_device(side, uplo, trans, diag, M, N, alpha, A, lda, B, ldb, stream=None):
+    """Device-resident DTRMM on device pointers (ints or tensors with data_ptr)."""
+    s = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else _addr(stream))
+    args = [SIDE.get(side, side), UPLO.get(uplo, uplo), TRANS.get(trans, trans), DIAG.get(diag, diag)]
+    return lib().blasx_dtrmm_device(*args, M, N, alpha, _addr(A), lda, _addr(B), ldb, s)
 
 
 def _cpair32(v) -> np.ndarray:

@@ -207,8 +207,11 @@ cplx c_scalar(const void *p) {
 
 }  // namespace
 
-int trsm_device_entry(DType dt, int side, int uplo, int trans, int diag, int M, int N, cplx alpha,
-                      const void *A, int lda, void *B, int ldb, cudaStream_t s) {
+// Device-resident TRSM (mult false) or TRMM (mult true) on the caller's
+// stream. TRMM's leaf scratch (one diagonal block, one leaf's vectors) is a
+// stream-ordered allocation on that stream, released after the last leaf.
+int tri_device_entry(bool mult, DType dt, int side, int uplo, int trans, int diag, int M, int N, cplx alpha,
+                     const void *A, int lda, void *B, int ldb, cudaStream_t s) {
     clear_error();
     int info = 0;
     const int nrowa = side == CblasLeft ? M : N;
@@ -220,7 +223,7 @@ int trsm_device_entry(DType dt, int side, int uplo, int trans, int diag, int M, 
     else if (N < 0) info = 6;
     else if (lda < std::max(1, nrowa)) info = 9;
     else if (ldb < std::max(1, M)) info = 11;
-    if (info) return set_error(BLASX_ERR_ARG, "device trsm parameter %d illegal", info);
+    if (info) return set_error(BLASX_ERR_ARG, "device %s parameter %d illegal", mult ? "trmm" : "trsm", info);
     if (M == 0 || N == 0) return BLASX_OK;
     if (!context()) return last_status();
     Trsm t;
@@ -234,7 +237,17 @@ int trsm_device_entry(DType dt, int side, int uplo, int trans, int diag, int M, 
     t.A = A; t.lda = lda;
     t.B = B; t.ldb = ldb;
     bool emulated = false;
-    return trsm_device(t, s, &emulated);
+    if (!mult) return trsm_device(t, s, &emulated);
+    TrmmScratch w = trmm_scratch_sizes(t);
+    BX_CUDA(cudaMallocAsync(&w.diag, w.diag_bytes, s));
+    if (cudaMallocAsync(&w.temp, w.temp_bytes, s) != cudaSuccess) {
+        cudaFreeAsync(w.diag, s);
+        return set_error(BLASX_ERR_NOMEM, "device trmm: no memory for %zu bytes of scratch", w.temp_bytes);
+    }
+    const int rc = trmm_device(t, w, s, &emulated);
+    cudaFreeAsync(w.temp, s);
+    cudaFreeAsync(w.diag, s);
+    return rc;
 }
 
 }  // namespace bx
@@ -331,8 +344,14 @@ BX_F77_TRI("ZTRSM ", ztrsm_, cblas_ztrsm, double, BX_PTR)
 
 int blasx_dtrsm_device(int side, int uplo, int trans, int diag, int M, int N, double alpha, const double *A,
                        int lda, double *B, int ldb, void *stream) {
-    return bx::trsm_device_entry(DType::F64, side, uplo, trans, diag, M, N, cplx{alpha, 0.0}, A, lda, B, ldb,
-                                 static_cast<cudaStream_t>(stream));
+    return bx::tri_device_entry(false, DType::F64, side, uplo, trans, diag, M, N, cplx{alpha, 0.0}, A, lda, B, ldb,
+                                static_cast<cudaStream_t>(stream));
+}
+
+int blasx_dtrmm_device(int side, int uplo, int trans, int diag, int M, int N, double alpha, const double *A,
+                       int lda, double *B, int ldb, void *stream) {
+    return bx::tri_device_entry(true, DType::F64, side, uplo, trans, diag, M, N, cplx{alpha, 0.0}, A, lda, B, ldb,
+                                static_cast<cudaStream_t>(stream));
 }
 #undef BX_REAL
 #undef BX_PTR

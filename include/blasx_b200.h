@@ -368,6 +368,13 @@ int blasx_dsyrk_device(int uplo, int trans, int N, int K, double alpha, const do
 int blasx_dtrsm_device(int side, int uplo, int trans, int diag, int M, int N, double alpha,
                        const double *A, int lda, double *B, int ldb, void *stream);
 
+/* Device-resident DTRMM (arguments as for cblas_dtrmm, column-major): B =
+ * alpha op(A) B or alpha B op(A) on the device matrix B, in place, enqueued on
+ * `stream`; returns a status. Its small leaf scratch is allocated and freed
+ * stream-ordered on `stream`. No counterpart in the reference. */
+int blasx_dtrmm_device(int side, int uplo, int trans, int diag, int M, int N, double alpha,
+                       const double *A, int lda, double *B, int ldb, void *stream);
+
 /* Device-resident DGEMM that allocates no memory. No counterpart in the
  * reference. It is meant for callers that cannot let a library call
  * cudaMalloc: a framework whose own allocator has already reserved the

@@ -393,3 +393,28 @@ def test_tri_beyond_the_budget(blx):
         assert np.array_equal(B, B0)
     finally:
         blx.set_hbm_budget(0)
+
+
+@pytest.mark.parametrize("fn", ["trmm", "trsm"])
+@pytest.mark.parametrize("mode", ["native", "ozaki"])
+def test_device_entries_match_host(blx, fn, mode):
+    """blasx_dtrmm_device / blasx_dtrsm_device on device pointers give the
+    host call's result (the other triangle of A holds NaN)."""
+    torch = pytest.importorskip("torch")
+    prev = blx.set_dgemm_mode(blx.MODE_NATIVE if mode == "native" else blx.MODE_OZAKI)
+    try:
+        M, N = 700, 900
+        A = dominant_triangle(np.float64, M, "U", "N", 101)
+        B0 = oracle.uniform((M, N), np.float64, 102)
+        Bh = B0.copy(order="F")
+        getattr(blx, f"cblas_d{fn}")(102, 141, 121, 111, 131, M, N, 0.5, A, M, Bh, M)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        dA = torch.from_numpy(A.T.copy()).cuda()
+        dB = torch.from_numpy(B0.T.copy()).cuda()
+        s = torch.cuda.Stream(); s.wait_stream(torch.cuda.current_stream())
+        rc = getattr(blx, f"d{fn}_device")("L", "U", "N", "N", M, N, 0.5, dA, M, dB, M, stream=s)
+        assert rc == 0, blx.last_error()
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(dB.cpu().numpy().T, Bh, rtol=1e-12, atol=1e-12)
+    finally:
+        blx.set_dgemm_mode(prev)
