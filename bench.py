@@ -797,6 +797,23 @@ def run_workloads(args):
         print(json.dumps(l), flush=True)
 
 
+def rank_barrier(dist) -> None:
+    """All ranks reach this point before any goes on (no-op on one rank)."""
+    if dist:
+        dist.barrier()
+
+
+def rank_max(x: float, dist, device: str) -> float:
+    """The largest x over all ranks (x itself on one rank): a step time is the
+    slowest rank's."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -846,15 +863,10 @@ def main():
     bx.set_dgemm_mode(mode)
 
     def barrier():
-        if dist:
-            dist.barrier()
+        rank_barrier(dist)
 
     def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, "cuda")
 
     # --- inputs (device-resident), C3 distribution ---
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
