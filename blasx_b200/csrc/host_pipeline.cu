@@ -372,49 +372,62 @@ bool want_ozaki(const Gemm &g, int mode) { return ozaki_selected(g, mode); }
 
 }  // namespace
 
-// TRSM and TRMM with their copies overlapped. Along the top-level split of
-// the triangle the H2D stream copies the first diagonal block of A and the
-// first part of B, then the off-diagonal block and the rest of B, then the
-// second diagonal block; the compute stream starts on the first part as
-// soon as its inputs landed; the D2H stream returns each part of B as soon
-// as it is final. The parts of B are rows (left) or columns (right).
-//   solve:    solve(first, alpha); second = alpha second - op(A)[second, first] X_first;
-//             solve(second); the first part is final after its solve.
-//   multiply: multiply(first); first += alpha op(A)[first, second] B_second (the
-//             second part's original values); multiply(second); the first
-//             part is final after the update.
-// The off-diagonal block is stored as op(A)[tgt, src] (left, NoTrans) or its
-// transpose.
-static int tri_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Context *c, bool mult,
-                         const TrmmScratch &w, int64_t f0, int64_t f1, int64_t s0, int64_t s1, bool *emulated,
-                         blasx_call_stats &st) {
+// The blocks of the streamed triangular pipeline: the order K of the
+// triangle cut into n blocks of b rows (left) or columns (right), taken in
+// substitution order (tri_forward: ascending), the block taken last ragged.
+// Up to 8 blocks of at least 2048 (2 for K below 4096): fewer blocks leave
+// longer copies at the start and end uncovered, more blocks shrink the
+// update GEMMs (the emulated path slices the blocks before each one again).
+struct TriBlocks {
+    int64_t K = 0, b = 0;
+    int n = 0;
+    bool fwd = true;
+    explicit TriBlocks(const Trsm &t) : K(t.order()), fwd(tri_forward(t)) {
+        const int64_t parts = std::min<int64_t>(8, std::max<int64_t>(2, K / 2048));
+        b = round_up((K + parts - 1) / parts, 256);
+        n = int((K + b - 1) / b);
+    }
+    // block i: [lo, hi); the blocks before it: [dlo, dhi) (empty for i == 0)
+    void block(int i, int64_t *lo, int64_t *hi, int64_t *dlo, int64_t *dhi) const {
+        if (fwd) {
+            *lo = i * b;
+            *hi = std::min(K, *lo + b);
+            *dlo = 0;
+            *dhi = *lo;
+        } else {
+            *hi = K - i * b;
+            *lo = std::max<int64_t>(0, *hi - b);
+            *dlo = *hi;
+            *dhi = K;
+        }
+    }
+};
+
+// TRSM and TRMM with the copies streamed against the compute. Block i of
+// the order needs its strip of A (its diagonal block and the rectangle of
+// op(A) against the blocks before it, inside the stored triangle) and its
+// part of B (rows for a left solve or multiply, columns for a right one);
+// the H2D stream copies these block after block, all enqueued at once, the
+// compute stream takes each block when its copies landed, and the D2H stream
+// returns each block of the result as soon as it is final.
+//   solve:    B_i = alpha B_i - op(A)[i, before] X_before (one GEMM), then
+//             the solve of block i against its diagonal block;
+//   multiply: out of place into R (the earlier blocks' original values are
+//             still needed): R_i = B_i, R_i = alpha S_ii R_i, then
+//             R_i += alpha op(A)[i, before] B_before (one GEMM).
+// The strip is stored as rows i x the blocks up to i (left NoTrans, right
+// Trans) or the transpose.
+static int tri_streamed(const Trsm &t, const Trsm &dt, const DeviceOps &d, Context *c, bool mult,
+                        const TrmmScratch &w, const TriBlocks &tb, bool *emulated, blasx_call_stats &st) {
     const size_t es = elem_size(t.dt);
     Events ev;
     cudaEvent_t start = ev.make();
     BX_CUDA(cudaEventRecord(start, c->compute));  // the device buffers are allocated on compute
     BX_CUDA(cudaStreamWaitEvent(c->h2d, start, 0));
     BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
-    auto copy_a = [&](int64_t r0, int64_t r1, int64_t c0, int64_t c1) -> int {
-        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.A) + (r0 + c0 * d.lda) * es, d.lda * es,
-                                  static_cast<const char *>(t.A) + (r0 + c0 * t.lda) * es, t.lda * es,
-                                  (r1 - r0) * es, c1 - c0, cudaMemcpyHostToDevice, c->h2d));
-        st.h2d_bytes += double(es) * (r1 - r0) * (c1 - c0);
-        return BLASX_OK;
-    };
-    // part [p0, p1) of B: rows (left) or columns (right)
-    auto copy_b = [&](int64_t p0, int64_t p1, bool in) -> int {
-        const int64_t off = t.left ? p0 : p0 * t.ldb, doff = t.left ? p0 : p0 * d.ldb;
-        const int64_t rows = t.left ? p1 - p0 : t.M, cols = t.left ? t.N : p1 - p0;
-        char *dev = static_cast<char *>(d.B) + doff * es;
-        char *host = static_cast<char *>(t.B) + off * es;
-        if (in)
-            BX_CUDA(cudaMemcpy2DAsync(dev, d.ldb * es, host, t.ldb * es, rows * es, cols, cudaMemcpyHostToDevice,
-                                      c->h2d));
-        else
-            BX_CUDA(cudaMemcpy2DAsync(host, t.ldb * es, dev, d.ldb * es, rows * es, cols, cudaMemcpyDeviceToHost,
-                                      c->d2h));
-        (in ? st.h2d_bytes : st.d2h_bytes) += double(es) * rows * cols;
-        return BLASX_OK;
+    // part [p0, p1) of a B-shaped buffer: rows (left) or columns (right)
+    auto part = [&](void *base, int64_t ld, int64_t p0) {
+        return static_cast<char *>(base) + (t.left ? p0 : p0 * ld) * int64_t(es);
     };
     auto handoff = [&](cudaStream_t from, cudaStream_t to) -> int {
         cudaEvent_t e = ev.make();
@@ -422,36 +435,39 @@ static int tri_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Cont
         BX_CUDA(cudaStreamWaitEvent(to, e, 0));
         return BLASX_OK;
     };
-    // the update writes tgt from src: the second part from the first (solve), or the reverse (multiply)
-    const int64_t t0 = mult ? f0 : s0, t1 = mult ? f1 : s1, r0 = mult ? s0 : f0, r1 = mult ? s1 : f1;
-    const bool off_tgt_first = t.left == (t.trans == NoTrans);  // stored rows of the off-diagonal block
-    BX_TRY(copy_a(f0, f1, f0, f1));
-    BX_TRY(copy_b(f0, f1, true));
-    BX_TRY(handoff(c->h2d, c->compute));
-    if (mult) {
-        BX_TRY(trmm_part(dt, f0, f1, w, c->compute, emulated));
-    } else {
-        BX_TRY(trsm_solve_part(dt, f0, f1, t.alpha, c->compute, emulated));
+    const bool strip_rows = t.left == (t.trans == NoTrans);
+    Trsm dr = dt;  // the multiply's view of the result buffer
+    dr.B = d.C;
+    for (int i = 0; i < tb.n; ++i) {
+        int64_t lo, hi, dlo, dhi;
+        tb.block(i, &lo, &hi, &dlo, &dhi);
+        const int64_t r0 = std::min(lo, dlo), r1 = std::max(hi, dhi);
+        const int64_t arow0 = strip_rows ? lo : r0, arow1 = strip_rows ? hi : r1;
+        const int64_t acol0 = strip_rows ? r0 : lo, acol1 = strip_rows ? r1 : hi;
+        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.A) + (arow0 + acol0 * d.lda) * es, d.lda * es,
+                                  static_cast<const char *>(t.A) + (arow0 + acol0 * t.lda) * es, t.lda * es,
+                                  (arow1 - arow0) * es, acol1 - acol0, cudaMemcpyHostToDevice, c->h2d));
+        const int64_t rows = t.left ? hi - lo : t.M, cols = t.left ? t.N : hi - lo;
+        BX_CUDA(cudaMemcpy2DAsync(part(d.B, d.ldb, lo), d.ldb * es, part(t.B, t.ldb, lo), t.ldb * es, rows * es, cols,
+                                  cudaMemcpyHostToDevice, c->h2d));
+        st.h2d_bytes += double(es) * (double(arow1 - arow0) * (acol1 - acol0) + double(rows) * cols);
+        BX_TRY(handoff(c->h2d, c->compute));
+        if (mult) {
+            BX_CUDA(cudaMemcpy2DAsync(part(d.C, d.ldb, lo), d.ldb * es, part(d.B, d.ldb, lo), d.ldb * es, rows * es,
+                                      cols, cudaMemcpyDeviceToDevice, c->compute));
+            BX_TRY(trmm_part(dr, lo, hi, w, c->compute, emulated));
+            if (dlo < dhi) BX_TRY(trmm_update_into(dt, d.C, lo, hi, dlo, dhi, c->compute, emulated));
+        } else if (dlo < dhi) {
+            BX_TRY(trsm_update_part(dt, lo, hi, dlo, dhi, t.alpha, c->compute, emulated));
+            BX_TRY(trsm_solve_part(dt, lo, hi, cplx{1.0, 0.0}, c->compute, emulated));
+        } else {
+            BX_TRY(trsm_solve_part(dt, lo, hi, t.alpha, c->compute, emulated));
+        }
         BX_TRY(handoff(c->compute, c->d2h));
-        BX_TRY(copy_b(f0, f1, false));
+        BX_CUDA(cudaMemcpy2DAsync(part(t.B, t.ldb, lo), t.ldb * es, part(mult ? d.C : d.B, d.ldb, lo), d.ldb * es,
+                                  rows * es, cols, cudaMemcpyDeviceToHost, c->d2h));
+        st.d2h_bytes += double(es) * rows * cols;
     }
-    if (off_tgt_first) BX_TRY(copy_a(t0, t1, r0, r1));
-    else BX_TRY(copy_a(r0, r1, t0, t1));
-    BX_TRY(copy_b(s0, s1, true));
-    BX_TRY(handoff(c->h2d, c->compute));
-    if (mult) {
-        BX_TRY(trmm_update_part(dt, f0, f1, s0, s1, c->compute, emulated));
-        BX_TRY(handoff(c->compute, c->d2h));
-        BX_TRY(copy_b(f0, f1, false));
-    } else {
-        BX_TRY(trsm_update_part(dt, s0, s1, f0, f1, t.alpha, c->compute, emulated));
-    }
-    BX_TRY(copy_a(s0, s1, s0, s1));
-    BX_TRY(handoff(c->h2d, c->compute));
-    if (mult) BX_TRY(trmm_part(dt, s0, s1, w, c->compute, emulated));
-    else BX_TRY(trsm_solve_part(dt, s0, s1, cplx{1.0, 0.0}, c->compute, emulated));
-    BX_TRY(handoff(c->compute, c->d2h));
-    BX_TRY(copy_b(s0, s1, false));
     BX_CUDA(cudaStreamSynchronize(c->h2d));
     BX_CUDA(cudaStreamSynchronize(c->compute));
     BX_CUDA(cudaStreamSynchronize(c->d2h));
@@ -464,7 +480,8 @@ static int tri_pipelined(const Trsm &t, const Trsm &dt, const DeviceOps &d, Cont
 // resident. Panel p + 1 is copied in while panel p computes, and each panel
 // goes back as soon as it is done; a panel buffer is refilled only after its
 // previous contents left. The panel width is the largest that fits (at least
-// 256 vectors); A itself must fit.
+// 256 vectors; all of B in one panel when only the streamed multiply's
+// result buffer did not fit); A itself must fit.
 static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t budget, blasx_call_stats &st) {
     const size_t es = elem_size(t.dt);
     const int64_t K = t.order(), nvec = t.left ? t.N : t.M;
@@ -489,7 +506,7 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
     };
     int64_t wv = nvec;
     while (wv > 256 && need(wv) > budget) wv = (wv / 2 + 31) / 32 * 32;
-    if (wv >= nvec || need(wv) > budget)
+    if (need(wv) > budget)
         return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: A (%zu bytes) leaves no room for panels of B in "
                          "the HBM budget", mult ? "multiply" : "solve", bytes_a);
     const Trsm full = panel_desc(wv);
@@ -563,10 +580,12 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
 }
 
 // TRSM (mult false) or TRMM (mult true) on host operands: A (the order-K
-// triangle) and B to the device, the recursive solve or multiply, B back;
-// copies overlap the compute along its top-level split (tri_pipelined). The
-// scratch of the largest update GEMM (and TRMM's leaf scratch) is part of
-// the budget; a B beyond it streams in panels (tri_panels).
+// triangle) and B to the device, the solve or multiply, B back. A triangle
+// of more than one block streams its copies against the compute block by
+// block (tri_streamed); one block is copied, solved or multiplied by the
+// recursion, and copied back. The scratch of the largest update GEMM (and
+// TRMM's leaf scratch and result buffer) is part of the budget; a B beyond
+// it streams in panels (tri_panels).
 static int host_tri(const Trsm &t, bool mult) {
     auto t0 = std::chrono::steady_clock::now();
     blasx_call_stats &st = call_stats();
@@ -588,12 +607,25 @@ static int host_tri(const Trsm &t, bool mult) {
     dt.ldb = d.ldb;
     const size_t bytes_a = need_a ? size_t(d.lda) * K * es : 0;
     const size_t bytes_b = size_t(d.ldb) * t.N * es;
-    const Gemm top = mult ? trmm_top_update(dt) : trsm_top_update(dt);
-    const size_t bytes_ws = need_a && top.K > 0 && ozaki_selected(top, mode) ? ozaki_scratch_bytes(top) : 0;
+    auto ws_of = [&](const Gemm &g) { return g.K > 0 && ozaki_selected(g, mode) ? ozaki_scratch_bytes(g) : size_t(0); };
+    const TriBlocks tb(dt);
+    const bool split = need_a && tb.n > 1;
+    size_t bytes_ws = 0, bytes_r = 0;
+    if (need_a) {
+        Trsm blk = dt;  // the recursion inside one block (the whole triangle unsplit)
+        if (split) (t.left ? blk.M : blk.N) = tb.b;
+        bytes_ws = ws_of(mult ? trmm_top_update(blk) : trsm_top_update(blk));
+        if (split) {  // the largest block update: the last block's, from all the others
+            int64_t lo, hi, dlo, dhi;
+            tb.block(tb.n - 1, &lo, &hi, &dlo, &dhi);
+            bytes_ws = std::max(bytes_ws, ws_of(tri_update_gemm(dt, lo, hi, dlo, dhi)));
+            if (mult) bytes_r = bytes_b;  // the out-of-place result
+        }
+    }
     TrmmScratch w = mult ? trmm_scratch_sizes(dt) : TrmmScratch{};
     const size_t bytes_w = need_a ? w.diag_bytes + w.temp_bytes : 0;
     const size_t budget = default_budget(c);
-    if (bytes_a + bytes_b + bytes_ws + bytes_w > budget) {
+    if (bytes_a + bytes_b + bytes_r + bytes_ws + bytes_w > budget) {
         const int rc = tri_panels(t, c, mult, mode, budget, st);
         st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return rc;
@@ -604,6 +636,7 @@ static int host_tri(const Trsm &t, bool mult) {
     cudaStream_t s = c->compute;
     if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, s));
     BX_CUDA(cudaMallocAsync(&d.B, bytes_b, s));  // alpha == 0 writes zeros without reading B
+    if (bytes_r) BX_CUDA(cudaMallocAsync(&d.C, bytes_r, s));
     if (bytes_w) {
         BX_CUDA(cudaMallocAsync(&d.diag, w.diag_bytes, s));
         BX_CUDA(cudaMallocAsync(&d.C0, w.temp_bytes, s));
@@ -613,8 +646,6 @@ static int host_tri(const Trsm &t, bool mult) {
     dt.A = d.A;
     dt.B = d.B;
     bool emulated = false;
-    int64_t f0, f1, s0, s1;
-    const bool split = need_a && (mult ? trmm_halves(dt, &f0, &f1, &s0, &s1) : trsm_halves(dt, &f0, &f1, &s0, &s1));
     if (!split) {
         if (need_a) {
             BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, s));
@@ -626,7 +657,8 @@ static int host_tri(const Trsm &t, bool mult) {
         st.d2h_bytes += double(es) * t.M * t.N;
         BX_CUDA(cudaStreamSynchronize(s));
     } else {
-        BX_TRY(tri_pipelined(t, dt, d, c, mult, w, f0, f1, s0, s1, &emulated, st));
+        BX_TRY(tri_streamed(t, dt, d, c, mult, w, tb, &emulated, st));
+        st.tile = int(tb.b);  // the block order
     }
     st.path = !need_a ? 3 : (emulated ? 2 : 1);
     if (emulated) {

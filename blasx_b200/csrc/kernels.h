@@ -49,13 +49,19 @@ int trsm_device(const Trsm &t, cudaStream_t s, bool *emulated);
 // The largest update GEMM trsm_device issues for t (its scratch bounds the
 // solve's), or a Gemm with K == 0 when the triangle is a single leaf.
 Gemm trsm_top_update(const Trsm &t);
-// The top-level split of trsm_device: solve order first, then second (false
-// when the triangle is a single leaf). trsm_solve_part solves rows (left) or
-// columns (right) [lo, hi) whose right-hand sides are scale * B;
+// Parts of a solve or multiply, for pipelines that work through the order in
+// blocks. trsm_solve_part solves rows (left) or columns (right) [lo, hi)
+// whose right-hand sides are scale * B, against their diagonal block;
 // trsm_update_part applies B[tgt] = scale B[tgt] - op(A)[tgt, src] X[src] (or
-// the right-side mirror). Together: solve(first, alpha), update(second, first,
-// alpha), solve(second, 1) is trsm_device.
-bool trsm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi);
+// the right-side mirror B[:, tgt] = scale B[:, tgt] - X[:, src] op(A)[src, tgt]).
+// Blocks solved in substitution order, each after the update from those
+// before it, give trsm_device. tri_forward: that order is ascending (the
+// system matrix, op(A) for a left solve and op(A)^T for a right one, is
+// lower); every update then reads op(A) inside the stored triangle.
+bool tri_forward(const Trsm &t);
+// The update of block tgt from block src as a GEMM on t's operands (alpha
+// t.alpha, beta 1): sizes the scratch of a block pipeline.
+Gemm tri_update_gemm(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi);
 // TRMM (a Trsm describes it: B = alpha op(A) B or alpha B op(A), in place):
 // recursive halving into GEMM updates plus leaves of at most 256 rows that
 // multiply by their completed diagonal block on the native kernels. Its
@@ -67,12 +73,15 @@ struct TrmmScratch {
 };
 TrmmScratch trmm_scratch_sizes(const Trsm &t);
 int trmm_device(const Trsm &t, const TrmmScratch &w, cudaStream_t s, bool *emulated);
-// The top-level split of trmm_device: multiply first, update first from
-// second (with second's original values), multiply second.
-bool trmm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi);
+// trmm_part multiplies rows (left) or columns (right) [lo, hi) of B in place
+// by alpha times their diagonal block; trmm_update_into adds alpha
+// op(A)[tgt, src] B[src] (or B[:, src] op(A)[src, tgt]) to block tgt of dst, a
+// device buffer with B's layout. Out of place, blocks multiplied in
+// substitution order, each followed by the update from the blocks before it
+// (B's original values), give trmm_device.
 int trmm_part(const Trsm &t, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s, bool *emulated);
-int trmm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cudaStream_t s,
-                     bool *emulated);
+int trmm_update_into(const Trsm &t, void *dst, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi,
+                     cudaStream_t s, bool *emulated);
 Gemm trmm_top_update(const Trsm &t);
 int trsm_solve_part(const Trsm &t, int64_t lo, int64_t hi, cplx scale, cudaStream_t s, bool *emulated);
 int trsm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cplx scale,

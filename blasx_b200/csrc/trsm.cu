@@ -344,14 +344,10 @@ int multiply(const Trsm &t, Range r, const TrmmScratch &w, cudaStream_t s, bool 
 
 }  // namespace
 
-bool trsm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi) {
-    const Range all{0, t.order()};
-    if (all.size() <= leaf_order(t.dt)) return false;
-    Range first, second;
-    split(t, all, &first, &second);
-    *first_lo = first.lo; *first_hi = first.hi;
-    *second_lo = second.lo; *second_hi = second.hi;
-    return true;
+bool tri_forward(const Trsm &t) { return forward_of(t); }
+
+Gemm tri_update_gemm(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi) {
+    return update_gemm(t, Range{tgt_lo, tgt_hi}, Range{src_lo, src_hi}, t.alpha, kOne);
 }
 
 int trsm_solve_part(const Trsm &t, int64_t lo, int64_t hi, cplx scale, cudaStream_t s, bool *emulated) {
@@ -406,23 +402,15 @@ TrmmScratch trmm_scratch_sizes(const Trsm &t) {
     return w;
 }
 
-bool trmm_halves(const Trsm &t, int64_t *first_lo, int64_t *first_hi, int64_t *second_lo, int64_t *second_hi) {
-    const Range all{0, t.order()};
-    if (all.size() <= kTrmmLeaf) return false;
-    Range first, second;
-    trmm_split(t, all, &first, &second);
-    *first_lo = first.lo; *first_hi = first.hi;
-    *second_lo = second.lo; *second_hi = second.hi;
-    return true;
-}
-
 int trmm_part(const Trsm &t, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s, bool *emulated) {
     return multiply(t, Range{lo, hi}, w, s, emulated);
 }
 
-int trmm_update_part(const Trsm &t, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi, cudaStream_t s,
-                     bool *emulated) {
-    BX_TRY(device_gemm(update_gemm(t, Range{tgt_lo, tgt_hi}, Range{src_lo, src_hi}, t.alpha, kOne), s));
+int trmm_update_into(const Trsm &t, void *dst, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi,
+                     cudaStream_t s, bool *emulated) {
+    Gemm g = update_gemm(t, Range{tgt_lo, tgt_hi}, Range{src_lo, src_hi}, t.alpha, kOne);
+    g.C = static_cast<char *>(dst) + (static_cast<char *>(g.C) - static_cast<char *>(t.B));
+    BX_TRY(device_gemm(g, s));
     if (call_stats().path == 2) *emulated = true;
     return BLASX_OK;
 }

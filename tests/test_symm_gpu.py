@@ -328,6 +328,41 @@ def test_symm_out_of_core(blx, side, uplo, dt, herm, emulated):
         blx.set_dgemm_mode(prev)
 
 
+@pytest.mark.parametrize("fn", ["trsm", "trmm"])
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "N"), ("U", "N", "U"), ("L", "T", "N")])
+def test_tri_streams_the_order_in_blocks(blx, mode, fn, side, uplo, trans, diag):
+    """An order of 6200 is copied, solved or multiplied and copied back in
+    three blocks of 2304 (the last ragged), ascending or descending with the
+    substitution order (both occur on each side); the result is within the
+    backward-error bound (solve) or the componentwise bound (multiply)."""
+    K, nv = 6200, 96
+    M, N = (K, nv) if side == "L" else (nv, K)
+    A = dominant_triangle(np.float64, K, uplo, diag, 111)
+    B0 = oracle.uniform((M + 1, N), np.float64, 112)
+    B = B0.copy(order="F")
+    getattr(blx, f"cblas_d{fn}")(102, blx.SIDE[side], blx.UPLO[uplo], blx.TRANS[trans], blx.DIAG[diag], M, N, 0.75,
+                                 A, K, B, M + 1)
+    assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+    st = blx.call_stats()
+    assert st["tile"] == 2304 and st["path"] == (2 if mode == "ozaki" else 1), st
+    assert np.array_equal(B[M:], B0[M:]) and np.all(np.isfinite(B))
+    Af = oracle.complete("T", uplo, A, K, diag)
+    if fn == "trmm":
+        Z = np.zeros_like(B0)
+        if side == "L":
+            check_dd(B, trans, "N", M, N, K, 0.75, Af, K, B0, M + 1, 0.0, Z, M + 1, 113)
+        else:
+            check_dd(B, "N", trans, M, N, K, 0.75, B0, M + 1, Af, K, 0.0, Z, M + 1, 113)
+        return
+    ii, jj = sample(M, N, 114)
+    if side == "L":
+        val, bound = oracle.dd_entries(trans, "N", M, N, K, 1.0, Af, K, B, M + 1, -0.75, B0, M + 1, ii, jj)
+    else:
+        val, bound = oracle.dd_entries("N", trans, M, N, K, 1.0, B, M + 1, Af, K, -0.75, B0, M + 1, ii, jj)
+    assert np.max(np.abs(val) / (2 * (K + 2) * 2.0 ** -53 * bound)) <= 1.0
+
+
 @pytest.mark.parametrize("emulated", [False, True])
 def test_trsm_streams_b_beyond_the_budget(blx, emulated):
     """B (74 MB) does not fit a 48 MiB budget beside A (8 MB): its columns
