@@ -370,6 +370,54 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
 
 bool want_ozaki(const Gemm &g, int mode) { return ozaki_selected(g, mode); }
 
+// Device bytes of host_gemm's in-core path for g: A, B (none when B is A's
+// buffer), C, the emulated path's scratch and, when it works in K-blocks
+// with C read, the input copy of C.
+struct IncoreBytes {
+    size_t a = 0, b = 0, c = 0, c0 = 0, ws = 0;
+    size_t total() const { return a + b + c + c0 + ws; }
+};
+IncoreBytes incore_bytes(const Gemm &g, int mode) {
+    const size_t es = elem_size(g.dt);
+    const bool need_ab = !(g.alpha_zero() || g.K == 0);
+    const bool read_c = !g.beta_zero() || g.uplo != 0;
+    const bool oz = need_ab && want_ozaki(g, mode);
+    const bool shared = need_ab && b_is_a(g);
+    IncoreBytes ib;
+    ib.a = need_ab ? size_t(round_up(g.rows_a(), 32)) * g.cols_a() * es : 0;
+    ib.b = need_ab && !shared ? size_t(round_up(g.rows_b(), 32)) * g.cols_b() * es : 0;
+    ib.c = size_t(round_up(g.M, 32)) * g.N * es;
+    Gemm probe = g;
+    probe.lda = round_up(g.rows_a(), 32);
+    probe.ldb = round_up(g.rows_b(), 32);
+    probe.ldc = round_up(g.M, 32);
+    if (!shared) probe.B = nullptr;  // the scratch shares slices only when the device copy is shared
+    probe.a_form = probe.b_form = 0;
+    ib.ws = oz ? ozaki_scratch_bytes(probe) : 0;
+    ib.c0 = (oz && read_c && kblock_count(g) > 1 && !(g.a_form || g.b_form)) ? ib.c : 0;
+    return ib;
+}
+
+// The emulated scratch of one tile-cache K-step of g with tile edge T (0
+// when the steps run natively).
+size_t tile_step_ws(const Gemm &g, int T, int mode) {
+    Gemm step = g;
+    step.M = std::min<int64_t>(g.M, T);
+    step.N = std::min<int64_t>(g.N, T);
+    step.K = std::min<int64_t>(g.K, T);
+    step.lda = step.ldb = step.ldc = T;
+    step.B = nullptr;  // a step's A and B tiles sit in separate slots, even for SYRK
+    return want_ozaki(step, mode) ? ozaki_scratch_bytes(step) : 0;
+}
+
+// Whether host_gemm runs g under the budget, in core or through the tile
+// cache (the C tiles and two operand tiles, and a step's scratch).
+bool host_gemm_fits(const Gemm &g, int mode, size_t budget) {
+    if (incore_bytes(g, mode).total() <= budget) return true;
+    const int T = pick_tile(g);
+    return tiled_min_bytes(g.dt, T, tile_step_ws(g, T, mode)) <= budget;
+}
+
 }  // namespace
 
 // The blocks of the streamed triangular pipeline: the order K of the
@@ -482,28 +530,41 @@ static int tri_streamed(const Trsm &t, const Trsm &dt, const DeviceOps &d, Conte
 // previous contents left. The panel width is the largest that fits (at least
 // 256 vectors; all of B in one panel when only the streamed multiply's
 // result buffer did not fit); A itself must fit.
+// The device layout of a panel of wv vectors of t (columns for a left call,
+// rows for a right one): K x wv (ld K padded) or wv x K (ld wv padded), A
+// with ld K padded.
+static Trsm tri_panel_desc(const Trsm &t, int64_t wv) {
+    const int64_t K = t.order();
+    Trsm p = t;
+    p.lda = round_up(K, 32);
+    if (t.left) { p.N = wv; p.ldb = round_up(K, 32); }
+    else { p.M = wv; p.ldb = round_up(wv, 32); }
+    return p;
+}
+
+// Device bytes of tri_panels with panels of wv vectors: A, two panels, the
+// scratch of the largest update GEMM, TRMM's leaf scratch.
+static size_t tri_panel_need(const Trsm &t, bool mult, int mode, int64_t wv) {
+    const size_t es = elem_size(t.dt);
+    const int64_t K = t.order();
+    const bool need_a = !(t.alpha.re == 0 && t.alpha.im == 0);  // alpha == 0: B = 0, A and B not read
+    const size_t bytes_a = need_a ? size_t(round_up(K, 32)) * K * es : 0;
+    const Trsm p = tri_panel_desc(t, wv);
+    const Gemm top = mult ? trmm_top_update(p) : trsm_top_update(p);
+    const size_t ws = top.K > 0 && ozaki_selected(top, mode) ? ozaki_scratch_bytes(top) : 0;
+    const TrmmScratch w = mult ? trmm_scratch_sizes(p) : TrmmScratch{};
+    const size_t panel = size_t(p.ldb) * size_t(t.left ? wv : K) * es;
+    return bytes_a + 2 * panel + ws + w.diag_bytes + w.temp_bytes;
+}
+
 static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t budget, blasx_call_stats &st) {
     const size_t es = elem_size(t.dt);
     const int64_t K = t.order(), nvec = t.left ? t.N : t.M;
     const int64_t lda = round_up(K, 32);
     const bool need_a = !(t.alpha.re == 0 && t.alpha.im == 0);  // alpha == 0: B = 0, A and B not read
     const size_t bytes_a = need_a ? size_t(lda) * K * es : 0;
-    // device extent of a panel of w vectors: K x w (left, ld K) or w x K (right, ld w)
-    auto panel_desc = [&](int64_t wv) {
-        Trsm p = t;
-        p.lda = lda;
-        if (t.left) { p.N = wv; p.ldb = round_up(K, 32); }
-        else { p.M = wv; p.ldb = round_up(wv, 32); }
-        return p;
-    };
-    auto need = [&](int64_t wv) {
-        const Trsm p = panel_desc(wv);
-        const Gemm top = mult ? trmm_top_update(p) : trsm_top_update(p);
-        const size_t ws = top.K > 0 && ozaki_selected(top, mode) ? ozaki_scratch_bytes(top) : 0;
-        const TrmmScratch w = mult ? trmm_scratch_sizes(p) : TrmmScratch{};
-        const size_t panel = size_t(p.ldb) * size_t(t.left ? wv : K) * es;
-        return bytes_a + 2 * panel + ws + w.diag_bytes + w.temp_bytes;
-    };
+    auto panel_desc = [&](int64_t wv) { return tri_panel_desc(t, wv); };
+    auto need = [&](int64_t wv) { return tri_panel_need(t, mult, mode, wv); };
     int64_t wv = nvec;
     while (wv > 256 && need(wv) > budget) wv = (wv / 2 + 31) / 32 * 32;
     if (need(wv) > budget)
@@ -671,8 +732,128 @@ static int host_tri(const Trsm &t, bool mult) {
     return BLASX_OK;
 }
 
-int host_trsm(const Trsm &t) { return host_tri(t, false); }
-int host_trmm(const Trsm &t) { return host_tri(t, true); }
+namespace {
+
+// ---- an A beyond the budget: the order halved on the host ---------------
+// When A leaves no room for panels of B, the order is halved on the host as
+// the device recursion halves it: each diagonal half is a solve or multiply
+// of its own (halved again until its A fits), on the host operands at an
+// offset, and the off-diagonal block is one host GEMM, through the tile
+// cache when it does not fit in core.
+//   solve:    solve(first, alpha); B_second = alpha B_second - op(A)[second, first] X_first;
+//             solve(second, 1)
+//   multiply: multiply(first); B_first += alpha op(A)[first, second] B_second (its
+//             original values); multiply(second)
+// with first the earlier half in substitution order for the solve, the later
+// one for the multiply.
+
+bool tri_fits(const Trsm &t, bool mult, int mode, size_t budget) {
+    const int64_t nvec = t.left ? t.N : t.M;
+    return tri_panel_need(t, mult, mode, std::min<int64_t>(nvec, 256)) <= budget;
+}
+
+// the split point of a host halving: the earlier part has m rows
+int64_t host_half(int64_t K) { return std::min(K - 1, round_up((K + 1) / 2, 256)); }
+
+// t with its order restricted to [lo, hi): A's diagonal block, B's rows
+// (left) or columns (right)
+Trsm tri_piece(const Trsm &t, int64_t lo, int64_t hi, cplx alpha) {
+    const size_t es = elem_size(t.dt);
+    Trsm p = t;
+    p.A = static_cast<const char *>(t.A) + (lo + lo * t.lda) * int64_t(es);
+    p.B = static_cast<char *>(t.B) + (t.left ? lo : lo * t.ldb) * int64_t(es);
+    (t.left ? p.M : p.N) = hi - lo;
+    p.alpha = alpha;
+    return p;
+}
+
+void merge_stats(blasx_call_stats &agg, const blasx_call_stats &s) {
+    agg.h2d_bytes += s.h2d_bytes;
+    agg.d2h_bytes += s.d2h_bytes;
+    agg.cache_hits += s.cache_hits;
+    agg.cache_misses += s.cache_misses;
+    agg.evictions += s.evictions;
+    auto rank = [](int p) { return p == 2 ? 3 : p == 4 ? 2 : p == 1 ? 1 : 0; };
+    if (rank(s.path) > rank(agg.path)) agg.path = s.path;
+    if (s.path == 2) agg.moduli = std::max(agg.moduli, s.moduli);
+}
+
+int tri_split(const Trsm &t, bool mult, int mode, size_t budget, blasx_call_stats &agg);
+
+int tri_run(const Trsm &t, bool mult, int mode, size_t budget, blasx_call_stats &agg) {
+    if (!tri_fits(t, mult, mode, budget)) return tri_split(t, mult, mode, budget, agg);
+    const int rc = host_tri(t, mult);
+    merge_stats(agg, call_stats());
+    agg.tile = std::max<int>(agg.tile, int(t.order()));
+    return rc;
+}
+
+int tri_split(const Trsm &t, bool mult, int mode, size_t budget, blasx_call_stats &agg) {
+    const int64_t K = t.order(), m = host_half(K);
+    const bool fwd = tri_forward(t);
+    // lower part [0, m), upper part [m, K)
+    const bool lower_first = mult ? !fwd : fwd;
+    const int64_t f0 = lower_first ? 0 : m, f1 = lower_first ? m : K;
+    const int64_t s0 = lower_first ? m : 0, s1 = lower_first ? K : m;
+    if (mult) {
+        BX_TRY(tri_run(tri_piece(t, f0, f1, t.alpha), true, mode, budget, agg));
+        BX_TRY(host_gemm(tri_update_gemm(t, f0, f1, s0, s1)));
+        merge_stats(agg, call_stats());
+        return tri_run(tri_piece(t, s0, s1, t.alpha), true, mode, budget, agg);
+    }
+    BX_TRY(tri_run(tri_piece(t, f0, f1, t.alpha), false, mode, budget, agg));
+    Gemm g = tri_update_gemm(t, s0, s1, f0, f1);
+    g.alpha = cplx{-1.0, 0.0};
+    g.beta = t.alpha;
+    BX_TRY(host_gemm(g));
+    merge_stats(agg, call_stats());
+    return tri_run(tri_piece(t, s0, s1, cplx{1.0, 0.0}), false, mode, budget, agg);
+}
+
+// TRSM / TRMM on host operands: one host_tri call, or the host halving when
+// A does not fit. The halving is checked whole before it starts (every
+// piece fits at the depth it reaches, and the largest update GEMM can run),
+// so that a call the budget cannot hold leaves B unchanged.
+int host_tri_entry(const Trsm &t, bool mult) {
+    const bool need_a = !(t.alpha.re == 0 && t.alpha.im == 0);
+    if (t.M == 0 || t.N == 0 || !need_a) return host_tri(t, mult);
+    Context *c = context();
+    if (!c) {
+        call_stats() = blasx_call_stats{};
+        return last_status();
+    }
+    const int mode = config().dgemm_mode.load();
+    const size_t budget = default_budget(c);
+    if (tri_fits(t, mult, mode, budget)) return host_tri(t, mult);
+    auto t0 = std::chrono::steady_clock::now();
+    call_stats() = blasx_call_stats{};
+    const int64_t K = t.order();
+    int64_t o = K;
+    while (o > 256 && !tri_fits(tri_piece(t, 0, o, t.alpha), mult, mode, budget)) o = std::max(host_half(o), o - host_half(o));
+    if (!tri_fits(tri_piece(t, 0, o, t.alpha), mult, mode, budget))
+        return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: the HBM budget (%zu bytes) holds no piece of A "
+                         "with room for panels of B", mult ? "multiply" : "solve", budget);
+    const int64_t m = host_half(K);
+    const Gemm top = tri_update_gemm(t, m, K, 0, m);  // the largest update (sizes only)
+    if (!host_gemm_fits(top, mode, budget))
+        return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: the HBM budget (%zu bytes) cannot hold the "
+                         "update GEMM of its halves (tile edge %d)", mult ? "multiply" : "solve", budget,
+                         pick_tile(top));
+    HostPin pins;  // once for every part: the parts' own registrations would overlap
+    const size_t es = elem_size(t.dt);
+    BX_TRY(pins.pin(t.A, host_extent(t.lda, K, K, es)));
+    BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
+    blasx_call_stats agg{};
+    const int rc = tri_split(t, mult, mode, budget, agg);
+    agg.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    call_stats() = agg;
+    return rc;
+}
+
+}  // namespace
+
+int host_trsm(const Trsm &t) { return host_tri_entry(t, false); }
+int host_trmm(const Trsm &t) { return host_tri_entry(t, true); }
 
 int host_gemm(const Gemm &g) {
     auto t0 = std::chrono::steady_clock::now();
@@ -687,7 +868,6 @@ int host_gemm(const Gemm &g) {
     // a triangular output keeps the other triangle: C always makes the round trip
     const bool read_c = !g.beta_zero() || g.uplo != 0;
     const int mode = config().dgemm_mode.load();
-    const bool formed = g.a_form || g.b_form;
     const bool oz = need_ab && want_ozaki(g, mode);
 
     DeviceOps d;
@@ -696,33 +876,17 @@ int host_gemm(const Gemm &g) {
     d.lda = round_up(g.rows_a(), 32);
     d.ldb = round_up(g.rows_b(), 32);
     d.ldc = round_up(g.M, 32);
-    const size_t bytes_a = need_ab ? size_t(d.lda) * g.cols_a() * es : 0;
-    const size_t bytes_b = need_ab && !d.b_is_a ? size_t(d.ldb) * g.cols_b() * es : 0;
-    const size_t bytes_c = size_t(d.ldc) * g.N * es;
-    Gemm probe = g;
-    probe.lda = d.lda; probe.ldb = d.ldb; probe.ldc = d.ldc;
-    if (!d.b_is_a) probe.B = nullptr;  // the scratch shares slices only when the device copy is shared
-    probe.a_form = probe.b_form = 0;
-    const size_t bytes_ws = oz ? ozaki_scratch_bytes(probe) : 0;
-    const size_t bytes_c0 = (oz && read_c && kblock_count(g) > 1 && !formed) ? bytes_c : 0;
+    const IncoreBytes ib = incore_bytes(g, mode);
     const size_t budget = default_budget(c);
 
     HostPin pins;
-    const size_t total = bytes_a + bytes_b + bytes_c + bytes_c0 + bytes_ws;
     // out of core, a symmetric / Hermitian operand (SYMM, HEMM) is read tile by
     // tile from its stored triangle (tiled_host_gemm)
-    if (total > budget && need_ab) {
+    if (ib.total() > budget && need_ab) {
         // out-of-core: HBM tile cache under the byte budget; each K-step on
         // the emulated path when the precision mode picks it for a step's shape
         const int T = pick_tile(g);
-        Gemm step = g;
-        step.M = std::min<int64_t>(g.M, T);
-        step.N = std::min<int64_t>(g.N, T);
-        step.K = std::min<int64_t>(g.K, T);
-        step.lda = step.ldb = step.ldc = T;
-        step.B = nullptr;  // a step's A and B tiles sit in separate slots, even for SYRK
-        const size_t step_ws = want_ozaki(step, mode) ? ozaki_scratch_bytes(step) : 0;
-        const int st_code = tiled_host_gemm(g, c, budget, T, 0, step_ws, mode);
+        const int st_code = tiled_host_gemm(g, c, budget, T, 0, tile_step_ws(g, T, mode), mode);
         st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return st_code;
     }
@@ -730,13 +894,13 @@ int host_gemm(const Gemm &g) {
     BX_TRY(pins.pin(g.B, need_ab && !d.b_is_a ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
     BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
     if (need_ab) {
-        BX_CUDA(cudaMallocAsync(&d.A, bytes_a ? bytes_a : 256, c->compute));
+        BX_CUDA(cudaMallocAsync(&d.A, ib.a ? ib.a : 256, c->compute));
         if (d.b_is_a) d.B = d.A;
-        else BX_CUDA(cudaMallocAsync(&d.B, bytes_b ? bytes_b : 256, c->compute));
+        else BX_CUDA(cudaMallocAsync(&d.B, ib.b ? ib.b : 256, c->compute));
     }
-    BX_CUDA(cudaMallocAsync(&d.C, bytes_c, c->compute));
-    if (oz) BX_CUDA(cudaMallocAsync(&d.ws, bytes_ws, c->compute));
-    if (bytes_c0) BX_CUDA(cudaMallocAsync(&d.C0, bytes_c0, c->compute));
+    BX_CUDA(cudaMallocAsync(&d.C, ib.c, c->compute));
+    if (oz) BX_CUDA(cudaMallocAsync(&d.ws, ib.ws, c->compute));
+    if (ib.c0) BX_CUDA(cudaMallocAsync(&d.C0, ib.c0, c->compute));
     const int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
                       : incore_native(g, c, d, need_ab, read_c, st);
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

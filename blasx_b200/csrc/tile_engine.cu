@@ -88,6 +88,11 @@ size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es) {
     return (size_t(ld) * size_t(cols - 1) + size_t(rows)) * es;
 }
 
+size_t tiled_min_bytes(DType dt, int T, size_t ws_bytes) {
+    const size_t ws_reserve = ws_bytes ? ((ws_bytes + 255) & ~size_t(255)) + 256 : 0;
+    return size_t(kCSlots + 2) * size_t(T) * T * elem_size(dt) + ws_reserve;
+}
+
 int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy, size_t ws_bytes,
                     int mode) {
     blasx_call_stats &st = call_stats();

@@ -29,6 +29,10 @@ size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es);
 int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int tile, int policy,
                     size_t ws_bytes = 0, int mode = 0);
 
+// The smallest budget tiled_host_gemm accepts for tile edge T and a step
+// scratch of ws_bytes: the C tiles and two operand tiles beside the scratch.
+size_t tiled_min_bytes(DType dt, int T, size_t ws_bytes);
+
 // Frees the arena (blasx_finalize).
 void release_tile_arena();
 

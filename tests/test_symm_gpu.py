@@ -409,9 +409,54 @@ def test_trmm_streams_b_rows_beyond_the_budget(blx):
         blx.set_hbm_budget(0)
 
 
+@pytest.mark.parametrize("fn", ["trsm", "trmm"])
+@pytest.mark.parametrize("side,uplo,trans,diag", [("L", "L", "N", "N"), ("L", "U", "T", "U"), ("R", "U", "N", "N"),
+                                                  ("R", "L", "T", "N")])
+def test_tri_halves_an_a_beyond_the_budget(blx, mode, fn, side, uplo, trans, diag):
+    """A of order 1700 (23 MB) under a 12 MiB budget with 256-edge tiles: the
+    order is halved on the host (pieces of at most 1024, some halved again),
+    the off-diagonal blocks run as host GEMMs through the tile cache, and the
+    result is within the backward-error bound (solve) or the componentwise
+    bound (multiply); B's padding rows are not touched."""
+    blx.set_hbm_budget(12 << 20)
+    blx.set_tile(256)
+    try:
+        K, nv = 1700, 300
+        M, N = (K, nv) if side == "L" else (nv, K)
+        A = dominant_triangle(np.float64, K, uplo, diag, 121)
+        B0 = oracle.uniform((M + 1, N), np.float64, 122)
+        B = B0.copy(order="F")
+        getattr(blx, f"cblas_d{fn}")(102, blx.SIDE[side], blx.UPLO[uplo], blx.TRANS[trans], blx.DIAG[diag], M, N,
+                                     0.75, A, K, B, M + 1)
+        assert blx.last_status() == blx.BLASX_OK, blx.last_error()
+        st = blx.call_stats()
+        assert 0 < st["tile"] <= 1024 and st["path"] == (2 if mode == "ozaki" else 1), st
+        assert st["h2d_bytes"] > 0 and st["d2h_bytes"] > 0
+    finally:
+        blx.set_hbm_budget(0)
+        blx.set_tile(0)
+    assert np.array_equal(B[M:], B0[M:]) and np.all(np.isfinite(B))
+    Af = oracle.complete("T", uplo, A, K, diag)
+    if fn == "trmm":
+        Z = np.zeros_like(B0)
+        if side == "L":
+            check_dd(B, trans, "N", M, N, K, 0.75, Af, K, B0, M + 1, 0.0, Z, M + 1, 123)
+        else:
+            check_dd(B, "N", trans, M, N, K, 0.75, B0, M + 1, Af, K, 0.0, Z, M + 1, 123)
+        return
+    ii, jj = sample(M, N, 124)
+    if side == "L":
+        val, bound = oracle.dd_entries(trans, "N", M, N, K, 1.0, Af, K, B, M + 1, -0.75, B0, M + 1, ii, jj)
+    else:
+        val, bound = oracle.dd_entries("N", trans, M, N, K, 1.0, B, M + 1, Af, K, -0.75, B0, M + 1, ii, jj)
+    assert np.max(np.abs(val) / (2 * (K + 2) * 2.0 ** -53 * bound)) <= 1.0
+
+
 def test_tri_beyond_the_budget(blx):
-    """alpha = 0 streams zeros into B without reading A; an A that does not fit
-    the budget is reported, and B is left unchanged."""
+    """alpha = 0 streams zeros into B without reading A. An A beyond a 4 MB
+    budget is halved on the host only when the halves' update GEMM can run:
+    with the default tile edge (4096) it cannot, the call is refused before
+    any work and B is left unchanged."""
     blx.set_hbm_budget(4 << 20)
     try:
         M, N = 1024, 1024  # A alone is 8 MB
