@@ -231,10 +231,33 @@ void cblas_ztrmm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
                  const enum CBLAS_DIAG Diag, const int M, const int N, const void *alpha,
                  const void *A, const int lda, void *B, const int ldb);
 
+/* Replace cblas_strsm / cblas_dtrsm / cblas_ctrsm / cblas_ztrsm
+ * (include/cblas.h:448,478,508,538; implementations blas/dtrsm.c:16-75 and
+ * siblings, host BLAS only): solves op(A) X = alpha B (Side Left) or
+ * X op(A) = alpha B (Right) for X, which overwrites B; A triangular (Uplo,
+ * Diag), op(A) = A, A^T or A^H. Only the Uplo triangle of A is read, and not
+ * its diagonal when Diag is CblasUnit. */
+void cblas_strsm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const float alpha,
+                 const float *A, const int lda, float *B, const int ldb);
+void cblas_dtrsm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const double alpha,
+                 const double *A, const int lda, double *B, const int ldb);
+void cblas_ctrsm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, void *B, const int ldb);
+void cblas_ztrsm(const enum CBLAS_ORDER Order, const enum CBLAS_SIDE Side,
+                 const enum CBLAS_UPLO Uplo, const enum CBLAS_TRANSPOSE TransA,
+                 const enum CBLAS_DIAG Diag, const int M, const int N, const void *alpha,
+                 const void *A, const int lda, void *B, const int ldb);
+
 /* Replace the F77 wrappers ?symm_ (blas/dsymm.c:74-95), ?hemm_ (blas/zhemm.c:
- * 80-99) and ?trmm_ (blas/dtrmm.c:67-91): side 'L'/'R', uplo 'U'/'L', transa
- * 'N'/'T'/'C', diag 'N'/'U', column-major, every argument by pointer; complex
- * scalars are (re, im) pairs. */
+ * 80-99), ?trmm_ (blas/dtrmm.c:67-91) and ?trsm_ (blas/dtrsm.c:78-100): side
+ * 'L'/'R', uplo 'U'/'L', transa 'N'/'T'/'C', diag 'N'/'U', column-major, every
+ * argument by pointer; complex scalars are (re, im) pairs. */
 void ssymm_(char *side, char *uplo, int *m, int *n, float *alpha, float *A, int *lda, float *B,
             int *ldb, float *beta, float *C, int *ldc);
 void dsymm_(char *side, char *uplo, int *m, int *n, double *alpha, double *A, int *lda, double *B,
@@ -254,6 +277,14 @@ void dtrmm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, do
 void ctrmm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, float *alpha,
             float *A, int *lda, float *B, int *ldb);
 void ztrmm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, double *alpha,
+            double *A, int *lda, double *B, int *ldb);
+void strsm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, float *alpha,
+            float *A, int *lda, float *B, int *ldb);
+void dtrsm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, double *alpha,
+            double *A, int *lda, double *B, int *ldb);
+void ctrsm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, float *alpha,
+            float *A, int *lda, float *B, int *ldb);
+void ztrsm_(char *side, char *uplo, char *transa, char *diag, int *m, int *n, double *alpha,
             double *A, int *lda, double *B, int *ldb);
 
 /* Replaces xerbla_, blas/error.c:5: prints

@@ -37,6 +37,12 @@ int main(void) {
     fflush(stdout);
     cblas_dtrmm(CblasColMajor, CblasRight, CblasLower, CblasTrans, (enum CBLAS_DIAG)7, 4, 4, 1.0, A, 4, C, 4);
     fflush(stdout);
+    /* DTRSM: ldb = 2 < M = 4: parameter 11; F77 dtrsm_: bad side */
+    cblas_dtrsm(CblasColMajor, CblasLeft, CblasUpper, CblasNoTrans, CblasNonUnit, 4, 4, 1.0, A, 4, C, 2);
+    fflush(stdout);
+    char sd = 'X', up = 'U', tn = 'N', dg = 'N';
+    dtrsm_(&sd, &up, &tn, &dg, &m, &n, &al, A, &ld, C, &ld);
+    fflush(stdout);
     /* M = 0: quick return, no device needed */
     cblas_dgemm(CblasColMajor, CblasNoTrans, CblasNoTrans, 0, 4, 4, 1.0, A, 4, B, 4, 0.0, C, 4);
     printf("status=%d C0=%g\n", blasx_last_status(), C[0]);

@@ -15,8 +15,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_library_exports_declared_symbols(blx):
     names = blx.declared_symbols()
-    for required in ("cblas_sgemm", "cblas_dgemm", "cblas_zgemm", "sgemm_", "dgemm_", "zgemm_", "xerbla_"):
-        assert required in names
+    required = ["cblas_sgemm", "cblas_dgemm", "cblas_zgemm", "sgemm_", "dgemm_", "zgemm_", "xerbla_",
+                "cblas_cgemm", "cgemm_"]
+    for fam, types in (("syrk", "sdcz"), ("syr2k", "sdcz"), ("herk", "cz"), ("her2k", "cz"), ("symm", "sdcz"),
+                       ("hemm", "cz"), ("trmm", "sdcz"), ("trsm", "sdcz")):
+        required += [f"cblas_{t}{fam}" for t in types] + [f"{t}{fam}_" for t in types]
+    missing_decl = [n for n in required if n not in names]
+    assert not missing_decl, missing_decl
     out = subprocess.run(["nm", "-D", "--defined-only", blx.LIB_PATH], capture_output=True, text=True).stdout
     exported = {l.split()[-1] for l in out.splitlines() if len(l.split()) >= 3}
     missing = [n for n in names if n not in exported]

@@ -24,5 +24,7 @@ def test_c_program_links_and_reports(blx, tmp_path):
     assert " ** On entry to DSYMM  parameter number  9 had an illegal value\n" in out
     assert " ** On entry to  ZHEMM parameter number  1 had an illegal value\n" in out
     assert " ** On entry to DTRMM  parameter number  4 had an illegal value\n" in out
+    assert " ** On entry to DTRSM  parameter number 11 had an illegal value\n" in out
+    assert " ** On entry to DTRSM  parameter number  1 had an illegal value\n" in out
     assert "status=1" in out and "status=0 C0=1" in out
     assert "plan rc=0 loads=200 min_ratio=1.000" in out
