@@ -461,7 +461,7 @@ struct TriBlocks {
 //   solve:    B_i = alpha B_i - op(A)[i, before] X_before (one GEMM), then
 //             the solve of block i against its diagonal block;
 //   multiply: out of place into R (the earlier blocks' original values are
-//             still needed): R_i = B_i, R_i = alpha S_ii R_i, then
+//             still needed): R_i = alpha S_ii B_i (trmm_part_into), then
 //             R_i += alpha op(A)[i, before] B_before (one GEMM).
 // The strip is stored as rows i x the blocks up to i (left NoTrans, right
 // Trans) or the transpose.
@@ -484,8 +484,6 @@ static int tri_streamed(const Trsm &t, const Trsm &dt, const DeviceOps &d, Conte
         return BLASX_OK;
     };
     const bool strip_rows = t.left == (t.trans == NoTrans);
-    Trsm dr = dt;  // the multiply's view of the result buffer
-    dr.B = d.C;
     for (int i = 0; i < tb.n; ++i) {
         int64_t lo, hi, dlo, dhi;
         tb.block(i, &lo, &hi, &dlo, &dhi);
@@ -501,9 +499,7 @@ static int tri_streamed(const Trsm &t, const Trsm &dt, const DeviceOps &d, Conte
         st.h2d_bytes += double(es) * (double(arow1 - arow0) * (acol1 - acol0) + double(rows) * cols);
         BX_TRY(handoff(c->h2d, c->compute));
         if (mult) {
-            BX_CUDA(cudaMemcpy2DAsync(part(d.C, d.ldb, lo), d.ldb * es, part(d.B, d.ldb, lo), d.ldb * es, rows * es,
-                                      cols, cudaMemcpyDeviceToDevice, c->compute));
-            BX_TRY(trmm_part(dr, lo, hi, w, c->compute, emulated));
+            BX_TRY(trmm_part_into(dt, d.C, lo, hi, w, c->compute, emulated));
             if (dlo < dhi) BX_TRY(trmm_update_into(dt, d.C, lo, hi, dlo, dhi, c->compute, emulated));
         } else if (dlo < dhi) {
             BX_TRY(trsm_update_part(dt, lo, hi, dlo, dhi, t.alpha, c->compute, emulated));

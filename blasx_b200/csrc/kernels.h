@@ -73,13 +73,16 @@ struct TrmmScratch {
 };
 TrmmScratch trmm_scratch_sizes(const Trsm &t);
 int trmm_device(const Trsm &t, const TrmmScratch &w, cudaStream_t s, bool *emulated);
-// trmm_part multiplies rows (left) or columns (right) [lo, hi) of B in place
-// by alpha times their diagonal block; trmm_update_into adds alpha
-// op(A)[tgt, src] B[src] (or B[:, src] op(A)[src, tgt]) to block tgt of dst, a
-// device buffer with B's layout. Out of place, blocks multiplied in
-// substitution order, each followed by the update from the blocks before it
-// (B's original values), give trmm_device.
-int trmm_part(const Trsm &t, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s, bool *emulated);
+// Parts of an out-of-place multiply into dst, a device buffer with B's
+// layout; B is left unchanged. trmm_part_into writes rows (left) or columns
+// (right) [lo, hi) of dst: alpha times their diagonal block times B's (its
+// leaves multiply straight from B, without the staging copy of the in-place
+// form). trmm_update_into adds alpha op(A)[tgt, src] B[src] (or B[:, src]
+// op(A)[src, tgt]) to block tgt of dst. Every block's product, followed by
+// the update from the blocks before it in substitution order, gives
+// trmm_device's result.
+int trmm_part_into(const Trsm &t, void *dst, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s,
+                   bool *emulated);
 int trmm_update_into(const Trsm &t, void *dst, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi,
                      cudaStream_t s, bool *emulated);
 Gemm trmm_top_update(const Trsm &t);

@@ -342,6 +342,53 @@ int multiply(const Trsm &t, Range r, const TrmmScratch &w, cudaStream_t s, bool 
     return multiply(t, second, w, s, emulated);
 }
 
+// The same product out of place: part r of dst (B's layout) = alpha S_rr
+// B_r, B unchanged. A leaf multiplies B's rows (or columns) by the completed
+// diagonal block straight into dst, with no staging copy; every update
+// reads B's original values, so the halves may go in either order.
+int leaf_into(const Trsm &t, void *dst, Range r, const TrmmScratch &w, cudaStream_t s) {
+    const size_t es = elem_size(t.dt);
+    const int64_t bs = r.size();
+    const char *A = static_cast<const char *>(t.A);
+    const char *B = static_cast<const char *>(t.B);
+    char *D = static_cast<char *>(dst);
+    BX_CUDA(cudaMemcpy2DAsync(w.diag, size_t(kTrmmLeaf) * es, A + (r.lo + r.lo * t.lda) * es, size_t(t.lda) * es,
+                              size_t(bs) * es, size_t(bs), cudaMemcpyDeviceToDevice, s));
+    const int form = t.lower ? (t.unit ? kTriLowerUnit : kTriLower) : (t.unit ? kTriUpperUnit : kTriUpper);
+    BX_TRY(launch_complete_operand(t.dt, form, w.diag, kTrmmLeaf, bs, s));
+    const int tr = (t.trans == ConjT && !is_complex(t.dt)) ? TransT : t.trans;
+    Gemm g;
+    g.dt = t.dt;
+    g.alpha = t.alpha;
+    g.beta = cplx{0.0, 0.0};
+    g.K = bs;
+    if (t.left) {  // rows r: D_r = alpha op(A_rr) B_r
+        g.M = bs; g.N = t.N;
+        g.ta = tr; g.A = w.diag; g.lda = kTrmmLeaf;
+        g.tb = NoTrans; g.B = B + r.lo * es; g.ldb = t.ldb;
+        g.C = D + r.lo * es;
+    } else {  // columns r: D_r = alpha B_r op(A_rr)
+        g.M = t.M; g.N = bs;
+        g.ta = NoTrans; g.A = B + r.lo * t.ldb * es; g.lda = t.ldb;
+        g.tb = tr; g.B = w.diag; g.ldb = kTrmmLeaf;
+        g.C = D + r.lo * t.ldb * es;
+    }
+    g.ldc = t.ldb;
+    return dmma_supported(g) ? launch_gemm_dmma(g, s) : launch_gemm_simt(g, s);
+}
+
+int multiply_into(const Trsm &t, void *dst, Range r, const TrmmScratch &w, cudaStream_t s, bool *emulated) {
+    if (r.size() <= kTrmmLeaf) return leaf_into(t, dst, r, w, s);
+    Range first, second;
+    trmm_split(t, r, &first, &second);
+    BX_TRY(multiply_into(t, dst, first, w, s, emulated));
+    Gemm g = update_gemm(t, first, second, t.alpha, kOne);
+    g.C = static_cast<char *>(dst) + (static_cast<char *>(g.C) - static_cast<char *>(t.B));
+    BX_TRY(device_gemm(g, s));
+    if (call_stats().path == 2) *emulated = true;
+    return multiply_into(t, dst, second, w, s, emulated);
+}
+
 }  // namespace
 
 bool tri_forward(const Trsm &t) { return forward_of(t); }
@@ -402,8 +449,9 @@ TrmmScratch trmm_scratch_sizes(const Trsm &t) {
     return w;
 }
 
-int trmm_part(const Trsm &t, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s, bool *emulated) {
-    return multiply(t, Range{lo, hi}, w, s, emulated);
+int trmm_part_into(const Trsm &t, void *dst, int64_t lo, int64_t hi, const TrmmScratch &w, cudaStream_t s,
+                   bool *emulated) {
+    return multiply_into(t, dst, Range{lo, hi}, w, s, emulated);
 }
 
 int trmm_update_into(const Trsm &t, void *dst, int64_t tgt_lo, int64_t tgt_hi, int64_t src_lo, int64_t src_hi,
