@@ -423,15 +423,19 @@ bool host_gemm_fits(const Gemm &g, int mode, size_t budget) {
 // The blocks of the streamed triangular pipeline: the order K of the
 // triangle cut into n blocks of b rows (left) or columns (right), taken in
 // substitution order (tri_forward: ascending), the block taken last ragged.
-// Up to 8 blocks of at least 2048 (2 for K below 4096): fewer blocks leave
-// longer copies at the start and end uncovered, more blocks shrink the
-// update GEMMs (the emulated path slices the blocks before each one again).
+// A solve takes up to 8 blocks of at least 2048, a multiply up to 16 of at
+// least 1024 (2 for smaller K): fewer blocks leave longer copies at the
+// start and end uncovered, more blocks shrink the update GEMMs (the emulated
+// path slices the blocks before each one again). At 16384 these counts
+// measured fastest among 4, 6, 8, 12 and 16: a multiply's diagonal blocks
+// of 1024 keep their inner updates on the native kernels.
 struct TriBlocks {
     int64_t K = 0, b = 0;
     int n = 0;
     bool fwd = true;
-    explicit TriBlocks(const Trsm &t) : K(t.order()), fwd(tri_forward(t)) {
-        const int64_t parts = std::min<int64_t>(8, std::max<int64_t>(2, K / 2048));
+    TriBlocks(const Trsm &t, bool mult) : K(t.order()), fwd(tri_forward(t)) {
+        const int64_t parts = mult ? std::min<int64_t>(16, std::max<int64_t>(2, K / 1024))
+                                   : std::min<int64_t>(8, std::max<int64_t>(2, K / 2048));
         b = round_up((K + parts - 1) / parts, 256);
         n = int((K + b - 1) / b);
     }
@@ -665,7 +669,7 @@ static int host_tri(const Trsm &t, bool mult) {
     const size_t bytes_a = need_a ? size_t(d.lda) * K * es : 0;
     const size_t bytes_b = size_t(d.ldb) * t.N * es;
     auto ws_of = [&](const Gemm &g) { return g.K > 0 && ozaki_selected(g, mode) ? ozaki_scratch_bytes(g) : size_t(0); };
-    const TriBlocks tb(dt);
+    const TriBlocks tb(dt, mult);
     const bool split = need_a && tb.n > 1;
     size_t bytes_ws = 0, bytes_r = 0;
     if (need_a) {

@@ -333,9 +333,10 @@ def test_symm_out_of_core(blx, side, uplo, dt, herm, emulated):
 @pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "N"), ("U", "N", "U"), ("L", "T", "N")])
 def test_tri_streams_the_order_in_blocks(blx, mode, fn, side, uplo, trans, diag):
     """An order of 6200 is copied, solved or multiplied and copied back in
-    three blocks of 2304 (the last ragged), ascending or descending with the
-    substitution order (both occur on each side); the result is within the
-    backward-error bound (solve) or the componentwise bound (multiply)."""
+    blocks: three of 2304 for the solve, five of 1280 for the multiply (the
+    last ragged), ascending or descending with the substitution order (both
+    occur on each side); the result is within the backward-error bound
+    (solve) or the componentwise bound (multiply)."""
     K, nv = 6200, 96
     M, N = (K, nv) if side == "L" else (nv, K)
     A = dominant_triangle(np.float64, K, uplo, diag, 111)
@@ -345,7 +346,7 @@ def test_tri_streams_the_order_in_blocks(blx, mode, fn, side, uplo, trans, diag)
                                  A, K, B, M + 1)
     assert blx.last_status() == blx.BLASX_OK, blx.last_error()
     st = blx.call_stats()
-    assert st["tile"] == 2304 and st["path"] == (2 if mode == "ozaki" else 1), st
+    assert st["tile"] == (1280 if fn == "trmm" else 2304) and st["path"] == (2 if mode == "ozaki" else 1), st
     assert np.array_equal(B[M:], B0[M:]) and np.all(np.isfinite(B))
     Af = oracle.complete("T", uplo, A, K, diag)
     if fn == "trmm":
