@@ -578,6 +578,7 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
     DeviceOps d;
     d.s = c->compute;
+    StreamDrain drain{c};  // before d and pins go, on every return
     if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, c->compute));
     BX_CUDA(cudaMallocAsync(&d.B, 2 * panel_bytes, c->compute));
     if (mult && need_a) {
@@ -694,6 +695,7 @@ static int host_tri(const Trsm &t, bool mult) {
     HostPin pins;
     BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
+    StreamDrain drain{c};  // before d and pins go, on every return
     cudaStream_t s = c->compute;
     if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, s));
     BX_CUDA(cudaMallocAsync(&d.B, bytes_b, s));  // alpha == 0 writes zeros without reading B
@@ -893,6 +895,7 @@ int host_gemm(const Gemm &g) {
     BX_TRY(pins.pin(g.A, need_ab ? host_extent(g.lda, g.rows_a(), g.cols_a(), es) : 0));
     BX_TRY(pins.pin(g.B, need_ab && !d.b_is_a ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
     BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
+    StreamDrain drain{c};  // before d and pins go, on every return
     if (need_ab) {
         BX_CUDA(cudaMallocAsync(&d.A, ib.a ? ib.a : 256, c->compute));
         if (d.b_is_a) d.B = d.A;

@@ -125,6 +125,7 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
     BX_TRY(pins.pin(g.A, host_extent(g.lda, g.rows_a(), g.cols_a(), es)));
     BX_TRY(pins.pin(g.B, host_extent(g.ldb, g.rows_b(), g.cols_b(), es)));
     BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
+    StreamDrain drain{c};  // before pins go, on every return
 
     EventPool pool;
     std::vector<cudaEvent_t> ready(static_cast<size_t>(op_slots)), lastuse(static_cast<size_t>(op_slots));

@@ -16,6 +16,21 @@ struct HostPin {
     ~HostPin();
 };
 
+// Waits for the context's three streams when it goes out of scope. Declared
+// after a call's device buffers and host pins, it runs before they are freed
+// or unregistered, so that an early error return does neither while a copy
+// or kernel of the call is still in flight. On the success path the streams
+// are already idle.
+struct StreamDrain {
+    Context *c;
+    ~StreamDrain() {
+        if (!c) return;
+        cudaStreamSynchronize(c->h2d);
+        cudaStreamSynchronize(c->compute);
+        cudaStreamSynchronize(c->d2h);
+    }
+};
+
 // Bytes spanned by a column-major rows x cols matrix with leading dimension ld.
 size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es);
 
