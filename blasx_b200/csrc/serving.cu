@@ -480,6 +480,12 @@ void finish(Server &s, Request *r, int status) {
     cudaStream_t st = s.streams[size_t(r->stream_slot)];
     const Gemm &g = r->g;
     const size_t es = elem_size(g.dt);
+    if (status != BLASX_OK) {
+        // a request that failed part-way may still have copies in flight on
+        // its stream: its blocks go back to the arena only after them
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+    }
     if (r->emulated && r->ws && status == BLASX_OK && s.err_words[r->stream_slot] != 0) {
         set_error(BLASX_ERR_TIMEOUT, "serving: emulated GEMM's bounded device wait expired (flag %d)",
                   s.err_words[r->stream_slot]);
