@@ -790,24 +790,39 @@ int tri_run(const Trsm &t, bool mult, int mode, size_t budget, blasx_call_stats 
     return rc;
 }
 
+// The halves of a host halving, in the order they run: first [f0, f1),
+// then second [s0, s1); the lower part is [0, m), the upper [m, K).
+struct TriHalves {
+    int64_t f0, f1, s0, s1;
+    TriHalves(const Trsm &t, bool mult) {
+        const int64_t K = t.order(), m = host_half(K);
+        const bool fwd = tri_forward(t);
+        const bool lower_first = mult ? !fwd : fwd;
+        f0 = lower_first ? 0 : m; f1 = lower_first ? m : K;
+        s0 = lower_first ? m : 0; s1 = lower_first ? K : m;
+    }
+    // the off-diagonal update: the second half from the first (solve), or
+    // the first from the second (multiply); alpha and beta as tri_split sets them
+    Gemm update(const Trsm &t, bool mult) const {
+        if (mult) return tri_update_gemm(t, f0, f1, s0, s1);
+        Gemm g = tri_update_gemm(t, s0, s1, f0, f1);
+        g.alpha = cplx{-1.0, 0.0};
+        g.beta = t.alpha;
+        return g;
+    }
+};
+
 int tri_split(const Trsm &t, bool mult, int mode, size_t budget, blasx_call_stats &agg) {
-    const int64_t K = t.order(), m = host_half(K);
-    const bool fwd = tri_forward(t);
-    // lower part [0, m), upper part [m, K)
-    const bool lower_first = mult ? !fwd : fwd;
-    const int64_t f0 = lower_first ? 0 : m, f1 = lower_first ? m : K;
-    const int64_t s0 = lower_first ? m : 0, s1 = lower_first ? K : m;
+    const TriHalves h(t, mult);
+    const int64_t f0 = h.f0, f1 = h.f1, s0 = h.s0, s1 = h.s1;
     if (mult) {
         BX_TRY(tri_run(tri_piece(t, f0, f1, t.alpha), true, mode, budget, agg));
-        BX_TRY(host_gemm(tri_update_gemm(t, f0, f1, s0, s1)));
+        BX_TRY(host_gemm(h.update(t, true)));
         merge_stats(agg, call_stats());
         return tri_run(tri_piece(t, s0, s1, t.alpha), true, mode, budget, agg);
     }
     BX_TRY(tri_run(tri_piece(t, f0, f1, t.alpha), false, mode, budget, agg));
-    Gemm g = tri_update_gemm(t, s0, s1, f0, f1);
-    g.alpha = cplx{-1.0, 0.0};
-    g.beta = t.alpha;
-    BX_TRY(host_gemm(g));
+    BX_TRY(host_gemm(h.update(t, false)));
     merge_stats(agg, call_stats());
     return tri_run(tri_piece(t, s0, s1, cplx{1.0, 0.0}), false, mode, budget, agg);
 }
@@ -835,8 +850,7 @@ int host_tri_entry(const Trsm &t, bool mult) {
     if (!tri_fits(tri_piece(t, 0, o, t.alpha), mult, mode, budget))
         return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: the HBM budget (%zu bytes) holds no piece of A "
                          "with room for panels of B", mult ? "multiply" : "solve", budget);
-    const int64_t m = host_half(K);
-    const Gemm top = tri_update_gemm(t, m, K, 0, m);  // the largest update (sizes only)
+    const Gemm top = TriHalves(t, mult).update(t, mult);  // the largest update
     if (!host_gemm_fits(top, mode, budget))
         return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: the HBM budget (%zu bytes) cannot hold the "
                          "update GEMM of its halves (tile edge %d)", mult ? "multiply" : "solve", budget,
