@@ -38,6 +38,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PUBLISHED_BLASX_1GPU_16384_GFLOPS = 1153.4  # performance_data/GEMM.xlsx row 17 col D
+# CPU seconds the whole reference arm (warm-up and timed slabs) aims at
+REFERENCE_ARM_SECONDS = 150.0
 
 
 def parse():
@@ -173,10 +175,11 @@ def reference_cpu_sample(n: int, seconds: float, cores: int, steps: int = 1, war
         gemm = ref.gemm
     T = 1000
 
+    A = oracle.spread((n, n), 1, 0.0)
+    B = oracle.spread((n, n), 2, 0.0)
+    C = oracle.spread((n, n), 3, 0.0)  # each slab updates its first ns columns in place
+
     def run(ns):
-        A = oracle.spread((n, n), 1, 0.0)
-        B = oracle.spread((n, ns), 2, 0.0)
-        C = oracle.spread((n, ns), 3, 0.0)
         t0 = time.perf_counter()
         for j0 in range(0, ns, T):
             nj = min(T, ns - j0)
@@ -188,9 +191,12 @@ def reference_cpu_sample(n: int, seconds: float, cores: int, steps: int = 1, war
                     gemm("N", "N", mi, nj, kk, 1.0, A[i0:, k0:], n, B[k0:, j0:], n, beta, C[i0:, j0:], n)
         return time.perf_counter() - t0
 
-    t = run(min(n, 1000))  # calibration slab
-    rate = 2.0 * n * n * min(n, 1000) / t
-    ns = int(max(1000, min(n, rate * seconds / (2.0 * n * n))) // 1000 * 1000)
+    # calibration on a slab of 250 columns (a quarter of a tile call); the
+    # timed slabs are whole multiples of 250 columns, at least one
+    cal = min(n, 250)
+    t = run(cal)
+    rate = 2.0 * n * n * cal / t
+    ns = int(max(cal, min(n, rate * seconds / (2.0 * n * n))) // cal * cal)
     out = []
     for s in range(warmup + steps):
         dt = run(ns)
@@ -198,7 +204,7 @@ def reference_cpu_sample(n: int, seconds: float, cores: int, steps: int = 1, war
             out.append(2.0 * n * n * ns / dt / 1e12)
     sample = (f"C[:, :{ns}] of the {n}^3 DGEMM ({2.0 * n * n * ns / 1e12:.2f} TFLOP) as {T}-sized tile calls "
               f"through the reference's cblas_dgemm CPU path")
-    return out, sample, kind, (ref.name if hasattr(ref, "name") else oracle.REF_PATH)
+    return out, sample, kind, (ref.name if hasattr(ref, "name") else oracle.REF_PATH), ns
 
 
 def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, seed: int = 7,
@@ -354,6 +360,37 @@ def _accuracy(C, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, dtype, n
     val, bound = oracle.dd_entries(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, ii, jj)
     dt = {"f64": np.float64, "f32": np.float32, "c128": np.complex128}[dtype]
     return oracle.componentwise_ratio(C, ii, jj, val, bound, K, dt)
+
+
+def sampled_error_device(torch, A, B, C0, C, n, alpha, beta, rows=100, cols=1000, seed=11):
+    """Componentwise error of a device-resident n^3 GEMM result on a sample of
+    rows x cols entries, against the double-double oracle.
+
+    A, B, C0, C are torch (n, n) tensors whose storage holds the column-major
+    matrices (element (i, j) at [j, i]); C = alpha A B + beta C0. Only the
+    sampled rows of A, columns of B and entries of C0 and C leave the device.
+    Returns {"samples", "bound_ratio", "max_norm_err"}: the largest ratio of
+    |C - C*| to the (K+2) u (|alpha||A||B| + |beta||C0|) bound, and the
+    largest |C - C*| / (|alpha||A||B| + |beta||C0|)."""
+    import numpy as np
+
+    import oracle
+    rng = np.random.default_rng(seed)
+    ri = np.sort(rng.choice(n, size=min(rows, n), replace=False))
+    cj = np.sort(rng.choice(n, size=min(cols, n), replace=False))
+    rt = torch.from_numpy(ri).to(A.device)
+    ct = torch.from_numpy(cj).to(A.device)
+    # op(A) rows as a K x R column-major block (transa 'T'), B columns as K x C
+    At = np.asfortranarray(A.index_select(1, rt).cpu().numpy())           # (K, R): At[k, r] = A(ri[r], k)
+    Bs = np.asfortranarray(B.index_select(0, ct).cpu().numpy().T)         # (K, C): Bs[k, c] = B(k, cj[c])
+    C0s = np.asfortranarray(C0.index_select(0, ct).index_select(1, rt).cpu().numpy().T)  # (R, C)
+    Cs = np.asfortranarray(C.index_select(0, ct).index_select(1, rt).cpu().numpy().T)
+    R, Cc = ri.size, cj.size
+    ii = np.repeat(np.arange(R), Cc)
+    jj = np.tile(np.arange(Cc), R)
+    val, bound = oracle.dd_entries("T", "N", R, Cc, n, alpha, At, n, Bs, n, beta, C0s, R, ii, jj)
+    ratio, err = oracle.componentwise_ratio(Cs, ii, jj, val, bound, n, np.float64)
+    return {"samples": int(ii.size), "bound_ratio": ratio, "max_norm_err": err}
 
 
 def measure_peaks(torch):
@@ -798,6 +835,11 @@ def run_workloads(args):
         print(json.dumps(l), flush=True)
 
 
+def path_name(code: int) -> str:
+    """The call path recorded in the call statistics."""
+    return {1: "native", 2: "ozaki", 3: "scale", 4: "native (device fallback)"}.get(code, "?")
+
+
 def rank_barrier(dist) -> None:
     """All ranks reach this point before any goes on (no-op on one rank)."""
     if dist:
@@ -831,12 +873,20 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        vals, sample, kind, lib = reference_cpu_sample(n, args.cpu_seconds, cores, args.steps, args.warmup)
+        # Each step is one slab of the GEMM, sized so that all warm-up and
+        # timed steps together take about REFERENCE_ARM_SECONDS of CPU time.
+        per_step = min(args.cpu_seconds, REFERENCE_ARM_SECONDS / max(1, args.steps + args.warmup))
+        vals, sample, kind, lib, slab = reference_cpu_sample(n, per_step, cores, args.steps, args.warmup)
         v = statistics.median(vals)
+        slab_ms = [2.0 * n * n * slab / (x * 1e12) * 1e3 for x in vals]
         line = {"impl": "reference", "metric": "DGEMM TFLOP/s (FP64-accurate, emulated vs native)",
                 "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 2.0 * n ** 3 / (v * 1e12) * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                # a step is the slab actually timed, not the full GEMM
+                "ms_per_step": statistics.mean(slab_ms), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(config, step=f"slab C[:, :{slab}] of the {n}^3 GEMM ({2.0 * n * n * slab / 1e12:.2f} "
+                                            f"TFLOP per step)", slab_columns=slab),
+                "full_gemm_ms_extrapolated": 2.0 * n ** 3 / (v * 1e12) * 1e3, "extrapolated": True,
                 "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": kind, "sample": sample,
                                  "library": lib},
                 "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -886,15 +936,39 @@ def main():
     torch.cuda.synchronize()
     flops = 2.0 * n ** 3
 
-    def step():
-        st = bx.gemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.5, C, n, stream=stream)
+    def step(Ct=None):
+        st = bx.gemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.5, C if Ct is None else Ct, n, stream=stream)
         if st != 0:
             raise RuntimeError(bx.last_error())
+
+    def check_timed(C_start, steps):
+        """Measured error of the last of `steps` steps that took C from C_start
+        to C: the steps are replayed on a copy (every call is deterministic),
+        the replay's last result must equal C bit for bit, and C is checked
+        against the double-double oracle with the replay's input to that step."""
+        # clones run on torch's stream, the steps on `stream`: synchronise between them
+        torch.cuda.synchronize()
+        Cr = C_start.clone()
+        torch.cuda.synchronize()
+        for _ in range(steps - 1):
+            step(Cr)
+        torch.cuda.synchronize()
+        C_prev = Cr.clone()
+        torch.cuda.synchronize()
+        step(Cr)
+        torch.cuda.synchronize()
+        same = bool(torch.equal(Cr, C))
+        del Cr
+        out = sampled_error_device(torch, A, B, C_prev, C, n, 1.0, 0.5)
+        out["replay_bitexact"] = same
+        return out
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     stats = bx.call_stats()
+    C_start = C.clone()  # input of the first timed step, for the accuracy check
+    torch.cuda.synchronize()
 
     # --- timed region (device-resident) ---
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -914,11 +988,18 @@ def main():
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
     value = world * flops / (ms * 1e-3) / 1e12
 
+    # --- measured error of the timed result (outside the timed region) ---
+    accuracy = {"oracle": "double-double (Dot2) on sampled entries; bound (K+2) u (|alpha||A||B| + |beta||C0|)",
+                path_name(stats["path"]): check_timed(C_start, args.steps)}
+    del C_start
+
     # --- native FP64 path on the same inputs ---
     native = None
     if mode != bx.MODE_NATIVE:
         bx.set_dgemm_mode(bx.MODE_NATIVE)
         step(); torch.cuda.synchronize()
+        Cn_start = C.clone()
+        torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ns = max(1, min(args.steps, 2))
         barrier(); e0.record(stream)
@@ -927,13 +1008,15 @@ def main():
         e1.record(stream); torch.cuda.synchronize(); barrier()
         nms = max_over_ranks(e0.elapsed_time(e1) / ns)
         native = {"value": world * flops / (nms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": nms}
+        accuracy["native"] = check_timed(Cn_start, ns)
+        del Cn_start
         bx.set_dgemm_mode(mode)
 
     # --- pipe peaks on this box, measured now with the vendor library ---
     fp64_peak, int8_peak = measure_peaks(torch)
 
     per_gpu = flops / (ms * 1e-3) / 1e12
-    path = {1: "native", 2: "ozaki", 3: "scale", 4: "native (device fallback)"}.get(stats["path"], "?")
+    path = path_name(stats["path"])
     phase_ms = {k: v["ms"] / max(1, args.steps) for k, v in phases.items()}
     if stats["path"] == 2:
         gemm_ms = phase_ms["residue_gemm"]
@@ -971,17 +1054,40 @@ def main():
 
         host_step()
         ts = []
-        for _ in range(max(1, min(args.steps, 3))):
+        for _ in range(args.steps):
             barrier()
             t0 = time.perf_counter()
             host_step()
             ts.append(time.perf_counter() - t0)
-        e2e_s = max_over_ranks(statistics.median(ts))
+        e2e_s = max_over_ranks(statistics.mean(ts))
         hs = bx.call_stats()
         e2e = {"value": world * flops / e2e_s / 1e12, "unit": "TFLOP/s", "ms_per_step": e2e_s * 1e3,
+               "median_ms": statistics.median(ts) * 1e3,
                "h2d_bytes_per_step": int(hs["h2d_bytes"]), "d2h_bytes_per_step": int(hs["d2h_bytes"]),
-               "timing": "host wall clock around the synchronous cblas_dgemm call, median"}
+               "timing": f"host wall clock around each of {args.steps} synchronous cblas_dgemm calls on "
+                         "pinned host buffers, mean"}
         del Ah, Bh, Ch
+        # the same call on pageable host memory (plain numpy arrays), as most BLAS callers pass it
+        Ap = np.empty((n, n)); Ap[...] = A.cpu().numpy()
+        Bp = np.empty((n, n)); Bp[...] = B.cpu().numpy()
+        Cp = np.empty((n, n)); Cp[...] = C.cpu().numpy()
+
+        def pageable_step():
+            bx.cblas_dgemm(bx.CblasColMajor, bx.CblasNoTrans, bx.CblasNoTrans, n, n, n, 1.0, Ap.ctypes.data, n,
+                           Bp.ctypes.data, n, 0.5, Cp.ctypes.data, n)
+            if bx.last_status() != 0:
+                raise RuntimeError(bx.last_error())
+
+        tp = []
+        for _ in range(2):
+            barrier()
+            t0 = time.perf_counter()
+            pageable_step()
+            tp.append(time.perf_counter() - t0)
+        p_s = max_over_ranks(statistics.mean(tp))
+        e2e["pageable"] = {"value": world * flops / p_s / 1e12, "unit": "TFLOP/s", "ms_per_step": p_s * 1e3,
+                           "calls": len(tp), "timing": "the same call on pageable (unpinned) host arrays, mean"}
+        del Ap, Bp, Cp
 
     serving = None
     if args.serving > 0 and rank == 0:
@@ -989,7 +1095,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        vals, sample, kind, lib = reference_cpu_sample(n, args.cpu_seconds, cores, 1, 0)
+        vals, sample, kind, lib, _ = reference_cpu_sample(n, args.cpu_seconds, cores, 1, 0)
         cpu = {"value": vals[0], "unit": "TFLOP/s", "cores": cores, "kind": kind, "sample": sample}
 
     if rank == 0:
@@ -999,6 +1105,7 @@ def main():
                 "data": "synthetic", "config": config,
                 "path": path, "moduli": stats["moduli"], "phases_ms_per_step": phase_ms,
                 "fp64_equivalent": fp64_equiv, "native": native, "e2e": e2e, "roofline": roofline,
+                "accuracy": accuracy,
                 "cpu_baseline": cpu, "serving": serving, "gpu_launches": launches, "clocks": clk.summary(),
                 "vs_published_blasx_1gpu_16384": value * 1e3 / PUBLISHED_BLASX_1GPU_16384_GFLOPS}
         print(json.dumps(line), flush=True)
@@ -1006,11 +1113,20 @@ def main():
         dist.destroy_process_group()
 
 
-if __name__ == "__main__":
-    main()
-    # The reference library loaded for the CPU legs prints a line from its ELF
-    # destructor at exit (blas/blasx_tile_resource.c:57-80); leave without
-    # running destructors so that the JSON line stays the last line of stdout.
+def quiet_stdout_at_exit() -> None:
+    """Sends whatever is written to stdout from here on to /dev/null.
+
+    The reference library loaded for the CPU legs prints a line from its ELF
+    destructor when the process exits (blas/blasx_tile_resource.c:57-80). The
+    interpreter still exits normally (exit handlers and library destructors
+    run); only that late output no longer follows the JSON line."""
     sys.stdout.flush()
     sys.stderr.flush()
-    os._exit(0)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    os.close(devnull)
+
+
+if __name__ == "__main__":
+    main()
+    quiet_stdout_at_exit()

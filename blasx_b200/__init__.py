@@ -128,6 +128,7 @@ def lib() -> ctypes.CDLL:
         L.blasx_zgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
         L.blasx_cgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
         L.blasx_dgemm_device_noalloc.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
+        L.blasx_dgemm_device_noalloc_status.argtypes = [_P]
         L.blasx_kernel_launch_count.restype = ctypes.c_uint64
         L.blasx_tile_plan.argtypes = [ctypes.c_longlong] * 5 + [_I, _I, ctypes.POINTER(TilePlanStats)]
         L.blasx_serve_start.argtypes = [ctypes.c_size_t, ctypes.c_size_t, _I]

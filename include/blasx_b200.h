@@ -411,21 +411,34 @@ int blasx_dtrmm_device(int side, int uplo, int trans, int diag, int M, int N, do
  * cudaMalloc: a framework whose own allocator has already reserved the
  * GPU's memory (a cudaMalloc would fail or fragment that pool), or
  * latency-critical code where cudaMalloc / cudaFree may synchronise the
- * device. Same arguments and result as blasx_dgemm_device on the emulated
- * (INT8 Ozaki) path, with the native FP64 kernel chosen on the device when
- * the operands' spread is too wide; the caller still provides A, B and C.
- * Its scratch is a fixed 64 MiB device array that every GPU loading this
- * library holds until the process exits; problems whose scratch would not
- * fit (M = N = K = 1024 fits; 2048 does not) are rejected with
- * BLASX_ERR_UNSUPPORTED and a message in blasx_last_error(). The first call
- * on each device performs a one-time set-up there (it looks up the array's
- * device address and uploads constant tables); make that first call before
- * any stream capture. All calls share the one array: calls that overlap on
- * the GPU (other streams, other threads) race and must be serialised by the
- * caller. Returns a blasx_status. */
+ * device. Arguments as for blasx_dgemm_device; the caller still provides A,
+ * B and C. The precision mode (blasx_set_dgemm_mode) applies: in native mode
+ * the FP64 kernel runs; in auto mode the emulated (INT8 Ozaki) path runs,
+ * with the native FP64 kernel chosen on the device when the operands' spread
+ * is too wide (unlike blasx_dgemm_device, auto mode does not send small
+ * problems to the native kernel by size); in ozaki mode the emulated path
+ * always runs. Its scratch is a fixed 64 MiB device array that every GPU
+ * loading this library holds until the process exits; emulated problems
+ * whose scratch would not fit (M = N = K = 1024 fits; 2048 does not) are
+ * rejected with BLASX_ERR_UNSUPPORTED and a message in blasx_last_error().
+ * The first call on each device context performs a one-time set-up there
+ * (it looks up the array's device address and uploads constant tables);
+ * make that first call before any stream capture. All calls share the one
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller. Returns a blasx_status for what
+ * the host could check; a failure on the device is reported by
+ * blasx_dgemm_device_noalloc_status. */
 int blasx_dgemm_device_noalloc(int transa, int transb, int M, int N, int K, double alpha,
                                const double *A, int lda, const double *B, int ldb,
                                double beta, double *C, int ldc, void *stream);
+
+/* Device status of the last blasx_dgemm_device_noalloc call on the current
+ * device: waits for `stream` (the stream that call was enqueued on), then
+ * reads the shared scratch's error word. Returns BLASX_ERR_TIMEOUT when a
+ * bounded wait of the residue GEMM ran out in that call (its C is then
+ * undefined), else BLASX_OK. Allocates nothing. No counterpart in the
+ * reference. */
+int blasx_dgemm_device_noalloc_status(void *stream);
 
 /* Number of kernels this library has launched since it was loaded (all
  * threads); lets a caller count the GPU work of a region. */

@@ -84,6 +84,68 @@ def test_alone_equals_mix(serving):
         assert np.all(np.abs(m - a) <= bound(r)), (r["M"], r["N"], r["K"], r["dt"])
 
 
+def make_large_requests(seed):
+    """Requests large enough for auto mode to emulate them (FP64 work >= 6e9
+    with K >= 512, FP32 >= 3e8 with K >= 256, complex128 >= 2e9), in a mix
+    with small native ones of every dtype."""
+    rng = np.random.default_rng(seed)
+    shapes = [(np.float64, 2048, 2048, 1536), (np.float64, 2304, 1792, 2048), (np.float64, 1800, 2100, 1700),
+              (np.float32, 1024, 1024, 512), (np.float32, 1500, 900, 700), (np.complex128, 1280, 1280, 1280),
+              (np.float64, 300, 200, 100), (np.float32, 200, 300, 150), (np.complex128, 100, 120, 90),
+              (np.float64, 700, 500, 300)]
+    reqs = []
+    for t, (dt, M, N, K) in enumerate(shapes):
+        ta = str(rng.choice(["N", "T"] + (["C"] if dt == np.complex128 else [])))
+        tb = str(rng.choice(["N", "T"] + (["C"] if dt == np.complex128 else [])))
+        ra, ca = oracle.shape_of_op(ta, M, K)
+        rb, cb = oracle.shape_of_op(tb, K, N)
+        A = oracle.uniform((ra, ca), dt, seed * 1000 + 3 * t)
+        B = oracle.uniform((rb, cb), dt, seed * 1000 + 3 * t + 1)
+        C0 = oracle.uniform((M, N), dt, seed * 1000 + 3 * t + 2)
+        alpha, beta = (1.5, -0.25) if dt != np.complex128 else (1 - 0.5j, 0.25 + 0.5j)
+        reqs.append(dict(dt=dt, ta=ta, tb=tb, M=M, N=N, K=K, A=A, ra=ra, B=B, rb=rb, C0=C0, alpha=alpha, beta=beta))
+    return reqs
+
+
+def test_alone_equals_mix_with_emulated_requests(serving):
+    """Emulated FP64, FP32 and complex128 requests beside small native ones:
+    each result in the concurrent mix equals the same request served alone
+    bit for bit when it was emulated (exact integer products, per-request
+    decision), and is within the bound of the unserved call's result."""
+    blx = serving
+    prev = blx.set_dgemm_mode(blx.MODE_AUTO)
+    try:
+        reqs = make_large_requests(3)
+        unserved = [run(blx, r) for r in reqs]
+        blx.serve_start(0, 0, 8)
+        alone = []
+        for r in reqs:
+            alone.append(run(blx, r))
+        out = [None] * len(reqs)
+        errs = []
+
+        def worker(w):
+            try:
+                for i in range(w, len(reqs), 10):
+                    out[i] = run(blx, reqs[i])
+            except Exception as e:  # pragma: no cover
+                errs.append(e)
+
+        for _ in range(2):
+            th = [threading.Thread(target=worker, args=(w,)) for w in range(10)]
+            [t.start() for t in th]
+            [t.join() for t in th]
+            assert not errs, errs
+            for r, a, u, m in zip(reqs, alone, unserved, out):
+                assert np.all(np.abs(m - u) <= 2 * bound(r)), (r["M"], r["N"], r["K"], r["dt"])
+                if r["M"] >= 1000:  # emulated in both runs
+                    assert np.array_equal(m, a), (r["M"], r["N"], r["K"], r["dt"])
+        st = blx.serve_stats()
+        assert st["failed"] == 0
+    finally:
+        blx.set_dgemm_mode(prev)
+
+
 def test_operand_cache_hits_and_identity(serving):
     blx = serving
     blx.serve_start(0, 1 << 30, 4)
