@@ -36,6 +36,9 @@ struct CrtTables {
     double Md[kNumN];                       // M as a double
     double invMd[kNumN];
     int Q[kNumN];                           // norm exponent bound: 2^(2Q) <= M/4
+    // the same 32-bit limbs as doubles (exact), operands of the FP64 CRT sums
+    double wd[kNumN][kMaxModuli][kLimbs];
+    double Ml[kNumN][kLimbs];
 };
 __constant__ CrtTables c_crt;
 
@@ -76,6 +79,7 @@ CrtTables build_tables() {
         uint32_t M[kLimbs] = {1, 0, 0, 0, 0, 0};
         for (int l = 0; l < n; ++l) big_mul_small(M, kLimbs, uint32_t(kModuli[l]));
         memcpy(t.M[ni], M, sizeof M);
+        for (int k = 0; k < kLimbs; ++k) t.Ml[ni][k] = double(M[k]);
         t.Md[ni] = big_to_double(M, kLimbs);
         t.invMd[ni] = 1.0 / t.Md[ni];
         t.Q[ni] = int(std::floor((std::log2(t.Md[ni]) - 2.0) / 2.0));
@@ -88,6 +92,7 @@ CrtTables build_tables() {
             const uint32_t r = big_div_small(tmp, kLimbs, uint32_t(kModuli[l]));  // (M/m_l) mod m_l
             big_mul_small(q, kLimbs, inv_mod(r, uint32_t(kModuli[l])));
             memcpy(t.w[ni][l], q, sizeof q);
+            for (int k = 0; k < kLimbs; ++k) t.wd[ni][l][k] = double(q[k]);
         }
     }
     return t;
@@ -284,7 +289,10 @@ template <int L> struct Mod {
     static constexpr uint32_t m = table[L];
     static constexpr uint32_t c21 = uint32_t((uint64_t(1) << 21) % m);
     static constexpr uint32_t c42 = uint32_t((uint64_t(1) << 42) % m);
-    static constexpr uint32_t cb = uint32_t((m - (uint64_t(1) << 62) % m) % m);
+    // half range of the symmetric residue (m odd): [-h, h]
+    static constexpr uint32_t h = (m - 1) / 2;
+    // -2^62 + h mod m: removes the bias of the digits and shifts by h
+    static constexpr uint32_t cbh = uint32_t(((m - (uint64_t(1) << 62) % m) % m + h) % m);
     static constexpr uint32_t magic = uint32_t(((uint64_t(1) << 39) + m - 1) / m);
 };
 
@@ -298,39 +306,40 @@ __device__ __forceinline__ Digits digits_of(int64_t v) {
     return {uint32_t(a) & 0x1FFFFFu, uint32_t(a >> 21) & 0x1FFFFFu, uint32_t(a >> 42)};
 }
 
-// Residue in [0, m) of the biased value minus the bias, for the L-th modulus:
-//   t = d2 (2^42 mod m) + d1 (2^21 mod m) + d0 + (-2^62 mod m) < 2^31,
+// Symmetric residue of v for the L-th modulus, in [-h, h] for odd m (the
+// low byte for m = 256, whose byte is already the two's complement of the
+// residue in [-128, 127]): with the bias removed and h added,
+//   t = d2 (2^42 mod m) + d1 (2^21 mod m) + d0 + (h - 2^62 mod m) < 2^30,
 //   t mod m = floor(t ceil(2^39/m) / 2^39), exact for t < 2^31 and m <= 256
-// (the rounding error of the magic multiplier stays below 1/m). Every
-// constant folds: two IMADs, one multiply-high, one shift, one IMAD.
-template <int L> __device__ __forceinline__ uint32_t residue_u(const Digits &x) {
+// (the rounding error of the magic multiplier stays below 1/m), and
+// (v + h) mod m - h is the residue of v in [-h, h]. Every constant folds: two
+// IMADs, one add, one multiply-high, one shift, one IMAD, one add.
+template <int L> __device__ __forceinline__ int32_t residue_s(const Digits &x) {
     using C = Mod<L>;
-    const uint32_t t = x.d2 * C::c42 + x.d1 * C::c21 + (x.d0 + C::cb);  // < 2^21 * 512 + 256 < 2^31
-    const uint32_t q = __umulhi(t, C::magic) >> 7;
-    return t - q * C::m;
-}
-
-// Four residues packed as bytes, mapped to the symmetric int8 range:
-// bytes above (m-1)/2 take m off (mod 256), 4 at a time with SIMD byte ops.
-// For m = 256 the byte already is the two's complement of the symmetric
-// residue.
-template <int L>
-__device__ __forceinline__ uint32_t pack4_sym(const Digits &a, const Digits &b, const Digits &c,
-                                              const Digits &d) {
-    constexpr uint32_t m = Mod<L>::m;
-    const uint32_t w = residue_u<L>(a) + (residue_u<L>(b) << 8) + (residue_u<L>(c) << 16) +
-                       (residue_u<L>(d) << 24);
-    if constexpr (m == 256) {
-        return w;
+    if constexpr (C::m == 256) {
+        return int32_t(x.d0);
     } else {
-        constexpr uint32_t half = ((m - 1) / 2) * 0x01010101u;
-        const uint32_t over = __vcmpgtu4(w, half);  // 0xff in every byte above (m-1)/2
-        return __vadd4(w, over & ((256 - m) * 0x01010101u));
+        const uint32_t t = x.d2 * C::c42 + x.d1 * C::c21 + (x.d0 + C::cbh);
+        const uint32_t q = __umulhi(t, C::magic) >> 7;
+        return int32_t(t - q * C::m) - int32_t(C::h);
     }
 }
 
+// The low bytes of four values packed into one word (byte k from value k).
+__device__ __forceinline__ uint32_t pack_bytes(int32_t a, int32_t b, int32_t c, int32_t d) {
+    return __byte_perm(__byte_perm(uint32_t(a), uint32_t(b), 0x0040u),
+                       __byte_perm(uint32_t(c), uint32_t(d), 0x0040u), 0x5410u);
+}
+
+// x * 2^e for a normal x: one multiply by a constructed power of two when
+// 2^e is a normal double, ldexp otherwise (both round the same way).
+__device__ __forceinline__ double scale_pow2(double x, int e) {
+    if (e >= -1022 && e <= 1023) return x * __longlong_as_double(int64_t(e + 1023) << 52);
+    return ldexp(x, e);
+}
+
 __device__ __forceinline__ int64_t scale_round(double x, int e) {
-    return __double2ll_rn(ldexp(x, e));
+    return __double2ll_rn(scale_pow2(x, e));
 }
 
 // Output geometry of one operand's slices.
@@ -351,7 +360,8 @@ template <int L> __device__ __forceinline__ uint4 pack16(const Digits (&x)[16]) 
     uint32_t w[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-        w[q] = pack4_sym<L>(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+        w[q] = pack_bytes(residue_s<L>(x[4 * q]), residue_s<L>(x[4 * q + 1]), residue_s<L>(x[4 * q + 2]),
+                          residue_s<L>(x[4 * q + 3]));
     return make_uint4(w[0], w[1], w[2], w[3]);
 }
 __device__ __forceinline__ uint4 neg16(uint4 a) {  // residue of -x, byte-wise
@@ -397,11 +407,28 @@ template <typename T, int ROLE, int COMP>
 __device__ __forceinline__ void slice_kc_comp(const View &v, int nmod, int e, int64_t r, int64_t k0,
                                               const SliceOut &o) {
     Digits d[16];
+    bool done = false;
+    if constexpr (!Elem<T>::cplx) {
+        // 16 whole elements in range and 16-byte aligned: vector loads
+        const T *p = static_cast<const T *>(v.p) + (r * v.ld + k0);
+        if (r < v.R && k0 + 16 <= v.K && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+            constexpr int PER = 16 / sizeof(T);  // elements per 16-byte load
+            using V = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+            T x[16];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        double re = 0, im = 0;
-        if (r < v.R && k0 + q < v.K) load_elem<T>(v, r, k0 + q, true, re, im);
-        d[q] = digits_of(scale_round(COMP ? im : re, e));
+            for (int q = 0; q < 16; q += PER) *reinterpret_cast<V *>(&x[q]) = __ldg(reinterpret_cast<const V *>(p + q));
+#pragma unroll
+            for (int q = 0; q < 16; ++q) d[q] = digits_of(scale_round(double(x[q]), e));
+            done = true;
+        }
+    }
+    if (!done) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            double re = 0, im = 0;
+            if (r < v.R && k0 + q < v.K) load_elem<T>(v, r, k0 + q, true, re, im);
+            d[q] = digits_of(scale_round(COMP ? im : re, e));
+        }
     }
     store_all<ROLE, COMP>(o, nmod, r, k0, d);
 }
@@ -473,63 +500,60 @@ __global__ void __launch_bounds__(256) slice_rc_kernel(View v, RowStats st, cons
 
 // ---- reconstruction -----------------------------------------------------------
 
-// 32-bit limbs that hold sum_l u_l w_l < N 2^8 M for N moduli.
+// 32-bit limbs that hold the weights w_l < M and M itself for N moduli; the
+// signed result |X| < M/4 then fits with its sign bit.
 __host__ __device__ constexpr int limbs_for(int n) {
-    return n <= 6 ? 2 : n <= 10 ? 3 : n <= 14 ? 4 : n <= 18 ? 5 : 6;
+    return n <= 8 ? 2 : n <= 12 ? 3 : n <= 16 ? 4 : 5;
 }
 
-// x * 2^e for a normal x: one multiply by a constructed power of two when
-// 2^e is a normal double, ldexp otherwise.
-__device__ __forceinline__ double scale_pow2(double x, int e) {
-    if (e >= -1022 && e <= 1023) return x * __longlong_as_double(int64_t(e + 1023) << 52);
-    return ldexp(x, e);
+// Residue l of element qb (byte qb of w[l], in [0, 256)) as an exact double:
+// the byte is placed in the low mantissa bits of 2^52 and 2^52 taken off.
+__device__ __forceinline__ double residue_as_double(uint32_t w, int qb) {
+    return __hiloint2double(0x43300000, int(__byte_perm(w, 0u, 0x4440u | uint32_t(qb)))) -
+           4503599627370496.0;
 }
 
-// CRT value of the residues u[0..N) times 2^scale as a double, correctly
-// rounded from the exact integer X (the scaling by a power of two is exact
-// unless the result leaves the normal range):
-//   S = sum_l u_l w_l (multi-limb) is congruent to X mod M, and the row and
-//   column scaling guarantees |X| < 2^(2Q) <= M/4. So X = S - q M with
-//   q = rint(S / M): S / M lies within 1/4 of an integer, and its double
-//   estimate (S < N 2^8 M, a few roundings of 2^-53) is off by far less, so
-//   the rounding is never ambiguous. X comes out in two's complement; its
-//   magnitude is converted with one rounding.
+// CRT value of the residues (byte qb of w[0..N)) times 2^scale as a double,
+// correctly rounded from the exact integer X (the scaling by a power of two
+// is exact unless the result leaves the normal range):
+//   S = sum_l u_l w_l is congruent to X mod M, and the row and column
+//   scaling guarantees |X| < 2^(2Q) <= M/4. With w_l and M split into L
+//   32-bit limbs, every limb sum S_t = sum_l u_l w_{l,t} < N 2^8 2^32 < 2^45
+//   is an exact FP64 value, summed with DFMAs on the FP64 pipe. X = S - q M
+//   with q = rint(S / M): S / M lies within 1/4 of an integer and its double
+//   estimate is off by far less, so the rounding is never ambiguous. The
+//   limb differences D_t = S_t - q M_t (|D_t| < 2^45) are exact as well; their
+//   two's complement words come out of the mantissa of D_t + 1.5 * 2^52, a
+//   carry pass assembles X in L words, and its magnitude is converted with
+//   one rounding.
 template <int N>
-__device__ __forceinline__ double crt_to_double(const uint32_t (&u)[N], int scale) {
+__device__ __forceinline__ double crt_to_double(const uint32_t (&w)[N], int qb, int scale) {
     constexpr int L = limbs_for(N);
     constexpr int ni = N - kMinModuli;
-    uint64_t acc[L];
+    double S[L];
 #pragma unroll
-    for (int t = 0; t < L; ++t) acc[t] = 0;
+    for (int t = 0; t < L; ++t) S[t] = 0.0;
 #pragma unroll
-    for (int l = 0; l < N; ++l)
+    for (int l = 0; l < N; ++l) {
+        const double u = residue_as_double(w[l], qb);
 #pragma unroll
-        for (int t = 0; t < L; ++t) acc[t] += uint64_t(u[l]) * c_crt.w[ni][l][t];
-    uint32_t s[L];
-    uint64_t carry = 0;
+        for (int t = 0; t < L; ++t) S[t] = fma(u, c_crt.wd[ni][l][t], S[t]);
+    }
+    double sa = S[L - 1];
+#pragma unroll
+    for (int t = L - 2; t >= 0; --t) sa = fma(sa, 4294967296.0, S[t]);
+    const double qd = rint(sa * c_crt.invMd[ni]);
+    // X in L two's complement words: word t of D_t plus the carry of the words below
+    uint32_t x[L];
+    int32_t carry = 0;
 #pragma unroll
     for (int t = 0; t < L; ++t) {
-        const uint64_t v = acc[t] + carry;
-        s[t] = uint32_t(v);
-        carry = v >> 32;
-    }
-    double sd = 0;
-#pragma unroll
-    for (int t = L - 1; t >= 0; --t) sd = sd * 4294967296.0 + double(s[t]);
-    const uint32_t q = uint32_t(rint(sd * c_crt.invMd[ni]));
-    // x = s - q M, L-limb two's complement
-    uint32_t x[L];
-    {
-        uint64_t qc = 0;
-        int64_t borrow = 0;
-#pragma unroll
-        for (int t = 0; t < L; ++t) {
-            const uint64_t qm = uint64_t(q) * c_crt.M[ni][t] + qc;
-            qc = qm >> 32;
-            const int64_t d = int64_t(s[t]) - int64_t(uint32_t(qm)) - borrow;
-            x[t] = uint32_t(d);
-            borrow = d < 0 ? 1 : 0;
-        }
+        const double d = fma(-qd, c_crt.Ml[ni][t], S[t]) + 6755399441055744.0;  // exact, |D_t| < 2^51
+        const uint32_t lo = uint32_t(__double2loint(d));
+        const int32_t hi = int32_t(uint32_t(__double2hiint(d)) & 0xFFFFFu) - 0x80000;  // floor(D_t / 2^32)
+        const int64_t v = int64_t(lo) + int64_t(carry);
+        x[t] = uint32_t(v);
+        carry = hi + int32_t(v >> 32);  // floor division: -1, 0 or 1 from the low word
     }
     const bool neg = int32_t(x[L - 1]) < 0;
     if (neg) {  // magnitude: ~x + 1
@@ -579,11 +603,6 @@ __device__ __forceinline__ void gather4(const uint8_t *U, int64_t plane, int64_t
 #pragma unroll
     for (int l = 0; l < N; ++l) w[l] = *reinterpret_cast<const uint32_t *>(U + l * plane + row_off);
 }
-template <int N>
-__device__ __forceinline__ void unpack(const uint32_t (&w)[N], int q, uint32_t (&u)[N]) {
-#pragma unroll
-    for (int l = 0; l < N; ++l) u[l] = (w[l] >> (8 * q)) & 0xffu;
-}
 
 struct ReconArgs {
     const uint8_t *U;
@@ -613,9 +632,7 @@ __device__ __forceinline__ void recon_real(const ReconArgs &a, int64_t i0, int64
         const int64_t i = i0 + q;
         if (i >= a.M) break;
         if (!recon_keep(a, i, j)) continue;
-        uint32_t u[N];
-        unpack<N>(w, q, u);
-        const double val = crt_to_double<N>(u, -(a.ea[i] + fj));
+        const double val = crt_to_double<N>(w, q, -(a.ea[i] + fj));
         T *cp = C + i + j * a.ldc;
         double r = a.ar * val;
         if (!a.beta_zero) r = fma(a.br, double(*cp), r);
@@ -639,12 +656,9 @@ __device__ __forceinline__ void recon_cplx(const ReconArgs &a, int64_t i0, int64
         const int64_t i = i0 + q;
         if (i >= a.M) break;
         if (!recon_keep(a, i, j)) continue;
-        uint32_t u[N];
         const int sc = -(a.ea[i] + fj);
-        unpack<N>(wr, q, u);
-        const double xr = crt_to_double<N>(u, sc);
-        unpack<N>(wi, q, u);
-        const double xi = crt_to_double<N>(u, sc);
+        const double xr = crt_to_double<N>(wr, q, sc);
+        const double xi = crt_to_double<N>(wi, q, sc);
         R *cp = C + 2 * (i + j * a.ldc);
         double vr = a.ar * xr - a.ai * xi, vi = a.ar * xi + a.ai * xr;
         if (!a.beta_zero) {
@@ -916,7 +930,7 @@ template <typename T> int ozaki_t(const Gemm &g, cudaStream_t s, int mode) {
     BX_TRY(oz::upload_crt_tables());
     const Plan pl = make_plan(g);
     void *ws = nullptr;
-    BX_CUDA(cudaMallocAsync(&ws, pl.bytes, s));
+    BX_CUDA(dev_malloc_async(&ws, pl.bytes, s));
     struct Free {
         void *p;
         cudaStream_t s;
