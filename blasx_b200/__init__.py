@@ -129,6 +129,8 @@ def lib() -> ctypes.CDLL:
         L.blasx_cgemm_device.argtypes = [_I] * 5 + [_P, _P, _I, _P, _I, _P, _P, _I, _P]
         L.blasx_dgemm_device_noalloc.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_dgemm_device_noalloc_status.argtypes = [_P]
+        L.blasx_test_stall_residue_gemm.argtypes = [_I, ctypes.c_longlong]
+        L.blasx_test_fail_allocation.argtypes = [_I]
         L.blasx_kernel_launch_count.restype = ctypes.c_uint64
         L.blasx_tile_plan.argtypes = [ctypes.c_longlong] * 5 + [_I, _I, ctypes.POINTER(TilePlanStats)]
         L.blasx_serve_start.argtypes = [ctypes.c_size_t, ctypes.c_size_t, _I]
@@ -568,6 +570,17 @@ def serve_start(hbm_budget: int = 0, cache_bytes: int = 0, max_inflight: int = 0
 
 def serve_stop() -> int:
     return lib().blasx_serve_stop()
+
+
+def test_stall_residue_gemm(launches: int, wait_cycles: int) -> int:
+    """Test hook: the next `launches` residue-GEMM launches stall one stage of
+    CTA 0 and give up after `wait_cycles` (the call reports BLASX_ERR_TIMEOUT)."""
+    return lib().blasx_test_stall_residue_gemm(launches, wait_cycles)
+
+
+def test_fail_allocation(nth: int) -> int:
+    """Test hook: the nth device allocation from now on fails (0 disarms)."""
+    return lib().blasx_test_fail_allocation(nth)
 
 
 def serve_invalidate(host_buffer) -> int:

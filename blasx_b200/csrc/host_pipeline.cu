@@ -579,11 +579,11 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
     DeviceOps d;
     d.s = c->compute;
     StreamDrain drain{c};  // before d and pins go, on every return
-    if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, c->compute));
-    BX_CUDA(cudaMallocAsync(&d.B, 2 * panel_bytes, c->compute));
+    if (need_a) BX_CUDA(dev_malloc_async(&d.A, bytes_a, c->compute));
+    BX_CUDA(dev_malloc_async(&d.B, 2 * panel_bytes, c->compute));
     if (mult && need_a) {
-        BX_CUDA(cudaMallocAsync(&d.diag, w.diag_bytes, c->compute));
-        BX_CUDA(cudaMallocAsync(&d.C0, w.temp_bytes, c->compute));
+        BX_CUDA(dev_malloc_async(&d.diag, w.diag_bytes, c->compute));
+        BX_CUDA(dev_malloc_async(&d.C0, w.temp_bytes, c->compute));
         w.diag = d.diag;
         w.temp = d.C0;
     }
@@ -697,12 +697,12 @@ static int host_tri(const Trsm &t, bool mult) {
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
     StreamDrain drain{c};  // before d and pins go, on every return
     cudaStream_t s = c->compute;
-    if (need_a) BX_CUDA(cudaMallocAsync(&d.A, bytes_a, s));
-    BX_CUDA(cudaMallocAsync(&d.B, bytes_b, s));  // alpha == 0 writes zeros without reading B
-    if (bytes_r) BX_CUDA(cudaMallocAsync(&d.C, bytes_r, s));
+    if (need_a) BX_CUDA(dev_malloc_async(&d.A, bytes_a, s));
+    BX_CUDA(dev_malloc_async(&d.B, bytes_b, s));  // alpha == 0 writes zeros without reading B
+    if (bytes_r) BX_CUDA(dev_malloc_async(&d.C, bytes_r, s));
     if (bytes_w) {
-        BX_CUDA(cudaMallocAsync(&d.diag, w.diag_bytes, s));
-        BX_CUDA(cudaMallocAsync(&d.C0, w.temp_bytes, s));
+        BX_CUDA(dev_malloc_async(&d.diag, w.diag_bytes, s));
+        BX_CUDA(dev_malloc_async(&d.C0, w.temp_bytes, s));
         w.diag = d.diag;
         w.temp = d.C0;
     }
@@ -911,13 +911,13 @@ int host_gemm(const Gemm &g) {
     BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
     StreamDrain drain{c};  // before d and pins go, on every return
     if (need_ab) {
-        BX_CUDA(cudaMallocAsync(&d.A, ib.a ? ib.a : 256, c->compute));
+        BX_CUDA(dev_malloc_async(&d.A, ib.a ? ib.a : 256, c->compute));
         if (d.b_is_a) d.B = d.A;
-        else BX_CUDA(cudaMallocAsync(&d.B, ib.b ? ib.b : 256, c->compute));
+        else BX_CUDA(dev_malloc_async(&d.B, ib.b ? ib.b : 256, c->compute));
     }
-    BX_CUDA(cudaMallocAsync(&d.C, ib.c, c->compute));
-    if (oz) BX_CUDA(cudaMallocAsync(&d.ws, ib.ws, c->compute));
-    if (ib.c0) BX_CUDA(cudaMallocAsync(&d.C0, ib.c0, c->compute));
+    BX_CUDA(dev_malloc_async(&d.C, ib.c, c->compute));
+    if (oz) BX_CUDA(dev_malloc_async(&d.ws, ib.ws, c->compute));
+    if (ib.c0) BX_CUDA(dev_malloc_async(&d.C0, ib.c0, c->compute));
     const int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
                       : incore_native(g, c, d, need_ab, read_c, st);
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -16,7 +16,8 @@
 //               let the epilogue of one tile overlap the MMAs of the next;
 //   warps 2..5  epilogue: tcgen05.ld 32x32b.x32, INT32 -> residue mod m_l,
 //               16-byte stores of uint8.
-// Every mbarrier wait is bounded (about one second of clock); on expiry the
+// Every mbarrier wait is bounded (about one second of clock by default; a
+// launch argument); on expiry the
 // CTA raises a device error flag and an abort flag in shared memory, the
 // producer waits (bounded) for its copies in flight, the MMA thread waits for
 // its MMAs, TMEM is freed and the kernel returns -- it never spins forever.
@@ -24,6 +25,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 
@@ -41,7 +43,7 @@ constexpr int kStageBytes = kXBytes + kYBytes;
 constexpr int kThreadsTC = 192;
 constexpr uint32_t kTmemCols = 512;
 constexpr int kAccCols = 256;
-constexpr long long kWaitCycles = 2000000000LL;  // ~1 s at 1.9 GHz
+constexpr long long kWaitCycles = 2000000000LL;  // default wait limit: ~1 s at 1.9 GHz
 constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 + 256;
 
 __constant__ int c_mod[kMaxModuli];
@@ -55,6 +57,8 @@ struct TcArgs {
     int uplo;      // triangular output: 0 all, 1 row - col <= diag, 2 row - col >= diag
     int jtiles;    // j-tiles per column block of X (complex X stacks two blocks)
     int64_t diag;
+    long long wait_cycles;  // limit of every mbarrier wait (clock cycles)
+    int stall_cta;          // test hook: this CTA skips the loads of its second stage (-1: none)
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
@@ -80,15 +84,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait for the phase of `parity` to complete. Returns false when the
-// time limit expires or (if given) the CTA abort flag is raised.
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
+// Bounded wait for the phase of `parity` to complete. Returns false when
+// `limit` clock cycles have passed or (if given) the CTA abort flag is raised.
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag, long long limit) {
     const long long t0 = clock64();
     for (uint32_t it = 0;; ++it) {
         if (mbar_try(bar, parity)) return true;
         if ((it & 63) == 63) {
             if (abort_flag && *abort_flag) return false;
-            if (clock64() - t0 > kWaitCycles) return false;
+            if (clock64() - t0 > limit) return false;
         }
     }
 }
@@ -243,18 +247,27 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             uint32_t phase = 0;
             uint32_t issued = 0, par = 0;  // bit s: stage s has a load issued / its parity
             bool ok = true;
+            // test hook: the stalled CTA issues nothing for its second stage,
+            // so that the MMA issuer's wait for that stage runs out
+            int skip = int(blockIdx.x) == a.stall_cta ? 1 : -1;
             for (int64_t tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
                 const TileCoord c = decode(tile, tiles_j, tiles_i, a.tj0);
                 if (!tile_needed(c, a)) continue;
                 for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!mbar_wait(empty0 + 8 * stage, phase ^ 1, abort_flag)) { ok = false; break; }
-                    const uint32_t fb = full0 + 8 * stage;
-                    mbar_expect_tx(fb, kStageBytes);
-                    const uint32_t sx = su32(smem + stage * kStageBytes);
-                    tma_load_3d(sx, &mapX, fb, kb * kTileK, c.tj * kTileJ, c.l);
-                    tma_load_3d(sx + kXBytes, &mapY, fb, kb * kTileK, c.ti * kTileI, c.l);
-                    issued |= 1u << stage;
-                    par = (par & ~(1u << stage)) | (phase << stage);
+                    if (!mbar_wait(empty0 + 8 * stage, phase ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
+                    const bool skip_this = skip == 0;
+                    if (skip >= 0) --skip;
+                    if (skip_this) {
+                        issued &= ~(1u << stage);  // no copy in flight for this stage
+                    } else {
+                        const uint32_t fb = full0 + 8 * stage;
+                        mbar_expect_tx(fb, kStageBytes);
+                        const uint32_t sx = su32(smem + stage * kStageBytes);
+                        tma_load_3d(sx, &mapX, fb, kb * kTileK, c.tj * kTileJ, c.l);
+                        tma_load_3d(sx + kXBytes, &mapY, fb, kb * kTileK, c.ti * kTileI, c.l);
+                        issued |= 1u << stage;
+                        par = (par & ~(1u << stage)) | (phase << stage);
+                    }
                     if (++stage == kStages) { stage = 0; phase ^= 1; }
                 }
             }
@@ -263,7 +276,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                 *abort_flag = 1;
                 // wait (bounded) for this thread's copies still in flight
                 for (int s = 0; s < kStages; ++s)
-                    if (issued & (1u << s)) mbar_wait(full0 + 8 * s, (par >> s) & 1u, nullptr);
+                    if (issued & (1u << s)) mbar_wait(full0 + 8 * s, (par >> s) & 1u, nullptr, a.wait_cycles);
             }
         }
     } else if (warp == 1) {
@@ -277,11 +290,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
                 if (!tile_needed(decode(tile, tiles_j, tiles_i, a.tj0), a)) continue;
-                if (!mbar_wait(tempty0 + 8 * acc, acc_phase ^ 1, abort_flag)) { ok = false; break; }
+                if (!mbar_wait(tempty0 + 8 * acc, acc_phase ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t d = tmem + uint32_t(acc * kAccCols);
                 for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!mbar_wait(full0 + 8 * stage, phase, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(full0 + 8 * stage, phase, abort_flag, a.wait_cycles)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t sx = su32(smem + stage * kStageBytes);
                     const uint64_t xd = sdesc(sx), yd = sdesc(sx + kXBytes);
@@ -302,7 +315,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             }
             // all MMAs of this thread complete before TMEM is released
             umma_commit(done);
-            mbar_wait(done, 0, nullptr);
+            mbar_wait(done, 0, nullptr, a.wait_cycles);
         }
     } else {
         // ---------------- epilogue (warps 2..5) ----------------
@@ -314,7 +327,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             if (!tile_needed(c, a)) continue;
             const int32_t m = c_mod[c.l];
             const float inv_m = 1.0f / float(m);
-            if (!mbar_wait(tfull0 + 8 * acc, acc_phase, abort_flag)) {
+            if (!mbar_wait(tfull0 + 8 * acc, acc_phase, abort_flag, a.wait_cycles)) {
                 if (lane == 0) atomicOr(a.err, 4);
                 *abort_flag = 1;
                 break;
@@ -352,6 +365,23 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"(kTmemCols)
                      : "memory");
+    }
+}
+
+// Test hook (blasx_test_stall_residue_gemm): the next g_stall_launches
+// launches run with a wait limit of g_stall_wait cycles and CTA 0 issues no
+// loads for its second pipeline stage.
+std::atomic<int> g_stall_launches{0};
+std::atomic<long long> g_stall_wait{kWaitCycles};
+
+void take_stall(long long *wait_cycles, int *stall_cta) {
+    int n = g_stall_launches.load();
+    while (n > 0) {
+        if (g_stall_launches.compare_exchange_weak(n, n - 1)) {
+            *wait_cycles = g_stall_wait.load();
+            *stall_cta = 0;
+            return;
+        }
     }
 }
 
@@ -420,7 +450,8 @@ int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp
     if (uplo && (jblock <= 0 || jblock % kTileJ || Jp % jblock))
         return set_error(BLASX_ERR_ARG, "residue GEMM: bad column block for a triangular output");
     TcArgs a{Jp, Ip, Kp, U, dec, err_flag, int(tj_begin), int(tj_count), uplo,
-             uplo ? int(jblock / kTileJ) : 1, diag};
+             uplo ? int(jblock / kTileJ) : 1, diag, kWaitCycles, -1};
+    take_stall(&a.wait_cycles, &a.stall_cta);
     const int64_t tiles_upper = int64_t(kMaxModuli) * tj_count * (Ip / kTileI);
     if (tiles_upper == 0) return BLASX_OK;
     int64_t grid = tiles_upper < num_sms ? tiles_upper : num_sms;
@@ -434,3 +465,10 @@ int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp
 
 }  // namespace oz
 }  // namespace bx
+
+extern "C" int blasx_test_stall_residue_gemm(int launches, long long wait_cycles) {
+    if (launches < 0 || wait_cycles <= 0) return BLASX_ERR_ARG;
+    bx::oz::g_stall_wait.store(wait_cycles);
+    bx::oz::g_stall_launches.store(launches);
+    return BLASX_OK;
+}

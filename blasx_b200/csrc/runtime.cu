@@ -79,6 +79,34 @@ blasx_call_stats &call_stats() { return t_stats; }
 
 void count_launch(int n) { g_launches.fetch_add(uint64_t(n), std::memory_order_relaxed); }
 
+namespace {
+std::atomic<int> g_fail_alloc_countdown{0};  // > 0: the allocation that brings it to 0 fails
+
+bool injected_alloc_failure() {
+    int n = g_fail_alloc_countdown.load();
+    while (n > 0) {
+        if (g_fail_alloc_countdown.compare_exchange_weak(n, n - 1)) return n == 1;
+    }
+    return false;
+}
+}  // namespace
+
+cudaError_t dev_malloc_async(void **p, size_t bytes, cudaStream_t s) {
+    if (injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMallocAsync(p, bytes, s);
+}
+
+cudaError_t dev_malloc(void **p, size_t bytes) {
+    if (injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
 void resolve_decision(blasx_call_stats &st) {
     if (st.path != 2 || !g_ctx) return;
     const oz::Decision *d = static_cast<const oz::Decision *>(g_ctx->last_decision);
@@ -193,3 +221,8 @@ int blasx_finalize(void) { return bx::release_context(); }
 uint64_t blasx_kernel_launch_count(void) { return bx::g_launches.load(); }
 
 }  // extern "C"
+
+extern "C" int blasx_test_fail_allocation(int nth) {
+    bx::g_fail_alloc_countdown.store(nth > 0 ? nth : 0);
+    return BLASX_OK;
+}

@@ -164,6 +164,12 @@ int gemm_arg_info(int order, int ta, int tb, int M, int N, int K, int lda, int l
 // Counts every kernel launch of the library (blasx_kernel_launch_count).
 void count_launch(int n = 1);
 
+// Every device allocation of the library goes through these two. A test hook
+// (blasx_test_fail_allocation) can make the n-th one from now report
+// cudaErrorMemoryAllocation without allocating, to drive the error paths.
+cudaError_t dev_malloc_async(void **p, size_t bytes, cudaStream_t s);
+cudaError_t dev_malloc(void **p, size_t bytes);
+
 // Thread-local statistics of the last host call.
 blasx_call_stats &call_stats();
 // Fills the modulus count / fallback of an emulated call from the pinned

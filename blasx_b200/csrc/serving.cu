@@ -171,7 +171,7 @@ public:
     int init(size_t bytes) {
         size_ = bytes & ~size_t(255);
         if (size_ == 0) return set_error(BLASX_ERR_ARG, "serving: HBM budget of %zu bytes", bytes);
-        if (cudaMalloc(&base_, size_) != cudaSuccess) {
+        if (dev_malloc(reinterpret_cast<void **>(&base_), size_) != cudaSuccess) {
             cudaGetLastError();
             base_ = nullptr;
             return set_error(BLASX_ERR_NOMEM, "serving: cannot reserve the HBM budget of %zu bytes", size_);

@@ -239,8 +239,8 @@ int tri_device_entry(bool mult, DType dt, int side, int uplo, int trans, int dia
     bool emulated = false;
     if (!mult) return trsm_device(t, s, &emulated);
     TrmmScratch w = trmm_scratch_sizes(t);
-    BX_CUDA(cudaMallocAsync(&w.diag, w.diag_bytes, s));
-    if (cudaMallocAsync(&w.temp, w.temp_bytes, s) != cudaSuccess) {
+    BX_CUDA(dev_malloc_async(&w.diag, w.diag_bytes, s));
+    if (dev_malloc_async(&w.temp, w.temp_bytes, s) != cudaSuccess) {
         cudaFreeAsync(w.diag, s);
         return set_error(BLASX_ERR_NOMEM, "device trmm: no memory for %zu bytes of scratch", w.temp_bytes);
     }

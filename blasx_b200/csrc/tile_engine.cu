@@ -46,7 +46,7 @@ int ensure_arena(size_t bytes) {
         g_arena = nullptr;
         g_arena_bytes = 0;
     }
-    BX_CUDA(cudaMalloc(&g_arena, bytes));
+    BX_CUDA(dev_malloc(&g_arena, bytes));
     g_arena_bytes = bytes;
     return BLASX_OK;
 }

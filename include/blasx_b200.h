@@ -444,6 +444,24 @@ int blasx_dgemm_device_noalloc_status(void *stream);
  * threads); lets a caller count the GPU work of a region. */
 uint64_t blasx_kernel_launch_count(void);
 
+/* Test hooks (no counterpart in the reference, which assert()s on every CUDA
+ * failure, blas/LRU.c:118,134). They drive the error paths without faulting
+ * the GPU.
+ *
+ * blasx_test_stall_residue_gemm: the next `launches` launches of the INT8
+ * residue GEMM run with every mbarrier wait limited to `wait_cycles` clock
+ * cycles (default about one second), and their CTA 0 issues no loads for
+ * its second pipeline stage, so the MMA issuer's wait for that stage runs
+ * out: the kernel raises its device error word, waits for its own copies and
+ * MMAs, frees its tensor memory and returns. The call that launched it
+ * reports BLASX_ERR_TIMEOUT; its C is undefined.
+ *
+ * blasx_test_fail_allocation: the nth device allocation of the library from
+ * now on (1 = the next one) reports an out-of-memory error without
+ * allocating; 0 disarms. */
+int blasx_test_stall_residue_gemm(int launches, long long wait_cycles);
+int blasx_test_fail_allocation(int nth);
+
 /* Serving loop (no counterpart in the reference, whose GEMM path is not
  * re-entrant). While it runs, cblas_?gemm / ?gemm_ calls from any number of
  * host threads are queued to one scheduler thread that owns the device: it

@@ -145,6 +145,42 @@ def test_noalloc_follows_native_mode(blx):
         blx.set_dgemm_mode(prev)
 
 
+def test_noalloc_reports_a_device_timeout(blx):
+    """A bounded wait of the residue GEMM that runs out (test hook: one stage
+    of CTA 0 is never loaded, every wait limited to about 1 ms) is reported by
+    the status query, and the next call, hook disarmed, is correct."""
+    torch = pytest.importorskip("torch")
+    L = blx.lib()
+    prev = blx.set_dgemm_mode(blx.MODE_OZAKI)
+    try:
+        M, N, K = 700, 513, 1000
+        A = oracle.uniform((M, K), np.float64, 41)
+        B = oracle.uniform((K, N), np.float64, 42)
+        C0 = oracle.uniform((M, N), np.float64, 43)
+        dA, dB = _device(A, torch), _device(B, torch)
+        d_ref = _device(C0, torch)
+        torch.cuda.synchronize()
+        assert blx.gemm_device("N", "N", M, N, K, 1.5, dA, M, dB, K, -0.25, d_ref, M) == blx.BLASX_OK
+        blx.test_stall_residue_gemm(1, 2_000_000)
+        d_new = _device(C0, torch)
+        torch.cuda.synchronize()
+        st = L.blasx_dgemm_device_noalloc(111, 111, M, N, K, 1.5, dA.data_ptr(), M, dB.data_ptr(), K, -0.25,
+                                          d_new.data_ptr(), M, None)
+        assert st == blx.BLASX_OK, blx.last_error()
+        assert L.blasx_dgemm_device_noalloc_status(None) == blx.BLASX_ERR_TIMEOUT
+        d_new = _device(C0, torch)
+        torch.cuda.synchronize()
+        st = L.blasx_dgemm_device_noalloc(111, 111, M, N, K, 1.5, dA.data_ptr(), M, dB.data_ptr(), K, -0.25,
+                                          d_new.data_ptr(), M, None)
+        assert st == blx.BLASX_OK, blx.last_error()
+        assert L.blasx_dgemm_device_noalloc_status(None) == blx.BLASX_OK
+        torch.cuda.synchronize()
+        assert torch.equal(d_new, d_ref)  # the same emulated pipeline on the same operands
+    finally:
+        blx.test_stall_residue_gemm(0, 1)
+        blx.set_dgemm_mode(prev)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(blx):
     torch = pytest.importorskip("torch")
     L = blx.lib()
