@@ -56,10 +56,11 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--serving", type=int, default=400,
                    help="requests of the serving load (0 = skip); 10000 with --serving-dmax 16384 is the full stream")
-    p.add_argument("--serving-dmax", type=int, default=4096)
+    p.add_argument("--serving-dmax", type=int, default=8192)
     p.add_argument("--serving-threads", type=int, default=16)
-    p.add_argument("--serving-rate", type=float, default=0.0,
+    p.add_argument("--serving-rate", type=float, default=200.0,
                    help="offered requests/s over all threads (Poisson); 0 = back to back")
+    p.add_argument("--serving-budget", type=float, default=120e9, help="serving HBM admission budget (bytes)")
     p.add_argument("--dtype", default="d", choices=["d", "s", "z", "c"],
                    help="--workload device: FP64, FP32, complex128 or complex64")
     p.add_argument("--rates", default="100,200,400",
@@ -305,7 +306,7 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
             "aggregate_tflops": flops / wall / 1e12, "wall_s": wall,
             "b_cache_hits": st["cache_hits"], "b_cache_misses": st["cache_misses"],
-            "grouped_launches": st["grouped_launches"], "grouped_requests": st["grouped_requests"],
+            "executor_launches": st["grouped_launches"], "executor_requests": st["grouped_requests"],
             "max_inflight": st["max_inflight_seen"], "failed": st["failed"] + len(errors),
             "by_size_call_latency": classes,
             "scheduler": {"admit_seconds": st["admit_seconds"], "admit_max_ms": st["admit_max_ms"],
@@ -1091,7 +1092,17 @@ def main():
 
     serving = None
     if args.serving > 0 and rank == 0:
-        serving = serving_load(bx, torch, args.serving, args.serving_dmax, args.serving_threads, args.serving_rate)
+        # the serving stream: Poisson arrivals at a stated rate from 16 threads,
+        # an HBM admission budget of 120 GB; FP64 (and complex) requests once in
+        # auto mode (emulated where it pays) and once native
+        serving = {"stream": f"{args.serving} calls, {args.serving_threads} threads, Poisson arrivals at "
+                             f"{args.serving_rate:g}/s, dims log-uniform in [64, {args.serving_dmax}], "
+                             f"HBM budget {args.serving_budget / 1e9:g} GB, 16 in flight"}
+        for mode_name, smode in (("auto", bx.MODE_AUTO), ("native", bx.MODE_NATIVE)):
+            bx.set_dgemm_mode(smode)
+            serving[mode_name] = serving_load(bx, torch, args.serving, args.serving_dmax, args.serving_threads,
+                                              args.serving_rate, budget=int(args.serving_budget), inflight=16)
+        bx.set_dgemm_mode(mode)
 
     cpu = None
     if rank == 0 and not args.no_cpu:

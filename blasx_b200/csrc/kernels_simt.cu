@@ -9,103 +9,28 @@
 
 #include "arith.cuh"
 #include "kernels.h"
+#include "simt_tile.cuh"
 
 namespace bx {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+using namespace dev;
+
+constexpr int BM = kSimtBM, BN = kSimtBN, NT = kSimtThreads;
 
 template <typename T>
-__global__ void __launch_bounds__(NT)
-    gemm_simt_kernel(int ta, int tb, int M, int N, int K, T alpha, const T *__restrict__ A,
-                     int64_t lda, const T *__restrict__ B, int64_t ldb, T beta, T *__restrict__ C,
-                     int64_t ldc, int beta_zero, const int *guard, int uplo, int64_t diag) {
-    using Ar = Arith<T>;
+__global__ void __launch_bounds__(NT) gemm_simt_kernel(const SimtParams<T> p, const int *guard) {
     if (guard && *guard != 0) return;  // the emulated path produced C
-    __shared__ T As[BK][BM + 1];
-    __shared__ T Bs[BK][BN + 1];
-    const int tid = threadIdx.x;
-    const int tx = tid % 16, ty = tid / 16;
-    const int64_t m0 = int64_t(blockIdx.x) * BM, n0 = int64_t(blockIdx.y) * BN;
-    // triangular output: a tile with no entry inside computes nothing
-    if (uplo == 1 && m0 - (n0 + BN - 1) > diag) return;
-    if (uplo == 2 && (m0 + BM - 1) - n0 < diag) return;
-    T acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = Ar::zero();
-
-    for (int64_t k0 = 0; k0 < K; k0 += BK) {
-        for (int e = tid; e < BM * BK; e += NT) {
-            int mm, kk;
-            if (ta == NoTrans) { mm = e % BM; kk = e / BM; }
-            else { kk = e % BK; mm = e / BK; }
-            const int64_t gm = m0 + mm, gk = k0 + kk;
-            T v = Ar::zero();
-            if (gm < M && gk < K) {
-                v = ta == NoTrans ? A[gm + gk * lda] : A[gk + gm * lda];
-                if (ta == ConjT) v = Ar::conj(v);
-            }
-            As[kk][mm] = v;
-        }
-        for (int e = tid; e < BN * BK; e += NT) {
-            int nn, kk;
-            if (tb == NoTrans) { kk = e % BK; nn = e / BK; }
-            else { nn = e % BN; kk = e / BN; }
-            const int64_t gn = n0 + nn, gk = k0 + kk;
-            T v = Ar::zero();
-            if (gn < N && gk < K) {
-                v = tb == NoTrans ? B[gk + gn * ldb] : B[gn + gk * ldb];
-                if (tb == ConjT) v = Ar::conj(v);
-            }
-            Bs[kk][nn] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            T a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = Ar::fma(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int64_t gn = n0 + ty + 16 * j;
-        if (gn >= N) continue;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int64_t gm = m0 + tx + 16 * i;
-            if (gm >= M) continue;
-            if (uplo && (uplo == 1 ? gm - gn > diag : gm - gn < diag)) continue;
-            T *cp = &C[gm + gn * ldc];
-            T v = Ar::mul(alpha, acc[i][j]);
-            if (!beta_zero) v = Ar::add(v, Ar::mul(beta, *cp));
-            *cp = v;
-        }
-    }
+    __shared__ T smem[2 * kSimtBK * (kSimtBM + 1)];
+    simt_tile<T>(p, blockIdx.x, blockIdx.y, smem);
 }
 
 template <typename T>
 __global__ void scale_kernel(int M, int N, T beta, T *__restrict__ C, int64_t ldc, int beta_zero,
                              int uplo, int64_t diag) {
-    using Ar = Arith<T>;
-    const int64_t total = int64_t(M) * N;
-    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total;
-         t += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t i = t % M, j = t / M;
-        if (uplo && (uplo == 1 ? i - j > diag : i - j < diag)) continue;
-        T *cp = &C[i + j * ldc];
-        *cp = beta_zero ? Ar::zero() : Ar::mul(beta, *cp);
-    }
+    scale_range<T>(M, beta, C, ldc, beta_zero, uplo, diag, blockIdx.x * int64_t(blockDim.x) + threadIdx.x,
+                   int64_t(M) * N, int64_t(gridDim.x) * blockDim.x);
 }
 
 // C(i, j) += beta X(i, j): blockIdx.y strides over columns, threads over rows.
@@ -167,10 +92,11 @@ template <typename T> int launch_complete_t(int form, void *X, int64_t ldx, int6
 template <typename T> int launch_simt_t(const Gemm &g, cudaStream_t s) {
     dim3 grid(unsigned((g.M + BM - 1) / BM), unsigned((g.N + BN - 1) / BN));
     if (grid.y > 65535) return set_error(BLASX_ERR_UNSUPPORTED, "N too large for SIMT grid");
-    gemm_simt_kernel<T><<<grid, NT, 0, s>>>(
-        g.ta, g.tb, int(g.M), int(g.N), int(g.K), from_cplx<T>(g.alpha),
-        static_cast<const T *>(g.A), g.lda, static_cast<const T *>(g.B), g.ldb,
-        from_cplx<T>(g.beta), static_cast<T *>(g.C), g.ldc, g.beta_zero() ? 1 : 0, g.guard, g.uplo, g.diag);
+    const SimtParams<T> p{g.ta, g.tb, int(g.M), int(g.N), int(g.K), from_cplx<T>(g.alpha),
+                          from_cplx<T>(g.beta), static_cast<const T *>(g.A), g.lda,
+                          static_cast<const T *>(g.B), g.ldb, static_cast<T *>(g.C), g.ldc,
+                          g.beta_zero() ? 1 : 0, g.uplo, g.diag};
+    gemm_simt_kernel<T><<<grid, NT, 0, s>>>(p, g.guard);
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;

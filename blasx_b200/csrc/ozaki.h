@@ -81,6 +81,11 @@ int upload_crt_tables();
 int prepare_crt_tables_current_device();
 int prepare_residue_gemm_current_device();
 
+// Test hook of the residue GEMM (blasx_test_stall_residue_gemm): true, with
+// the wait limit to use, when the next launch (or executor task) is to stall
+// one pipeline stage; each true answer uses up one of the armed stalls.
+bool take_residue_stall(long long *wait_cycles);
+
 // The moduli (largest first).
 extern const int kModuli[kMaxModuli];
 

@@ -1,26 +1,7 @@
-// ozaki_gemm_tc.cu -- INT8 residue GEMM on the sm_100a tensor cores (tcgen05).
-//
-// For every modulus l chosen on the device:
-//     U_l[j][i] = (sum_k X_l[j][k] * Y_l[i][k]) mod m_l
-// with X_l, Y_l int8 K-major slices and exact INT32 accumulation in TMEM.
-// X holds the columns of op(B) (MMA M = 128 rows), Y the rows of op(A)
-// (MMA N = 256), so a TMEM lane is a column j of C and a thread of the
-// epilogue writes 256 consecutive rows i -- the column-major layout of C.
-//
-// Persistent, warp-specialised CTA (one per SM, 192 threads):
-//   warp 0      TMA producer: 3-D tensor maps (k, row, modulus), 128-byte
-//               swizzle, a 4-stage ring of 16 KB (X) + 32 KB (Y) stages;
-//   warp 1      allocates 512 TMEM columns and issues the MMAs from one
-//               thread: 4 x tcgen05.mma.kind::i8 (M128 N256 K32) per stage,
-//               tcgen05.commit frees the stage; two 256-column accumulators
-//               let the epilogue of one tile overlap the MMAs of the next;
-//   warps 2..5  epilogue: tcgen05.ld 32x32b.x32, INT32 -> residue mod m_l,
-//               16-byte stores of uint8.
-// Every mbarrier wait is bounded (about one second of clock by default; a
-// launch argument); on expiry the
-// CTA raises a device error flag and an abort flag in shared memory, the
-// producer waits (bounded) for its copies in flight, the MMA thread waits for
-// its MMAs, TMEM is freed and the kernel returns -- it never spins forever.
+// ozaki_gemm_tc.cu -- the standalone INT8 residue GEMM launch: one persistent
+// CTA per SM (or CTAs of bounded life when a launch asks for it), each
+// running the tcgen05 pipeline of residue_tc.cuh over a strided walk of the
+// output tiles, with the test hook that stalls one pipeline stage.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -30,170 +11,12 @@
 #include <mutex>
 
 #include "ozaki.h"
+#include "residue_tc.cuh"
 
 namespace bx {
 namespace oz {
 
 namespace {
-
-constexpr int kStages = 4;
-constexpr int kXBytes = kTileJ * kTileK;  // 16 KB
-constexpr int kYBytes = kTileI * kTileK;  // 32 KB
-constexpr int kStageBytes = kXBytes + kYBytes;
-constexpr int kThreadsTC = 192;
-constexpr uint32_t kTmemCols = 512;
-constexpr int kAccCols = 256;
-constexpr long long kWaitCycles = 2000000000LL;  // default wait limit: ~1 s at 1.9 GHz
-constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 + 256;
-
-__constant__ int c_mod[kMaxModuli];
-
-struct TcArgs {
-    int64_t Jp, Ip, Kp;
-    uint8_t *U;
-    const Decision *dec;
-    int *err;
-    int tj0, tjn;  // range of j-tiles (128 columns of C each) this launch covers
-    int uplo;      // triangular output: 0 all, 1 row - col <= diag, 2 row - col >= diag
-    int jtiles;    // j-tiles per column block of X (complex X stacks two blocks)
-    int64_t diag;
-    long long wait_cycles;  // limit of every mbarrier wait (clock cycles)
-    int stall_cta;          // test hook: this CTA skips the loads of its second stage (-1: none)
-};
-
-__device__ __forceinline__ uint32_t su32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        "selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase of `parity` to complete. Returns false when
-// `limit` clock cycles have passed or (if given) the CTA abort flag is raised.
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag, long long limit) {
-    const long long t0 = clock64();
-    for (uint32_t it = 0;; ++it) {
-        if (mbar_try(bar, parity)) return true;
-        if ((it & 63) == 63) {
-            if (abort_flag && *abort_flag) return false;
-            if (clock64() - t0 > limit) return false;
-        }
-    }
-}
-
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
-                                            int c0, int c1, int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
-// Shared-memory matrix descriptor: K-major operand, rows of 128 bytes with
-// the 128-byte swizzle, 8-row core groups 1024 bytes apart (SBO), sm_100
-// descriptor version 1, layout SWIZZLE_128B (2).
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-    uint64_t d = uint64_t((saddr & 0x3FFFF) >> 4);
-    // leading byte offset (bits 16..29) stays 0: ignored for swizzled K-major
-    d |= uint64_t(1024 >> 4) << 32;    // stride byte offset
-    d |= uint64_t(1) << 46;            // descriptor version
-    d |= uint64_t(2) << 61;            // SWIZZLE_128B
-    return d;
-}
-
-// Instruction descriptor, kind::i8: D s32, A s8, B s8, both K-major, N, M.
-constexpr uint32_t idesc_i8(int M, int N) {
-    return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                        uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-    asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-        : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-          "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// x mod m in [0, m) for |x| < 2^31, m <= 256: a float quotient estimate is off
-// by at most one (|x| * 2^-24 / m < 1), corrected by two compares.
-__device__ __forceinline__ uint32_t mod_small(int32_t x, int32_t m, float inv_m) {
-    const int32_t q = __float2int_rd(__int2float_rn(x) * inv_m);
-    int32_t r = x - q * m;
-    r += (r < 0) ? m : 0;
-    r -= (r >= m) ? m : 0;
-    return uint32_t(r);
-}
-
-struct TileCoord {
-    int l, tj, ti;
-};
-__device__ __forceinline__ TileCoord decode(int64_t tile, int tiles_j, int tiles_i, int tj0) {
-    constexpr int GJ = 16;  // j-tiles per raster group (operand panels stay in L2)
-    const int64_t per_mod = int64_t(tiles_j) * tiles_i;
-    TileCoord c;
-    c.l = int(tile / per_mod);
-    const int64_t t = tile % per_mod;
-    const int64_t per_group = int64_t(GJ) * tiles_i;
-    const int group = int(t / per_group);
-    const int first = group * GJ;
-    const int gsize = min(GJ, tiles_j - first);
-    const int64_t in = t % per_group;
-    c.tj = tj0 + first + int(in % gsize);
-    c.ti = int(in / gsize);
-    return c;
-}
-
-// Triangular output: whether the C tile (rows ti*256.., columns tj*128..) has
-// an entry inside the triangle. Every role of the kernel skips the same tiles.
-__device__ __forceinline__ bool tile_needed(const TileCoord &c, const TcArgs &a) {
-    if (a.uplo == 0) return true;
-    const int64_t r0 = int64_t(c.ti) * kTileI, c0 = int64_t(c.tj % a.jtiles) * kTileJ;
-    if (a.uplo == 1) return r0 - (c0 + kTileJ - 1) <= a.diag;
-    return (r0 + kTileI - 1) - c0 >= a.diag;
-}
 
 __global__ void __launch_bounds__(kThreadsTC, 1)
     residue_gemm_kernel(const __grid_constant__ CUtensorMap mapX,
@@ -202,169 +25,37 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     const int tiles_j = a.tjn, tiles_i = int(a.Ip / kTileI);
     const int64_t total = int64_t(nmod) * tiles_j * tiles_i;
     if (total == 0) return;  // native fallback chosen on the device
-    const int num_kb = int(a.Kp / kTileK);
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kStages * kStageBytes);
-    const uint32_t full0 = su32(bars), empty0 = su32(bars + kStages);
-    const uint32_t tfull0 = su32(bars + 2 * kStages), tempty0 = su32(bars + 2 * kStages + 2);
-    const uint32_t done = su32(bars + 2 * kStages + 4);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 5);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
-
+    const ResiduePipe p = residue_pipe_at(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            mbar_init(full0 + 8 * s, 1);
-            mbar_init(empty0 + 8 * s, 1);
-        }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(tfull0 + 8 * b, 1);
-            mbar_init(tempty0 + 8 * b, 4);
-        }
-        mbar_init(done, 1);
-        *abort_flag = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         su32(tmem_slot)),
-                     "r"(kTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
+    if (threadIdx.x == 0) residue_pipe_init(p);
+    if (warp == 1) tmem_alloc_all(p.tmem_slot);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem = *p.tmem_slot;
 
-    if (warp == 0) {
-        if (lane == 0) {
-            // ---------------- TMA producer ----------------
-            int stage = 0;
-            uint32_t phase = 0;
-            uint32_t issued = 0, par = 0;  // bit s: stage s has a load issued / its parity
-            bool ok = true;
-            // test hook: the stalled CTA issues nothing for its second stage,
-            // so that the MMA issuer's wait for that stage runs out
-            int skip = int(blockIdx.x) == a.stall_cta ? 1 : -1;
-            for (int64_t tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
-                const TileCoord c = decode(tile, tiles_j, tiles_i, a.tj0);
-                if (!tile_needed(c, a)) continue;
-                for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!mbar_wait(empty0 + 8 * stage, phase ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
-                    const bool skip_this = skip == 0;
-                    if (skip >= 0) --skip;
-                    if (skip_this) {
-                        issued &= ~(1u << stage);  // no copy in flight for this stage
-                    } else {
-                        const uint32_t fb = full0 + 8 * stage;
-                        mbar_expect_tx(fb, kStageBytes);
-                        const uint32_t sx = su32(smem + stage * kStageBytes);
-                        tma_load_3d(sx, &mapX, fb, kb * kTileK, c.tj * kTileJ, c.l);
-                        tma_load_3d(sx + kXBytes, &mapY, fb, kb * kTileK, c.ti * kTileI, c.l);
-                        issued |= 1u << stage;
-                        par = (par & ~(1u << stage)) | (phase << stage);
-                    }
-                    if (++stage == kStages) { stage = 0; phase ^= 1; }
-                }
-            }
-            if (!ok) {
-                atomicOr(a.err, 1);
-                *abort_flag = 1;
-                // wait (bounded) for this thread's copies still in flight
-                for (int s = 0; s < kStages; ++s)
-                    if (issued & (1u << s)) mbar_wait(full0 + 8 * s, (par >> s) & 1u, nullptr, a.wait_cycles);
-            }
-        }
-    } else if (warp == 1) {
-        if (lane == 0) {
-            // ---------------- MMA issuer ----------------
-            constexpr uint32_t idesc = idesc_i8(kTileJ, kTileI);
-            int stage = 0;
-            uint32_t phase = 0;
-            int acc = 0;
-            uint32_t acc_phase = 0;
-            bool ok = true;
-            for (int64_t tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
-                if (!tile_needed(decode(tile, tiles_j, tiles_i, a.tj0), a)) continue;
-                if (!mbar_wait(tempty0 + 8 * acc, acc_phase ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
-                tc_fence_after();
-                const uint32_t d = tmem + uint32_t(acc * kAccCols);
-                for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!mbar_wait(full0 + 8 * stage, phase, abort_flag, a.wait_cycles)) { ok = false; break; }
-                    tc_fence_after();
-                    const uint32_t sx = su32(smem + stage * kStageBytes);
-                    const uint64_t xd = sdesc(sx), yd = sdesc(sx + kXBytes);
-#pragma unroll
-                    for (int k = 0; k < kTileK / 32; ++k)
-                        umma_i8(d, xd + uint64_t(2 * k), yd + uint64_t(2 * k), idesc,
-                                (kb | k) != 0 ? 1u : 0u);
-                    umma_commit(empty0 + 8 * stage);
-                    if (++stage == kStages) { stage = 0; phase ^= 1; }
-                }
-                if (!ok) break;
-                umma_commit(tfull0 + 8 * acc);
-                if (++acc == 2) { acc = 0; acc_phase ^= 1; }
-            }
-            if (!ok) {
-                atomicOr(a.err, 2);
-                *abort_flag = 1;
-            }
-            // all MMAs of this thread complete before TMEM is released
-            umma_commit(done);
-            mbar_wait(done, 0, nullptr, a.wait_cycles);
-        }
-    } else {
-        // ---------------- epilogue (warps 2..5) ----------------
-        const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
-        int acc = 0;
-        uint32_t acc_phase = 0;
-        for (int64_t tile = blockIdx.x; tile < total; tile += gridDim.x) {
-            const TileCoord c = decode(tile, tiles_j, tiles_i, a.tj0);
-            if (!tile_needed(c, a)) continue;
-            const int32_t m = c_mod[c.l];
-            const float inv_m = 1.0f / float(m);
-            if (!mbar_wait(tfull0 + 8 * acc, acc_phase, abort_flag, a.wait_cycles)) {
-                if (lane == 0) atomicOr(a.err, 4);
-                *abort_flag = 1;
-                break;
-            }
-            tc_fence_after();
-            const int64_t j = int64_t(c.tj) * kTileJ + quarter * 32 + lane;
-            uint8_t *out = a.U + int64_t(c.l) * a.Jp * a.Ip + j * a.Ip + int64_t(c.ti) * kTileI;
-            const uint32_t tbase = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(acc * kAccCols);
-#pragma unroll 1
-            for (int ch = 0; ch < kTileI / 32; ++ch) {
-                uint32_t r[32];
-                tmem_ld32(tbase + uint32_t(ch * 32), r);
-                uint32_t w[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    w[q] = mod_small(int32_t(r[4 * q]), m, inv_m) |
-                           (mod_small(int32_t(r[4 * q + 1]), m, inv_m) << 8) |
-                           (mod_small(int32_t(r[4 * q + 2]), m, inv_m) << 16) |
-                           (mod_small(int32_t(r[4 * q + 3]), m, inv_m) << 24);
-                }
-                uint4 *o = reinterpret_cast<uint4 *>(out + ch * 32);
-                o[0] = make_uint4(w[0], w[1], w[2], w[3]);
-                o[1] = make_uint4(w[4], w[5], w[6], w[7]);
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(tempty0 + 8 * acc);
-            if (++acc == 2) { acc = 0; acc_phase ^= 1; }
-        }
-    }
+    // this CTA's tiles: a strided walk over the raster order
+    TileSeq q;
+    q.raster = true;
+    q.first = blockIdx.x;
+    q.step = gridDim.x;
+    q.end = total;
+    q.tiles_j = tiles_j;
+    q.tiles_i = tiles_i;
+    q.tj0 = a.tj0;
+    q.tj = q.ti = 0;
+    RolePos pos;
+    residue_roles(&mapX, &mapY, a, q, seq_count(q, nmod), p, tmem, pos, warp, lane,
+                  int(blockIdx.x) == a.stall_cta);
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(kTmemCols)
-                     : "memory");
+        tmem_free_all(tmem);
     }
 }
 
@@ -375,49 +66,24 @@ std::atomic<int> g_stall_launches{0};
 std::atomic<long long> g_stall_wait{kWaitCycles};
 
 void take_stall(long long *wait_cycles, int *stall_cta) {
-    int n = g_stall_launches.load();
-    while (n > 0) {
-        if (g_stall_launches.compare_exchange_weak(n, n - 1)) {
-            *wait_cycles = g_stall_wait.load();
-            *stall_cta = 0;
-            return;
-        }
-    }
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaDriverEntryPointQueryResult q;
-        void *p = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    });
-    return fn;
-}
-
-// 3-D map over [kMaxModuli][rows][Kp] int8 with a (128 k, box_rows, 1) box.
-int make_map(CUtensorMap *map, const void *base, int64_t rows, int64_t kp, int box_rows) {
-    auto enc = encode_fn();
-    if (!enc) return set_error(BLASX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    cuuint64_t dims[3] = {cuuint64_t(kp), cuuint64_t(rows), cuuint64_t(kMaxModuli)};
-    cuuint64_t strides[2] = {cuuint64_t(kp), cuuint64_t(rows * kp)};
-    cuuint32_t box[3] = {cuuint32_t(kTileK), cuuint32_t(box_rows), 1};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(base), dims, strides,
-                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return set_error(BLASX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
-    return BLASX_OK;
+    if (take_residue_stall(wait_cycles)) *stall_cta = 0;
 }
 
 }  // namespace
 
+bool take_residue_stall(long long *wait_cycles) {
+    int n = g_stall_launches.load();
+    while (n > 0) {
+        if (g_stall_launches.compare_exchange_weak(n, n - 1)) {
+            *wait_cycles = g_stall_wait.load();
+            return true;
+        }
+    }
+    return false;
+}
+
 int prepare_residue_gemm_current_device() {
-    BX_CUDA(cudaMemcpyToSymbol(c_mod, kModuli, sizeof(kModuli)));
+    BX_CUDA(upload_moduli());
     BX_CUDA(cudaFuncSetAttribute(residue_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(kSmemBytes)));
     return BLASX_OK;
@@ -432,7 +98,7 @@ int launch_residue_gemm(const int8_t *X, const int8_t *Y, uint8_t *U, int64_t Jp
     static std::once_flag once;
     static int init_status = BLASX_OK;
     std::call_once(once, [] {
-        if (cudaMemcpyToSymbol(c_mod, kModuli, sizeof(kModuli)) != cudaSuccess ||
+        if (upload_moduli() != cudaSuccess ||
             cudaFuncSetAttribute(residue_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(kSmemBytes)) != cudaSuccess)
             init_status = BLASX_ERR_CUDA;

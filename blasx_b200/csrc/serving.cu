@@ -10,16 +10,21 @@
 //               operand cache is not copied again and not charged again.
 //               Requests behind one that waits for memory may pass it if they
 //               fit, until it has waited 50 ms (then its memory is kept free);
-//   in flight   every admitted request gets its own stream: its copies in,
-//               compute and copy out overlap with other requests' on the
-//               device, and requests that arrive meanwhile are admitted as
-//               slots and memory free up;
-//   mixing      small native FP64 / complex128 requests wait for their
-//               operands and are then run together by ONE grouped kernel
-//               launch whose grid holds the tiles of all of them, on the
-//               highest-priority stream; an emulated request's residue GEMM
-//               runs CTAs of bounded life (not one persistent CTA per SM),
-//               so that small requests' CTAs are scheduled in between;
+//   in flight   every admitted request gets its own stream for its copies in
+//               and out, which overlap with other requests' compute, and
+//               requests that arrive meanwhile are admitted as slots and
+//               memory free up;
+//   mixing      one persistent kernel (executor.cu) runs the work of every
+//               request in flight: native FP64 / complex128 DMMA tiles, FP32 /
+//               complex64 SIMT tiles, and each stage of emulated requests
+//               (statistics, decision, slices, tcgen05 residue tiles,
+//               reconstruction). The scheduler publishes a request's stage
+//               into the executor's task ring once its copies (or its
+//               previous stage) completed; the kernel's CTAs claim tasks of
+//               all requests in publication order, so their tiles share the
+//               SMs. Requests whose operand is stored as one triangle (SYMM,
+//               HEMM) or whose output is Hermitian run on their own kernels,
+//               alone, with the executor stopped;
 //   completion  detected by polling each request's last event; device memory
 //               is released, the B copy is kept in the operand cache (LRU,
 //               byte budget, pinned while in use) and the caller wakes up.
@@ -49,6 +54,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "executor.h"
 #include "host_pipeline.h"
 #include "kernels.h"
 #include "ozaki.h"
@@ -243,6 +249,7 @@ struct Request {
     Key bkey{};
     bool bkey_valid = false;
     bool grouped = false;
+    bool on_exec = false;  // computed by the persistent executor
     int stream_slot = -1;
     cudaEvent_t ev_in = nullptr, ev_done = nullptr;
     int stage = 0;  // 1 copying in (grouped: waiting for operands), 3 in flight to completion
@@ -267,6 +274,8 @@ struct Server {
     cudaStream_t batch_stream = nullptr;
     std::vector<std::shared_ptr<Request>> pending, inflight;
     Arena arena;
+    exec::Executor *ex = nullptr;
+    long long exec_launch_base = 0;  // executor launches before the last statistics reset
     int *err_words = nullptr;  // pinned, one per stream slot: the emulated path's device error word
 
     std::mutex cache_mu;
@@ -400,15 +409,18 @@ int admit(Server &s, Request *r, int slot) {
                                   cudaMemcpyHostToDevice, st));
         r->stats.h2d_bytes += double(es) * g.M * g.N;
     }
-    BX_CUDA(cudaEventRecord(r->ev_in, st));
-    if (r->grouped) {
-        r->stage = 1;  // compute joins the next grouped launch once the copies landed
-        return BLASX_OK;
-    }
     Gemm d = g;
     d.A = r->dA; d.lda = r->lda;
     d.B = r->dB; d.ldb = r->ldb;
     d.C = r->dC; d.ldc = r->ldc;
+    if (r->on_exec) {
+        // the executor runs its tiles once the copies (and its descriptor) landed
+        BX_TRY(exec::prepare(s.ex, slot, d, r->emulated, config().dgemm_mode.load(), r->ws, st));
+        BX_CUDA(cudaEventRecord(r->ev_in, st));
+        r->stage = 1;
+        return BLASX_OK;
+    }
+    BX_CUDA(cudaEventRecord(r->ev_in, st));
     d.max_cta_tiles = kResidueTilesPerCta;  // emulated path: let other requests' kernels in
     {
         HostTimer t(s.enqueue_s);
@@ -432,48 +444,64 @@ int admit(Server &s, Request *r, int slot) {
     return BLASX_OK;
 }
 
-// One grouped launch for every grouped request whose operands have landed.
-int launch_groups(Server &s) {
-    for (DType dt : {DType::F64, DType::C128}) {
-        std::vector<Request *> ready;
-        for (const auto &r : s.inflight)
-            if (r->grouped && r->stage == 1 && r->g.dt == dt && cudaEventQuery(r->ev_in) == cudaSuccess)
-                ready.push_back(r.get());
-        cudaGetLastError();
-        for (size_t off = 0; off < ready.size(); off += kMaxGroup) {
-            const size_t n = std::min(ready.size() - off, size_t(kMaxGroup));
-            std::vector<Gemm> gs;
-            for (size_t i = 0; i < n; ++i) {
-                Request *r = ready[off + i];
-                Gemm d = r->g;
-                d.A = r->dA; d.lda = r->lda;
-                d.B = r->dB; d.ldb = r->ldb;
-                d.C = r->dC; d.ldc = r->ldc;
-                gs.push_back(d);
+// Moves the executor's requests along: a request whose copies landed has its
+// first stage published; one whose device work completed gets its C copied
+// back. Returns whether anything moved.
+bool exec_progress(Server &s) {
+    bool progress = false;
+    for (const auto &rp : s.inflight) {
+        Request *r = rp.get();
+        if (!r->on_exec) continue;
+        if (r->stage == 1) {
+            const cudaError_t q = cudaEventQuery(r->ev_in);
+            if (q == cudaErrorNotReady) continue;
+            if (q != cudaSuccess) {
+                cudaGetLastError();
+                r->status = BLASX_ERR_CUDA;
+                r->stage = 4;  // failed: finished by the completion pass
+                progress = true;
+                continue;
             }
-            BX_TRY(launch_gemm_dmma_grouped(gs.data(), int(n), s.batch_stream));
-            cudaEvent_t ev;
-            BX_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-            BX_CUDA(cudaEventRecord(ev, s.batch_stream));
-            for (size_t i = 0; i < n; ++i) {
-                Request *r = ready[off + i];
-                cudaStream_t st = s.streams[size_t(r->stream_slot)];
-                const size_t es = elem_size(r->g.dt);
-                BX_CUDA(cudaStreamWaitEvent(st, ev, 0));
-                BX_CUDA(cudaMemcpy2DAsync(r->g.C, r->g.ldc * es, r->dC, r->ldc * es,
-                                          r->g.M * es, r->g.N, cudaMemcpyDeviceToHost, st));
-                r->stats.d2h_bytes += double(es) * r->g.M * r->g.N;
-                BX_CUDA(cudaEventRecord(r->ev_done, st));
-                r->stats.path = 1;
-                r->stage = 3;
+            if (exec::start(s.ex, r->stream_slot) != BLASX_OK) {
+                r->status = last_status();
+                r->stage = 4;
+            } else {
+                r->stage = 2;
             }
-            cudaEventDestroy(ev);
+            progress = true;
+        } else if (r->stage == 2) {
+            const int rc = exec::advance(s.ex, r->stream_slot);
+            if (rc == 0) continue;
+            progress = true;
+            int path = 1, moduli = 0;
+            exec::path_of(s.ex, r->stream_slot, &path, &moduli);
+            r->stats.path = path;
+            r->stats.moduli = moduli;
+            if (rc < 0) {
+                set_error(BLASX_ERR_TIMEOUT, "serving: a bounded device wait of the executor ran out");
+                r->status = BLASX_ERR_TIMEOUT;
+                r->stage = 4;
+                continue;
+            }
+            cudaStream_t st = s.streams[size_t(r->stream_slot)];
+            const Gemm &g = r->g;
+            const size_t es = elem_size(g.dt);
+            if (cudaMemcpy2DAsync(g.C, g.ldc * es, r->dC, r->ldc * es, g.M * es, g.N, cudaMemcpyDeviceToHost,
+                                  st) != cudaSuccess ||
+                cudaEventRecord(r->ev_done, st) != cudaSuccess) {
+                cudaGetLastError();
+                r->status = BLASX_ERR_CUDA;
+                r->stage = 4;
+                continue;
+            }
+            r->stats.d2h_bytes += double(es) * g.M * g.N;
+            r->stage = 3;
             std::lock_guard<std::mutex> lk(s.stat_mu);
-            s.grouped_launches += 1;
-            s.grouped_requests += static_cast<long long>(n);
+            s.grouped_requests += 1;
         }
     }
-    return BLASX_OK;
+    exec::pump(s.ex);
+    return progress;
 }
 
 void finish(Server &s, Request *r, int status) {
@@ -582,6 +610,12 @@ void loop(Server *sp) {
         // completions
         for (size_t i = 0; i < s.inflight.size();) {
             Request *r = s.inflight[i].get();
+            if (r->stage == 4) {
+                finish(s, r, r->status != BLASX_OK ? r->status : BLASX_ERR_CUDA);
+                s.inflight.erase(s.inflight.begin() + long(i));
+                progress = true;
+                continue;
+            }
             if (r->stage == 3) {
                 const cudaError_t q = cudaEventQuery(r->ev_done);
                 if (q == cudaSuccess || (q != cudaErrorNotReady)) {
@@ -594,8 +628,8 @@ void loop(Server *sp) {
             }
             ++i;
         }
-        // grouped launches of small native requests whose operands landed
-        launch_groups(s);
+        // the executor's requests: publish stages, copy finished results back
+        if (exec_progress(s)) progress = true;
         // admission: arrival order, except that while the oldest pending
         // request waits for memory, up to kLookahead requests behind it that
         // fit may pass it -- until it has waited kHeadWait; from then on
@@ -609,6 +643,17 @@ void loop(Server *sp) {
             std::shared_ptr<Request> rp = s.pending[idx];
             Request *r = rp.get();
             ++scanned;
+            if (!r->on_exec) {
+                // SYMM / HEMM operand forms and Hermitian outputs run on their own
+                // kernels, which cannot share the SMs with the executor: only
+                // when nothing else is in flight, with the executor stopped
+                if (!s.inflight.empty()) {
+                    if (idx == 0) break;  // keeps its place at the head
+                    ++idx;
+                    continue;
+                }
+                exec::stop(s.ex);
+            }
             // operand cache lookup for B
             Entry *hit = nullptr;
             {
@@ -680,7 +725,8 @@ void loop(Server *sp) {
             }
             progress = true;
         }
-        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(50));
+        // requests on the executor move on its completions: poll them closely
+        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(s.inflight.empty() ? 50 : 10));
     }
 }
 
@@ -705,8 +751,8 @@ int submit(const Gemm &g) {
     // small native requests are mixed into grouped launches
     r->flops = 0;
     r->emulated = need_ab && ozaki_selected(g, config().dgemm_mode.load());
-    r->grouped = need_ab && !r->emulated && (g.dt == DType::F64 || g.dt == DType::C128) && g.uplo == 0 &&
-                 g.flops() <= s->group_flops;
+    r->on_exec = exec::supports(g);
+    r->grouped = false;
     if (need_ab) {
         r->bkey = Key{g.B, g.ldb, g.rows_b(), g.cols_b(), int(g.dt),
                       fingerprint(g.B, g.ldb, g.rows_b(), g.cols_b(), es)};
@@ -755,10 +801,12 @@ int blasx_serve_start(size_t hbm_budget, size_t cache_bytes, int max_inflight) {
     s->max_inflight = max_inflight > 0 ? std::min(max_inflight, 64) : 8;
     int rc = s->arena.init(s->budget);
     if (rc == BLASX_OK) rc = bx::oz::upload_crt_tables();
+    if (rc == BLASX_OK) rc = bx::exec::create(s->max_inflight, &s->ex);
     if (rc == BLASX_OK && cudaHostAlloc(reinterpret_cast<void **>(&s->err_words),
                                         sizeof(int) * size_t(s->max_inflight), cudaHostAllocDefault) != cudaSuccess)
         rc = bx::set_error(BLASX_ERR_NOMEM, "serving: pinned error words");
     if (rc != BLASX_OK) {
+        bx::exec::destroy(s->ex);
         s->arena.release();
         delete s;
         return rc;
@@ -792,6 +840,7 @@ int blasx_serve_stop(void) {
     }
     s->cv.notify_all();
     s->thread.join();  // the loop drains queued and in-flight requests first
+    bx::exec::destroy(s->ex);
     {
         std::lock_guard<std::mutex> lk(s->cache_mu);
         for (auto &kv : s->cache) delete kv.second;
@@ -832,7 +881,11 @@ void blasx_serve_get_stats(blasx_serve_stats *out) {
     out->failed = s.failed;
     out->cache_hits = s.hits;
     out->cache_misses = s.misses;
-    out->grouped_launches = s.grouped_launches;
+    {
+        long long launches = 0, tasks = 0;
+        bx::exec::counters(s.ex, &launches, &tasks);
+        out->grouped_launches = launches - s.exec_launch_base;
+    }
     out->grouped_requests = s.grouped_requests;
     out->max_inflight_seen = s.max_seen;
     out->flops = s.flops;
@@ -870,6 +923,11 @@ int blasx_serve_reset_stats(void) {
     s.flops = 0;
     s.t_first = s.t_last = 0;
     s.submitted = s.completed = s.hits = s.misses = s.grouped_launches = s.grouped_requests = 0;
+    {
+        long long launches = 0, tasks = 0;
+        bx::exec::counters(s.ex, &launches, &tasks);
+        s.exec_launch_base = launches;
+    }
     s.failed = 0;
     s.max_seen = 0;
     s.memory_waits = s.head_holds = 0;

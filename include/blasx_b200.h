@@ -466,10 +466,13 @@ int blasx_test_fail_allocation(int nth);
  * re-entrant). While it runs, cblas_?gemm / ?gemm_ calls from any number of
  * host threads are queued to one scheduler thread that owns the device: it
  * admits requests when an in-flight slot is free and their device memory
- * fits hbm_budget (0 = 85% of free HBM), runs several at once on their own
- * streams (continuous batching), mixes small native FP64 / complex128
- * requests into one grouped kernel launch, and keeps copies of B operands in
- * an HBM operand cache of cache_bytes (0 = a quarter of the budget).
+ * fits hbm_budget (0 = 85% of free HBM), copies each one's operands on its
+ * own stream, and runs the compute of every request in flight in one
+ * persistent kernel whose CTAs take the tiles of all of them from a task
+ * queue the scheduler fills (continuous batching: native FP64 / complex128 /
+ * FP32 / complex64 tiles and every stage of emulated requests mix on the
+ * SMs); it keeps copies of B operands in an HBM operand cache of cache_bytes
+ * (0 = a quarter of the budget).
  * Operand identity: host pointer, leading dimension, stored shape, dtype and
  * a fingerprint of 1024 sampled elements plus the first and last column; a
  * caller that modifies an operand in place without touching those must call
@@ -484,7 +487,7 @@ int blasx_serve_invalidate(const void *host_ptr);
 typedef struct blasx_serve_stats {
     long long submitted, completed, failed;
     long long cache_hits, cache_misses;        /* B operands reused / copied */
-    long long grouped_launches, grouped_requests;
+    long long grouped_launches, grouped_requests; /* persistent-kernel launches; requests run by it */
     int max_inflight_seen, reserved;
     double p50_ms, p99_ms, mean_ms, max_ms;    /* submit -> completion */
     double flops, seconds, tflops;             /* first submit -> last completion */

@@ -123,8 +123,10 @@ def test_allocation_failure_returns_nomem(mode, case):
     else:
         blx.set_dgemm_mode(blx.MODE_NATIVE)
         M, N, K = 2048, 2048, 2048
-        budget = 48 << 20  # the operands do not fit: tile cache
+        budget = 48 << 20  # the operands do not fit: tile cache of 512^2 tiles
     blx.set_hbm_budget(budget)
+    if case == "out_of_core":
+        blx.set_tile(512)
     try:
         if case == "out_of_core":
             blx.finalize()  # the tile arena is allocated again by the next call
@@ -150,6 +152,7 @@ def test_allocation_failure_returns_nomem(mode, case):
         assert check(C)
     finally:
         blx.set_hbm_budget(0)
+        blx.set_tile(0)
 
 
 def test_allocation_failure_in_trsm(mode):
