@@ -263,6 +263,7 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
         cbuf.append(torch.empty(need, dtype=torch.uint8, pin_memory=True))
     errors = []
     lat = []  # (flops, seconds) per call, measured around the blocking call
+    slow = []  # (seconds, dtype, M, N, K, path) per call
 
     def worker(t):
         r = random.Random(seed + t)
@@ -282,6 +283,7 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
             fn(bx.CblasColMajor, bx.TRANS[ta], bx.TRANS[tb], M, N, K, alpha, a.data_ptr(), lda, b.data_ptr(), ldb,
                0.0, cbuf[t].data_ptr(), M)
             lat.append(((8.0 if dt == np.complex128 else 2.0) * M * N * K, time.perf_counter() - c0))
+            slow.append((time.perf_counter() - c0, np.dtype(dt).name, M, N, K, bx.call_stats()["path"]))
             if bx.last_status() != 0:
                 errors.append(bx.last_error())
 
@@ -309,10 +311,14 @@ def serving_load(bx, torch, n_req: int, dmax: int, threads: int, rate: float, se
             "executor_launches": st["grouped_launches"], "executor_requests": st["grouped_requests"],
             "max_inflight": st["max_inflight_seen"], "failed": st["failed"] + len(errors),
             "by_size_call_latency": classes,
+            "slowest_calls": [{"ms": 1e3 * t, "dtype": d, "mnk": [m, n, k], "path": pth}
+                              for t, d, m, n, k, pth in sorted(slow, reverse=True)[:5]],
             "scheduler": {"admit_seconds": st["admit_seconds"], "admit_max_ms": st["admit_max_ms"],
                           "memory_waits": st["memory_waits"], "head_holds": st["head_holds"],
                           "alloc_seconds": st["alloc_seconds"], "copy_seconds": st["copy_seconds"],
-                          "compute_enqueue_seconds": st["compute_enqueue_seconds"]},
+                          "compute_enqueue_seconds": st["compute_enqueue_seconds"],
+                          "mean_copy_in_ms": st["mean_copy_in_ms"], "mean_compute_ms": st["mean_compute_ms"],
+                          "mean_copy_out_ms": st["mean_copy_out_ms"]},
             "mix": "60% f64 / 30% f32 / 10% c128, dims log-uniform [64, dmax], 30% B reuse"}
 
 

@@ -56,7 +56,8 @@ class ServeStats(ctypes.Structure):
                 ("flops", _D), ("seconds", _D), ("tflops", _D),
                 ("admit_seconds", _D), ("admit_max_ms", _D), ("memory_waits", ctypes.c_longlong),
                 ("head_holds", ctypes.c_longlong), ("alloc_seconds", _D), ("copy_seconds", _D),
-                ("compute_enqueue_seconds", _D)]
+                ("compute_enqueue_seconds", _D), ("mean_copy_in_ms", _D), ("mean_compute_ms", _D),
+                ("mean_copy_out_ms", _D)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

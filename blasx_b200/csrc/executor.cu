@@ -36,6 +36,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -57,8 +58,19 @@ using dev::DmmaParams;
 using dev::SimtParams;
 
 constexpr int kThreads = 256;
-constexpr int64_t kRing = int64_t(1) << 16;  // task entries of the ring
-constexpr long long kIdleCycles = 4000000;    // ~2 ms without a task: the CTA exits
+constexpr int64_t kRing = int64_t(1) << 16;  // task entries of each ring
+// Two rings: lane 0 for requests of fewer than kFastFlops, lane 1 for the
+// rest. A CTA always looks at lane 0 first, so that small requests do not
+// wait behind the tiles of large ones.
+constexpr int kLanes = 2;
+constexpr double kFastFlops = 2e9;
+// The kernel's CTAs stay while the host keeps it running and leave together
+// when the host raises the stop flag (kLinger without work). A CTA that sees
+// no task for kIdleCycles leaves on its own: a bound for the case of a host
+// that stopped publishing without stopping the kernel, long enough not to
+// fire between the arrivals of a live request stream.
+constexpr long long kIdleCycles = 400000000;  // ~0.2 s
+constexpr double kLinger = 0.005;             // s without pending tasks before the host stops the kernel
 
 enum Kind : int32_t {
     kNone = 0,
@@ -112,13 +124,16 @@ struct alignas(128) ReqDesc {
 static_assert(sizeof(ReqDesc) % 16 == 0, "descriptor copied in 16-byte words");
 
 struct ExecArgs {
-    const Task *ring;                 // pinned host, device view
-    volatile uint32_t *done;          // pinned host: task i done <=> done[i % kRing] == i + 1
-    const volatile long long *tail;   // pinned host: tasks published
-    const volatile int *stop;         // pinned host: exit at the next claim
-    volatile int *err_host;           // pinned host, per slot: device error word seen
-    oz::Decision *dec_host;           // pinned host, per slot: the decision
-    unsigned long long *next;         // device: next task to claim
+    const Task *ring[kLanes];               // pinned host, device view
+    volatile uint32_t *done[kLanes];        // pinned host: task i done <=> done[i % kRing] == i + 1
+    const volatile long long *tail[kLanes]; // pinned host: tasks published
+    const volatile int *stop;               // pinned host: exit at the next claim
+    volatile int *err_host;                 // pinned host, per slot: device error word seen
+    oz::Decision *dec_host;                 // pinned host, per slot: the decision
+    unsigned long long *next;               // device, per lane: next task to claim
+    long long *dev_tail;                    // device, per lane: tasks known to be published
+    unsigned *poll_lock;              // device: one CTA at a time reads the host's tail
+    int *dev_stop;                    // device: the host's stop flag was seen
     const ReqDesc *descs;             // device, per slot
     unsigned long long *tasks_run;    // device counter
     long long idle_cycles;
@@ -155,33 +170,73 @@ __device__ __forceinline__ void st_release_sys(volatile uint32_t *p, uint32_t v)
     asm volatile("st.release.sys.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Claims the next published task (thread 0). False when the stop flag is
-// raised or no task came for idle_cycles.
-__device__ bool claim(const ExecArgs &a, Task *task, long long *index) {
+__device__ __forceinline__ long long ld_acquire_gpu(const long long *p) {
+    long long v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void max_release_gpu(long long *p, long long v) {
+    asm volatile("red.release.gpu.global.max.s64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Claims the next published task (thread 0), lane 0 first. False when the
+// stop flag is raised or no task came for idle_cycles. The tasks known to be
+// published are mirrored in device memory (dev_tail): the CTAs poll that,
+// and only when it shows nothing new does one of them at a time (poll_lock)
+// read the host's tails and stop flag across PCIe, with a growing pause
+// between looks while the rings stay empty.
+__device__ bool claim(const ExecArgs &a, Task *task, long long *index, int *lane) {
     const long long t0 = clock64();
+    unsigned pause = 64;  // ns
     for (;;) {
-        if (ld_acquire_sys(a.stop)) return false;
-        const long long tail = ld_acquire_sys(a.tail);
-        const unsigned long long i = ld_relaxed_gpu(a.next);
-        if (static_cast<long long>(i) < tail) {
-            if (atomicCAS(a.next, i, i + 1) == i) {
-                const volatile int4 *src = reinterpret_cast<const volatile int4 *>(a.ring + (i % kRing));
-                int4 *dst = reinterpret_cast<int4 *>(task);
+        bool known = false;
+#pragma unroll 1
+        for (int l = 0; l < kLanes; ++l) {
+            const long long tail = ld_acquire_gpu(a.dev_tail + l);
+            const unsigned long long i = ld_relaxed_gpu(a.next + l);
+            if (static_cast<long long>(i) >= tail) continue;
+            known = true;
+            if (atomicCAS(a.next + l, i, i + 1) != i) break;  // lost the race: look again from lane 0
+            const volatile int4 *src = reinterpret_cast<const volatile int4 *>(a.ring[l] + (i % kRing));
+            int4 v[sizeof(Task) / 16];
 #pragma unroll
-                for (int w = 0; w < int(sizeof(Task) / 16); ++w) {
-                    const int4 v = {src[w].x, src[w].y, src[w].z, src[w].w};
-                    dst[w] = v;
-                }
-                *index = static_cast<long long>(i);
-                // what the task reads was written before it was published: order
-                // the CTA's coming loads after that (no stale cached lines)
-                asm volatile("fence.acq_rel.gpu;" ::: "memory");
-                return true;
-            }
+            for (int w = 0; w < int(sizeof(Task) / 16); ++w) v[w] = {src[w].x, src[w].y, src[w].z, src[w].w};
+            int4 *dst = reinterpret_cast<int4 *>(task);
+#pragma unroll
+            for (int w = 0; w < int(sizeof(Task) / 16); ++w) dst[w] = v[w];
+            *index = static_cast<long long>(i);
+            *lane = l;
+            // what the task reads was written before it was published: order
+            // the CTA's coming loads after that (no stale cached lines)
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
+            return true;
+        }
+        if (known) {
+            pause = 64;
             continue;
         }
+        if (atomicCAS(a.poll_lock, 0u, 1u) == 0u) {
+            const int stop = ld_acquire_sys(a.stop);
+            bool more = false;
+#pragma unroll 1
+            for (int l = 0; l < kLanes; ++l) {
+                const long long host_tail = ld_acquire_sys(a.tail[l]);
+                if (host_tail > ld_acquire_gpu(a.dev_tail + l)) {
+                    max_release_gpu(a.dev_tail + l, host_tail);
+                    more = true;
+                }
+            }
+            if (stop) atomicExch(a.dev_stop, 1);
+            atomicExch(a.poll_lock, 0u);
+            if (more) {
+                pause = 64;
+                continue;
+            }
+        }
+        if (*reinterpret_cast<volatile int *>(a.dev_stop)) return false;
         if (clock64() - t0 > a.idle_cycles) return false;
-        __nanosleep(1000);
+        __nanosleep(pause);
+        if (pause < 8192) pause *= 2;
     }
 }
 
@@ -250,8 +305,10 @@ __device__ __forceinline__ void emulated_task(const ReqDesc &d, const Task &t, i
     }
 }
 
+// Not inlined: the tile's accumulators get the registers that the
+// executor's own loop state would otherwise take from them.
 template <bool CPLX, int KI>
-__device__ __forceinline__ void dmma_task(const ReqDesc &d, const Task &t, uint8_t *work) {
+__device__ __noinline__ void dmma_task(const ReqDesc &d, const Task &t, uint8_t *work) {
     double *smem = reinterpret_cast<double *>(work);
     for (int64_t tile = t.first; tile < t.first + t.count; ++tile) {
         if (d.akc) {
@@ -281,6 +338,7 @@ __global__ void __launch_bounds__(kThreads, 1) executor_kernel(const ExecArgs a)
     __shared__ int s_abort;
     __shared__ Task s_task;
     __shared__ long long s_index;
+    __shared__ int s_lane;
     __shared__ ReqDesc s_desc;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -306,9 +364,11 @@ __global__ void __launch_bounds__(kThreads, 1) executor_kernel(const ExecArgs a)
         if (tid == 0) {
             Task t;
             long long i = 0;
-            if (!claim(a, &t, &i)) t.kind = kNone;
+            int lane = 0;
+            if (!claim(a, &t, &i, &lane)) t.kind = kNone;
             s_task = t;
             s_index = i;
+            s_lane = lane;
         }
         __syncthreads();
         const Task t = s_task;
@@ -398,7 +458,7 @@ __global__ void __launch_bounds__(kThreads, 1) executor_kernel(const ExecArgs a)
                 if (e) a.err_host[t.slot] = e;
             }
             __threadfence_system();
-            st_release_sys(a.done + (s_index % kRing), uint32_t(s_index + 1));
+            st_release_sys(a.done[s_lane] + (s_index % kRing), uint32_t(s_index + 1));
             atomicAdd(a.tasks_run, 1ull);
         }
     }
@@ -425,7 +485,16 @@ struct Slot {
     int decide_stage = -1;        // index of the decision stage (emulated)
     int stage = -1;               // current stage
     long long first = 0, count = 0, scan = 0;  // ring indices of the current stage, first not yet seen done
+    int lane = 1;                 // its ring
     int path = 0, moduli = 0;
+};
+
+struct Lane {
+    Task *ring = nullptr;             // pinned host
+    volatile uint32_t *done = nullptr;
+    volatile long long *tail = nullptr;
+    long long published = 0, floor = 0;  // tasks published / first not seen done
+    bool is_done(long long i) const { return done[i % kRing] == uint32_t(i + 1); }
 };
 
 }  // namespace
@@ -438,49 +507,63 @@ public:
     cudaEvent_t ev_end = nullptr;
     bool launched = false;
     // pinned host
-    Task *ring = nullptr;
-    volatile uint32_t *done = nullptr;
-    volatile long long *tail = nullptr;
+    Lane lanes[kLanes];
     volatile int *stop_flag = nullptr;
     volatile int *err_host = nullptr;
     oz::Decision *dec_host = nullptr;
     ReqDesc *staging = nullptr;  // per slot, source of the descriptor copies
+    void *host_words = nullptr;  // the tails and the stop flag
     // device
-    unsigned long long *next = nullptr;
+    unsigned long long *next = nullptr;  // per lane, then the task counter, tails, lock and stop word
     unsigned long long *tasks_run = nullptr;
     ReqDesc *descs = nullptr;
-    long long published = 0, floor = 0;  // tasks published / first not seen done
     long long launches = 0;
     std::vector<Slot> state;
 
-    bool is_done(long long i) const { return done[i % kRing] == uint32_t(i + 1); }
+    bool stopping = false;       // the stop flag is raised; the kernel is draining
+    double idle_since = -1.0;    // when the last pending task completed (s), -1 while tasks are pending
     bool running() {
         if (!launched) return false;
         const cudaError_t q = cudaEventQuery(ev_end);
         if (q == cudaErrorNotReady) return true;
         if (q != cudaSuccess) cudaGetLastError();
         launched = false;
+        if (stopping) {
+            *stop_flag = 0;
+            stopping = false;
+        }
         return false;
+    }
+    static double now_s() {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
     }
     int launch() {
         ExecArgs a;
         void *p = nullptr;
-        BX_CUDA(cudaHostGetDevicePointer(&p, ring, 0));
-        a.ring = static_cast<const Task *>(p);
-        BX_CUDA(cudaHostGetDevicePointer(&p, const_cast<uint32_t *>(done), 0));
-        a.done = static_cast<volatile uint32_t *>(p);
-        BX_CUDA(cudaHostGetDevicePointer(&p, const_cast<long long *>(tail), 0));
-        a.tail = static_cast<const volatile long long *>(p);
+        for (int l = 0; l < kLanes; ++l) {
+            BX_CUDA(cudaHostGetDevicePointer(&p, lanes[l].ring, 0));
+            a.ring[l] = static_cast<const Task *>(p);
+            BX_CUDA(cudaHostGetDevicePointer(&p, const_cast<uint32_t *>(lanes[l].done), 0));
+            a.done[l] = static_cast<volatile uint32_t *>(p);
+            BX_CUDA(cudaHostGetDevicePointer(&p, const_cast<long long *>(lanes[l].tail), 0));
+            a.tail[l] = static_cast<const volatile long long *>(p);
+        }
         BX_CUDA(cudaHostGetDevicePointer(&p, const_cast<int *>(stop_flag), 0));
         a.stop = static_cast<const volatile int *>(p);
         BX_CUDA(cudaHostGetDevicePointer(&p, const_cast<int *>(err_host), 0));
         a.err_host = static_cast<volatile int *>(p);
         BX_CUDA(cudaHostGetDevicePointer(&p, dec_host, 0));
         a.dec_host = static_cast<oz::Decision *>(p);
-        a.next = next;
-        a.descs = descs;
+        a.next = next;  // next[0..kLanes)
         a.tasks_run = tasks_run;
+        a.dev_tail = reinterpret_cast<long long *>(next + kLanes + 1);
+        a.poll_lock = reinterpret_cast<unsigned *>(next + 2 * kLanes + 1);
+        a.dev_stop = reinterpret_cast<int *>(next + 2 * kLanes + 2);
+        a.descs = descs;
         a.idle_cycles = kIdleCycles;
+        *stop_flag = 0;
+        stopping = false;
+        BX_CUDA(cudaMemsetAsync(a.poll_lock, 0, 2 * sizeof(unsigned long long), stream));  // lock and stop word
         executor_kernel<<<unsigned(num_sms), kThreads, kDynSmem, stream>>>(a);
         BX_CUDA(cudaGetLastError());
         count_launch();
@@ -489,28 +572,51 @@ public:
         ++launches;
         return BLASX_OK;
     }
-    // Ring entry i is free once task i - kRing is done.
-    int publish(const Task &t) {
-        const long long i = published;
-        while (i >= kRing && !is_done(i - kRing)) {
+    // Entry i of a ring is free once its task i - kRing is done.
+    int publish(int l, const Task &t) {
+        Lane &ln = lanes[l];
+        const long long i = ln.published;
+        while (i >= kRing && !ln.is_done(i - kRing)) {
             BX_TRY(pump_kernel());
             std::this_thread::yield();
         }
-        ring[i % kRing] = t;
+        ln.ring[i % kRing] = t;
         std::atomic_thread_fence(std::memory_order_release);
-        *tail = i + 1;
-        published = i + 1;
+        *ln.tail = i + 1;
+        ln.published = i + 1;
         return BLASX_OK;
     }
+    bool pending() {
+        bool any = false;
+        for (Lane &ln : lanes) {
+            while (ln.floor < ln.published && ln.is_done(ln.floor)) ++ln.floor;
+            any = any || ln.floor < ln.published;
+        }
+        return any;
+    }
+    // Launches the kernel when tasks are pending and it is not running; stops
+    // it (without waiting) once nothing has been pending for kLinger.
     int pump_kernel() {
-        while (floor < published && is_done(floor)) ++floor;
-        if (floor < published && !running()) BX_TRY(launch());
+        const bool busy = pending();
+        const bool live = running();
+        if (busy) {
+            idle_since = -1.0;
+            if (!live) BX_TRY(launch());
+        } else if (live && !stopping) {
+            const double t = now_s();
+            if (idle_since < 0) idle_since = t;
+            else if (t - idle_since > kLinger) {
+                *stop_flag = 1;
+                std::atomic_thread_fence(std::memory_order_seq_cst);
+                stopping = true;
+            }
+        }
         return BLASX_OK;
     }
     int publish_stage(int slot, int k) {
         Slot &sl = state[size_t(slot)];
         sl.stage = k;
-        sl.first = published;
+        sl.first = lanes[sl.lane].published;
         sl.count = int64_t(sl.stages[size_t(k)].tasks.size());
         sl.scan = sl.first;
         for (Task t : sl.stages[size_t(k)].tasks) {
@@ -521,7 +627,7 @@ public:
                     t.wait = w;
                 }
             }
-            BX_TRY(publish(t));
+            BX_TRY(publish(sl.lane, t));
         }
         return pump_kernel();
     }
@@ -596,13 +702,19 @@ int create(int slots, Executor **out) {
         return true;
     };
     void *p = nullptr;
-    if (!host(&p, size_t(kRing) * sizeof(Task), cudaHostAllocMapped)) return fail(set_error(BLASX_ERR_NOMEM, "executor: ring"));
-    e->ring = static_cast<Task *>(p);
-    if (!host(&p, size_t(kRing) * sizeof(uint32_t), cudaHostAllocMapped)) return fail(set_error(BLASX_ERR_NOMEM, "executor: done flags"));
-    e->done = static_cast<volatile uint32_t *>(p);
-    if (!host(&p, 256, cudaHostAllocMapped)) return fail(set_error(BLASX_ERR_NOMEM, "executor: tail"));
-    e->tail = static_cast<volatile long long *>(p);
-    e->stop_flag = reinterpret_cast<volatile int *>(static_cast<char *>(p) + 128);
+    for (int l = 0; l < kLanes; ++l) {
+        if (!host(&p, size_t(kRing) * sizeof(Task), cudaHostAllocMapped))
+            return fail(set_error(BLASX_ERR_NOMEM, "executor: ring"));
+        e->lanes[l].ring = static_cast<Task *>(p);
+        if (!host(&p, size_t(kRing) * sizeof(uint32_t), cudaHostAllocMapped))
+            return fail(set_error(BLASX_ERR_NOMEM, "executor: done flags"));
+        e->lanes[l].done = static_cast<volatile uint32_t *>(p);
+    }
+    if (!host(&p, 256, cudaHostAllocMapped)) return fail(set_error(BLASX_ERR_NOMEM, "executor: tails"));
+    e->host_words = p;
+    for (int l = 0; l < kLanes; ++l)
+        e->lanes[l].tail = reinterpret_cast<volatile long long *>(static_cast<char *>(p) + 64 * l);
+    e->stop_flag = reinterpret_cast<volatile int *>(static_cast<char *>(p) + 64 * kLanes);
     if (!host(&p, sizeof(int) * size_t(slots), cudaHostAllocMapped)) return fail(set_error(BLASX_ERR_NOMEM, "executor: error words"));
     e->err_host = static_cast<volatile int *>(p);
     if (!host(&p, sizeof(oz::Decision) * size_t(slots), cudaHostAllocMapped)) return fail(set_error(BLASX_ERR_NOMEM, "executor: decisions"));
@@ -614,7 +726,7 @@ int create(int slots, Executor **out) {
         cudaGetLastError();
         return fail(set_error(BLASX_ERR_NOMEM, "executor: device tables"));
     }
-    e->tasks_run = e->next + 1;
+    e->tasks_run = e->next + kLanes;
     if (cudaMemset(e->next, 0, 256) != cudaSuccess ||
         cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_end, cudaEventDisableTiming) != cudaSuccess ||
@@ -635,9 +747,11 @@ void destroy(Executor *e) {
     if (e->stream) cudaStreamDestroy(e->stream);
     if (e->next) cudaFree(e->next);
     if (e->descs) cudaFree(e->descs);
-    if (e->ring) cudaFreeHost(e->ring);
-    if (e->done) cudaFreeHost(const_cast<uint32_t *>(e->done));
-    if (e->tail) cudaFreeHost(const_cast<long long *>(e->tail));
+    for (Lane &ln : e->lanes) {
+        if (ln.ring) cudaFreeHost(ln.ring);
+        if (ln.done) cudaFreeHost(const_cast<uint32_t *>(ln.done));
+    }
+    if (e->host_words) cudaFreeHost(e->host_words);
     if (e->err_host) cudaFreeHost(const_cast<int *>(e->err_host));
     if (e->dec_host) cudaFreeHost(e->dec_host);
     if (e->staging) cudaFreeHost(e->staging);
@@ -652,6 +766,7 @@ int prepare(Executor *e, int slot, const Gemm &g, bool emulated, int mode, void 
     sl = Slot{};
     sl.active = true;
     sl.dt = int(g.dt);
+    sl.lane = g.flops() < kFastFlops ? 0 : 1;
     ReqDesc &d = e->staging[slot];
     memset(static_cast<void *>(&d), 0, sizeof d);
     d.dt = int(g.dt);
@@ -751,7 +866,7 @@ int start(Executor *e, int slot) {
 int advance(Executor *e, int slot) {
     Slot &sl = e->state[size_t(slot)];
     if (!sl.active || sl.stage < 0) return 1;
-    while (sl.scan < sl.first + sl.count && e->is_done(sl.scan)) ++sl.scan;
+    while (sl.scan < sl.first + sl.count && e->lanes[sl.lane].is_done(sl.scan)) ++sl.scan;
     if (sl.scan < sl.first + sl.count) return 0;
     std::atomic_thread_fence(std::memory_order_acquire);
     if (e->err_host[slot]) {
@@ -760,6 +875,7 @@ int advance(Executor *e, int slot) {
     }
     if (sl.emulated && sl.stage == sl.decide_stage) {
         const int nmod = static_cast<volatile oz::Decision *>(e->dec_host)[slot].nmod;
+
         sl.moduli = nmod > 0 ? nmod : 0;
         if (nmod <= 0) {  // the native fallback, chosen on the device
             sl.stages.resize(size_t(sl.decide_stage + 1));
@@ -785,10 +901,7 @@ void path_of(Executor *e, int slot, int *path, int *moduli) {
 
 int pump(Executor *e) { return e->pump_kernel(); }
 
-bool idle(Executor *e) {
-    while (e->floor < e->published && e->is_done(e->floor)) ++e->floor;
-    return e->floor == e->published;
-}
+bool idle(Executor *e) { return !e->pending(); }
 
 int stop(Executor *e) {
     *e->stop_flag = 1;
@@ -798,6 +911,8 @@ int stop(Executor *e) {
         e->launched = false;
     }
     *e->stop_flag = 0;
+    e->stopping = false;
+    e->idle_since = -1.0;
     return BLASX_OK;
 }
 

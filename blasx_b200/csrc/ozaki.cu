@@ -228,6 +228,7 @@ int ozaki_run(const Gemm &g, cudaStream_t s, int mode, void *ws, int num_sms, vo
         BX_CUDA(cudaMemcpyAsync(dec_host, dec, sizeof(oz::Decision), cudaMemcpyDeviceToHost, s));
     if (err_host) BX_CUDA(cudaMemcpyAsync(err_host, err, sizeof(int), cudaMemcpyDeviceToHost, s));
     call_stats().path = 2;
+    call_stats().moduli = -1;  // decided on the device: resolved from dec_host once the stream has passed
     return BLASX_OK;
 }
 

@@ -108,7 +108,8 @@ cudaError_t dev_malloc(void **p, size_t bytes) {
 }
 
 void resolve_decision(blasx_call_stats &st) {
-    if (st.path != 2 || !g_ctx) return;
+    // moduli >= 0: already known (a served request reports its own decision)
+    if (st.path != 2 || st.moduli >= 0 || !g_ctx) return;
     const oz::Decision *d = static_cast<const oz::Decision *>(g_ctx->last_decision);
     st.moduli = d->nmod;
     if (d->nmod == 0) st.path = 4;  // native fallback chosen on the device

@@ -238,6 +238,7 @@ private:
 struct Request {
     Gemm g;
     double t_submit = 0, t_done = 0;
+    double t_admit = 0, t_in = 0, t_exec = 0;  // admitted, copies in landed, executor done
     std::promise<int> done;
     int status = BLASX_OK;
     // device side
@@ -292,6 +293,8 @@ struct Server {
     int max_seen = 0;
     double admit_s = 0, admit_max_s = 0;
     double alloc_s = 0, copy_s = 0, enqueue_s = 0;  // parts of admit_s
+    double phase_in_s = 0, phase_exec_s = 0, phase_out_s = 0;  // executor requests: summed phases
+    long long phase_n = 0;
 };
 
 std::mutex g_server_mu;
@@ -380,6 +383,7 @@ int admit(Server &s, Request *r, int slot) {
     const size_t es = elem_size(g.dt);
     cudaStream_t st = s.streams[size_t(slot)];
     r->stream_slot = slot;
+    r->t_admit = now_s();
     const bool need_ab = !(g.alpha_zero() || g.K == 0);
     const bool read_c = !g.beta_zero() || g.uplo != 0;  // a triangular output keeps the rest of C
     BX_CUDA(cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming));
@@ -462,6 +466,7 @@ bool exec_progress(Server &s) {
                 progress = true;
                 continue;
             }
+            r->t_in = now_s();
             if (exec::start(s.ex, r->stream_slot) != BLASX_OK) {
                 r->status = last_status();
                 r->stage = 4;
@@ -473,6 +478,7 @@ bool exec_progress(Server &s) {
             const int rc = exec::advance(s.ex, r->stream_slot);
             if (rc == 0) continue;
             progress = true;
+            r->t_exec = now_s();
             int path = 1, moduli = 0;
             exec::path_of(s.ex, r->stream_slot, &path, &moduli);
             r->stats.path = path;
@@ -561,6 +567,12 @@ void finish(Server &s, Request *r, int status) {
     r->stats.seconds = r->t_done - r->t_submit;
     {
         std::lock_guard<std::mutex> lk(s.stat_mu);
+        if (r->on_exec && status == BLASX_OK && r->t_exec > 0) {
+            s.phase_in_s += r->t_in - r->t_admit;
+            s.phase_exec_s += r->t_exec - r->t_in;
+            s.phase_out_s += r->t_done - r->t_exec;
+            s.phase_n += 1;
+        }
         s.completed += 1;
         if (status != BLASX_OK) s.failed += 1;
         s.latencies.push_back(r->t_done - r->t_submit);
@@ -598,6 +610,12 @@ void loop(Server *sp) {
         {
             std::unique_lock<std::mutex> lk(s.mu);
             if (s.pending.empty() && s.inflight.empty()) {
+                if (s.queue.empty() && !s.stopping) {
+                    // nothing to do: give the SMs back before sleeping
+                    lk.unlock();
+                    exec::stop(s.ex);
+                    lk.lock();
+                }
                 s.cv.wait(lk, [&] { return s.stopping || !s.queue.empty(); });
                 if (s.stopping && s.queue.empty()) return;
             }
@@ -898,6 +916,11 @@ void blasx_serve_get_stats(blasx_serve_stats *out) {
     out->alloc_seconds = s.alloc_s;
     out->copy_seconds = s.copy_s;
     out->compute_enqueue_seconds = s.enqueue_s;
+    if (s.phase_n) {
+        out->mean_copy_in_ms = s.phase_in_s / double(s.phase_n) * 1e3;
+        out->mean_compute_ms = s.phase_exec_s / double(s.phase_n) * 1e3;
+        out->mean_copy_out_ms = s.phase_out_s / double(s.phase_n) * 1e3;
+    }
     if (!s.latencies.empty()) {
         std::vector<double> l = s.latencies;
         std::sort(l.begin(), l.end());
@@ -933,6 +956,8 @@ int blasx_serve_reset_stats(void) {
     s.memory_waits = s.head_holds = 0;
     s.admit_s = s.admit_max_s = 0;
     s.alloc_s = s.copy_s = s.enqueue_s = 0;
+    s.phase_in_s = s.phase_exec_s = s.phase_out_s = 0;
+    s.phase_n = 0;
     return BLASX_OK;
 }
 

@@ -496,6 +496,8 @@ typedef struct blasx_serve_stats {
     long long head_holds;                      /* passes stopped to keep memory for the oldest request */
     double alloc_seconds, copy_seconds;        /* parts of admit_seconds: device allocation, copy calls */
     double compute_enqueue_seconds;            /* part of admit_seconds: enqueueing the GEMM kernels */
+    double mean_copy_in_ms, mean_compute_ms, mean_copy_out_ms; /* per request: admitted -> operands on the
+                                                  device -> result computed -> result on the host */
 } blasx_serve_stats;
 void blasx_serve_get_stats(blasx_serve_stats *out);
 int blasx_serve_reset_stats(void);

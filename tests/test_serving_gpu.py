@@ -121,6 +121,8 @@ def test_alone_equals_mix_with_emulated_requests(serving):
         alone = []
         for r in reqs:
             alone.append(run(blx, r))
+            if r["M"] >= 1000:  # large enough for auto mode: the executor runs it emulated
+                assert blx.call_stats()["path"] == 2, (r["M"], r["N"], r["K"], r["dt"], blx.call_stats())
         out = [None] * len(reqs)
         errs = []
 
