@@ -10,7 +10,8 @@
 // Task bodies are the same device code as the standalone kernels:
 //   kDmma     one C tile of a native FP64 (128x128) or complex128 (64x128)
 //             request on the FP64 tensor pipe (dmma_tile.cuh)
-//   kSimt     one 64x64 C tile of a native FP32 or complex64 request
+//   kSimt     one C tile of a native FP32 (128x128) or complex64 (64x64)
+//             request on the CUDA cores (simt_tile.cuh)
 //   kScale    beta-scaling of a range of C (alpha == 0 or K == 0)
 //   kZero     clearing of an emulated request's statistics and error word
 //   kStats    row statistics of op(A) or op(B), a range of blocks
@@ -107,6 +108,7 @@ struct alignas(128) ReqDesc {
     SimtParams<double> sd;  // scale only
     SimtParams<z2> sz;      // scale only
     int64_t simt_tm;        // SIMT tiles along M
+    int64_t simt_edge;      // SIMT tile edge: 128 (FP32) or 64 (complex64)
     // emulated
     oz::View va, vb;
     oz::RowStats sa, sb, sbd;
@@ -148,7 +150,8 @@ constexpr size_t kWorkBytes = cmax(
          cmax(dev::dmma_smem_bytes<false, false, true>(), dev::dmma_smem_bytes<false, false, false>())),
     cmax(cmax(cmax(dev::dmma_smem_bytes<true, true, true>(), dev::dmma_smem_bytes<true, true, false>()),
               cmax(dev::dmma_smem_bytes<true, false, true>(), dev::dmma_smem_bytes<true, false, false>())),
-         cmax(oz::kRingBytes, cmax(oz::slice_rc_smem_bytes<1>(), dev::simt_smem_bytes<c2>()))));
+         cmax(oz::kRingBytes, cmax(oz::slice_rc_smem_bytes<1>(),
+                                   cmax(dev::simt_smem_bytes<c2>(), dev::sgemm128_smem_bytes())))));
 constexpr size_t kDynSmem = kWorkBytes + 1024;
 
 __device__ __forceinline__ long long ld_acquire_sys(const volatile long long *p) {
@@ -425,8 +428,14 @@ __global__ void __launch_bounds__(kThreads, 1) executor_kernel(const ExecArgs a)
                 else dmma_task<false, 16>(d, t, work);
                 break;
             case kSimt:
-                if (dt == DType::F32) simt_task<float>(d.sf, d.simt_tm, t, work);
-                else simt_task<c2>(d.sc, d.simt_tm, t, work);
+                if (dt == DType::F32) {
+                    for (int64_t tile = t.first; tile < t.first + t.count; ++tile) {
+                        dev::sgemm128_tile(d.sf, tile % d.simt_tm, tile / d.simt_tm, reinterpret_cast<float *>(work));
+                        __syncthreads();
+                    }
+                } else {
+                    simt_task<c2>(d.sc, d.simt_tm, t, work);
+                }
                 break;
             case kScale:
                 if (dt == DType::F32) scale_task<float>(d, t, tid);
@@ -673,10 +682,12 @@ Stage native_stage(ReqDesc &d, const Gemm &g, int slot) {
         d.dp = g.dt == DType::F64 ? dev::make_params<false, 0>(g) : dev::make_params<true, 0>(g);
         add_tasks(st, kDmma, slot, 0, int64_t(d.dp.tiles_m) * d.dp.tiles_n, 1);
     } else {
+        // FP32 on the 128 x 128 tile, complex64 on the 64 x 64 one
         if (g.dt == DType::F32) d.sf = simt_params<float>(g);
         else d.sc = simt_params<c2>(g);
-        d.simt_tm = cdiv(g.M, dev::kSimtBM);
-        add_tasks(st, kSimt, slot, 0, d.simt_tm * cdiv(g.N, dev::kSimtBN), 1);
+        d.simt_edge = g.dt == DType::F32 ? dev::sg::TM : dev::kSimtBM;
+        d.simt_tm = cdiv(g.M, d.simt_edge);
+        add_tasks(st, kSimt, slot, 0, d.simt_tm * cdiv(g.N, d.simt_edge), 1);
     }
     return st;
 }

@@ -28,11 +28,6 @@ int launch_gemm_simt(const Gemm &g, cudaStream_t s);
 int launch_gemm_dmma(const Gemm &g, cudaStream_t s);
 bool dmma_supported(const Gemm &g);
 
-// Up to kMaxGroup problems of one dtype (FP64 or complex128) in a single
-// launch: the tiles of all of them share one grid (device pointers, no
-// allocation; alpha == 0 / K == 0 problems must be scaled separately).
-constexpr int kMaxGroup = 96;
-int launch_gemm_dmma_grouped(const Gemm *gs, int n, cudaStream_t s);
 
 // Device-resident GEMM of any dtype through the best available path.
 // Uses library-owned scratch memory for the Ozaki path.

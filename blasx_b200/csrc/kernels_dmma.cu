@@ -5,23 +5,10 @@
 // sm_100a kernel built on DMMA (mma.sync m16n8k{4,8,16}, f64 in, f64
 // accumulate).
 //
-// Structure (one CTA per 128x128 C tile for FP64, 64x128 for complex128):
-//   * 8 warps in a 2 x 4 grid; a warp owns a 64x32 (FP64) or 32x32 (complex)
-//     accumulator block in registers;
-//   * operand tiles are staged global -> shared through a 3-stage cp.async
-//     ring. Each operand keeps the contiguity it has in global memory: a
-//     k-contiguous source (A transposed, B not) lands as [m][k] rows padded
-//     by 4 doubles, an m/n-contiguous source as [k][m] rows padded by 4, so
-//     every copy is a 16-byte cp.async along the contiguous direction and
-//     every fragment load (8 rows x 4 doubles or 4 rows x 8 doubles) falls on
-//     disjoint bank groups;
-//   * ragged edges: the src-size operand of cp.async zero-fills the part of
-//     a chunk beyond M, N or K, so nothing outside the matrices is read;
-//   * the epilogue applies alpha / beta in FP64 and never reads C when
-//     beta == 0 (BLAS semantics).
-// Complex128 keeps real and imaginary planes separately in shared memory and
-// issues four real DMMAs per fragment pair (re += ar br - ai bi,
-// im += ar bi + ai br); conjugation flips the sign of the imaginary fragment.
+// The tile itself (DMMA fragments, the cp.async ring, the alpha / beta
+// epilogue) is dmma_tile.cuh, shared with the serving executor; this file
+// holds the launches: one CTA per C tile, with the CTA geometry chosen by
+// the estimated SM utilisation.
 #include <cstdint>
 #include <cstdlib>
 
@@ -39,43 +26,6 @@ __global__ void __launch_bounds__(Tile<CPLX, G>::THREADS, 1) dmma_gemm_kernel(co
     if (p.guard && *p.guard != 0) return;  // the emulated path produced C
     extern __shared__ __align__(16) double smem[];
     dmma_tile<CPLX, AKC, BKC, KI, G>(p, blockIdx.x, smem);
-}
-
-// Several problems in one launch: CTA b works on tile b - start[q] of the
-// problem q with start[q] <= b < start[q + 1]; the operand layouts of each
-// problem are chosen at run time (uniform within a CTA).
-// Problem table of a grouped launch, passed by value as a kernel parameter
-// (no device allocation): problem q owns CTAs [start[q], start[q + 1]).
-struct GroupTable {
-    int n;
-    int start[kMaxGroup + 1];
-    DmmaParams p[kMaxGroup];
-};
-
-// Several problems in one launch: CTA b works on tile b - start[q] of the
-// problem q with start[q] <= b < start[q + 1]; the operand layouts of each
-// problem are chosen at run time (uniform within a CTA).
-template <bool CPLX, int KI>
-__global__ void __launch_bounds__(Tile<CPLX>::THREADS, 1)
-    dmma_grouped_kernel(const __grid_constant__ GroupTable tab) {
-    extern __shared__ __align__(16) double smem[];
-    const int b = int(blockIdx.x);
-    int lo = 0, hi = tab.n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (tab.start[mid] <= b) lo = mid;
-        else hi = mid - 1;
-    }
-    const DmmaParams p = tab.p[lo];
-    const int tile = b - tab.start[lo];
-    const bool akc = p.ta != NoTrans, bkc = p.tb == NoTrans;
-    if (akc) {
-        if (bkc) dmma_tile<CPLX, true, true, KI>(p, tile, smem);
-        else dmma_tile<CPLX, true, false, KI>(p, tile, smem);
-    } else {
-        if (bkc) dmma_tile<CPLX, false, true, KI>(p, tile, smem);
-        else dmma_tile<CPLX, false, false, KI>(p, tile, smem);
-    }
 }
 
 template <bool CPLX, bool AKC, bool BKC, int KI, int G>
@@ -169,57 +119,11 @@ template <bool CPLX> int launch_t(const Gemm &g, cudaStream_t s) {
     else return dmma_geometry(g.M, g.N) == 1 ? launch_g<CPLX, 1>(g, s) : launch_g<CPLX, 0>(g, s);
 }
 
-template <bool CPLX, int KI> int launch_grouped_t(const GroupTable &tab, int tiles, cudaStream_t s) {
-    using TL = Tile<CPLX>;
-    constexpr int PLANES = CPLX ? 2 : 1;
-    constexpr int pa = SmemOp<TL::BM, TL::BK, true>::plane > SmemOp<TL::BM, TL::BK, false>::plane
-                           ? SmemOp<TL::BM, TL::BK, true>::plane
-                           : SmemOp<TL::BM, TL::BK, false>::plane;
-    constexpr int pb = SmemOp<TL::BN, TL::BK, true>::plane > SmemOp<TL::BN, TL::BK, false>::plane
-                           ? SmemOp<TL::BN, TL::BK, true>::plane
-                           : SmemOp<TL::BN, TL::BK, false>::plane;
-    // each layout combination places sB after its own A stages: size for the largest
-    constexpr size_t smem = size_t(TL::STAGES) * PLANES * (pa + pb) * sizeof(double);
-    static_assert(smem <= 227 * 1024, "shared memory budget");
-    auto kern = dmma_grouped_kernel<CPLX, KI>;
-    BX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kern<<<unsigned(tiles), TL::THREADS, smem, s>>>(tab);
-    BX_CUDA(cudaGetLastError());
-    count_launch();
-    return BLASX_OK;
-}
-
 }  // namespace
 
 bool dmma_supported(const Gemm &g) {
     return (g.dt == DType::F64 || g.dt == DType::C128) && g.M <= INT32_MAX && g.N <= INT32_MAX &&
            g.K <= INT32_MAX;
-}
-
-int launch_gemm_dmma_grouped(const Gemm *gs, int n, cudaStream_t s) {
-    if (n <= 0) return BLASX_OK;
-    if (n > kMaxGroup) return set_error(BLASX_ERR_ARG, "grouped launch of %d > %d problems", n, kMaxGroup);
-    const bool cplx = gs[0].dt == DType::C128;
-    GroupTable tab;
-    tab.n = n;
-    int64_t tiles = 0;
-    for (int i = 0; i < n; ++i) {
-        if (gs[i].dt != gs[0].dt || (gs[i].dt != DType::F64 && gs[i].dt != DType::C128))
-            return set_error(BLASX_ERR_ARG, "grouped launch needs one FP64 or complex128 dtype");
-        tab.p[i] = cplx ? make_params<true>(gs[i]) : make_params<false>(gs[i]);
-        tab.p[i].guard = nullptr;
-        tab.start[i] = int(tiles);
-        tiles += int64_t(tab.p[i].tiles_m) * tab.p[i].tiles_n;
-    }
-    tab.start[n] = int(tiles);
-    if (tiles == 0) return BLASX_OK;
-    if (tiles > INT32_MAX) return set_error(BLASX_ERR_UNSUPPORTED, "grouped launch too large");
-    if (cplx) return launch_grouped_t<true, 4>(tab, int(tiles), s);
-    switch (dmma_k()) {
-        case 4: return launch_grouped_t<false, 4>(tab, int(tiles), s);
-        case 8: return launch_grouped_t<false, 8>(tab, int(tiles), s);
-        default: return launch_grouped_t<false, 16>(tab, int(tiles), s);
-    }
 }
 
 int launch_gemm_dmma(const Gemm &g, cudaStream_t s) {

@@ -44,13 +44,13 @@ __global__ void decide_kernel(RowStats sa, int64_t Ra, RowStats sb, int64_t Rb, 
 }
 
 template <typename T, int ROLE>
-__global__ void __launch_bounds__(256) slice_kc_kernel(View v, RowStats st, const Decision *dec, int *expo,
+__global__ void __launch_bounds__(256, ROLE == 0 ? 4 : (ROLE == 1 ? 3 : 2)) slice_kc_kernel(View v, RowStats st, const Decision *dec, int *expo,
                                                        SliceOut o) {
     slice_kc_body<T, ROLE>(v, st, dec, expo, o, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
 template <typename T, int ROLE>
-__global__ void __launch_bounds__(256) slice_rc_kernel(View v, RowStats st, const Decision *dec, int *expo,
+__global__ void __launch_bounds__(256, ROLE == 0 ? 4 : (ROLE == 1 ? 3 : 2)) slice_rc_kernel(View v, RowStats st, const Decision *dec, int *expo,
                                                        SliceOut o) {
     __shared__ __align__(16) unsigned char smem[slice_rc_smem_bytes<ROLE>()];
     slice_rc_body<T, ROLE>(v, st, dec, expo, o, blockIdx.x, blockIdx.y, threadIdx.x, smem);

@@ -475,7 +475,31 @@ __device__ __forceinline__ void slice_rc_body(const View &v, const RowStats &st,
         if (bx == 0 && r < v.R) expo[r] = e;
     }
     __syncthreads();
-    {
+    bool paired = false;
+    if constexpr (std::is_same<T, double>::value) {
+        // FP64 rows in pairs: one 16-byte load covers rows r, r + 1 of one k
+        // (ld even, 16-byte aligned base; the block's first row is even)
+        const double *p = static_cast<const double *>(v.p);
+        if ((v.ld & 1) == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+            paired = true;
+            const int tr = (tid & 31) * 2, tk = tid >> 5;  // tk in 0..7
+            const int64_t r = r0 + tr;
+            const int e0 = s_e[tr], e1 = s_e[tr + 1];
+#pragma unroll
+            for (int i = 0; i < KT / 8; ++i) {
+                const int kk = tk + 8 * i;
+                double2 x = make_double2(0.0, 0.0);
+                if (k0 + kk < v.K) {
+                    const double *q = p + r + (k0 + kk) * v.ld;
+                    if (r + 1 < v.R) x = __ldcg(reinterpret_cast<const double2 *>(q));
+                    else if (r < v.R) x.x = q[0];
+                }
+                tile[0][kk][tr] = scale_round(x.x, e0);
+                tile[0][kk][tr + 1] = scale_round(x.y, e1);
+            }
+        }
+    }
+    if (!paired) {
         const int tr = tid & 63, tk = tid >> 6;  // tk in 0..3
         const int64_t r = r0 + tr;
         const int e = s_e[tr];
@@ -491,8 +515,9 @@ __device__ __forceinline__ void slice_rc_body(const View &v, const RowStats &st,
     __syncthreads();
     constexpr int TPR = KT / 16;  // threads per row and component
     static_assert(64 * TPR * CPL == 256, "one 16-k word per thread");
+    // a warp reads 32 consecutive rows of one k-group: conflict-free
     const int comp = tid / (64 * TPR), idx = tid % (64 * TPR);
-    const int wr = idx / TPR, wk = (idx % TPR) * 16;
+    const int wr = idx % 64, wk = (idx / 64) * 16;
     Digits d[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) d[q] = digits_of(tile[comp][wk + q][wr]);

@@ -249,11 +249,10 @@ struct Request {
     Entry *bcache = nullptr;  // cached B in use
     Key bkey{};
     bool bkey_valid = false;
-    bool grouped = false;
     bool on_exec = false;  // computed by the persistent executor
     int stream_slot = -1;
     cudaEvent_t ev_in = nullptr, ev_done = nullptr;
-    int stage = 0;  // 1 copying in (grouped: waiting for operands), 3 in flight to completion
+    int stage = 0;  // 1 copying in, 2 on the executor, 3 copying out, 4 failed
     double flops = 0;
     blasx_call_stats stats{};
 };
@@ -261,7 +260,6 @@ struct Request {
 struct Server {
     size_t budget = 0, cache_budget = 0;
     int max_inflight = 8;
-    double group_flops = 4e9;
 
     std::mutex mu;
     std::condition_variable cv;
@@ -272,7 +270,6 @@ struct Server {
     // scheduler-owned
     std::vector<cudaStream_t> streams;
     std::vector<bool> stream_busy;
-    cudaStream_t batch_stream = nullptr;
     std::vector<std::shared_ptr<Request>> pending, inflight;
     Arena arena;
     exec::Executor *ex = nullptr;
@@ -766,11 +763,9 @@ int submit(const Gemm &g) {
     Request *r = rp.get();
     r->g = g;
     r->t_submit = now_s();
-    // small native requests are mixed into grouped launches
     r->flops = 0;
     r->emulated = need_ab && ozaki_selected(g, config().dgemm_mode.load());
     r->on_exec = exec::supports(g);
-    r->grouped = false;
     if (need_ab) {
         r->bkey = Key{g.B, g.ldb, g.rows_b(), g.cols_b(), int(g.dt),
                       fingerprint(g.B, g.ldb, g.rows_b(), g.cols_b(), es)};
@@ -832,12 +827,9 @@ int blasx_serve_start(size_t hbm_budget, size_t cache_bytes, int max_inflight) {
     memset(s->err_words, 0, sizeof(int) * size_t(s->max_inflight));
     s->streams.resize(size_t(s->max_inflight));
     s->stream_busy.assign(size_t(s->max_inflight), false);
-    // the grouped launches of small requests get the highest stream priority:
-    // when CTAs of a large request's kernel retire, theirs are scheduled first
-    int prio_low = 0, prio_high = 0;
-    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
-    for (auto &st : s->streams) cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_low);
-    cudaStreamCreateWithPriority(&s->batch_stream, cudaStreamNonBlocking, prio_high);
+    // the requests' streams carry their copies (and, for requests the executor
+    // does not run, their kernels)
+    for (auto &st : s->streams) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     s->thread = std::thread(loop, s);
     g_server = s;
     g_active.store(true, std::memory_order_release);
@@ -864,7 +856,6 @@ int blasx_serve_stop(void) {
         for (auto &kv : s->cache) delete kv.second;
     }
     for (auto st : s->streams) cudaStreamDestroy(st);
-    cudaStreamDestroy(s->batch_stream);
     s->arena.release();
     cudaFreeHost(s->err_words);
     std::lock_guard<std::mutex> lk(g_server_mu);
