@@ -66,7 +66,7 @@ class ServeStats(ctypes.Structure):
 class CallStats(ctypes.Structure):
     _fields_ = [("seconds", _D), ("h2d_bytes", _D), ("d2h_bytes", _D), ("cache_hits", _D),
                 ("cache_misses", _D), ("evictions", _D), ("path", _I), ("moduli", _I),
-                ("tile", _I), ("reserved", _I)]
+                ("tile", _I), ("host_copy", _I)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -123,6 +123,7 @@ def lib() -> ctypes.CDLL:
         L.blasx_set_dgemm_mode.argtypes = [_I]
         L.blasx_set_hbm_budget.argtypes = [ctypes.c_size_t]
         L.blasx_set_tile.argtypes = [_I]
+        L.blasx_set_host_staging.argtypes = [_I]
         L.blasx_get_call_stats.argtypes = [ctypes.POINTER(CallStats)]
         L.blasx_dgemm_device.argtypes = [_I] * 5 + [_D, _P, _I, _P, _I, _D, _P, _I, _P]
         L.blasx_sgemm_device.argtypes = [_I] * 5 + [_F, _P, _I, _P, _I, _F, _P, _I, _P]
@@ -558,6 +559,13 @@ def set_hbm_budget(nbytes: int) -> int:
 
 def set_tile(tile: int) -> int:
     return lib().blasx_set_tile(tile)
+
+
+def set_host_staging(on: bool) -> int:
+    """Pageable host operands: staged through pinned bounce buffers (True,
+    the default) or registered for the call (False). Returns the previous
+    setting."""
+    return lib().blasx_set_host_staging(1 if on else 0)
 
 
 def finalize() -> int:

@@ -17,8 +17,9 @@
 //   tiled     otherwise: the HBM tile cache with an explicit byte budget
 //             (tile_engine.cu), native kernels.
 //
-// Host buffers that are not pinned are registered for the call (full
-// ld x columns extent) so that every copy is an asynchronous DMA.
+// Host buffers that are not pinned are staged through pinned bounce buffers
+// (staging.h), or registered for the call (full ld x columns extent) when
+// staging is switched off, so that every copy is an asynchronous DMA.
 #include <algorithm>
 #include <chrono>
 #include <vector>
@@ -89,16 +90,16 @@ int copy_panel_in(const Gemm &g, const DeviceOps &d, int64_t j0, int64_t j1, boo
         const char *hb = static_cast<const char *>(g.B);
         char *db = static_cast<char *>(d.B);
         if (g.tb == NoTrans) {  // K x N stored: columns j0..j1
-            BX_CUDA(cudaMemcpy2DAsync(db + j0 * d.ldb * es, d.ldb * es, hb + j0 * g.ldb * es,
+            BX_TRY(copy2d(db + j0 * d.ldb * es, d.ldb * es, hb + j0 * g.ldb * es,
                                       g.ldb * es, g.K * es, w, cudaMemcpyHostToDevice, s));
         } else {  // N x K stored: rows j0..j1
-            BX_CUDA(cudaMemcpy2DAsync(db + j0 * es, d.ldb * es, hb + j0 * es, g.ldb * es, w * es,
+            BX_TRY(copy2d(db + j0 * es, d.ldb * es, hb + j0 * es, g.ldb * es, w * es,
                                       g.K, cudaMemcpyHostToDevice, s));
         }
         st.h2d_bytes += double(w) * g.K * es;
     }
     if (read_c) {
-        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.C) + j0 * d.ldc * es, d.ldc * es,
+        BX_TRY(copy2d(static_cast<char *>(d.C) + j0 * d.ldc * es, d.ldc * es,
                                   static_cast<const char *>(g.C) + j0 * g.ldc * es, g.ldc * es,
                                   g.M * es, w, cudaMemcpyHostToDevice, s));
         st.h2d_bytes += double(w) * g.M * es;
@@ -109,7 +110,7 @@ int copy_panel_in(const Gemm &g, const DeviceOps &d, int64_t j0, int64_t j1, boo
 int copy_panel_out(const Gemm &g, const DeviceOps &d, int64_t j0, int64_t j1, cudaStream_t s,
                    blasx_call_stats &st) {
     const size_t es = elem_size(g.dt);
-    BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(g.C) + j0 * g.ldc * es, g.ldc * es,
+    BX_TRY(copy2d(static_cast<char *>(g.C) + j0 * g.ldc * es, g.ldc * es,
                               static_cast<const char *>(d.C) + j0 * d.ldc * es, d.ldc * es,
                               g.M * es, j1 - j0, cudaMemcpyDeviceToHost, s));
     st.d2h_bytes += double(j1 - j0) * g.M * es;
@@ -142,11 +143,11 @@ int incore_native(const Gemm &g, Context *c, DeviceOps &d, bool need_ab, bool re
     BX_CUDA(cudaStreamWaitEvent(c->h2d, start, 0));
     BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
     if (need_ab) {
-        BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
+        BX_TRY(copy2d(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
                                   cudaMemcpyHostToDevice, c->h2d));
         st.h2d_bytes += double(es) * g.rows_a() * g.cols_a();
         if (g.b_form) {  // a stored triangle is completed whole: B lands before the panels
-            BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
+            BX_TRY(copy2d(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
                                       cudaMemcpyHostToDevice, c->h2d));
             st.h2d_bytes += double(es) * g.rows_b() * g.cols_b();
         }
@@ -250,10 +251,10 @@ int copy_kblock_in(const Gemm &g, const DeviceOps &d, int64_t k0, int64_t k1, cu
     const size_t es = elem_size(g.dt);
     const Gemm h = kblock_of(g, g.A, g.lda, g.B, g.ldb, k0, k1);
     const Gemm v = kblock_of(g, d.A, d.lda, d.B, d.ldb, k0, k1);
-    BX_CUDA(cudaMemcpy2DAsync(const_cast<void *>(v.A), d.lda * es, h.A, g.lda * es, h.rows_a() * es,
+    BX_TRY(copy2d(const_cast<void *>(v.A), d.lda * es, h.A, g.lda * es, h.rows_a() * es,
                               h.cols_a(), cudaMemcpyHostToDevice, s));
     if (!d.b_is_a)
-        BX_CUDA(cudaMemcpy2DAsync(const_cast<void *>(v.B), d.ldb * es, h.B, g.ldb * es, h.rows_b() * es,
+        BX_TRY(copy2d(const_cast<void *>(v.B), d.ldb * es, h.B, g.ldb * es, h.rows_b() * es,
                                   h.cols_b(), cudaMemcpyHostToDevice, s));
     st.h2d_bytes += double(es) * (h.rows_a() * h.cols_a() + (d.b_is_a ? 0 : h.rows_b() * h.cols_b()));
     return BLASX_OK;
@@ -266,7 +267,7 @@ int oz_after_panel_kblocks(void *vctx, int64_t j0, int64_t j1) {
     const DeviceOps &d = *x->d;
     const size_t es = elem_size(g.dt);
     if (!g.beta_zero()) {
-        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.C0) + j0 * d.ldc * es, d.ldc * es,
+        BX_TRY(copy2d(static_cast<char *>(d.C0) + j0 * d.ldc * es, d.ldc * es,
                                   static_cast<const char *>(g.C) + j0 * g.ldc * es, g.ldc * es,
                                   g.M * es, j1 - j0, cudaMemcpyHostToDevice, x->c->h2d));
         x->st->h2d_bytes += double(j1 - j0) * g.M * es;
@@ -309,18 +310,18 @@ int incore_ozaki_kblocks(const Gemm &g, Context *c, DeviceOps &d, int mode, blas
     BX_CUDA(cudaEventRecord(start, c->compute));
     BX_CUDA(cudaStreamWaitEvent(c->h2d, start, 0));
     BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
-    std::vector<cudaEvent_t> in(static_cast<size_t>(blocks));
-    for (int b = 0; b < blocks; ++b) {
-        BX_TRY(copy_kblock_in(g, d, kblock_edge(g, b, blocks), kblock_edge(g, b + 1, blocks), c->h2d, st));
-        in[size_t(b)] = ev.make();
-        BX_CUDA(cudaEventRecord(in[size_t(b)], c->h2d));
-    }
     Gemm dg = g;
     dg.C = d.C;
     dg.ldc = d.ldc;
     OzPanelCtx pctx{&g, &d, c, &ev, &st};
+    // each block's compute is enqueued right after its copies: with staged
+    // host memory the next block's copies keep this thread busy (packing)
+    // while the block computes
     for (int b = 0; b < blocks; ++b) {
-        BX_CUDA(cudaStreamWaitEvent(c->compute, in[size_t(b)], 0));
+        BX_TRY(copy_kblock_in(g, d, kblock_edge(g, b, blocks), kblock_edge(g, b + 1, blocks), c->h2d, st));
+        cudaEvent_t in = ev.make();
+        BX_CUDA(cudaEventRecord(in, c->h2d));
+        BX_CUDA(cudaStreamWaitEvent(c->compute, in, 0));
         Gemm kb = kblock_of(dg, d.A, d.lda, d.B, d.ldb, kblock_edge(g, b, blocks),
                             kblock_edge(g, b + 1, blocks));
         kb.beta = b == 0 ? cplx{0.0, 0.0} : cplx{1.0, 0.0};
@@ -346,10 +347,10 @@ int incore_ozaki(const Gemm &g, Context *c, DeviceOps &d, bool read_c, int mode,
     BX_CUDA(cudaStreamWaitEvent(c->d2h, start, 0));
     // A and B first (the slicing needs them whole); C follows panel by panel,
     // each reconstruction waiting only for its own panel
-    BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
+    BX_TRY(copy2d(d.A, d.lda * es, g.A, g.lda * es, g.rows_a() * es, g.cols_a(),
                               cudaMemcpyHostToDevice, c->h2d));
     if (!d.b_is_a)
-        BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
+        BX_TRY(copy2d(d.B, d.ldb * es, g.B, g.ldb * es, g.rows_b() * es, g.cols_b(),
                                   cudaMemcpyHostToDevice, c->h2d));
     st.h2d_bytes += double(es) * (g.rows_a() * g.cols_a() + (d.b_is_a ? 0 : g.rows_b() * g.cols_b()));
     cudaEvent_t ab = ev.make();
@@ -494,11 +495,11 @@ static int tri_streamed(const Trsm &t, const Trsm &dt, const DeviceOps &d, Conte
         const int64_t r0 = std::min(lo, dlo), r1 = std::max(hi, dhi);
         const int64_t arow0 = strip_rows ? lo : r0, arow1 = strip_rows ? hi : r1;
         const int64_t acol0 = strip_rows ? r0 : lo, acol1 = strip_rows ? r1 : hi;
-        BX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(d.A) + (arow0 + acol0 * d.lda) * es, d.lda * es,
+        BX_TRY(copy2d(static_cast<char *>(d.A) + (arow0 + acol0 * d.lda) * es, d.lda * es,
                                   static_cast<const char *>(t.A) + (arow0 + acol0 * t.lda) * es, t.lda * es,
                                   (arow1 - arow0) * es, acol1 - acol0, cudaMemcpyHostToDevice, c->h2d));
         const int64_t rows = t.left ? hi - lo : t.M, cols = t.left ? t.N : hi - lo;
-        BX_CUDA(cudaMemcpy2DAsync(part(d.B, d.ldb, lo), d.ldb * es, part(t.B, t.ldb, lo), t.ldb * es, rows * es, cols,
+        BX_TRY(copy2d(part(d.B, d.ldb, lo), d.ldb * es, part(t.B, t.ldb, lo), t.ldb * es, rows * es, cols,
                                   cudaMemcpyHostToDevice, c->h2d));
         st.h2d_bytes += double(es) * (double(arow1 - arow0) * (acol1 - acol0) + double(rows) * cols);
         BX_TRY(handoff(c->h2d, c->compute));
@@ -512,7 +513,7 @@ static int tri_streamed(const Trsm &t, const Trsm &dt, const DeviceOps &d, Conte
             BX_TRY(trsm_solve_part(dt, lo, hi, t.alpha, c->compute, emulated));
         }
         BX_TRY(handoff(c->compute, c->d2h));
-        BX_CUDA(cudaMemcpy2DAsync(part(t.B, t.ldb, lo), t.ldb * es, part(mult ? d.C : d.B, d.ldb, lo), d.ldb * es,
+        BX_TRY(copy2d(part(t.B, t.ldb, lo), t.ldb * es, part(mult ? d.C : d.B, d.ldb, lo), d.ldb * es,
                                   rows * es, cols, cudaMemcpyDeviceToHost, c->d2h));
         st.d2h_bytes += double(es) * rows * cols;
     }
@@ -576,6 +577,7 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
     HostPin pins;
     BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
+    st.host_copy = pins.mode();
     DeviceOps d;
     d.s = c->compute;
     StreamDrain drain{c};  // before d and pins go, on every return
@@ -596,7 +598,7 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
     };
     BX_TRY(handoff(c->compute, c->h2d));  // the buffers are allocated on compute
     if (need_a) {
-        BX_CUDA(cudaMemcpy2DAsync(d.A, lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, c->h2d));
+        BX_TRY(copy2d(d.A, lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, c->h2d));
         st.h2d_bytes += double(es) * K * K;
     }
     cudaEvent_t out_done[2] = {nullptr, nullptr};
@@ -612,7 +614,7 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
         const int64_t rows = t.left ? t.M : n, cols = t.left ? n : t.N;
         if (out_done[buf]) BX_CUDA(cudaStreamWaitEvent(c->h2d, out_done[buf], 0));
         if (need_a) {
-            BX_CUDA(cudaMemcpy2DAsync(tp.B, tp.ldb * es, host, t.ldb * es, rows * es, cols, cudaMemcpyHostToDevice,
+            BX_TRY(copy2d(tp.B, tp.ldb * es, host, t.ldb * es, rows * es, cols, cudaMemcpyHostToDevice,
                                       c->h2d));
             st.h2d_bytes += double(es) * rows * cols;
         }
@@ -621,7 +623,7 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
         BX_TRY(mult ? trmm_device(tp, w, c->compute, &e) : trsm_device(tp, c->compute, &e));
         emulated |= e;
         BX_TRY(handoff(c->compute, c->d2h));
-        BX_CUDA(cudaMemcpy2DAsync(host, t.ldb * es, tp.B, tp.ldb * es, rows * es, cols, cudaMemcpyDeviceToHost,
+        BX_TRY(copy2d(host, t.ldb * es, tp.B, tp.ldb * es, rows * es, cols, cudaMemcpyDeviceToHost,
                                   c->d2h));
         st.d2h_bytes += double(es) * rows * cols;
         if (!out_done[buf]) out_done[buf] = ev.make();
@@ -630,6 +632,7 @@ static int tri_panels(const Trsm &t, Context *c, bool mult, int mode, size_t bud
     BX_CUDA(cudaStreamSynchronize(c->h2d));
     BX_CUDA(cudaStreamSynchronize(c->compute));
     BX_CUDA(cudaStreamSynchronize(c->d2h));
+    BX_TRY(pins.finish());  // staged write-backs in host memory
     st.path = !need_a ? 3 : (emulated ? 2 : 1);
     st.tile = int(wv);  // the panel width, in vectors
     if (emulated) {
@@ -695,6 +698,7 @@ static int host_tri(const Trsm &t, bool mult) {
     HostPin pins;
     BX_TRY(pins.pin(t.A, need_a ? host_extent(t.lda, K, K, es) : 0));
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
+    st.host_copy = pins.mode();
     StreamDrain drain{c};  // before d and pins go, on every return
     cudaStream_t s = c->compute;
     if (need_a) BX_CUDA(dev_malloc_async(&d.A, bytes_a, s));
@@ -711,18 +715,19 @@ static int host_tri(const Trsm &t, bool mult) {
     bool emulated = false;
     if (!split) {
         if (need_a) {
-            BX_CUDA(cudaMemcpy2DAsync(d.A, d.lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, s));
-            BX_CUDA(cudaMemcpy2DAsync(d.B, d.ldb * es, t.B, t.ldb * es, t.M * es, t.N, cudaMemcpyHostToDevice, s));
+            BX_TRY(copy2d(d.A, d.lda * es, t.A, t.lda * es, K * es, K, cudaMemcpyHostToDevice, s));
+            BX_TRY(copy2d(d.B, d.ldb * es, t.B, t.ldb * es, t.M * es, t.N, cudaMemcpyHostToDevice, s));
             st.h2d_bytes += double(es) * (double(K) * K + double(t.M) * t.N);
         }
         BX_TRY(mult ? trmm_device(dt, w, s, &emulated) : trsm_device(dt, s, &emulated));
-        BX_CUDA(cudaMemcpy2DAsync(t.B, t.ldb * es, d.B, d.ldb * es, t.M * es, t.N, cudaMemcpyDeviceToHost, s));
+        BX_TRY(copy2d(t.B, t.ldb * es, d.B, d.ldb * es, t.M * es, t.N, cudaMemcpyDeviceToHost, s));
         st.d2h_bytes += double(es) * t.M * t.N;
         BX_CUDA(cudaStreamSynchronize(s));
     } else {
         BX_TRY(tri_streamed(t, dt, d, c, mult, w, tb, &emulated, st));
         st.tile = int(tb.b);  // the block order
     }
+    BX_TRY(pins.finish());  // staged write-backs in host memory
     st.path = !need_a ? 3 : (emulated ? 2 : 1);
     if (emulated) {
         resolve_decision(st);
@@ -855,11 +860,14 @@ int host_tri_entry(const Trsm &t, bool mult) {
         return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: the HBM budget (%zu bytes) cannot hold the "
                          "update GEMM of its halves (tile edge %d)", mult ? "multiply" : "solve", budget,
                          pick_tile(top));
-    HostPin pins;  // once for every part: the parts' own registrations would overlap
+    // registered once for every part (the parts' own registrations would
+    // overlap); staged ranges are staged again by each part's own call
+    HostPin pins;
     const size_t es = elem_size(t.dt);
     BX_TRY(pins.pin(t.A, host_extent(t.lda, K, K, es)));
     BX_TRY(pins.pin(t.B, host_extent(t.ldb, t.M, t.N, es)));
     blasx_call_stats agg{};
+    agg.host_copy = pins.mode();
     const int rc = tri_split(t, mult, mode, budget, agg);
     agg.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     call_stats() = agg;
@@ -909,6 +917,7 @@ int host_gemm(const Gemm &g) {
     BX_TRY(pins.pin(g.A, need_ab ? host_extent(g.lda, g.rows_a(), g.cols_a(), es) : 0));
     BX_TRY(pins.pin(g.B, need_ab && !d.b_is_a ? host_extent(g.ldb, g.rows_b(), g.cols_b(), es) : 0));
     BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
+    st.host_copy = pins.mode();
     StreamDrain drain{c};  // before d and pins go, on every return
     if (need_ab) {
         BX_CUDA(dev_malloc_async(&d.A, ib.a ? ib.a : 256, c->compute));
@@ -918,8 +927,9 @@ int host_gemm(const Gemm &g) {
     BX_CUDA(dev_malloc_async(&d.C, ib.c, c->compute));
     if (oz) BX_CUDA(dev_malloc_async(&d.ws, ib.ws, c->compute));
     if (ib.c0) BX_CUDA(dev_malloc_async(&d.C0, ib.c0, c->compute));
-    const int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
-                      : incore_native(g, c, d, need_ab, read_c, st);
+    int rc = oz ? incore_ozaki(g, c, d, read_c, mode, st)
+                : incore_native(g, c, d, need_ab, read_c, st);
+    if (rc == BLASX_OK) rc = pins.finish();  // staged write-backs in host memory
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }

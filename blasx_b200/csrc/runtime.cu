@@ -13,6 +13,7 @@
 
 #include "ozaki.h"
 #include "runtime.h"
+#include "staging.h"
 #include "tile_engine.h"
 
 namespace bx {
@@ -48,6 +49,7 @@ void read_env(Config &c) {
     }
     if (const char *b = getenv("BLASX_HBM_BUDGET")) c.hbm_budget = parse_bytes(b);
     if (const char *t = getenv("BLASX_TILE")) c.tile = atoi(t);
+    if (const char *h = getenv("BLASX_HOST_STAGING")) c.host_staging = strcmp(h, "0") && strcmp(h, "off") ? 1 : 0;
 }
 }  // namespace
 
@@ -176,6 +178,7 @@ int release_context() {
     cudaSetDevice(g_ctx->device);
     cudaDeviceSynchronize();
     release_tile_arena();
+    release_staging();
     cudaStreamDestroy(g_ctx->compute);
     cudaStreamDestroy(g_ctx->h2d);
     cudaStreamDestroy(g_ctx->d2h);
@@ -204,6 +207,8 @@ int blasx_set_hbm_budget(size_t bytes) {
     bx::config().hbm_budget = bytes;
     return 0;
 }
+
+int blasx_set_host_staging(int on) { return bx::config().host_staging.exchange(on ? 1 : 0); }
 
 int blasx_set_tile(int tile) {
     if (tile != 0 && (tile < 256 || tile > 16384 || tile % 256)) return -1;

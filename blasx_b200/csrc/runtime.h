@@ -136,6 +136,7 @@ struct Config {
     std::atomic<int> dgemm_mode{0};    // 0 auto, 1 native, 2 ozaki
     std::atomic<size_t> hbm_budget{0}; // 0 = default
     std::atomic<int> tile{0};          // 0 = automatic
+    std::atomic<int> host_staging{1};  // pageable host memory: 1 staged, 0 registered
 };
 Config &config();
 

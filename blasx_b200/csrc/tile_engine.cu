@@ -15,10 +15,13 @@
 //                   GEMMs and adds alpha X into the C tile in FP64, with its
 //                   own modulus decision (native fallback on the device);
 //   D2H stream      writes a finished C tile back to the host.
-// The host thread never blocks until the final synchronisation, so copies
-// run ahead of compute as far as slot reuse allows. Host operands that are
-// not pinned are registered for the duration of the call over their full
-// ld x columns extent (the reference registers rows x columns,
+// With pinned host operands the host thread never blocks until the final
+// synchronisation, so copies run ahead of compute as far as slot reuse
+// allows. Pageable host operands are staged through pinned bounce buffers
+// (staging.h): the host thread then packs each inbound tile and waits for
+// outbound buffers, which keeps the copies about one C tile ahead. With
+// staging switched off they are registered for the duration of the call over
+// their full ld x columns extent (the reference registers rows x columns,
 // blas/dgemm.c:88-90, which misses the ld padding).
 #include <chrono>
 #include <mutex>
@@ -65,24 +68,6 @@ struct EventPool {
 
 }  // namespace
 
-int HostPin::pin(const void *p, size_t bytes) {
-    if (!p || !bytes) return BLASX_OK;
-    cudaPointerAttributes attr;
-    if (cudaPointerGetAttributes(&attr, p) == cudaSuccess && attr.type == cudaMemoryTypeHost)
-        return BLASX_OK;  // already pinned by the caller
-    cudaGetLastError();
-    if (cudaHostRegister(const_cast<void *>(p), bytes, cudaHostRegisterDefault) == cudaSuccess) {
-        regs.push_back(const_cast<void *>(p));
-    } else {
-        cudaGetLastError();  // not registrable: copies fall back to staged transfers
-    }
-    return BLASX_OK;
-}
-
-HostPin::~HostPin() {
-    for (void *p : regs) cudaHostUnregister(p);
-}
-
 size_t host_extent(int64_t ld, int64_t rows, int64_t cols, size_t es) {
     if (rows <= 0 || cols <= 0) return 0;
     return (size_t(ld) * size_t(cols - 1) + size_t(rows)) * es;
@@ -125,6 +110,7 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
     BX_TRY(pins.pin(g.A, host_extent(g.lda, g.rows_a(), g.cols_a(), es)));
     BX_TRY(pins.pin(g.B, host_extent(g.ldb, g.rows_b(), g.cols_b(), es)));
     BX_TRY(pins.pin(g.C, host_extent(g.ldc, g.M, g.N, es)));
+    st.host_copy = pins.mode();
     StreamDrain drain{c};  // before pins go, on every return
 
     EventPool pool;
@@ -185,7 +171,7 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
         const int64_t ld = isA ? g.lda : g.ldb;
         const char *src = (isA ? hA : hB) + (srow + scol * ld) * int64_t(es);
         if (used[size_t(u.slot)]) BX_CUDA(cudaStreamWaitEvent(c->h2d, lastuse[size_t(u.slot)], 0));
-        BX_CUDA(cudaMemcpy2DAsync(op_ptr(u.slot), size_t(T) * es, src, size_t(ld) * es,
+        BX_TRY(copy2d(op_ptr(u.slot), size_t(T) * es, src, size_t(ld) * es,
                                   size_t(nrow) * es, size_t(ncol), cudaMemcpyHostToDevice, c->h2d));
         if (kind == kDiagonal)
             BX_TRY(launch_complete_operand(g.dt, form_of(u.key.op), op_ptr(u.slot), T, rows_op, c->h2d));
@@ -226,7 +212,7 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
             c_used[cs] = true;
             if (!g.beta_zero() || g.uplo != 0) {  // a triangular tile keeps its other entries
                 char *src = hC + (int64_t(s.i) * T + int64_t(s.j) * T * g.ldc) * int64_t(es);
-                BX_CUDA(cudaMemcpy2DAsync(c_ptr(cs), size_t(T) * es, src, size_t(g.ldc) * es,
+                BX_TRY(copy2d(c_ptr(cs), size_t(T) * es, src, size_t(g.ldc) * es,
                                           size_t(m) * es, size_t(n), cudaMemcpyHostToDevice, c->h2d));
                 BX_CUDA(cudaEventRecord(c_ready[cs], c->h2d));
                 BX_CUDA(cudaStreamWaitEvent(c->compute, c_ready[cs], 0));
@@ -262,7 +248,7 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
             BX_CUDA(cudaEventRecord(c_done[cs], c->compute));
             BX_CUDA(cudaStreamWaitEvent(c->d2h, c_done[cs], 0));
             char *dst = hC + (int64_t(s.i) * T + int64_t(s.j) * T * g.ldc) * int64_t(es);
-            BX_CUDA(cudaMemcpy2DAsync(dst, size_t(g.ldc) * es, c_ptr(cs), size_t(T) * es,
+            BX_TRY(copy2d(dst, size_t(g.ldc) * es, c_ptr(cs), size_t(T) * es,
                                       size_t(m) * es, size_t(n), cudaMemcpyDeviceToHost, c->d2h));
             BX_CUDA(cudaEventRecord(c_out[cs], c->d2h));
             st.d2h_bytes += double(m) * n * es;
@@ -271,6 +257,7 @@ int tiled_host_gemm(const Gemm &g, Context *c, size_t budget, int T, int policy,
     BX_CUDA(cudaStreamSynchronize(c->h2d));
     BX_CUDA(cudaStreamSynchronize(c->compute));
     BX_CUDA(cudaStreamSynchronize(c->d2h));
+    BX_TRY(pins.finish());  // staged write-backs in host memory
     st.cache_hits = double(plan.hits);
     st.cache_misses = double(plan.loads);
     st.evictions = double(plan.evictions);

@@ -1,20 +1,13 @@
 // tile_engine.h -- out-of-core execution of a host GEMM through the HBM tile
-// cache, and host-memory pinning helpers shared by the host pipelines.
+// cache, and the stream drain shared by the host pipelines.
 #pragma once
 
 #include <vector>
 
 #include "runtime.h"
+#include "staging.h"
 
 namespace bx {
-
-// Pins host ranges for the lifetime of the object (no-op for memory that is
-// already pinned); unregisters what it registered on destruction.
-struct HostPin {
-    std::vector<void *> regs;
-    int pin(const void *p, size_t bytes);
-    ~HostPin();
-};
 
 // Waits for the context's three streams when it goes out of scope. Declared
 // after a call's device buffers and host pins, it runs before they are freed

@@ -328,6 +328,15 @@ int blasx_set_hbm_budget(size_t bytes);
  * (env BLASX_TILE). Multiple of 256, between 256 and 16384. */
 int blasx_set_tile(int tile);
 
+/* Pageable host memory passed to a host call (memory that is neither
+ * pinned nor device memory): 1 = staged through a ring of pinned bounce
+ * buffers, packed and unpacked by host threads while the copy engines run
+ * (default); 0 = registered for the duration of the call (cudaHostRegister,
+ * as the reference does in blas/dgemm.c:88-121). Also read once from the
+ * environment variable BLASX_HOST_STAGING (0/off). Returns the previous
+ * setting. */
+int blasx_set_host_staging(int on);
+
 /* Per-call statistics of the calling thread's last host GEMM call. */
 typedef struct blasx_call_stats {
     double seconds;           /* wall time of the call */
@@ -341,7 +350,9 @@ typedef struct blasx_call_stats {
                                  device (spread too wide or non-finite input) */
     int moduli;               /* Ozaki moduli used (0 when native) */
     int tile;                 /* tile edge used */
-    int reserved;
+    int host_copy;            /* host memory: 0 copied directly (pinned by
+                                 the caller), 1 staged through bounce buffers,
+                                 2 registered for the call */
 } blasx_call_stats;
 void blasx_get_call_stats(blasx_call_stats *out);
 
