@@ -21,6 +21,8 @@ namespace oz {
 namespace {
 
 constexpr int kNumN = kMaxModuli - kMinModuli + 1;
+// The largest modulus count whose CRT runs on 40-bit FP64 limbs (M < 2^133).
+constexpr int kMaxFpCrt = 17;
 constexpr int kP = 62;  // |scaled integer| < 2^62
 
 struct CrtTables {
@@ -30,8 +32,15 @@ struct CrtTables {
     double invMd[kNumN];
     int Q[kNumN];                           // norm exponent bound: 2^(2Q) <= M/4
     // the same 32-bit limbs as doubles (exact), operands of the FP64 CRT sums
+    // of more than kMaxFpCrt moduli
     double wd[kNumN][kMaxModuli][kLimbs];
     double Ml[kNumN][kLimbs];
+    // 40-bit limbs kept at their weight, for up to kMaxFpCrt moduli: limb k
+    // of a value v is (bits [40k, 40k + 40) of v) * 2^(40k). wq: the weight
+    // limbs times 2^8; cq: their sum over the N moduli; M40: M's limbs.
+    double wq[kNumN][kMaxModuli][4];
+    double cq[kNumN][4];
+    double M40[kNumN][4];
 };
 __constant__ CrtTables c_crt;
 
@@ -52,6 +61,15 @@ uint32_t big_div_small(uint32_t *a, int n, uint32_t s) {  // a /= s, returns rem
         rem = cur % s;
     }
     return uint32_t(rem);
+}
+// bits [40k, 40k + 40) of a (n 32-bit limbs) times 2^(40k), as an exact double
+double limb40(const uint32_t *a, int n, int k, int shift) {
+    uint64_t v = 0;
+    for (int b = 0; b < 40; ++b) {
+        const int bit = 40 * k + b;
+        if (bit / 32 < n && ((a[bit / 32] >> (bit % 32)) & 1u)) v |= uint64_t(1) << b;
+    }
+    return std::ldexp(double(v), 40 * k + shift);
 }
 double big_to_double(const uint32_t *a, int n) {
     double d = 0;
@@ -86,7 +104,12 @@ CrtTables build_tables() {
             big_mul_small(q, kLimbs, inv_mod(r, uint32_t(kModuli[l])));
             memcpy(t.w[ni][l], q, sizeof q);
             for (int k = 0; k < kLimbs; ++k) t.wd[ni][l][k] = double(q[k]);
+            for (int k = 0; k < 4; ++k) {
+                t.wq[ni][l][k] = limb40(q, kLimbs, k, 8);
+                t.cq[ni][k] += t.wq[ni][l][k];  // exact: multiples of 2^(40k+8) below 2^(40k+53)
+            }
         }
+        for (int k = 0; k < 4; ++k) t.M40[ni][k] = limb40(M, kLimbs, k, 0);
     }
     return t;
 }
@@ -540,76 +563,136 @@ __device__ __forceinline__ double residue_as_double(uint32_t w, int qb) {
            4503599627370496.0;
 }
 
-// CRT value of the residues (byte qb of w[0..N)) times 2^scale as a double,
+// 1 + u / 256 for the residue u = byte qb of w: exact (9 significant bits),
+// built in the high word alone.
+__device__ __forceinline__ double residue_plus_one(uint32_t w, int qb) {
+    const uint32_t u = __byte_perm(w, 0u, 0x4440u | uint32_t(qb));
+    return __hiloint2double(int(u * 4096u + 0x3FF00000u), 0);
+}
+
+// s + e = a + b exactly (Knuth's TwoSum).
+__device__ __forceinline__ double two_sum(double a, double b, double &e) {
+    const double s = __dadd_rn(a, b);
+    const double bb = __dsub_rn(s, a);
+    e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+    return s;
+}
+
+// a + b rounded to odd: the truncation of the exact sum, its last mantissa
+// bit set when the sum is inexact (the neighbour of the round-to-nearest
+// result toward the exact sum, when that result's last bit is even).
+__device__ __forceinline__ double add_round_odd(double a, double b) {
+    double e;
+    const double s = two_sum(a, b, e);
+    long long bits = __double_as_longlong(s);
+    if (e != 0.0 && !(bits & 1)) bits += ((e > 0.0) == (s > 0.0)) ? 1 : -1;
+    return __longlong_as_double(bits);
+}
+
+// The CRT value of one entry's residues times 2^scale as a double,
 // correctly rounded from the exact integer X (the scaling by a power of two
 // is exact unless the result leaves the normal range):
 //   S = sum_l u_l w_l is congruent to X mod M, and the row and column
-//   scaling guarantees |X| < 2^(2Q) <= M/4. With w_l and M split into L
-//   32-bit limbs, every limb sum S_t = sum_l u_l w_{l,t} < N 2^8 2^32 < 2^45
-//   is an exact FP64 value, summed with DFMAs on the FP64 pipe. X = S - q M
-//   with q = rint(S / M): S / M lies within 1/4 of an integer and its double
-//   estimate is off by far less, so the rounding is never ambiguous. The
-//   limb differences D_t = S_t - q M_t (|D_t| < 2^45) are exact as well; their
-//   two's complement words come out of the mantissa of D_t + 1.5 * 2^52, a
-//   carry pass assembles X in L words, and its magnitude is converted with
-//   one rounding.
+//   scaling guarantees |X| < 2^(2Q) <= M/4. X = S - q M with q = rint(S / M):
+//   S / M lies within 1/4 of an integer and its double estimate is off by
+//   far less, so the rounding is never ambiguous.
+// Up to kMaxFpCrt moduli (M < 2^133) everything runs on the FP64 pipe. With
+// w_l and M cut into L limbs of 40 bits kept at their weight 2^(40k), every
+// limb sum S_k = sum_l u_l w_{l,k} is a multiple of 2^(40k) below
+// 2^(40k+53): exact. It is accumulated as sum_l (1 + u_l/256) (256 w_{l,k})
+// from -sum_l 256 w_{l,k}, each product exact (9 x 40 significant bits) and
+// each partial sum exact, so the residue enters as a bit pattern, without a
+// conversion. The differences D_k = S_k - q M_k (|D_k| < 2^(40k+53), one
+// DFMA each) are exact, and X = D_0 + D_1 + D_2 (with D_3 + D_2, exact since
+// |X| < 2^131, as the top term for four limbs). The sum of the three is
+// rounded correctly by the round-to-odd method of Boldo and Melquiond
+// ("Emulation of FMA and correctly rounded sums: proved algorithms using
+// rounding to odd", IEEE Trans. Computers 57(4), 2008):
+//   (uh, ul) = TwoSum(D_1, D_0), (th, tl) = TwoSum(D_2, uh),
+//   RN(X) = RN(th + RO(tl + ul)).
+// More moduli use 32-bit limbs: D_t = S_t - q M_t with |D_t| < 2^45, whose
+// two's complement words come out of the mantissa of D_t + 1.5 * 2^52; a
+// carry pass assembles X in L words, and its magnitude is converted with one
+// rounding from a 64-bit window and a sticky bit.
+
+// 40-bit limbs of M for the FP64 CRT of N <= kMaxFpCrt moduli.
+template <int N> __host__ __device__ constexpr int fp_limbs() { return N <= 10 ? 2 : N <= 15 ? 3 : 4; }
+
+// The FP64 CRT's limb sums S_k of the 4 rows whose residues w packs (byte q
+// of w[l]: row q, modulus l), all rows at once: every weight limb is read once
+// and serves the 4 rows.
 template <int N>
-__device__ __forceinline__ double crt_to_double(const uint32_t (&w)[N], int qb, int scale) {
-    constexpr int L = limbs_for(N);
-    constexpr int ni = N - kMinModuli;
-    double S[L];
+__device__ __forceinline__ void crt_sums4(const uint32_t (&w)[N], double (&S)[4][fp_limbs<N>()]) {
+    constexpr int L = fp_limbs<N>(), ni = N - kMinModuli;
 #pragma unroll
-    for (int t = 0; t < L; ++t) S[t] = 0.0;
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int k = 0; k < L; ++k) S[q][k] = -c_crt.cq[ni][k];
 #pragma unroll
     for (int l = 0; l < N; ++l) {
-        const double u = residue_as_double(w[l], qb);
 #pragma unroll
-        for (int t = 0; t < L; ++t) S[t] = fma(u, c_crt.wd[ni][l][t], S[t]);
-    }
-    double sa = S[L - 1];
+        for (int q = 0; q < 4; ++q) {
+            const double d = residue_plus_one(w[l], q);
 #pragma unroll
-    for (int t = L - 2; t >= 0; --t) sa = fma(sa, 4294967296.0, S[t]);
-    const double qd = rint(sa * c_crt.invMd[ni]);
-    // X in L two's complement words: word t of D_t plus the carry of the words
-    // below. D_t + 1.5 * 2^52 holds D_t + 2^51 in its 52 mantissa bits (exact,
-    // |D_t| < 2^51): the low word is D_t mod 2^32, the high word minus
-    // 0x43380000 is floor(D_t / 2^32).
-    uint32_t x[L];
-    int32_t carry = 0;
-#pragma unroll
-    for (int t = 0; t < L; ++t) {
-        const double d = fma(-qd, c_crt.Ml[ni][t], S[t]) + 6755399441055744.0;
-        const uint32_t lo = uint32_t(__double2loint(d));
-        const int32_t hi = __double2hiint(d) - 0x43380000;
-        const int64_t v = int64_t(lo) + int64_t(carry);
-        x[t] = uint32_t(v);
-        carry = hi + int32_t(v >> 32);  // floor division: -1, 0 or 1 from the low word
-    }
-    if constexpr (L <= 4) {
-        // |X| < 2^126: two 64-bit halves of a 128-bit two's complement value
-        // (words above L are the sign), its magnitude, and one correctly
-        // rounded conversion: a 64-bit window whose bit 63 is the leading one,
-        // every lower bit folded into a sticky bit 0 (bit 0 lies below the
-        // 53-bit rounding point, so round-to-nearest-even stays exact).
-        const uint32_t sw = uint32_t(int32_t(x[L - 1]) >> 31);
-        uint64_t lo = (uint64_t(L > 1 ? x[1] : sw) << 32) | x[0];
-        uint64_t hi = (uint64_t(L > 3 ? x[3] : sw) << 32) | (L > 2 ? x[2] : sw);
-        const bool neg = sw != 0;
-        if (neg) {  // magnitude: ~X + 1
-            lo = ~lo + 1;
-            hi = ~hi + (lo == 0 ? 1 : 0);
+            for (int k = 0; k < L; ++k) S[q][k] = __fma_rn(d, c_crt.wq[ni][l][k], S[q][k]);
         }
-        double d;
-        if (hi) {
-            const int lz = __clzll(hi);
-            const uint64_t win = lz ? (hi << lz) | (lo >> (64 - lz)) : hi;
-            const uint64_t rest = lz ? lo << lz : lo;
-            d = scale_pow2(__ull2double_rn(win | (rest ? 1 : 0)), 64 - lz + scale);
-        } else {
-            d = scale_pow2(__ull2double_rn(lo), scale);
-        }
-        return neg ? -d : d;
+    }
+}
+
+// RN(X) * 2^scale from one row's limb sums (N <= kMaxFpCrt).
+template <int N>
+__device__ __forceinline__ double crt_round(const double (&S)[fp_limbs<N>()], int scale) {
+    constexpr int L = fp_limbs<N>(), ni = N - kMinModuli;
+    const double qd = rint(__dmul_rn(__dadd_rn(S[L - 1], S[L - 2]), c_crt.invMd[ni]));
+    double D[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) D[k] = __fma_rn(-qd, c_crt.M40[ni][k], S[k]);
+    double x;
+    if constexpr (L == 2) {
+        x = __dadd_rn(D[1], D[0]);
     } else {
+        const double top = L == 4 ? __dadd_rn(D[3], D[2]) : D[2];
+        double ul, tl;
+        const double uh = two_sum(D[1], D[0], ul);
+        const double th = two_sum(top, uh, tl);
+        x = __dadd_rn(th, add_round_odd(tl, ul));
+    }
+    return scale_pow2(__dadd_rn(x, 0.0), scale);  // + 0: a zero sum is +0
+}
+
+// CRT of more than kMaxFpCrt moduli for row qb of w (the 32-bit-limb method).
+// Out of line: its registers would otherwise size every reconstruction
+// kernel, whose common path (fewer moduli) needs far fewer.
+template <int N>
+__device__ __noinline__ double crt_to_double(const uint32_t (&w)[N], int qb, int scale) {
+    constexpr int ni = N - kMinModuli;
+    static_assert(N > kMaxFpCrt, "the FP64-limb CRT serves fewer moduli");
+    {
+        constexpr int L = limbs_for(N);
+        double S[L];
+#pragma unroll
+        for (int t = 0; t < L; ++t) S[t] = 0.0;
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            const double u = residue_as_double(w[l], qb);
+#pragma unroll
+            for (int t = 0; t < L; ++t) S[t] = fma(u, c_crt.wd[ni][l][t], S[t]);
+        }
+        double sa = S[L - 1];
+#pragma unroll
+        for (int t = L - 2; t >= 0; --t) sa = fma(sa, 4294967296.0, S[t]);
+        const double qd = rint(sa * c_crt.invMd[ni]);
+        uint32_t x[L];
+        int32_t carry = 0;
+#pragma unroll
+        for (int t = 0; t < L; ++t) {
+            const double d = fma(-qd, c_crt.Ml[ni][t], S[t]) + 6755399441055744.0;
+            const uint32_t lo = uint32_t(__double2loint(d));
+            const int32_t hi = __double2hiint(d) - 0x43380000;
+            const int64_t v = int64_t(lo) + int64_t(carry);
+            x[t] = uint32_t(v);
+            carry = hi + int32_t(v >> 32);  // floor division: -1, 0 or 1 from the low word
+        }
         const bool neg = int32_t(x[L - 1]) < 0;
         if (neg) {  // magnitude: ~x + 1
             uint32_t c = 1;
@@ -620,8 +703,10 @@ __device__ __forceinline__ double crt_to_double(const uint32_t (&w)[N], int qb, 
                 c = uint32_t(v >> 32);
             }
         }
-        // magnitude -> double, correctly rounded, as above with a window
-        // taken at the top non-zero word
+        // magnitude -> double, correctly rounded: a 64-bit window whose bit
+        // 63 is the leading one, every lower bit folded into a sticky bit 0
+        // (bit 0 lies below the 53-bit rounding point, so round-to-nearest-
+        // even stays exact)
         int top = -1;
 #pragma unroll
         for (int t = L - 1; t >= 0; --t)
@@ -682,21 +767,64 @@ __device__ __forceinline__ void recon_real(const ReconArgs &a, int64_t i0, int64
     gather4<N>(a.U, a.Jp * a.Ip, j * a.Ip + i0, w);
     const int fj = a.fb[j];
     T *C = static_cast<T *>(a.C);
-#pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
-        const int64_t i = i0 + q;
-        if (i >= a.M) break;
-        if (!recon_keep(a, i, j)) continue;
-        const double val = crt_to_double<N>(w, q, -(a.ea[i] + fj));
+    auto put = [&](int64_t i, double val) {
         T *cp = C + i + j * a.ldc;
         double r = a.ar * val;
         if (!a.beta_zero) r = fma(a.br, double(*cp), r);
         *cp = T(r);
+    };
+    if constexpr (N <= kMaxFpCrt) {
+        double S[4][fp_limbs<N>()];
+        crt_sums4<N>(w, S);
+        T *cp = C + i0 + j * a.ldc;
+        if (a.uplo == 0 && i0 + 3 < a.M && (reinterpret_cast<uintptr_t>(cp) & 15) == 0) {
+            // 4 whole rows, 16-byte aligned: vector loads and stores of C and
+            // the row exponents, the same arithmetic per entry as put
+            const int4 e = *reinterpret_cast<const int4 *>(a.ea + i0);
+            double r[4] = {crt_round<N>(S[0], -(e.x + fj)), crt_round<N>(S[1], -(e.y + fj)),
+                           crt_round<N>(S[2], -(e.z + fj)), crt_round<N>(S[3], -(e.w + fj))};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r[q] = a.ar * r[q];
+            if constexpr (std::is_same<T, double>::value) {
+                double2 *v = reinterpret_cast<double2 *>(cp);
+                if (!a.beta_zero) {
+                    const double2 c0 = v[0], c1 = v[1];
+                    r[0] = fma(a.br, c0.x, r[0]);
+                    r[1] = fma(a.br, c0.y, r[1]);
+                    r[2] = fma(a.br, c1.x, r[2]);
+                    r[3] = fma(a.br, c1.y, r[3]);
+                }
+                v[0] = make_double2(r[0], r[1]);
+                v[1] = make_double2(r[2], r[3]);
+            } else {
+                float4 *v = reinterpret_cast<float4 *>(cp);
+                if (!a.beta_zero) {
+                    const float4 c = *v;
+                    r[0] = fma(a.br, double(c.x), r[0]);
+                    r[1] = fma(a.br, double(c.y), r[1]);
+                    r[2] = fma(a.br, double(c.z), r[2]);
+                    r[3] = fma(a.br, double(c.w), r[3]);
+                }
+                *v = make_float4(float(r[0]), float(r[1]), float(r[2]), float(r[3]));
+            }
+            return;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int64_t i = i0 + q;
+            if (i < a.M && recon_keep(a, i, j)) put(i, crt_round<N>(S[q], -(a.ea[i] + fj)));
+        }
+    } else {
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+            const int64_t i = i0 + q;
+            if (i >= a.M) break;
+            if (!recon_keep(a, i, j)) continue;
+            put(i, crt_to_double<N>(w, q, -(a.ea[i] + fj)));
+        }
     }
 }
 
-// Complex outputs: residues of Re(C) are rows [0, Jp) of U, Im(C) rows
-// [Jp, 2 Jp); U planes are 2 Jp x Ip.
 template <typename T, int N>
 __device__ __forceinline__ void recon_cplx(const ReconArgs &a, int64_t i0, int64_t j) {
     using R = typename Elem<T>::R;
@@ -706,23 +834,62 @@ __device__ __forceinline__ void recon_cplx(const ReconArgs &a, int64_t i0, int64
     gather4<N>(a.U, plane, (a.Jp + j) * a.Ip + i0, wi);
     const int fj = a.fb[j];
     R *C = static_cast<R *>(a.C);
-#pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
-        const int64_t i = i0 + q;
-        if (i >= a.M) break;
-        if (!recon_keep(a, i, j)) continue;
-        const int sc = -(a.ea[i] + fj);
-        const double xr = crt_to_double<N>(wr, q, sc);
-        const double xi = crt_to_double<N>(wi, q, sc);
+    // one entry: (re, im) loaded and stored as one vector (16 bytes for
+    // complex128, 8 for complex64) when C is aligned to that size
+    using V = typename std::conditional<std::is_same<R, double>::value, double2, float2>::type;
+    const bool vec = (reinterpret_cast<uintptr_t>(a.C) & (sizeof(V) - 1)) == 0;
+    auto put = [&](int64_t i, double xr, double xi) {
         R *cp = C + 2 * (i + j * a.ldc);
         double vr = a.ar * xr - a.ai * xi, vi = a.ar * xi + a.ai * xr;
-        if (!a.beta_zero) {
-            const double cr = double(cp[0]), ci = double(cp[1]);
-            vr += a.br * cr - a.bi * ci;
-            vi += a.br * ci + a.bi * cr;
+        if (vec) {
+            V *vp = reinterpret_cast<V *>(cp);
+            if (!a.beta_zero) {
+                const V c = *vp;
+                const double cr = double(c.x), ci = double(c.y);
+                vr += a.br * cr - a.bi * ci;
+                vi += a.br * ci + a.bi * cr;
+            }
+            V o;
+            o.x = R(vr);
+            o.y = R(vi);
+            *vp = o;
+        } else {
+            if (!a.beta_zero) {
+                const double cr = double(cp[0]), ci = double(cp[1]);
+                vr += a.br * cr - a.bi * ci;
+                vi += a.br * ci + a.bi * cr;
+            }
+            cp[0] = R(vr);
+            cp[1] = R(vi);
         }
-        cp[0] = R(vr);
-        cp[1] = R(vi);
+    };
+    if constexpr (N <= kMaxFpCrt) {
+        // the real parts of the 4 rows, then the imaginary parts
+        double xr[4], S[4][fp_limbs<N>()];
+        int sc[4];
+        bool live[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int64_t i = i0 + q;
+            live[q] = i < a.M && recon_keep(a, i, j);
+            sc[q] = live[q] ? -(a.ea[i] + fj) : 0;
+        }
+        crt_sums4<N>(wr, S);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) xr[q] = crt_round<N>(S[q], sc[q]);
+        crt_sums4<N>(wi, S);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (live[q]) put(i0 + q, xr[q], crt_round<N>(S[q], sc[q]));
+    } else {
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+            const int64_t i = i0 + q;
+            if (i >= a.M) break;
+            if (!recon_keep(a, i, j)) continue;
+            const int sc = -(a.ea[i] + fj);
+            put(i, crt_to_double<N>(wr, q, sc), crt_to_double<N>(wi, q, sc));
+        }
     }
 }
 
