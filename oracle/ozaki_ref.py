@@ -87,3 +87,83 @@ def emulate(A: np.ndarray, B: np.ndarray, n: int, P: int = 62, verify: bool = Fa
                 assert x == exact, (i, j)
             C[i, j] = math.ldexp(float(x), -int(ea[i]) - int(eb[j])) if x else 0.0
     return C, Q
+
+
+# ---- the device's FP64-limb reconstruction, restated ---------------------------
+# The reconstruction kernel (blasx_b200/csrc/ozaki_dev.cuh: crt_sums4 and
+# crt_round) turns the unsigned residues u_l = X mod m_l of an entry into
+# RN(X) without integer arithmetic: 40-bit limbs of the CRT weights, exact
+# FP64 limb sums, the quotient by M, the exact limb differences, and a
+# correctly rounded sum of three doubles by rounding to odd (Boldo and
+# Melquiond, IEEE Trans. Computers 57(4), 2008). Every product and sum below
+# is exact by the bounds the kernel's comments state, so plain Python float
+# arithmetic (round to nearest) reproduces the kernel's fused multiply-adds
+# bit for bit; ``fp_limb_tables`` asserts those bounds.
+
+FP_CRT_MAX = 17  # moduli the FP64-limb method serves (M < 2^133)
+
+
+def fp_limbs(n: int) -> int:
+    return 2 if n <= 10 else 3 if n <= 15 else 4
+
+
+def _limb40(v: int, k: int) -> int:
+    return ((v >> (40 * k)) & ((1 << 40) - 1)) << (40 * k)
+
+
+def fp_limb_tables(n: int):
+    """(moduli, M, wq, cq, M40, invM) as the kernel's constant tables hold
+    them: wq[l][k] = limb k of weight l times 2^8, cq[k] = sum_l wq[l][k],
+    M40[k] = limb k of M."""
+    assert n <= FP_CRT_MAX
+    ms, M, w, _ = crt(n)
+    L = fp_limbs(n)
+    assert M < 2 ** (40 * L) and M < 2 ** 133
+    wq = [[float(_limb40(wl, k) << 8) for k in range(L)] for wl in w]
+    cq = [float(sum(_limb40(wl, k) << 8 for wl in w)) for k in range(L)]
+    M40 = [float(_limb40(M, k)) for k in range(L)]
+    for k in range(L):
+        assert int(cq[k]) == sum(_limb40(wl, k) << 8 for wl in w)  # exact
+        assert all(int(wq[l][k]) == _limb40(w[l], k) << 8 for l in range(n))
+        assert int(M40[k]) == _limb40(M, k)
+        # every partial limb sum lies in (-cq, S_k] and S_k < n 255 2^(40k+40)
+        assert cq[k] < 2.0 ** (40 * k + 53) and n * 255 * 2.0 ** (40 * k + 40) < 2.0 ** (40 * k + 53)
+    return ms, M, wq, cq, M40, 1.0 / float(M)
+
+
+def _two_sum(a: float, b: float):
+    s = a + b
+    bb = s - a
+    return s, (a - (s - bb)) + (b - bb)
+
+
+def _add_round_odd(a: float, b: float) -> float:
+    s, e = _two_sum(a, b)
+    if e != 0.0:
+        bits = int(np.float64(s).view(np.int64))
+        if not bits & 1:
+            bits += 1 if (e > 0.0) == (s > 0.0) else -1
+            s = float(np.int64(bits).view(np.float64))
+    return s
+
+
+def crt_fp64(u, tables) -> float:
+    """RN(X) for the residues u_l = X mod m_l (|X| < M / 4), as the kernel
+    computes it."""
+    ms, M, wq, cq, M40, invM = tables
+    L = len(cq)
+    S = [-c for c in cq]
+    for l, ul in enumerate(u):
+        d = 1.0 + ul / 256.0  # the bit pattern 0x3FF00000 | u << 12 in the high word
+        for k in range(L):
+            S[k] = d * wq[l][k] + S[k]
+    q = float(round((S[L - 1] + S[L - 2]) * invM))
+    D = [S[k] - q * M40[k] for k in range(L)]
+    if L == 2:
+        x = D[1] + D[0]
+    else:
+        top = D[3] + D[2] if L == 4 else D[2]
+        uh, ul = _two_sum(D[1], D[0])
+        th, tl = _two_sum(top, uh)
+        x = th + _add_round_odd(tl, ul)
+    return x + 0.0

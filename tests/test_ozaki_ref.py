@@ -46,3 +46,27 @@ def test_calibrated_modulus_counts_beat_native(phi, n):
     B = oracle.spread((2048, 10), 6, phi)
     C, _ = ozaki_ref.emulate(A, B, n)
     assert _normerr(C, A, B) <= _normerr(A @ B, A, B) + 1e-3
+
+
+@pytest.mark.parametrize("n", range(6, ozaki_ref.FP_CRT_MAX + 1))
+def test_fp64_limb_crt_rounds_correctly(n):
+    # the device's reconstruction, restated, against exact rounding of the
+    # CRT value: random magnitudes and values next to rounding midpoints
+    # (ties included), both signs and zero
+    import random
+    tables = ozaki_ref.fp_limb_tables(n)
+    ms, M = tables[0], tables[1]
+    rng = random.Random(n)
+    xs = [0, 1, -1, M // 4 - 1, -(M // 4 - 1)]
+    top = M.bit_length() - 3
+    for _ in range(1500):
+        bits = rng.randint(1, top)
+        x = rng.getrandbits(bits)
+        if x.bit_length() > 60 and rng.random() < 0.5:  # a midpoint of two doubles, or one away
+            s = x.bit_length() - 53
+            x = ((x >> s) << s) + (1 << (s - 1)) + rng.choice((-1, 0, 1))
+        xs.append(x if rng.random() < 0.5 else -x)
+    for x in xs:
+        assert abs(x) < M // 4
+        got = ozaki_ref.crt_fp64([x % m for m in ms], tables)
+        assert got == float(x) and (x != 0 or math.copysign(1.0, got) > 0), (n, x, got)
