@@ -57,33 +57,57 @@ template <typename T> int launch_add_scaled_t(const Gemm &g, const void *X, int6
     return BLASX_OK;
 }
 
-// One thread per entry of column j = blockIdx.y (grid-strided over j).
+// One CTA of 32 x 8 threads per 32 x 32 tile of X that holds entries to
+// complete (the other triangle and the diagonal). A mirrored tile is read
+// from the stored triangle with coalesced column reads into shared memory and
+// written back transposed, again column by column; a diagonal tile reads
+// itself whole before writing only its other triangle.
+constexpr int kCompTile = 32, kCompRows = 8;
+
 template <typename T>
-__global__ void complete_operand_kernel(int form, T *__restrict__ X, int64_t ldx, int n) {
+__global__ void __launch_bounds__(kCompTile * kCompRows)
+complete_operand_kernel(int form, T *__restrict__ X, int64_t ldx, int n) {
     using Ar = Arith<T>;
     const bool upper = form == kSymUpper || form == kHermUpper || form == kTriUpper || form == kTriUpperUnit;
     const bool herm = form == kHermUpper || form == kHermLower;
     const bool tri = form >= kTriUpper;
     const bool unit = form == kTriUpperUnit || form == kTriLowerUnit;
-    for (int64_t j = blockIdx.y; j < n; j += gridDim.y)
-        for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
-             i += int64_t(gridDim.x) * blockDim.x) {
-            T *xp = &X[i + j * ldx];
-            if (i == j) {
-                if (unit) *xp = Ar::one();
-                else if (herm) *xp = Ar::real_part(*xp);
-                continue;
-            }
-            const bool stored = upper ? i < j : i > j;
-            if (stored) continue;
-            if (tri) *xp = Ar::zero();
-            else *xp = herm ? Ar::conj(X[j + i * ldx]) : X[j + i * ldx];
+    // target tile: rows r0.., columns c0..; with the upper triangle stored the
+    // targets lie on or below the diagonal (tile row >= tile column)
+    const int tr = blockIdx.x, tc = blockIdx.y;
+    if (upper ? tr < tc : tr > tc) return;
+    const int64_t r0 = int64_t(tr) * kCompTile, c0 = int64_t(tc) * kCompTile;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    __shared__ T sm[kCompTile][kCompTile + 1];  // sm[i - r0][j - c0] = X(j, i)
+    if (!tri) {
+#pragma unroll
+        for (int k = 0; k < kCompTile; k += kCompRows) {
+            const int64_t j = c0 + tx, i = r0 + ty + k;  // source X(j, i): column i
+            if (j < n && i < n) sm[ty + k][tx] = X[j + i * ldx];
         }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int k = 0; k < kCompTile; k += kCompRows) {
+        const int64_t i = r0 + tx, j = c0 + ty + k;  // target X(i, j): column j
+        if (i >= n || j >= n) continue;
+        T *xp = &X[i + j * ldx];
+        if (i == j) {
+            if (unit) *xp = Ar::one();
+            else if (herm) *xp = Ar::real_part(*xp);
+            continue;
+        }
+        if (upper ? i < j : i > j) continue;  // stored
+        if (tri) *xp = Ar::zero();
+        else *xp = herm ? Ar::conj(sm[tx][ty + k]) : sm[tx][ty + k];
+    }
 }
 
 template <typename T> int launch_complete_t(int form, void *X, int64_t ldx, int64_t n, cudaStream_t s) {
-    dim3 grid(unsigned(std::min<int64_t>(8, (n + 255) / 256)), unsigned(std::min<int64_t>(n, 65535)));
-    complete_operand_kernel<T><<<grid, 256, 0, s>>>(form, static_cast<T *>(X), ldx, int(n));
+    const int64_t tiles = (n + kCompTile - 1) / kCompTile;
+    if (tiles > 65535) return set_error(BLASX_ERR_UNSUPPORTED, "operand order too large to complete");
+    complete_operand_kernel<T><<<dim3(unsigned(tiles), unsigned(tiles)), dim3(kCompTile, kCompRows), 0, s>>>(
+        form, static_cast<T *>(X), ldx, int(n));
     BX_CUDA(cudaGetLastError());
     count_launch();
     return BLASX_OK;
