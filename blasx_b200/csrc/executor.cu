@@ -67,9 +67,9 @@ constexpr int kLanes = 2;
 constexpr double kFastFlops = 2e9;
 // The kernel's CTAs stay while the host keeps it running and leave together
 // when the host raises the stop flag (kLinger without work). A CTA that sees
-// no task for kIdleCycles leaves on its own: a bound for the case of a host
-// that stopped publishing without stopping the kernel, long enough not to
-// fire between the arrivals of a live request stream.
+// no task for kIdleCycles makes them all leave: a bound for the case of a
+// host that stopped publishing without stopping the kernel. The host
+// launches the kernel again when tasks are pending and it has ended.
 constexpr long long kIdleCycles = 400000000;  // ~0.2 s
 constexpr double kLinger = 0.005;             // s without pending tasks before the host stops the kernel
 
@@ -182,8 +182,9 @@ __device__ __forceinline__ void max_release_gpu(long long *p, long long v) {
     asm volatile("red.release.gpu.global.max.s64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Claims the next published task (thread 0), lane 0 first. False when the
-// stop flag is raised or no task came for idle_cycles. The tasks known to be
+// Claims the next published task (thread 0), lane 0 first. False once a
+// stop was seen (the host's flag, or a CTA that found no task for
+// idle_cycles): then every CTA leaves at its next claim. The tasks known to be
 // published are mirrored in device memory (dev_tail): the CTAs poll that,
 // and only when it shows nothing new does one of them at a time (poll_lock)
 // read the host's tails and stop flag across PCIe, with a growing pause
@@ -192,6 +193,12 @@ __device__ bool claim(const ExecArgs &a, Task *task, long long *index, int *lane
     const long long t0 = clock64();
     unsigned pause = 64;  // ns
     for (;;) {
+        // a stop, once seen by any CTA, ends every CTA at its next claim,
+        // tasks left or not: the kernel then ends as a whole and the host
+        // launches it again for what is pending (a kernel that went on with
+        // the CTAs that still found tasks would look live to the host with a
+        // fraction of the SMs)
+        if (*reinterpret_cast<volatile int *>(a.dev_stop)) return false;
         bool known = false;
 #pragma unroll 1
         for (int l = 0; l < kLanes; ++l) {
@@ -237,7 +244,10 @@ __device__ bool claim(const ExecArgs &a, Task *task, long long *index, int *lane
             }
         }
         if (*reinterpret_cast<volatile int *>(a.dev_stop)) return false;
-        if (clock64() - t0 > a.idle_cycles) return false;
+        if (clock64() - t0 > a.idle_cycles) {  // the whole kernel leaves, not this CTA alone
+            atomicExch(a.dev_stop, 1);
+            return false;
+        }
         __nanosleep(pause);
         if (pause < 8192) pause *= 2;
     }

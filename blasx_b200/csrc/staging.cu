@@ -113,7 +113,7 @@ public:
     Stager() {
         int n = 0;
         if (const char *e = getenv("BLASX_STAGING_THREADS")) n = atoi(e);
-        if (n <= 0) n = std::clamp(int(std::thread::hardware_concurrency()) / 2, 1, 8);
+        if (n <= 0) n = std::clamp(int(std::thread::hardware_concurrency()) / 2, 1, 16);
         workers_ = new Workers(n - 1);
         writer_ = std::thread([this] { write_loop(); });
         writer_.detach();
