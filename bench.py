@@ -475,6 +475,7 @@ def run_workloads(args):
         link = h2d_min / 55.6e9  # measured pinned H2D rate on this pool
         sweep = [("native", bx.MODE_NATIVE, t) for t in (1024, 1536, 2048, 3072, 4096)]
         sweep += [("auto", bx.MODE_AUTO, t) for t in (2048, 4096, 8192)]
+        sweep += [("auto, library's tile", bx.MODE_AUTO, 0), ("native, library's tile", bx.MODE_NATIVE, 0)]
         for mode_name, mode, tile in sweep:
             C[:, :64] = C0
             bx.set_dgemm_mode(mode)
@@ -492,7 +493,7 @@ def run_workloads(args):
             roof = max(pipe, link)
             ratio, err = _accuracy(C[:, :64], "N", "N", n, 64, n, 1.0, A, n, B, n, 0.5, C0, n, "f64",
                                    min(args.samples, 512))
-            lines.append({"workload": f"out-of-core dgemm NN {n}^3, HBM cache 24 GiB, tile {tile}, {mode_name}",
+            lines.append({"workload": f"out-of-core dgemm NN {n}^3, HBM cache 24 GiB, tile {st['tile']}, {mode_name}",
                           "path": {1: "native", 2: "emulated", 4: "native (device fallback)"}.get(st["path"], "?"),
                           "moduli": st["moduli"], "tflops_e2e": fl / dt / 1e12, "seconds": dt,
                           "roofline_seconds": roof, "roofline_bound": "link" if link >= pipe else

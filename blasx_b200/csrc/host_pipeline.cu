@@ -75,10 +75,23 @@ size_t default_budget(const Context *c) {
     return b ? std::min(b, total_b) : cap;
 }
 
-int pick_tile(const Gemm &g) {
+size_t tile_step_ws(const Gemm &g, int T, int mode);
+
+// Tile edge of the out-of-core path: BLASX_TILE / blasx_set_tile when set;
+// otherwise 4096 (complex128: 2048), or twice that when the K-steps of that
+// edge run emulated and the budget holds 16 operand tiles of it beside the C
+// tiles and the step scratch. An emulated K-step slices its tiles and
+// reconstructs its C tile every time, work that a larger edge spreads over
+// more multiply-adds (40960^3 through a 24 GiB cache: 1.18 s at 8192 against
+// 1.51 s at 4096); native K-steps peak at 4096.
+int pick_tile(const Gemm &g, int mode, size_t budget) {
     const int t = config().tile.load();
     if (t) return t;
-    return g.dt == DType::C128 ? 2048 : 4096;
+    const int base = g.dt == DType::C128 ? 2048 : 4096, big = 2 * base;
+    const size_t ws = tile_step_ws(g, big, mode);
+    const size_t slot = size_t(big) * big * elem_size(g.dt);
+    if (ws && budget >= tiled_min_bytes(g.dt, big, ws) + 14 * slot) return big;
+    return base;
 }
 
 // Copies the column panel [j0, j1) of op(B) (and of C) host -> device.
@@ -415,7 +428,7 @@ size_t tile_step_ws(const Gemm &g, int T, int mode) {
 // cache (the C tiles and two operand tiles, and a step's scratch).
 bool host_gemm_fits(const Gemm &g, int mode, size_t budget) {
     if (incore_bytes(g, mode).total() <= budget) return true;
-    const int T = pick_tile(g);
+    const int T = pick_tile(g, mode, budget);
     return tiled_min_bytes(g.dt, T, tile_step_ws(g, T, mode)) <= budget;
 }
 
@@ -859,7 +872,7 @@ int host_tri_entry(const Trsm &t, bool mult) {
     if (!host_gemm_fits(top, mode, budget))
         return set_error(BLASX_ERR_UNSUPPORTED, "triangular %s: the HBM budget (%zu bytes) cannot hold the "
                          "update GEMM of its halves (tile edge %d)", mult ? "multiply" : "solve", budget,
-                         pick_tile(top));
+                         pick_tile(top, mode, budget));
     // registered once for every part (the parts' own registrations would
     // overlap); staged ranges are staged again by each part's own call
     HostPin pins;
@@ -909,7 +922,7 @@ int host_gemm(const Gemm &g) {
     if (ib.total() > budget && need_ab) {
         // out-of-core: HBM tile cache under the byte budget; each K-step on
         // the emulated path when the precision mode picks it for a step's shape
-        const int T = pick_tile(g);
+        const int T = pick_tile(g, mode, budget);
         const int st_code = tiled_host_gemm(g, c, budget, T, 0, tile_step_ws(g, T, mode), mode);
         st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return st_code;
