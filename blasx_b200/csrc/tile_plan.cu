@@ -21,35 +21,43 @@ struct KeyHash {
 
 }  // namespace
 
-bool plan_tiles(int64_t M, int64_t N, int64_t K, int64_t T, int slots, int policy, TilePlan *out) {
-    if (slots < 2 || T <= 0 || M <= 0 || N <= 0 || K <= 0) return false;
-    TilePlan &p = *out;
-    p = TilePlan{};
-    p.tiles_m = int((M + T - 1) / T);
-    p.tiles_n = int((N + T - 1) / T);
-    p.tiles_k = int((K + T - 1) / T);
-    p.slots = slots;
+namespace {
 
-    // 1. reference string: C tiles in snake order, K-steps inside
-    for (int i = 0; i < p.tiles_m; ++i) {
+// The reference string: C tiles in `rows`-row bands, the bands taken top to
+// bottom, a band's tiles column by column (the columns snaking from band to
+// band, the rows inside a column snaking from column to column), K-steps
+// inside. rows = 1 is the plain snake order (row by row, alternate rows
+// reversed).
+void band_order(TilePlan &p, int rows) {
+    p.steps.clear();
+    for (int b0 = 0, band = 0; b0 < p.tiles_m; b0 += rows, ++band) {
+        const int b1 = std::min(p.tiles_m, b0 + rows);
         for (int jj = 0; jj < p.tiles_n; ++jj) {
-            const int j = (i % 2 == 0) ? jj : p.tiles_n - 1 - jj;
-            for (int k = 0; k < p.tiles_k; ++k) {
-                TileStep s;
-                s.i = i; s.j = j; s.k = k;
-                s.first_k = (k == 0);
-                s.last_k = (k == p.tiles_k - 1);
-                s.a = TileUse{TileKey{0, i, k}, -1, false, 0};
-                s.b = TileUse{TileKey{1, k, j}, -1, false, 0};
-                p.steps.push_back(s);
+            const int j = band % 2 == 0 ? jj : p.tiles_n - 1 - jj;
+            for (int ii = 0; ii < b1 - b0; ++ii) {
+                const int i = jj % 2 == 0 ? b0 + ii : b1 - 1 - ii;
+                for (int k = 0; k < p.tiles_k; ++k) {
+                    TileStep s;
+                    s.i = i; s.j = j; s.k = k;
+                    s.first_k = (k == 0);
+                    s.last_k = (k == p.tiles_k - 1);
+                    s.a = TileUse{TileKey{0, i, k}, -1, false, 0};
+                    s.b = TileUse{TileKey{1, k, j}, -1, false, 0};
+                    p.steps.push_back(s);
+                }
             }
         }
     }
+}
+
+// Simulates the cache over p.steps: slot, load and eviction of every use.
+void simulate(TilePlan &p, int slots, int policy) {
+    p.loads = p.hits = p.evictions = 0;
     const int64_t nuse = int64_t(p.steps.size()) * 2;
     auto use_key = [&](int64_t u) -> const TileKey & {
         return (u & 1) ? p.steps[size_t(u >> 1)].b.key : p.steps[size_t(u >> 1)].a.key;
     };
-    // 2. next use of the same tile after every use (for Belady)
+    // next use of the same tile after every use (for Belady)
     std::vector<int64_t> next(size_t(nuse), std::numeric_limits<int64_t>::max());
     {
         std::unordered_map<TileKey, int64_t, KeyHash> last;
@@ -59,7 +67,6 @@ bool plan_tiles(int64_t M, int64_t N, int64_t K, int64_t T, int slots, int polic
             last[use_key(u)] = u;
         }
     }
-    // 3. simulate the cache
     std::unordered_map<TileKey, int, KeyHash> where;  // resident tile -> slot
     std::vector<TileKey> holder(size_t(slots), TileKey{-1, -1, -1});
     std::vector<int64_t> prio(size_t(slots), 0);  // Belady: next use; LRU: last use
@@ -118,6 +125,30 @@ bool plan_tiles(int64_t M, int64_t N, int64_t K, int64_t T, int slots, int polic
         use.slot = s;
         use.load = true;
         ++p.loads;
+    }
+}
+
+}  // namespace
+
+bool plan_tiles(int64_t M, int64_t N, int64_t K, int64_t T, int slots, int policy, TilePlan *out) {
+    if (slots < 2 || T <= 0 || M <= 0 || N <= 0 || K <= 0) return false;
+    TilePlan &p = *out;
+    p = TilePlan{};
+    p.tiles_m = int((M + T - 1) / T);
+    p.tiles_n = int((N + T - 1) / T);
+    p.tiles_k = int((K + T - 1) / T);
+    p.slots = slots;
+    // Bands of two tile rows, unless they load more tiles than the snake
+    // order: the snake's first row of C tiles needs every B tile, and while
+    // those cross the host link the compute waits; a band needs them for
+    // twice the C tiles, so the link keeps pace with the compute sooner.
+    band_order(p, 1);
+    simulate(p, slots, policy);
+    if (p.tiles_m >= 2) {
+        TilePlan b = p;
+        band_order(b, 2);
+        simulate(b, slots, policy);
+        if (b.loads <= p.loads) p = std::move(b);
     }
     return true;
 }

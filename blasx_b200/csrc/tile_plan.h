@@ -5,8 +5,10 @@
 // (blas/LRU.c, blas/red_black_tree.c, blas/blasx_mem_control.c:222-340) and
 // its reader refcounts (blas/blasx_mem_control.c:45-63) with one planner:
 //   * C is cut into T x T tiles (edge tiles clipped, as margin_adjustment in
-//     blas/blasx_mem_control.c:24-42) visited in snake order (row by row,
-//     alternate rows reversed), so B tiles of one row are reused by the next;
+//     blas/blasx_mem_control.c:24-42) visited in bands of two tile rows,
+//     column by column inside a band, snaking, so the tiles of A and B in
+//     use are reused by the next C tiles (the plain row-by-row snake when
+//     bands would load more tiles);
 //   * every K-step of a C tile needs one A tile and one B tile; they live in
 //     fixed-size slots of an HBM arena whose size is an explicit byte budget
 //     (the reference has none: it evicts when cudaMalloc fails);

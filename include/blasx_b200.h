@@ -360,7 +360,8 @@ void blasx_get_call_stats(blasx_call_stats *out);
  * the host without touching a GPU (no counterpart in the reference; it
  * replaces the reference's task queue and LRU tile cache,
  * blas/blasx_task_queue.c, blas/LRU.c). C is cut into tile x tile blocks
- * visited in snake order; operand tiles occupy budget_bytes / (tile^2 *
+ * visited in bands of two block rows, column by column, snaking (row by row
+ * when that loads fewer tiles); operand tiles occupy budget_bytes / (tile^2 *
  * elem_bytes) - 3 slots (3 hold C tiles); policy 0 = Belady (farthest next
  * use), 1 = LRU. */
 typedef struct blasx_tile_plan_stats {

@@ -6,7 +6,7 @@ G = 1 << 30
 
 def test_c2_config_reaches_minimum_h2d(blx):
     # 40960^3 FP64 with a 24 GB cache: every operand element crosses PCIe once
-    for tile in (1024, 2048, 3072, 4096):
+    for tile in (1024, 2048, 3072, 4096, 8192):
         for pol in (blx.POLICY_BELADY, blx.POLICY_LRU):
             s = blx.tile_plan(40960, 40960, 40960, tile, 24 * G, 8, pol)
             assert s["operand_h2d_bytes"] == pytest.approx(s["min_operand_h2d_bytes"])
