@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target CPU time per reference sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-ooc", action="store_true", help="skip the out-of-core 40960^3 point of the headline line")
     p.add_argument("--serving", type=int, default=400,
                    help="requests of the serving load (0 = skip); 10000 with --serving-dmax 16384 is the full stream")
     p.add_argument("--serving-dmax", type=int, default=8192)
@@ -356,6 +357,58 @@ def _host(torch, shape, dtype, seed, lo=-1.0, hi=1.0, phi=None):
     return t, np.asarray(t.numpy()).T  # (rows x cols) Fortran-ordered view
 
 
+def ooc_runs(bx, torch, sweep, fp64_peak: float, int8_peak: float, samples: int):
+    """DGEMM NN 40960^3 through cblas_dgemm on pinned host arrays
+    (13.4 GB each), beta = 0.5, with the HBM tile cache capped at 24 GiB.
+    sweep: (name, precision mode, tile edge; 0 = the library's choice). Each
+    run reports e2e TF/s, its roofline (the slower of the pipe -- FP64 for
+    native K-steps, INT8 moduli x 2n^3 for emulated ones, at the rates measured
+    in this process -- and the host link), H2D bytes against the minimum, the
+    tile-cache hit rate and the error of 64 columns against the dd oracle."""
+    n = 40960
+    tA, A = _host(torch, (n, n), "f64", 1)
+    tB, B = _host(torch, (n, n), "f64", 2)
+    tC, C = _host(torch, (n, n), "f64", 3)
+    C0 = C[:, :64].copy(order="F")  # columns checked against the oracle
+    bx.set_hbm_budget(24 << 30)
+    fl = 2.0 * n ** 3
+    h2d_min = 8.0 * 3 * n * n
+    link = h2d_min / 55.6e9  # measured pinned H2D rate on this pool
+    out = []
+    for mode_name, mode, tile in sweep:
+        C[:, :64] = C0
+        bx.set_dgemm_mode(mode)
+        bx.set_tile(tile)
+        t0 = time.perf_counter()
+        bx.cblas_dgemm(bx.CblasColMajor, bx.CblasNoTrans, bx.CblasNoTrans, n, n, n, 1.0, tA.data_ptr(), n,
+                       tB.data_ptr(), n, 0.5, tC.data_ptr(), n)
+        dt = time.perf_counter() - t0
+        assert bx.last_status() == 0, bx.last_error()
+        st = bx.call_stats()
+        emulated = st["path"] == 2
+        pipe = (st["moduli"] * fl / (int8_peak * 1e12)) if emulated else fl / (fp64_peak * 1e12)
+        roof = max(pipe, link)
+        ratio, err = _accuracy(C[:, :64], "N", "N", n, 64, n, 1.0, A, n, B, n, 0.5, C0, n, "f64", samples)
+        out.append({"workload": f"out-of-core dgemm NN {n}^3, HBM cache 24 GiB, tile {st['tile']}, {mode_name}",
+                    "path": {1: "native", 2: "emulated", 4: "native (device fallback)"}.get(st["path"], "?"),
+                    "moduli": st["moduli"], "tflops_e2e": fl / dt / 1e12, "seconds": dt,
+                    "roofline_seconds": roof, "roofline_bound": "link" if link >= pipe else
+                    ("int8" if emulated else "fp64"), "frac_of_roofline": roof / dt,
+                    "fp64_roofline_seconds": max(fl / (fp64_peak * 1e12), link),
+                    "frac_of_fp64_roofline": max(fl / (fp64_peak * 1e12), link) / dt,
+                    "fp64_peak": fp64_peak, "int8_peak": int8_peak,
+                    "h2d_bytes": st["h2d_bytes"], "h2d_min_bytes": h2d_min,
+                    "h2d_over_min": st["h2d_bytes"] / h2d_min, "tile_hits": st["cache_hits"],
+                    "tile_loads": st["cache_misses"], "evictions": st["evictions"],
+                    "hit_rate": st["cache_hits"] / max(1.0, st["cache_hits"] + st["cache_misses"]),
+                    "bound_ratio": ratio, "max_normalised_error": err})
+    bx.set_tile(0)
+    bx.set_hbm_budget(0)
+    bx.set_dgemm_mode(bx.MODE_AUTO)
+    del tA, tB, tC
+    return out
+
+
 def _accuracy(C, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C0, ldc, dtype, n):
     """(ratio to the (K+2)u componentwise bound, max normalised error) on n
     sampled entries against the double-double oracle."""
@@ -463,53 +516,13 @@ def run_workloads(args):
                           "host": "pinned", **res})
             del tA, tB, tC
     elif args.workload == "ooc":
-        n = 40960
         fp64_peak, int8_peak = measure_peaks(torch)
-        tA, A = _host(torch, (n, n), "f64", 1)
-        tB, B = _host(torch, (n, n), "f64", 2)
-        tC, C = _host(torch, (n, n), "f64", 3)
-        C0 = C[:, :64].copy(order="F")  # columns checked against the oracle
-        bx.set_hbm_budget(24 << 30)
-        fl = 2.0 * n ** 3
-        h2d_min = 8.0 * 3 * n * n
-        link = h2d_min / 55.6e9  # measured pinned H2D rate on this pool
         sweep = [("native", bx.MODE_NATIVE, t) for t in (1024, 1536, 2048, 3072, 4096)]
         sweep += [("auto", bx.MODE_AUTO, t) for t in (2048, 4096, 8192)]
         sweep += [("auto, library's tile", bx.MODE_AUTO, 0), ("native, library's tile", bx.MODE_NATIVE, 0)]
-        for mode_name, mode, tile in sweep:
-            C[:, :64] = C0
-            bx.set_dgemm_mode(mode)
-            bx.set_tile(tile)
-            t0 = time.perf_counter()
-            bx.cblas_dgemm(bx.CblasColMajor, bx.CblasNoTrans, bx.CblasNoTrans, n, n, n, 1.0, tA.data_ptr(), n,
-                           tB.data_ptr(), n, 0.5, tC.data_ptr(), n)
-            dt = time.perf_counter() - t0
-            assert bx.last_status() == 0, bx.last_error()
-            st = bx.call_stats()
-            # roofline: the slower of the pipe bound and the host-link bytes; the
-            # pipe is FP64 for native K-steps, INT8 (moduli x 2n^3 ops) for emulated ones
-            emulated = st["path"] == 2
-            pipe = (st["moduli"] * fl / (int8_peak * 1e12)) if emulated else fl / (fp64_peak * 1e12)
-            roof = max(pipe, link)
-            ratio, err = _accuracy(C[:, :64], "N", "N", n, 64, n, 1.0, A, n, B, n, 0.5, C0, n, "f64",
-                                   min(args.samples, 512))
-            lines.append({"workload": f"out-of-core dgemm NN {n}^3, HBM cache 24 GiB, tile {st['tile']}, {mode_name}",
-                          "path": {1: "native", 2: "emulated", 4: "native (device fallback)"}.get(st["path"], "?"),
-                          "moduli": st["moduli"], "tflops_e2e": fl / dt / 1e12, "seconds": dt,
-                          "roofline_seconds": roof, "roofline_bound": "link" if link >= pipe else
-                          ("int8" if emulated else "fp64"), "frac_of_roofline": roof / dt,
-                          "fp64_roofline_seconds": max(fl / (fp64_peak * 1e12), link),
-                          "frac_of_fp64_roofline": max(fl / (fp64_peak * 1e12), link) / dt,
-                          "fp64_peak": fp64_peak, "int8_peak": int8_peak,
-                          "h2d_bytes": st["h2d_bytes"], "h2d_min_bytes": h2d_min,
-                          "h2d_over_min": st["h2d_bytes"] / h2d_min, "tile_hits": st["cache_hits"],
-                          "tile_loads": st["cache_misses"], "evictions": st["evictions"],
-                          "hit_rate": st["cache_hits"] / max(1.0, st["cache_hits"] + st["cache_misses"]),
-                          "bound_ratio": ratio, "max_normalised_error": err})
-            print(json.dumps(lines[-1]), file=sys.stderr, flush=True)
-        bx.set_tile(0)
-        bx.set_hbm_budget(0)
-        bx.set_dgemm_mode(bx.MODE_AUTO)
+        for res in ooc_runs(bx, torch, sweep, fp64_peak, int8_peak, min(args.samples, 512)):
+            lines.append(res)
+            print(json.dumps(res), file=sys.stderr, flush=True)
     elif args.workload == "c0":
         # cblas_dgemm NN 4096^3 on the native path, U[-1,1], alpha = 1, beta = 0.5, pinned host arrays;
         # checked against OpenBLAS (full matrix) and the double-double oracle (sampled)
@@ -1126,6 +1139,13 @@ def main():
                                               args.serving_rate, budget=int(args.serving_budget), inflight=16)
         bx.set_dgemm_mode(mode)
 
+    ooc = None
+    if world == 1 and not args.no_ooc:
+        # one C2 point, emulated and native, each at the library's own tile choice
+        ooc = ooc_runs(bx, torch, [("auto", bx.MODE_AUTO, 0), ("native", bx.MODE_NATIVE, 0)], fp64_peak,
+                       int8_peak, 256)
+        bx.set_dgemm_mode(mode)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         vals, sample, kind, lib, _ = reference_cpu_sample(n, args.cpu_seconds, cores, 1, 0)
@@ -1139,7 +1159,8 @@ def main():
                 "path": path, "moduli": stats["moduli"], "phases_ms_per_step": phase_ms,
                 "fp64_equivalent": fp64_equiv, "native": native, "e2e": e2e, "roofline": roofline,
                 "accuracy": accuracy,
-                "cpu_baseline": cpu, "serving": serving, "gpu_launches": launches, "clocks": clk.summary(),
+                "cpu_baseline": cpu, "serving": serving, "out_of_core": ooc, "gpu_launches": launches,
+                "clocks": clk.summary(),
                 "vs_published_blasx_1gpu_16384": value * 1e3 / PUBLISHED_BLASX_1GPU_16384_GFLOPS}
         print(json.dumps(line), flush=True)
     if dist:
