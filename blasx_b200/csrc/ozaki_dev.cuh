@@ -309,40 +309,46 @@ template <int L> struct Mod {
                                                    233, 229, 227, 223, 217, 211, 199,
                                                    197, 193, 191, 181, 179, 173};
     static constexpr uint32_t m = table[L];
-    static constexpr uint32_t c21 = uint32_t((uint64_t(1) << 21) % m);
-    static constexpr uint32_t c42 = uint32_t((uint64_t(1) << 42) % m);
+    static constexpr uint32_t pw(int bits) { return uint32_t((uint64_t(1) << bits) % m); }
+    // 2^(8k) mod m, one byte each: bytes 0-3 of the biased value (lo) and
+    // bytes 4-7 (hi)
+    static constexpr uint32_t wlo = pw(0) | pw(8) << 8 | pw(16) << 16 | pw(24) << 24;
+    static constexpr uint32_t whi = pw(32) | pw(40) << 8 | pw(48) << 16 | pw(56) << 24;
     // half range of the symmetric residue (m odd): [-h, h]
     static constexpr uint32_t h = (m - 1) / 2;
-    // -2^62 + h mod m: removes the bias of the digits and shifts by h
+    // -2^62 + h mod m: removes the bias and shifts by h
     static constexpr uint32_t cbh = uint32_t(((m - (uint64_t(1) << 62) % m) % m + h) % m);
-    static constexpr uint32_t magic = uint32_t(((uint64_t(1) << 39) + m - 1) / m);
+    // ceil(2^32 / m): the quotient of t < 2^20 by m is its product's high word
+    static constexpr uint32_t magic = uint32_t(((uint64_t(1) << 32) + m - 1) / m);
 };
 
-// v + 2^62 (|v| < 2^62, so the biased value is in [0, 2^63)) split into
-// 21-bit digits, computed once per element and shared by all moduli.
+// v + 2^62 (|v| < 2^62, so the biased value is in [0, 2^63)) as two 32-bit
+// words, computed once per element and shared by all moduli.
 struct Digits {
-    uint32_t d0, d1, d2;
+    uint32_t lo, hi;
 };
 __device__ __forceinline__ Digits digits_of(int64_t v) {
     const uint64_t a = uint64_t(v) + (uint64_t(1) << 62);
-    return {uint32_t(a) & 0x1FFFFFu, uint32_t(a >> 21) & 0x1FFFFFu, uint32_t(a >> 42)};
+    return {uint32_t(a), uint32_t(a >> 32)};
 }
 
 // Symmetric residue of v for the L-th modulus, in [-h, h] for odd m (the
 // low byte for m = 256, whose byte is already the two's complement of the
-// residue in [-128, 127]): with the bias removed and h added,
-//   t = d2 (2^42 mod m) + d1 (2^21 mod m) + d0 + (h - 2^62 mod m) < 2^30,
-//   t mod m = floor(t ceil(2^39/m) / 2^39), exact for t < 2^31 and m <= 256
-// (the rounding error of the magic multiplier stays below 1/m), and
-// (v + h) mod m - h is the residue of v in [-h, h]. Every constant folds: two
-// IMADs, one add, one multiply-high, one shift, one IMAD, one add.
+// residue in [-128, 127]): with the bias removed and h added, the bytes b_k
+// of the biased value give
+//   t = sum_k b_k (2^(8k) mod m) + (h - 2^62 mod m) < 8 * 255 * 255 + 256 < 2^20,
+// two byte dot products (DP4A) against constant weight words;
+//   floor(t / m) = floor(t ceil(2^32/m) / 2^32), exact for t < 2^20 and
+// m <= 256 (the rounding error of the magic multiplier, below 2^-12, stays
+// under 1/m), and (v + h) mod m - h is the residue of v in [-h, h]. Every
+// constant folds: two DP4As, one multiply-high, one IMAD, one add.
 template <int L> __device__ __forceinline__ int32_t residue_s(const Digits &x) {
     using C = Mod<L>;
     if constexpr (C::m == 256) {
-        return int32_t(x.d0);
+        return int32_t(x.lo);
     } else {
-        const uint32_t t = x.d2 * C::c42 + x.d1 * C::c21 + (x.d0 + C::cbh);
-        const uint32_t q = __umulhi(t, C::magic) >> 7;
+        const uint32_t t = __dp4a(x.hi, C::whi, __dp4a(x.lo, C::wlo, C::cbh));
+        const uint32_t q = __umulhi(t, C::magic);
         return int32_t(t - q * C::m) - int32_t(C::h);
     }
 }
