@@ -167,3 +167,25 @@ def crt_fp64(u, tables) -> float:
         th, tl = _two_sum(top, uh)
         x = th + _add_round_odd(tl, ul)
     return x + 0.0
+
+
+# ---- the device's residue computation, restated --------------------------------
+# The slicing kernels (blasx_b200/csrc/ozaki_dev.cuh: residue_s) take the
+# symmetric residue of a scaled integer v (|v| < 2^62) for an odd modulus m
+# from the eight bytes b_k of the biased value v + 2^62: two byte dot products
+# against the constants 2^(8k) mod m plus (h - 2^62) mod m (h = (m - 1) / 2)
+# give t < 2^20, the quotient of t by m is the high word of t * ceil(2^32 / m),
+# and t - m floor(t / m) - h lies in [-h, h]. For m = 256 the residue is the
+# low byte of v.
+
+def residue_bytes(v: int, m: int) -> int:
+    a = v + (1 << 62)
+    if m == 256:
+        b = a & 255
+        return b - 256 if b >= 128 else b
+    h = (m - 1) // 2
+    t = sum(((a >> (8 * k)) & 255) * ((1 << (8 * k)) % m) for k in range(8))
+    t += ((m - (1 << 62) % m) % m + h) % m
+    assert t < (1 << 20)
+    q = (t * (((1 << 32) + m - 1) // m)) >> 32
+    return t - q * m - h

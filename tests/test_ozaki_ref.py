@@ -70,3 +70,20 @@ def test_fp64_limb_crt_rounds_correctly(n):
         assert abs(x) < M // 4
         got = ozaki_ref.crt_fp64([x % m for m in ms], tables)
         assert got == float(x) and (x != 0 or math.copysign(1.0, got) > 0), (n, x, got)
+
+
+def test_byte_dot_residues_match_symmetric_residues():
+    # the device's residue formula, restated, against the symmetric residue
+    # by definition, for every modulus, at the range ends and at random
+    import random
+    rng = random.Random(3)
+    vs = [0, 1, -1, (1 << 62) - 1, -(1 << 62), (1 << 53) + 1, -(1 << 40)]
+    vs += [rng.randrange(-(1 << 62), 1 << 62) for _ in range(3000)]
+    for m in ozaki_ref.MODULI:
+        for v in vs:
+            r = ozaki_ref.residue_bytes(v, m)
+            if m == 256:
+                assert r % 256 == v % 256 and -128 <= r <= 127
+            else:
+                h = (m - 1) // 2
+                assert r == (v + h) % m - h, (m, v)
