@@ -316,10 +316,12 @@ template <int L> struct Mod {
     static constexpr uint32_t whi = pw(32) | pw(40) << 8 | pw(48) << 16 | pw(56) << 24;
     // half range of the symmetric residue (m odd): [-h, h]
     static constexpr uint32_t h = (m - 1) / 2;
-    // -2^62 + h mod m: removes the bias and shifts by h
-    static constexpr uint32_t cbh = uint32_t(((m - (uint64_t(1) << 62) % m) % m + h) % m);
+    // -2^62 mod m: removes the bias
+    static constexpr uint32_t cb = uint32_t((m - (uint64_t(1) << 62) % m) % m);
     // ceil(2^32 / m): the quotient of t < 2^20 by m is its product's high word
     static constexpr uint32_t magic = uint32_t(((uint64_t(1) << 32) + m - 1) / m);
+    // h * magic: (s + h) * magic as one 64-bit multiply-add of s
+    static constexpr uint64_t hmagic = uint64_t(h) * magic;
 };
 
 // v + 2^62 (|v| < 2^62, so the biased value is in [0, 2^63)) as two 32-bit
@@ -334,22 +336,24 @@ __device__ __forceinline__ Digits digits_of(int64_t v) {
 
 // Symmetric residue of v for the L-th modulus, in [-h, h] for odd m (the
 // low byte for m = 256, whose byte is already the two's complement of the
-// residue in [-128, 127]): with the bias removed and h added, the bytes b_k
-// of the biased value give
-//   t = sum_k b_k (2^(8k) mod m) + (h - 2^62 mod m) < 8 * 255 * 255 + 256 < 2^20,
-// two byte dot products (DP4A) against constant weight words;
-//   floor(t / m) = floor(t ceil(2^32/m) / 2^32), exact for t < 2^20 and
+// residue in [-128, 127]): with the bias removed, the bytes b_k of the
+// biased value give
+//   s = sum_k b_k (2^(8k) mod m) + (-2^62 mod m) <= 8 * 255 * 255 + 255,
+// two byte dot products (DP4A) against constant weight words, s = v (mod m).
+// With t = s + h < 2^20,
+//   q = floor(t / m) = floor(t ceil(2^32/m) / 2^32), exact for t < 2^20 and
 // m <= 256 (the rounding error of the magic multiplier, below 2^-12, stays
-// under 1/m), and (v + h) mod m - h is the residue of v in [-h, h]. Every
-// constant folds: two DP4As, one multiply-high, one IMAD, one add.
+// under 1/m), is the high word of s * magic + h * magic, and
+// s - q m = (v + h) mod m - h is the residue of v in [-h, h]. Every constant
+// folds: two DP4As, one wide multiply-add, one IMAD.
 template <int L> __device__ __forceinline__ int32_t residue_s(const Digits &x) {
     using C = Mod<L>;
     if constexpr (C::m == 256) {
         return int32_t(x.lo);
     } else {
-        const uint32_t t = __dp4a(x.hi, C::whi, __dp4a(x.lo, C::wlo, C::cbh));
-        const uint32_t q = __umulhi(t, C::magic);
-        return int32_t(t - q * C::m) - int32_t(C::h);
+        const uint32_t s = __dp4a(x.hi, C::whi, __dp4a(x.lo, C::wlo, C::cb));
+        const uint32_t q = uint32_t((uint64_t(s) * C::magic + C::hmagic) >> 32);
+        return int32_t(s - q * C::m);
     }
 }
 

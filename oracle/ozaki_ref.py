@@ -173,10 +173,10 @@ def crt_fp64(u, tables) -> float:
 # The slicing kernels (blasx_b200/csrc/ozaki_dev.cuh: residue_s) take the
 # symmetric residue of a scaled integer v (|v| < 2^62) for an odd modulus m
 # from the eight bytes b_k of the biased value v + 2^62: two byte dot products
-# against the constants 2^(8k) mod m plus (h - 2^62) mod m (h = (m - 1) / 2)
-# give t < 2^20, the quotient of t by m is the high word of t * ceil(2^32 / m),
-# and t - m floor(t / m) - h lies in [-h, h]. For m = 256 the residue is the
-# low byte of v.
+# against the constants 2^(8k) mod m plus -2^62 mod m give s = v (mod m); with
+# h = (m - 1) / 2 and t = s + h < 2^20, the quotient q of t by m is the high
+# word of s * ceil(2^32 / m) + h * ceil(2^32 / m), and s - q m lies in [-h, h].
+# For m = 256 the residue is the low byte of v.
 
 def residue_bytes(v: int, m: int) -> int:
     a = v + (1 << 62)
@@ -184,8 +184,10 @@ def residue_bytes(v: int, m: int) -> int:
         b = a & 255
         return b - 256 if b >= 128 else b
     h = (m - 1) // 2
-    t = sum(((a >> (8 * k)) & 255) * ((1 << (8 * k)) % m) for k in range(8))
-    t += ((m - (1 << 62) % m) % m + h) % m
-    assert t < (1 << 20)
-    q = (t * (((1 << 32) + m - 1) // m)) >> 32
-    return t - q * m - h
+    s = sum(((a >> (8 * k)) & 255) * ((1 << (8 * k)) % m) for k in range(8))
+    s += (m - (1 << 62) % m) % m
+    assert s + h < (1 << 20)
+    magic = ((1 << 32) + m - 1) // m
+    q = (s * magic + h * magic) >> 32
+    assert q == (s + h) // m
+    return s - q * m
