@@ -358,7 +358,7 @@ def _host(torch, shape, dtype, seed, lo=-1.0, hi=1.0, phi=None):
 
 
 def ooc_runs(bx, torch, sweep, fp64_peak: float, int8_peak: float, samples: int):
-    """DGEMM NN 40960^3 through cblas_dgemm on pinned host arrays
+    """The out-of-core workload: DGEMM NN 40960^3 through cblas_dgemm on pinned host arrays
     (13.4 GB each), beta = 0.5, with the HBM tile cache capped at 24 GiB.
     sweep: (name, precision mode, tile edge; 0 = the library's choice). Each
     run reports e2e TF/s, its roofline (the slower of the pipe -- FP64 for
@@ -940,7 +940,7 @@ def main():
     def max_over_ranks(x: float) -> float:
         return rank_max(x, dist, "cuda")
 
-    # --- inputs (device-resident), C3 distribution ---
+    # --- inputs (device-resident), entries U[-0.5, 0.5] * exp(phi * g) ---
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
 
     def gen():
@@ -1141,7 +1141,8 @@ def main():
 
     ooc = None
     if world == 1 and not args.no_ooc:
-        # one C2 point, emulated and native, each at the library's own tile choice
+        # one out-of-core point (40960^3 through a 24 GiB cache), emulated and native, each at the
+        # library's own tile choice
         ooc = ooc_runs(bx, torch, [("auto", bx.MODE_AUTO, 0), ("native", bx.MODE_NATIVE, 0)], fp64_peak,
                        int8_peak, 256)
         bx.set_dgemm_mode(mode)
