@@ -1,7 +1,7 @@
 """CPU oracle for the GEMM path -- TEST INFRASTRUCTURE ONLY.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
-and reference legs import this package, and only as the checker: nothing in
+and reference legs import this package, and only to check results: nothing in
 ``blasx_b200`` imports it, and the shipped library never routes through it.
 
 It wraps ``oracle/liboracle.so`` (built by ``oracle/Makefile``):

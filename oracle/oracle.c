@@ -1,7 +1,7 @@
 /*
  * oracle.c -- CPU oracle for the GEMM path. TEST INFRASTRUCTURE ONLY (see
  * oracle.h). Only tests/, the smoke check and bench.py's CPU-baseline leg load
- * this file's library, and only as the checker.
+ * this file's library, and only to check results.
  */
 #define _GNU_SOURCE
 #include "oracle.h"

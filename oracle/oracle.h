@@ -3,7 +3,7 @@
  *
  * Nothing in the shipped library links or calls this code. It is used by the
  * test-suite, by the smoke check and by bench.py's CPU-baseline leg, always as
- * the checker and never as the thing that is measured or shipped.
+ * a check of results and never as the thing that is measured or shipped.
  *
  * Contents:
  *   - oracle_?gemm_tiled: a plain-C restatement of the reference's tiled GEMM
